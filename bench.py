@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Throughput of the MPPI control step on B200.
+
+Workload (per GPU): 4 agents, each an MPPI controller with K = 4096 samples, horizon
+H = 64 (dense controls), 2 opponent hypotheses, one policy opponent, plan verification
+with V = 2^17 samples over 40 steps (the reference front-end's setting), on a seeded
+synthetic track (closed Catmull-Rom through 12 control points jittered +-5 m around a
+40 m circle). One control step = every agent's getControl once.
+
+value : control steps/s with inputs resident in HBM (device pipeline, CUDA events)
+e2e   : control steps/s through the C ABI with host buffers (dr_mppi_batch_step: inputs
+        copied from pinned host memory, results copied back, host tail included)
+
+Multi-GPU: one process per GPU, each running its own 4-agent race (replicas, weak
+scaling, no data-path collective); timing is the max over ranks.
+
+--impl reference times the reference's own CPU implementation of the path (its model
+functions compiled from the reference sources, oracle/_ref, OpenMP over all host
+threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "drone-race_b200"
+
+AGENTS = 4
+K = 4096
+H = 64
+N_THETA = 2
+V = 2**17
+VERIF_H = 40
+
+# Algorithmic FP32 work of one environment step of the rollout (unit = one (agent,
+# sample, hypothesis, timestep) step), counted by running the FP64 transcription of the
+# model with an operation-counting scalar (oracle/port, counted over the benchmark
+# workload's own trajectories): add/sub/mul/compare = 1, fma = 2, div and sqrt = 1 each
+# plus exp/log/pow counted as 1 (their internal instructions are not algorithmic work).
+FLOPS_PER_ROLLOUT_STEP = 1076.0   # MPPI rollout step (belief update over 2 hypotheses)
+FLOPS_PER_VERIFY_STEP = 1076.0    # verification step (same model, noise-free ego plan)
+
+
+def _package():
+    if "drone_race_b200" in sys.modules:
+        return sys.modules["drone_race_b200"]
+    spec = importlib.util.spec_from_file_location("drone_race_b200", PKG_DIR / "__init__.py", submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["drone_race_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(rank: int):
+    drb = _package()
+    S = drb.scenarios
+    return [S.circle_race(agent=a, seed=rank, K=K, T=H, use_splines=False, n_theta=N_THETA, n_verif=V) for a in range(AGENTS)]
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(f"/tmp/dr_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        q = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        for line in self.path.read_text().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        try:
+            self.path.unlink()
+        except Exception:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and not dist.is_initialized():
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def _max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_baseline_reference(scs, target_s: float = 12.0) -> dict:
+    """The reference's CPU path (its model functions from oracle/_ref, OpenMP) on a bounded
+    sample of one agent's control step, scaled to the 4-agent control step."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O
+
+    drb = _package()
+    O.set_abi(drb.abi)
+    variant = O.ref_variant_name(N_THETA, False)
+    kind = "reference"
+    if not O.ref_available(variant):
+        kind = "port"
+    threads = os.cpu_count() or 1
+    sc = scs[0]
+    c = sc.mppi
+    belief = sc.belief()
+    # sample: k_s rollout samples and v_s verification samples
+    k_s, v_s = 256, 2048
+    c_small = type(c).from_buffer_copy(c)
+    c_small.n_samples = k_s
+    c_small.n_verif_samples = v_s
+    sc.mppi = c_small
+    nominal = np.zeros((N_THETA + 1, H, 2), np.float32)
+    noise = O.mppi_noise(sc, 0)
+    t0 = time.perf_counter()
+    reps = 0
+    t_roll = t_ver = 0.0
+    while True:
+        a = time.perf_counter()
+        if kind == "reference":
+            O.mppi_rollout(sc, belief, nominal, noise, None, 0, impl=variant, nthreads=threads)
+        else:
+            O.mppi_rollout(sc, belief, nominal, noise, None, 0, prec=32)
+        b = time.perf_counter()
+        if kind == "reference":
+            O.mppi_verify(sc, belief, nominal, 0, 0, impl=variant, nthreads=threads)
+        else:
+            O.mppi_verify(sc, belief, nominal.astype(np.float64), 0, 0, prec=32)
+        e = time.perf_counter()
+        t_roll += b - a
+        t_ver += e - b
+        reps += 1
+        if e - t0 > target_s or reps >= 50:
+            break
+    sc.mppi = c
+    t_roll /= reps
+    t_ver /= reps
+    # scale: rollout work ~ samples, verification ~ samples (x2 plans); 4 agents
+    step_s = AGENTS * (t_roll * (K / k_s) + 2 * t_ver * (V / v_s))
+    return {"value": 1.0 / step_s, "unit": "control_steps/s", "cores": threads, "kind": kind,
+            "sample": f"1 agent: rollout of {k_s} samples x {N_THETA} hypotheses x {H} steps and one verification pass of {v_s} samples x {VERIF_H} steps, "
+                      f"{reps} repetitions ({time.perf_counter() - t0:.1f} s), scaled to 4 agents x K={K} and 2 x V={V}",
+            "ms_per_control_step": step_s * 1e3}
+
+
+def run_ours(args) -> None:
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    drb = _package()
+    import drone_race_b200.controllers as ctl_mod
+
+    abi = drb.abi
+    scs = workload(rank)
+    stream = torch.cuda.Stream()  # non-default stream: the batch captures a CUDA graph on it
+    ctls = [ctl_mod.MPPIController(s.env, s.mppi, s.seed, device=local, stream=stream.cuda_stream) for s in scs]
+    batch = ctl_mod.MPPIBatch(ctls, stream=stream.cuda_stream)
+    n = len(ctls)
+    states = [s.state for s in scs]
+    beliefs = np.stack([s.belief() for s in scs])
+    # device-resident inputs
+    st_bytes = bytes((abi.dr_sim_state * n)(*states))
+    st_dev = torch.frombuffer(bytearray(st_bytes), dtype=torch.uint8).to("cuda")
+    bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+    bel[:, :N_THETA] = beliefs
+    bel_dev = torch.from_numpy(bel).to("cuda")
+
+    # ---- device-resident throughput -------------------------------------------------------
+    for _ in range(args.warmup):
+        batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+    torch.cuda.synchronize()
+    batch.set_profiling(True)
+    _barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    _barrier(world)
+    ms = e0.elapsed_time(e1)
+    ms = _max_over_ranks(ms, world)
+    kt = batch.kernel_times()
+    batch.set_profiling(False)
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers -----------------------------------
+    for c in ctls:
+        c.engine = object()
+    for _ in range(args.warmup):
+        batch.step(states, beliefs)
+    torch.cuda.synchronize()
+    _barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch.step(states, beliefs)
+    t1 = time.perf_counter()
+    _barrier(world)
+    e2e_s = _max_over_ranks(t1 - t0, world)
+    h2d = d2h = 0
+    for c in ctls:
+        a, b = C.c_size_t(), C.c_size_t()
+        abi.lib().dr_mppi_io_bytes(c.handle, C.byref(a), C.byref(b))
+        h2d += a.value
+        d2h += b.value
+
+    # ---- roofline of the dominant kernel --------------------------------------------------
+    dom = max(kt, key=kt.get) if kt else None
+    units = {"rollout": AGENTS * K * N_THETA * H, "verify": AGENTS * 2 * V * VERIF_H}
+    flops_unit = {"rollout": FLOPS_PER_ROLLOUT_STEP, "verify": FLOPS_PER_VERIFY_STEP}
+    roof = None
+    if dom in units and clk.get("sm_mhz"):
+        achieved = units[dom] * flops_unit[dom] / (kt[dom] / 1e3) / 1e12
+        peak = 2 * 128 * 148 * clk["sm_mhz"] * 1e6 / 1e12
+        roof = {"bound": "fp32", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "FP32 FMA rate of 148 SMs x 128 lanes at the median SM clock sampled during the timed region (MEASURED_PEAKS.json has no FP32 figure)",
+                "units_per_launch": units[dom], "flops_per_unit": flops_unit[dom], "kernel_ms": kt[dom]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_reference(scs)
+        cpu.pop("ms_per_control_step", None)
+
+    rollout_steps = AGENTS * K * N_THETA * H
+    line = {
+        "metric": "control_steps_per_s",
+        "value": value,
+        "unit": "control steps/s (4 agents x K=4096 x H=64 MPPI, verification V=2^17 x 40, all agents advanced once)",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded tracks and states; no dataset)",
+        "config": {"workload": "mppi_4x4096x64", "agents": AGENTS, "K": K, "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
+                   "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": f"replicas x{world}",
+                   "l2": "working set per step < L2; steps are dependent control steps of the same controllers"},
+        "rollout_steps_per_s": world * rollout_steps * args.steps / (ms / 1e3),
+        "verify_steps_per_s": world * AGENTS * 2 * V * VERIF_H * args.steps / (ms / 1e3),
+        "kernel_ms": kt,
+        "e2e": {"value": world * args.steps / e2e_s, "unit": "control steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_s / args.steps * 1e3},
+        "gpu_launches": (4 if ctls[0].mppiConfig.verify else 3) * args.steps,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for c in ctls:
+        c.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_reference(args) -> None:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    scs = workload(0)
+    steps_ms = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline_reference(scs, target_s=min(20.0, 120.0 / max(1, args.warmup + args.steps)))
+        if i >= args.warmup:
+            steps_ms.append(r["ms_per_control_step"])
+        base = r
+    ms = statistics.mean(steps_ms)
+    value = 1e3 / ms
+    line = {
+        "impl": "reference",
+        "metric": "control_steps_per_s",
+        "value": value,
+        "unit": "control steps/s (4 agents x K=4096 x H=64 MPPI, verification V=2^17 x 40, all agents advanced once)",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded tracks and states; no dataset)",
+        "config": {"workload": "mppi_4x4096x64", "agents": AGENTS, "K": K, "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
+                   "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "control_steps/s", "cores": base["cores"], "kind": base["kind"], "sample": base["sample"]},
+        "e2e": {"value": value, "unit": "control steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,300 @@
+"""Controller classes over the C ABI, mirroring the reference's controller interface
+(include/controllers.h:12-179): `getControl(state) -> action`, with the public fields
+the reference's simulation engine reads after each call (src/engine.cpp:73-212).
+
+All compute happens in lib/libdrmppi.so; these classes only marshal arguments.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .abi import check, lib
+
+
+def _state(s) -> abi.dr_sim_state:
+    if isinstance(s, abi.dr_sim_state):
+        return s
+    raise TypeError("state must be a dr_sim_state")
+
+
+class Controller:
+    """include/controllers.h:12-21."""
+
+    def __init__(self, n_theta: int, init_belief: np.ndarray):
+        self.engine = None
+        self.h_belief = np.array(init_belief[:n_theta], dtype=np.float32)
+
+    def getControl(self, state) -> np.ndarray:  # noqa: N802 (reference name)
+        raise NotImplementedError
+
+
+class MPPIController(Controller):
+    """MPPIController (include/controllers.h:23-111, src/mppi_controller.cu)."""
+
+    def __init__(self, env: abi.dr_env_config, cfg: abi.dr_mppi_config, seed: int, nominal: np.ndarray | None = None, device: int = 0, stream=None):
+        super().__init__(env.n_theta, np.array(env.init_belief))
+        self.mppiConfig = cfg
+        self.n_theta = int(env.n_theta)
+        self.T = int(cfg.n_timesteps)
+        self.nbp = self.n_theta + 1
+        h = C.c_void_p()
+        nom = None
+        if nominal is not None:
+            nominal = np.ascontiguousarray(nominal, np.float32)
+            if nominal.size != self.nbp * self.T * 2:
+                raise ValueError(f"Invalid MPPI construction: expected nominal size {self.nbp * self.T * 2}, got {nominal.size}")
+            nom = abi.fptr(nominal)
+        check(lib().dr_mppi_create(C.byref(env), C.byref(cfg), seed, nom, device, C.c_void_p(stream) if stream else None, C.byref(h)), "dr_mppi_create")
+        self._h = h
+        self.info = abi.dr_mppi_info()
+        self.failCount = np.zeros(self.T, np.uint32)
+        self.failCountNew = np.zeros(self.T, np.uint32)
+        self.failCountOld = np.zeros(self.T, np.uint32)
+        self.min_nu = float(cfg.min_nu) or 0.0005
+        self.max_nu = float(cfg.max_nu) or 0.001
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib().dr_mppi_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def getControl(self, state) -> np.ndarray:  # noqa: N802
+        if self.engine is None:
+            raise RuntimeError("MPPI: engine not set")
+        out = np.zeros(2, np.float32)
+        check(lib().dr_mppi_step(self._h, C.byref(_state(state)), abi.fptr(self.h_belief), abi.fptr(out), C.byref(self.info)), "dr_mppi_step")
+        self._pull()
+        return out
+
+    def _pull(self) -> None:
+        check(lib().dr_mppi_get_fail_counts(self._h, abi.uptr(self.failCountNew), abi.uptr(self.failCountOld), abi.uptr(self.failCount), self.T),
+              "dr_mppi_get_fail_counts")
+
+    # public fields of the reference controller
+    @property
+    def h_nominal(self) -> np.ndarray:
+        out = np.zeros(self.nbp * self.T * 2, np.float32)
+        check(lib().dr_mppi_get_nominal(self._h, abi.fptr(out), out.size), "dr_mppi_get_nominal")
+        return out
+
+    def knots(self) -> np.ndarray:
+        M = int(self.mppiConfig.n_knots) if self.mppiConfig.use_splines else self.T
+        out = np.zeros(self.nbp * M * 2, np.float32)
+        check(lib().dr_mppi_get_knots(self._h, abi.fptr(out), out.size), "dr_mppi_get_knots")
+        return out.reshape(self.nbp, M, 2)
+
+    @property
+    def epsilon(self) -> float:
+        return self.info.epsilon
+
+    @property
+    def epsilonPartial(self) -> float:  # noqa: N802
+        return self.info.epsilon_partial
+
+    @property
+    def certifiedLoss(self) -> float:  # noqa: N802
+        return self.info.certified_loss
+
+    @property
+    def useNewPlan(self) -> bool:  # noqa: N802
+        return bool(self.info.use_new_plan)
+
+    @property
+    def invTemperature(self) -> float:  # noqa: N802
+        return float(lib().dr_mppi_get_temperature(self._h))
+
+    @property
+    def step_index(self) -> int:
+        return int(lib().dr_mppi_get_step(self._h))
+
+    def set_profiling(self, on: bool) -> None:
+        check(lib().dr_mppi_set_profiling(self._h, int(on)), "dr_mppi_set_profiling")
+
+    def kernel_times(self) -> dict[str, float]:
+        return _kernel_times(lib().dr_mppi_get_kernel_times, self._h)
+
+
+class PRMPPIController(Controller):
+    """PRMPPIController (include/controllers.h:114-179, src/prmppi_controller.cu)."""
+
+    def __init__(self, env: abi.dr_env_config, cfg: abi.dr_prmppi_config, seed: int, nominal: np.ndarray | None = None, device: int = 0, stream=None):
+        super().__init__(env.n_theta, np.array(env.init_belief))
+        self.mppiConfig = cfg
+        self.T = int(cfg.n_timesteps)
+        h = C.c_void_p()
+        nom = None
+        if nominal is not None:
+            nominal = np.ascontiguousarray(nominal, np.float32)
+            if nominal.size != self.T * 2:
+                raise ValueError(f"Invalid PRMPPI construction: expected nominal size {self.T * 2}, got {nominal.size}")
+            nom = abi.fptr(nominal)
+        check(lib().dr_prmppi_create(C.byref(env), C.byref(cfg), seed, nom, device, C.c_void_p(stream) if stream else None, C.byref(h)), "dr_prmppi_create")
+        self._h = h
+        self.info = abi.dr_prmppi_info()
+        self.min_nu = float(cfg.min_nu) or 0.0005
+        self.max_nu = float(cfg.max_nu) or 0.001
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib().dr_prmppi_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def getControl(self, state) -> np.ndarray:  # noqa: N802
+        if self.engine is None:
+            raise RuntimeError("PRMPPI: engine not set")
+        out = np.zeros(2, np.float32)
+        check(lib().dr_prmppi_step(self._h, C.byref(_state(state)), abi.fptr(self.h_belief), abi.fptr(out), C.byref(self.info)), "dr_prmppi_step")
+        return out
+
+    def nominals(self) -> tuple[np.ndarray, np.ndarray]:
+        a = np.zeros(self.T * 2, np.float32)
+        b = np.zeros(self.T * 2, np.float32)
+        check(lib().dr_prmppi_get_nominals(self._h, abi.fptr(a), abi.fptr(b), a.size), "dr_prmppi_get_nominals")
+        return a, b
+
+    @property
+    def h_nom_nominal(self) -> np.ndarray:
+        return self.nominals()[0]
+
+    @property
+    def h_rob_nominal(self) -> np.ndarray:
+        return self.nominals()[1]
+
+    @property
+    def useNomPlan(self) -> bool:  # noqa: N802
+        return bool(self.info.use_nom_plan)
+
+    @property
+    def resetNom(self) -> bool:  # noqa: N802
+        return bool(self.info.reset_nom)
+
+    def set_profiling(self, on: bool) -> None:
+        check(lib().dr_prmppi_set_profiling(self._h, int(on)), "dr_prmppi_set_profiling")
+
+    def kernel_times(self) -> dict[str, float]:
+        return _kernel_times(lib().dr_prmppi_get_kernel_times, self._h)
+
+
+def _kernel_times(fn, h) -> dict[str, float]:
+    names = (C.c_char_p * 16)()
+    ms = (C.c_float * 16)()
+    cnt = C.c_int()
+    check(fn(h, names, ms, 16, C.byref(cnt)), "get_kernel_times")
+    return {names[i].decode(): float(ms[i]) for i in range(cnt.value)}
+
+
+class MPPIBatch:
+    """Several MPPI controllers (one per agent) advanced by one launch sequence."""
+
+    def __init__(self, controllers: list[MPPIController], stream=None):
+        self.ctls = controllers
+        arr = (C.c_void_p * len(controllers))(*[c.handle.value for c in controllers])
+        b = C.c_void_p()
+        check(lib().dr_mppi_batch_create(arr, len(controllers), C.c_void_p(stream) if stream else None, C.byref(b)), "dr_mppi_batch_create")
+        self._b = b
+        self.infos = (abi.dr_mppi_info * len(controllers))()
+
+    def step(self, states, beliefs: np.ndarray) -> np.ndarray:
+        n = len(self.ctls)
+        st = (abi.dr_sim_state * n)(*states)
+        bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+        bel[:, : beliefs.shape[1]] = beliefs
+        out = np.zeros((n, 2), np.float32)
+        check(lib().dr_mppi_batch_step(self._b, st, abi.fptr(bel), abi.fptr(out), self.infos), "dr_mppi_batch_step")
+        return out
+
+    def set_graph(self, on: bool) -> None:
+        check(lib().dr_mppi_batch_set_graph(self._b, int(on)), "dr_mppi_batch_set_graph")
+
+    def step_dev(self, states_dev_ptr: int, beliefs_dev_ptr: int) -> None:
+        check(lib().dr_mppi_batch_step_dev(self._b, C.c_void_p(states_dev_ptr), C.c_void_p(beliefs_dev_ptr)), "dr_mppi_batch_step_dev")
+
+    def set_profiling(self, on: bool) -> None:
+        check(lib().dr_mppi_batch_set_profiling(self._b, int(on)), "dr_mppi_batch_set_profiling")
+
+    def kernel_times(self) -> dict[str, float]:
+        return _kernel_times(lib().dr_mppi_batch_get_kernel_times, self._b)
+
+    def close(self) -> None:
+        if self._b:
+            lib().dr_mppi_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PRMPPIBatch:
+    def __init__(self, controllers: list[PRMPPIController], stream=None):
+        self.ctls = controllers
+        arr = (C.c_void_p * len(controllers))(*[c.handle.value for c in controllers])
+        b = C.c_void_p()
+        check(lib().dr_prmppi_batch_create(arr, len(controllers), C.c_void_p(stream) if stream else None, C.byref(b)), "dr_prmppi_batch_create")
+        self._b = b
+        self.infos = (abi.dr_prmppi_info * len(controllers))()
+
+    def step(self, states, beliefs: np.ndarray) -> np.ndarray:
+        n = len(self.ctls)
+        st = (abi.dr_sim_state * n)(*states)
+        bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+        bel[:, : beliefs.shape[1]] = beliefs
+        out = np.zeros((n, 2), np.float32)
+        check(lib().dr_prmppi_batch_step(self._b, st, abi.fptr(bel), abi.fptr(out), self.infos), "dr_prmppi_batch_step")
+        return out
+
+    def step_dev(self, states_dev_ptr: int, beliefs_dev_ptr: int) -> None:
+        check(lib().dr_prmppi_batch_step_dev(self._b, C.c_void_p(states_dev_ptr), C.c_void_p(beliefs_dev_ptr)), "dr_prmppi_batch_step_dev")
+
+    def set_profiling(self, on: bool) -> None:
+        check(lib().dr_prmppi_batch_set_profiling(self._b, int(on)), "dr_prmppi_batch_set_profiling")
+
+    def kernel_times(self) -> dict[str, float]:
+        return _kernel_times(lib().dr_prmppi_batch_get_kernel_times, self._b)
+
+    def close(self) -> None:
+        if self._b:
+            lib().dr_prmppi_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def env_step(env: abi.dr_env_config, true_theta: int, action, state: abi.dr_sim_state, belief: np.ndarray, update_belief: bool, seed: int,
+             step: int) -> int:
+    """One true-dynamics step on the device (engine dynStep, src/engine.cpp:286-312);
+    state and belief are updated in place; returns the terminal type."""
+    a = np.ascontiguousarray(action, np.float32)
+    term = C.c_int()
+    check(lib().dr_env_step(C.byref(env), true_theta, abi.fptr(a), C.byref(state), abi.fptr(belief), int(update_belief), seed, step, C.byref(term)),
+          "dr_env_step")
+    return term.value

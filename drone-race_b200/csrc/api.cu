@@ -1,0 +1,932 @@
+// C ABI of the control step (include/drmppi.h): controller objects, device memory,
+// batched launches, CUDA-graph replay and the host tails of the reference controllers
+// (src/mppi_controller.cu:363-466, src/prmppi_controller.cu:232-349).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/drmppi.h"
+#include "cp.hpp"
+#include "hostutil.hpp"
+#include "instance.cuh"
+#include "launch.h"
+
+using namespace dr;
+
+namespace dr
+{
+std::string& lastError()
+{
+    static thread_local std::string e;
+    return e;
+}
+} // namespace dr
+
+
+// ============================================================================================
+// MPPI controller
+// ============================================================================================
+struct dr_mppi
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    dr_env_config env{};
+    dr_mppi_config cfg{};
+    uint64_t seed = 0;
+    int nth = 0, nopp = 0, K = 0, T = 0, M = 0, nbp = 0, V = 0, H = 0;
+    bool spl = false;
+    Arena arena;
+    MppiDev desc{};
+    unsigned char* hRes = nullptr; // pinned copy of the result block
+    // host mirrors of the reference controller's public fields
+    std::vector<float> hNominal;
+    std::vector<uint32_t> fcNew, fcOld, fc;
+    double epsilon = 0, epsilonPartial = 0, certifiedLoss = -1;
+    bool useNewPlan = true;
+    float lambda = 1.0f;
+    uint64_t step = 0;
+    int pendBranch = -1, pendUseNew = 0;
+    ClopperPearson cp;
+    dr_mppi_batch* self = nullptr; // batch of one used by dr_mppi_step
+
+    MppiIn input(const dr_sim_state& s, const float* belief) const
+    {
+        MppiIn in{};
+        in.state = s;
+        for (int i = 0; i < DR_MAX_THETA; i++)
+            in.belief[i] = i < nth ? belief[i] : 0.0f;
+        in.lambda = lambda;
+        in.step = (uint32_t)step;
+        in.pendBranch = pendBranch;
+        in.pendUseNew = pendUseNew;
+        return in;
+    }
+
+    // host tail of MPPIController::getControl (mppi_controller.cu:363-456)
+    void finish(const float* belief, float* outAction, dr_mppi_info* info)
+    {
+        const unsigned char* r = hRes;
+        const uint32_t* fail = (const uint32_t*)(r + ((const unsigned char*)desc.fail - (const unsigned char*)desc.fail));
+        const float* dense = (const float*)(r + ((const unsigned char*)desc.dense - (const unsigned char*)desc.fail));
+        const float* prevDense = (const float*)(r + ((const unsigned char*)desc.prevDense - (const unsigned char*)desc.fail));
+        const float* nu = (const float*)(r + ((const unsigned char*)desc.nu - (const unsigned char*)desc.fail));
+        const float* minCosts = (const float*)(r + ((const unsigned char*)desc.minCosts - (const unsigned char*)desc.fail));
+        const int* stats = (const int*)(r + ((const unsigned char*)desc.stats - (const unsigned char*)desc.fail));
+        fcNew.assign(fail, fail + T);
+        fcOld.assign(fail + T, fail + 2 * T);
+        if (cfg.verify)
+        {
+            // computeCertifiedLoss (mppi_controller.cu:468-501)
+            certifiedLoss = -1.0;
+            uint32_t totOld = 0, totNew = 0;
+            for (int t = 0; t < T; t++)
+            {
+                totOld += fcOld[t];
+                totNew += fcNew[t];
+                double eps1 = cp.upper(totNew, (uint32_t)V, cfg.beta / 2.0);
+                double eps2 = cp.lower(totOld, (uint32_t)V, cfg.beta / 2.0);
+                if (eps1 - eps2 > certifiedLoss)
+                    certifiedLoss = eps1 - eps2;
+            }
+            useNewPlan = certifiedLoss < cfg.max_verif_eps;
+        }
+        else
+        {
+            certifiedLoss = -1.0;
+            useNewPlan = true;
+        }
+        fc = useNewPlan ? fcNew : fcOld;
+        // computeEpsilon (mppi_controller.cu:503-514)
+        uint32_t totFail = std::accumulate(fc.begin(), fc.end(), 0u);
+        epsilonPartial = cp.upper(totFail, (uint32_t)std::max(V, 1), cfg.beta);
+        epsilon = epsilonPartial + (float)(cfg.verif_horizon * cfg.max_verif_eps);
+        const float* chosen = useNewPlan ? dense : prevDense;
+        hNominal.assign(chosen, chosen + (size_t)nbp * T * 2);
+        int branchIdx = findConfidentHost(belief, nth, cfg.min_confidence);
+        for (int d = 0; d < 2; d++)
+            outAction[d] = hNominal[(size_t)branchIdx * T * 2 + d];
+        float usedNu = nu[branchIdx];
+        float before = lambda;
+        if (usedNu > cfg.max_nu * (float)K)
+            lambda *= 0.9f;
+        else if (usedNu < cfg.min_nu * (float)K)
+            lambda *= 1.2f;
+        (void)before;
+        // shift the chosen branch (mppi_controller.cu:430-436)
+        size_t base = (size_t)branchIdx * T * 2;
+        for (int t = 0; t < T - 1; t++)
+            for (int d = 0; d < 2; d++)
+                hNominal[base + t * 2 + d] = hNominal[base + (t + 1) * 2 + d];
+        for (int d = 0; d < 2; d++)
+            hNominal[base + (T - 1) * 2 + d] = 0.0f;
+        pendBranch = branchIdx;
+        pendUseNew = useNewPlan ? 1 : 0;
+        step++;
+        if (info)
+        {
+            info->fail_count_total = totFail;
+            info->use_new_plan = useNewPlan ? 1 : 0;
+            info->epsilon = epsilon;
+            info->epsilon_partial = epsilonPartial;
+            info->certified_loss = certifiedLoss;
+            info->branch_idx = branchIdx;
+            info->min_cost = minCosts[branchIdx * M];
+            info->nu = usedNu;
+            info->inv_temperature = lambda;
+            info->nonfinite_costs = stats[0];
+            info->verif_timeouts = stats[1];
+        }
+    }
+};
+
+struct dr_mppi_batch
+{
+    std::vector<dr_mppi*> hs;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    int nopp = 0, nth = 0;
+    bool spl = false, verify = true;
+    MppiDev* dDesc = nullptr;
+    MppiIn* dIn = nullptr;
+    MppiIn* hIn = nullptr;
+    Tile *dRoll = nullptr, *dUpd = nullptr, *dVer = nullptr;
+    int nRoll = 0, nUpd = 0, nVer = 0;
+    size_t rollSmem = 0, verSmem = 0, proSmem = 0;
+    bool useGraph = true;
+    bool profiling = false;
+    Timer timer;
+    int runs = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graphExec = nullptr;
+    const MppiIn* graphIn = nullptr;
+
+    LaunchArgs args(const Tile* tiles, int n, const MppiIn* in) const
+    {
+        LaunchArgs a;
+        a.stream = stream;
+        a.mppi = dDesc;
+        a.mppiIn = in;
+        a.tiles = tiles;
+        a.nTiles = n;
+        return a;
+    }
+
+    // kernels of one control step, reading inputs from `in` (device)
+    int launchAll(const MppiIn* in, bool profile, Timer* timer)
+    {
+        const int n = (int)hs.size();
+        if (profile)
+        {
+            timer->begin();
+            timer->mark("prologue", stream);
+        }
+        CK(launchMppiPrologue(args(nullptr, 0, in), n, proSmem));
+        if (profile)
+            timer->mark("rollout", stream);
+        CK(launchMppiRollout(args(dRoll, nRoll, in), nopp, nth, spl, rollSmem));
+        if (profile)
+            timer->mark("update", stream);
+        CK(launchMppiUpdate(args(dUpd, nUpd, in), nth));
+        if (verify && nVer > 0)
+        {
+            if (profile)
+                timer->mark("verify", stream);
+            CK(launchMppiVerify(args(dVer, nVer, in), nopp, nth, verSmem, nullptr, nullptr));
+        }
+        if (profile)
+        {
+            timer->mark("end", stream);
+            timer->end();
+        }
+        return DR_OK;
+    }
+
+    int copyResults()
+    {
+        for (auto* h : hs)
+            CK(cudaMemcpyAsync(h->hRes, h->desc.fail, h->desc.resBytes, cudaMemcpyDeviceToHost, stream));
+        return DR_OK;
+    }
+
+    // H2D inputs + kernels + D2H results, replayed from a CUDA graph after the first run
+    int enqueue(bool profile)
+    {
+        const int n = (int)hs.size();
+        if (profile || !useGraph || runs == 0)
+        {
+            CK(cudaMemcpyAsync(dIn, hIn, sizeof(MppiIn) * n, cudaMemcpyHostToDevice, stream));
+            int rc = launchAll(dIn, profile, &timer);
+            if (rc)
+                return rc;
+            rc = copyResults();
+            runs++;
+            return rc;
+        }
+        if (!graphExec)
+        {
+            CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            cudaMemcpyAsync(dIn, hIn, sizeof(MppiIn) * n, cudaMemcpyHostToDevice, stream);
+            int rc = launchAll(dIn, false, nullptr);
+            if (rc == DR_OK)
+                rc = copyResults();
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(stream, &g);
+            if (rc)
+                return rc;
+            CK(e);
+            graph = g;
+            CK(cudaGraphInstantiate(&graphExec, graph, 0));
+        }
+        CK(cudaGraphLaunch(graphExec, stream));
+        runs++;
+        return DR_OK;
+    }
+
+    int step(const dr_sim_state* states, const float* beliefs, int beliefStride, float* actions, dr_mppi_info* infos)
+    {
+        const int n = (int)hs.size();
+        CK(cudaSetDevice(device));
+        for (int i = 0; i < n; i++)
+            hIn[i] = hs[i]->input(states[i], beliefs + (size_t)i * beliefStride);
+        bool profile = profiling;
+        int rc = enqueue(profile);
+        if (rc)
+            return rc;
+        CK(cudaStreamSynchronize(stream));
+        for (int i = 0; i < n; i++)
+            hs[i]->finish(beliefs + (size_t)i * beliefStride, actions + 2 * i, infos ? infos + i : nullptr);
+        return DR_OK;
+    }
+
+    void release()
+    {
+        if (graphExec)
+            cudaGraphExecDestroy(graphExec);
+        if (graph)
+            cudaGraphDestroy(graph);
+        graphExec = nullptr;
+        graph = nullptr;
+        cudaFree(dDesc);
+        cudaFree(dIn);
+        cudaFree(dRoll);
+        cudaFree(dUpd);
+        cudaFree(dVer);
+        if (hIn)
+            cudaFreeHost(hIn);
+        if (ownStream && stream)
+            cudaStreamDestroy(stream);
+    }
+};
+
+namespace
+{
+
+int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStream, dr_mppi_batch** out)
+{
+    if (n <= 0 || !hs)
+        return fail(DR_ERR_INVALID_ARG, "empty batch");
+    auto b = std::make_unique<dr_mppi_batch>();
+    b->hs.assign(hs, hs + n);
+    b->device = hs[0]->device;
+    b->nopp = hs[0]->nopp;
+    b->nth = hs[0]->nth;
+    b->spl = hs[0]->spl;
+    b->verify = hs[0]->cfg.verify != 0;
+    for (int i = 0; i < n; i++)
+        if (!hs[i] || hs[i]->device != b->device || hs[i]->nopp != b->nopp || hs[i]->nth != b->nth || hs[i]->spl != b->spl ||
+            (hs[i]->cfg.verify != 0) != b->verify)
+            return fail(DR_ERR_INVALID_ARG, "a batch needs controllers on one device with equal n_opp, n_theta, use_splines and verify");
+    CK(cudaSetDevice(b->device));
+    b->stream = stream;
+    b->ownStream = ownStream;
+    std::vector<MppiDev> descs;
+    std::vector<Tile> roll, upd, ver;
+    const int spb = rolloutSamplesPerBlock(b->nth);
+    int maxT = 0, maxM = 0, maxNbpT = 0;
+    for (int i = 0; i < n; i++)
+    {
+        dr_mppi* h = hs[i];
+        descs.push_back(h->desc);
+        for (int s0 = 0; s0 < h->K; s0 += spb)
+            roll.push_back(Tile{i, s0, std::min(spb, h->K - s0), 0});
+        for (int bk = 0; bk < h->nbp * h->M; bk++)
+            upd.push_back(Tile{i, bk, 0, 0});
+        if (b->verify)
+            for (int plan = 0; plan < 2; plan++)
+                for (int v0 = 0; v0 < h->V; v0 += 128)
+                    ver.push_back(Tile{i, v0, std::min(128, h->V - v0), plan});
+        maxT = std::max(maxT, h->T);
+        maxM = std::max(maxM, h->M);
+        maxNbpT = std::max(maxNbpT, h->nbp * h->T);
+    }
+    for (int i = 0; i < n; i++)
+    {
+        b->rollSmem = std::max(b->rollSmem, mppiRolloutSmem(b->nth, hs[i]->T, hs[i]->M, b->spl));
+        b->verSmem = std::max(b->verSmem, mppiVerifySmem(b->nth, hs[i]->T));
+    }
+    b->proSmem = ((size_t)maxNbpT * 2 + (size_t)maxM * 2) * 4;
+    if (b->rollSmem > 227 * 1024)
+        return fail(DR_ERR_INVALID_ARG, "horizon x knots too large for shared memory");
+    b->nRoll = (int)roll.size();
+    b->nUpd = (int)upd.size();
+    b->nVer = (int)ver.size();
+    CK(cudaMalloc(&b->dDesc, sizeof(MppiDev) * n));
+    CK(cudaMemcpy(b->dDesc, descs.data(), sizeof(MppiDev) * n, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&b->dIn, sizeof(MppiIn) * n));
+    CK(cudaMallocHost(&b->hIn, sizeof(MppiIn) * n));
+    CK(cudaMalloc(&b->dRoll, sizeof(Tile) * std::max<size_t>(roll.size(), 1)));
+    CK(cudaMemcpy(b->dRoll, roll.data(), sizeof(Tile) * roll.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&b->dUpd, sizeof(Tile) * std::max<size_t>(upd.size(), 1)));
+    CK(cudaMemcpy(b->dUpd, upd.data(), sizeof(Tile) * upd.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&b->dVer, sizeof(Tile) * std::max<size_t>(ver.size(), 1)));
+    if (!ver.empty())
+        CK(cudaMemcpy(b->dVer, ver.data(), sizeof(Tile) * ver.size(), cudaMemcpyHostToDevice));
+    *out = b.release();
+    return DR_OK;
+}
+
+int checkMppiCfg(const dr_env_config* env, const dr_mppi_config* c)
+{
+    if (!c)
+        return fail(DR_ERR_INVALID_ARG, "cfg is NULL");
+    if (c->n_samples < 1 || c->n_samples > (1 << 24))
+        return fail(DR_ERR_INVALID_ARG, "n_samples must be in [1, 2^24]");
+    if (c->n_timesteps < 2 || c->n_timesteps > DR_MAX_T)
+        return fail(DR_ERR_INVALID_ARG, "n_timesteps must be in [2, 256]");
+    if (c->use_splines)
+    {
+        if (c->n_knots < 2 || c->n_knots > DR_MAX_KNOTS)
+            return fail(DR_ERR_INVALID_ARG, "n_knots must be in [2, 64]");
+        for (int i = 0; i < c->n_knots; i++)
+        {
+            if (c->knots[i] < 0 || c->knots[i] > c->n_timesteps - 2)
+                return fail(DR_ERR_INVALID_ARG, "knots must lie in [0, T-2]");
+            if (i > 0 && c->knots[i] <= c->knots[i - 1])
+                return fail(DR_ERR_INVALID_ARG, "knots must be strictly increasing");
+        }
+    }
+    if (c->verify)
+    {
+        if (c->n_verif_samples < 1)
+            return fail(DR_ERR_INVALID_ARG, "n_verif_samples must be positive");
+        if (c->verif_horizon < 1 || c->verif_horizon > c->n_timesteps)
+            return fail(DR_ERR_INVALID_ARG, "verif_horizon must be in [1, n_timesteps]");
+    }
+    if (!(c->inv_temperature > 0.0f) || !std::isfinite(c->inv_temperature))
+        return fail(DR_ERR_INVALID_ARG, "inv_temperature must be positive");
+    if (!mppiSupported(env->n_opp, env->n_theta))
+        return fail(DR_ERR_UNSUPPORTED, "(n_opp, n_theta) combination not compiled in");
+    return DR_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int dr_abi_version(void)
+{
+    return DR_ABI_VERSION;
+}
+
+int dr_supported(int n_opp, int n_theta)
+{
+    return mppiSupported(n_opp, n_theta) && prSupported(n_opp, n_theta);
+}
+
+const char* dr_last_error(void)
+{
+    return lastError().c_str();
+}
+
+const char* dr_status_string(int s)
+{
+    switch (s)
+    {
+    case DR_OK: return "ok";
+    case DR_ERR_INVALID_ARG: return "invalid argument";
+    case DR_ERR_UNSUPPORTED: return "unsupported configuration";
+    case DR_ERR_CUDA: return "CUDA error";
+    case DR_ERR_OOM: return "out of device memory";
+    case DR_ERR_NO_DEVICE: return "no CUDA device";
+    case DR_ERR_TIMEOUT: return "device wait timed out";
+    case DR_ERR_STATE: return "invalid state";
+    default: return "unknown";
+    }
+}
+
+int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream, dr_mppi** out)
+{
+    if (!out)
+        return fail(DR_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = checkEnv(env);
+    if (rc)
+        return rc;
+    rc = checkMppiCfg(env, cfg);
+    if (rc)
+        return rc;
+    rc = selectDevice(device);
+    if (rc)
+        return rc;
+    auto h = std::make_unique<dr_mppi>();
+    h->device = device;
+    h->env = *env;
+    h->env.p_grid = h->env.dp_grid = h->env.t_grid = h->env.kappa_grid = nullptr;
+    h->cfg = *cfg;
+    h->seed = seed;
+    h->nth = env->n_theta;
+    h->nopp = env->n_opp;
+    h->K = cfg->n_samples;
+    h->T = cfg->n_timesteps;
+    h->spl = cfg->use_splines != 0;
+    h->M = h->spl ? cfg->n_knots : h->T;
+    if (!h->spl)
+        for (int i = 0; i < DR_MAX_KNOTS; i++)
+            h->cfg.knots[i] = i; // unused in dense mode
+    h->nbp = h->nth + 1;
+    h->V = cfg->verify ? cfg->n_verif_samples : 0;
+    h->H = cfg->verif_horizon;
+    h->lambda = cfg->inv_temperature;
+    const int K = h->K, T = h->T, M = h->M, nbp = h->nbp, nth = h->nth;
+    MppiDev& D = h->desc;
+    D.env = toEnvParams(*env);
+    D.cfg.K = K;
+    D.cfg.T = T;
+    D.cfg.M = M;
+    D.cfg.useSplines = h->spl ? 1 : 0;
+    D.cfg.V = h->V;
+    D.cfg.H = h->H;
+    D.cfg.nth = nth;
+    D.cfg.nopp = h->nopp;
+    for (int i = 0; i < DR_MAX_KNOTS; i++)
+        D.cfg.knots[i] = h->cfg.knots[i];
+    float s0 = cfg->sampling_noise_dim[0], s1 = cfg->sampling_noise_dim[1];
+    if (s0 == 0.0f && s1 == 0.0f)
+        s0 = s1 = cfg->sampling_noise;
+    D.cfg.sigma0 = s0;
+    D.cfg.sigma1 = s1;
+    D.cfg.minConf = cfg->min_confidence;
+    D.cfg.w = MppiCostW{cfg->coll_dist_factor, cfg->boundary_cost, cfg->boundary_threshold_factor, cfg->outside_cost,
+                        cfg->win_cost,         cfg->opp_win_cost,  cfg->final_adv_weight,          cfg->final_opp_adv_weight};
+    D.cfg.k0 = (uint32_t)seed;
+    D.cfg.k1 = (uint32_t)(seed >> 32);
+    if (h->cfg.min_nu == 0.0f && h->cfg.max_nu == 0.0f)
+    {
+        h->cfg.min_nu = 0.0005f; // controllers.h:47-48
+        h->cfg.max_nu = 0.001f;
+    }
+
+    // device memory
+    float *grids, *B, *knots, *costsTrue, *costs, *dense, *prevDense, *nu, *minCosts;
+    int *binfo, *stats;
+    unsigned *counter, *failc;
+    Arena& A = h->arena;
+    A.add(grids, GRID_FLOATS * 4);
+    A.add(B, a16((size_t)T * M * 4));
+    A.add(knots, a16((size_t)nbp * M * 2 * 4));
+    A.add(costsTrue, (size_t)nth * K * 4);
+    A.add(binfo, (size_t)nth * K * 4);
+    A.add(costs, (size_t)nbp * K * 4);
+    A.add(counter, 16);
+    // result block, one contiguous range
+    size_t oFail = 0, oDense = a16(oFail + (size_t)2 * T * 4), oPrev = oDense + a16((size_t)nbp * T * 2 * 4), oNu = oPrev + a16((size_t)nbp * T * 2 * 4),
+           oMin = oNu + a16((size_t)nbp * 4), oStats = oMin + a16((size_t)nbp * M * 4), resBytes = oStats + 16;
+    unsigned char* res;
+    A.add(res, resBytes);
+    CK(A.alloc());
+    failc = (unsigned*)(res + oFail);
+    dense = (float*)(res + oDense);
+    prevDense = (float*)(res + oPrev);
+    nu = (float*)(res + oNu);
+    minCosts = (float*)(res + oMin);
+    stats = (int*)(res + oStats);
+    D.grids = grids;
+    D.B = B;
+    D.knots = knots;
+    D.costsTrue = costsTrue;
+    D.binfo = binfo;
+    D.costs = costs;
+    D.counter = counter;
+    D.fail = failc;
+    D.dense = dense;
+    D.prevDense = prevDense;
+    D.nu = nu;
+    D.minCosts = minCosts;
+    D.stats = stats;
+    D.resBytes = resBytes;
+    std::vector<float> g = packGrids(*env);
+    CK(cudaMemcpy(grids, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    if (h->spl)
+    {
+        std::vector<float> Bm = splineMatrix(T, M, h->cfg.knots);
+        CK(cudaMemcpy(B, Bm.data(), Bm.size() * 4, cudaMemcpyHostToDevice));
+    }
+    h->hNominal.assign((size_t)nbp * T * 2, 0.0f);
+    if (nominal)
+        std::memcpy(h->hNominal.data(), nominal, h->hNominal.size() * 4);
+    CK(cudaMemcpy(dense, h->hNominal.data(), h->hNominal.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(prevDense, h->hNominal.data(), h->hNominal.size() * 4, cudaMemcpyHostToDevice));
+    if (!h->spl)
+        CK(cudaMemcpy(knots, h->hNominal.data(), h->hNominal.size() * 4, cudaMemcpyHostToDevice)); // spline knots start at 0 (mppi_controller.cu:205)
+    CK(cudaMallocHost(&h->hRes, resBytes));
+    h->fcNew.assign(T, 0u);
+    h->fcOld.assign(T, 0u);
+    h->fc.assign(T, 0u);
+    cudaStream_t s = (cudaStream_t)stream;
+    bool own = false;
+    if (!s)
+    {
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        own = true;
+    }
+    h->stream = s;
+    h->ownStream = own;
+    dr_mppi* raw = h.get();
+    rc = buildMppiBatch(&raw, 1, s, false, &h->self);
+    if (rc)
+        return rc;
+    *out = h.release();
+    return DR_OK;
+}
+
+int dr_mppi_destroy(dr_mppi* h)
+{
+    if (!h)
+        return DR_OK;
+    cudaSetDevice(h->device);
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    if (h->self)
+    {
+        h->self->release();
+        delete h->self;
+    }
+    h->arena.release();
+    if (h->hRes)
+        cudaFreeHost(h->hRes);
+    if (h->ownStream && h->stream)
+        cudaStreamDestroy(h->stream);
+    delete h;
+    return DR_OK;
+}
+
+int dr_mppi_step(dr_mppi* h, const dr_sim_state* state, const float* belief, float* out_action, dr_mppi_info* info)
+{
+    if (!h || !state || !belief || !out_action)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->step(state, belief, h->nth, out_action, info);
+}
+
+int dr_mppi_get_nominal(const dr_mppi* h, float* out, size_t n)
+{
+    if (!h || !out || n < h->hNominal.size())
+        return fail(DR_ERR_INVALID_ARG, "output too small");
+    std::memcpy(out, h->hNominal.data(), h->hNominal.size() * 4);
+    return DR_OK;
+}
+
+int dr_mppi_get_knots(dr_mppi* h, float* out, size_t n)
+{
+    size_t need = (size_t)h->nbp * h->M * 2;
+    if (!h || !out || n < need)
+        return fail(DR_ERR_INVALID_ARG, "output too small");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(out, h->desc.knots, need * 4, cudaMemcpyDeviceToHost));
+    return DR_OK;
+}
+
+int dr_mppi_get_fail_counts(const dr_mppi* h, uint32_t* a, uint32_t* b, uint32_t* c, size_t n)
+{
+    if (!h || n < (size_t)h->T)
+        return fail(DR_ERR_INVALID_ARG, "output too small");
+    if (a)
+        std::memcpy(a, h->fcNew.data(), h->T * 4);
+    if (b)
+        std::memcpy(b, h->fcOld.data(), h->T * 4);
+    if (c)
+        std::memcpy(c, h->fc.data(), h->T * 4);
+    return DR_OK;
+}
+
+float dr_mppi_get_temperature(const dr_mppi* h)
+{
+    return h ? h->lambda : NAN;
+}
+
+int dr_mppi_set_temperature(dr_mppi* h, float v)
+{
+    if (!h || !(v > 0.0f))
+        return fail(DR_ERR_INVALID_ARG, "temperature must be positive");
+    h->lambda = v;
+    return DR_OK;
+}
+
+uint64_t dr_mppi_get_step(const dr_mppi* h)
+{
+    return h ? h->step : 0;
+}
+
+int dr_mppi_io_bytes(const dr_mppi* h, size_t* h2d, size_t* d2h)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    if (h2d)
+        *h2d = sizeof(MppiIn);
+    if (d2h)
+        *d2h = h->desc.resBytes;
+    return DR_OK;
+}
+
+int dr_mppi_set_step(dr_mppi* h, uint64_t step)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    h->step = step;
+    return DR_OK;
+}
+
+int dr_mppi_set_profiling(dr_mppi* h, int on)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    h->self->profiling = on != 0;
+    h->self->timer.reset();
+    return DR_OK;
+}
+
+int dr_mppi_get_kernel_times(dr_mppi* h, const char** names, float* ms, int n, int* count)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    return kernelTimes(h->self->timer, names, ms, n, count);
+}
+
+int dr_mppi_batch_create(dr_mppi* const* hs, int n, void* stream, dr_mppi_batch** out)
+{
+    if (!out)
+        return fail(DR_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (n <= 0 || !hs || !hs[0])
+        return fail(DR_ERR_INVALID_ARG, "empty batch");
+    CK(cudaSetDevice(hs[0]->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    bool own = false;
+    if (!s)
+    {
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        own = true;
+    }
+    return buildMppiBatch(hs, n, s, own, out);
+}
+
+int dr_mppi_batch_destroy(dr_mppi_batch* b)
+{
+    if (!b)
+        return DR_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    b->release();
+    delete b;
+    return DR_OK;
+}
+
+int dr_mppi_batch_step(dr_mppi_batch* b, const dr_sim_state* states, const float* beliefs, float* out_actions, dr_mppi_info* infos)
+{
+    if (!b || !states || !beliefs || !out_actions)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return b->step(states, beliefs, DR_MAX_THETA, out_actions, infos);
+}
+
+int dr_mppi_batch_set_graph(dr_mppi_batch* b, int use_graph)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    b->useGraph = use_graph != 0;
+    return DR_OK;
+}
+
+// Device-resident step for throughput measurement: inputs are MppiIn-compatible states
+// and beliefs already on the device; the controllers' host state (temperature, shift
+// decision, step counter) is not advanced and no results are copied back.
+int dr_mppi_batch_step_dev(dr_mppi_batch* b, const dr_sim_state* states_dev, const float* beliefs_dev)
+{
+    if (!b || !states_dev || !beliefs_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    CK(cudaSetDevice(b->device));
+    const int n = (int)b->hs.size();
+    for (int i = 0; i < n; i++)
+    {
+        MppiIn tmp = b->hs[i]->input(dr_sim_state{}, std::vector<float>(DR_MAX_THETA, 0.0f).data());
+        b->hIn[i] = tmp;
+    }
+    // host part of the record (temperature, step, pending shift), then state and belief device-to-device
+    CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(MppiIn) * n, cudaMemcpyHostToDevice, b->stream));
+    for (int i = 0; i < n; i++)
+    {
+        CK(cudaMemcpyAsync(&b->dIn[i].state, states_dev + i, sizeof(dr_sim_state), cudaMemcpyDeviceToDevice, b->stream));
+        CK(cudaMemcpyAsync(&b->dIn[i].belief, beliefs_dev + (size_t)i * DR_MAX_THETA, DR_MAX_THETA * 4, cudaMemcpyDeviceToDevice, b->stream));
+    }
+    return b->launchAll(b->dIn, b->profiling, &b->timer);
+}
+
+// ---- test hooks -------------------------------------------------------------------------------
+
+int dr_mppi_debug_noise(dr_mppi* h, float* noise, size_t n)
+{
+    size_t need = (size_t)h->nbp * h->M * h->K * 2;
+    if (!h || !noise || n < need)
+        return fail(DR_ERR_INVALID_ARG, "output too small");
+    CK(cudaSetDevice(h->device));
+    dr_mppi_batch* b = h->self;
+    b->hIn[0] = h->input(dr_sim_state{}, std::vector<float>(DR_MAX_THETA, 0.0f).data());
+    float* d = nullptr;
+    CK(cudaMalloc(&d, need * 4));
+    cudaMemcpyAsync(b->dIn, b->hIn, sizeof(MppiIn), cudaMemcpyHostToDevice, h->stream);
+    LaunchArgs a = b->args(nullptr, 0, b->dIn);
+    cudaError_t e = launchMppiNoise(a, need / 2, d);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(noise, d, need * 4, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    CK(e);
+    return DR_OK;
+}
+
+static int applyPending(dr_mppi* h, const dr_sim_state* state, const float* belief)
+{
+    dr_mppi_batch* b = h->self;
+    b->hIn[0] = h->input(*state, belief);
+    CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(MppiIn), cudaMemcpyHostToDevice, h->stream));
+    CK(launchMppiPrologue(b->args(nullptr, 0, b->dIn), 1, b->proSmem));
+    // the shift is now applied; the next step must not apply it again
+    h->pendBranch = -1;
+    b->hIn[0].pendBranch = -1;
+    CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(MppiIn), cudaMemcpyHostToDevice, h->stream));
+    return DR_OK;
+}
+
+int dr_mppi_debug_rollout(dr_mppi* h, const dr_sim_state* state, const float* belief, float* costs_true, int32_t* branch_used, int32_t* branch_time,
+                          float* costs)
+{
+    if (!h || !state || !belief)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    CK(cudaSetDevice(h->device));
+    int rc = applyPending(h, state, belief);
+    if (rc)
+        return rc;
+    dr_mppi_batch* b = h->self;
+    CK(launchMppiRollout(b->args(b->dRoll, b->nRoll, b->dIn), h->nopp, h->nth, h->spl, b->rollSmem));
+    const size_t nk = (size_t)h->nth * h->K;
+    std::vector<int> info(nk);
+    if (costs_true)
+        CK(cudaMemcpyAsync(costs_true, h->desc.costsTrue, nk * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(info.data(), h->desc.binfo, nk * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (costs)
+        CK(cudaMemcpyAsync(costs, h->desc.costs, (size_t)h->nbp * h->K * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < nk; i++)
+    {
+        if (branch_used)
+            branch_used[i] = info[i] >> 16;
+        if (branch_time)
+            branch_time[i] = (int)(short)(info[i] & 0xffff);
+    }
+    return DR_OK;
+}
+
+int dr_mppi_debug_update(dr_mppi* h, const float* belief, const float* costs_true, const int32_t* branch_used, const int32_t* branch_time,
+                         float* dense_nominal, float* min_costs, float* nu)
+{
+    if (!h || !belief || !costs_true || !branch_used || !branch_time)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    CK(cudaSetDevice(h->device));
+    dr_sim_state st{};
+    int rc = applyPending(h, &st, belief);
+    if (rc)
+        return rc;
+    dr_mppi_batch* b = h->self;
+    const size_t nk = (size_t)h->nth * h->K;
+    std::vector<int> info(nk);
+    for (size_t i = 0; i < nk; i++)
+        info[i] = (branch_used[i] << 16) | (branch_time[i] & 0xffff);
+    CK(cudaMemcpyAsync(h->desc.costsTrue, costs_true, nk * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->desc.binfo, info.data(), nk * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(launchMppiAggregate(b->args(nullptr, 0, b->dIn), h->nth, h->K));
+    CK(launchMppiUpdate(b->args(b->dUpd, b->nUpd, b->dIn), h->nth));
+    if (dense_nominal)
+        CK(cudaMemcpyAsync(dense_nominal, h->desc.dense, (size_t)h->nbp * h->T * 2 * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (min_costs)
+        CK(cudaMemcpyAsync(min_costs, h->desc.minCosts, (size_t)h->nbp * h->M * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (nu)
+        CK(cudaMemcpyAsync(nu, h->desc.nu, (size_t)h->nbp * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return DR_OK;
+}
+
+int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* belief, const float* dense_plan, int plan, uint32_t* fail_count,
+                         int32_t* fail_time, int32_t* thetas)
+{
+    if (!h || !state || !belief || !dense_plan || plan < 0 || plan > 1 || h->V <= 0)
+        return fail(DR_ERR_INVALID_ARG, "bad argument (verification disabled?)");
+    CK(cudaSetDevice(h->device));
+    const int V = h->V, T = h->T;
+    // a private copy of the instance with its own plan and histogram buffers
+    MppiDev D = h->desc;
+    float* dPlan = nullptr;
+    unsigned* dFail = nullptr;
+    int *dFt = nullptr, *dTh = nullptr, *dStats = nullptr;
+    MppiDev* dD = nullptr;
+    MppiIn* dIn = nullptr;
+    Tile* dT = nullptr;
+    std::vector<Tile> tiles;
+    for (int v0 = 0; v0 < V; v0 += 128)
+        tiles.push_back(Tile{0, v0, std::min(128, V - v0), plan});
+    size_t planBytes = a16((size_t)h->nbp * T * 2 * 4);
+    cudaError_t e = cudaMalloc(&dPlan, planBytes);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dFail, 2 * T * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dFt, V * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dTh, V * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dStats, 16);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dD, sizeof(MppiDev));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dIn, sizeof(MppiIn));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dT, sizeof(Tile) * tiles.size());
+    if (e == cudaSuccess)
+    {
+        D.dense = dPlan;
+        D.prevDense = dPlan;
+        D.fail = dFail;
+        D.stats = dStats;
+        MppiIn in = h->input(*state, belief);
+        cudaMemsetAsync(dFail, 0, 2 * T * 4, h->stream);
+        cudaMemsetAsync(dStats, 0, 16, h->stream);
+        cudaMemcpyAsync(dPlan, dense_plan, (size_t)h->nbp * T * 2 * 4, cudaMemcpyHostToDevice, h->stream);
+        cudaMemcpyAsync(dD, &D, sizeof(MppiDev), cudaMemcpyHostToDevice, h->stream);
+        cudaMemcpyAsync(dIn, &in, sizeof(MppiIn), cudaMemcpyHostToDevice, h->stream);
+        cudaMemcpyAsync(dT, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, h->stream);
+        LaunchArgs a;
+        a.stream = h->stream;
+        a.mppi = dD;
+        a.mppiIn = dIn;
+        a.tiles = dT;
+        a.nTiles = (int)tiles.size();
+        e = launchMppiVerify(a, h->nopp, h->nth, mppiVerifySmem(h->nth, T), dFt, dTh);
+        std::vector<unsigned> fc(2 * T);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(fc.data(), dFail, 2 * T * 4, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess && fail_time)
+            e = cudaMemcpyAsync(fail_time, dFt, V * 4, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess && thetas)
+            e = cudaMemcpyAsync(thetas, dTh, V * 4, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(h->stream);
+        if (e == cudaSuccess && fail_count)
+            std::memcpy(fail_count, fc.data() + plan * T, T * 4);
+    }
+    cudaFree(dPlan);
+    cudaFree(dFail);
+    cudaFree(dFt);
+    cudaFree(dTh);
+    cudaFree(dStats);
+    cudaFree(dD);
+    cudaFree(dIn);
+    cudaFree(dT);
+    CK(e);
+    return DR_OK;
+}
+
+} // extern "C"
+
+extern "C" int dr_mppi_batch_set_profiling(dr_mppi_batch* b, int on)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    b->profiling = on != 0;
+    b->timer.reset();
+    return DR_OK;
+}
+
+extern "C" int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** names, float* ms, int n, int* count)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    CK(cudaSetDevice(b->device));
+    return kernelTimes(b->timer, names, ms, n, count);
+}

@@ -1,0 +1,735 @@
+// C ABI of the PR-MPPI controller (reference PRMPPIController, src/prmppi_controller.cu)
+// and of the device environment step (reference SimulationEngine::dynStep,
+// src/engine.cpp:286-312).
+#include <algorithm>
+#include <memory>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/drmppi.h"
+#include "common.cuh"
+#include "hostutil.hpp"
+#include "instance.cuh"
+#include "launch.h"
+
+using namespace dr;
+
+struct dr_prmppi
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    dr_env_config env{};
+    dr_prmppi_config cfg{};
+    uint64_t seed = 0;
+    int nth = 0, nopp = 0, K = 0, T = 0, P = 0;
+    Arena arena;
+    PrDev desc{};
+    unsigned char* hRes = nullptr;
+    std::vector<float> hNom, hRob;
+    bool useNomPlan = true, resetNom = false;
+    float lambda[3] = {1, 1, 1}; // invTempNomFull, invTempRobFull, invTempRobSafe
+    uint64_t step = 0;
+    dr_prmppi_batch* self = nullptr;
+
+    PrIn input(const dr_sim_state& s, const float* belief) const
+    {
+        PrIn in{};
+        in.state = s;
+        for (int i = 0; i < DR_MAX_THETA; i++)
+            in.belief[i] = i < nth ? belief[i] : 0.0f;
+        for (int i = 0; i < 3; i++)
+            in.lambda[i] = lambda[i];
+        in.step = (uint32_t)step;
+        return in;
+    }
+
+    template <typename T_> const T_* at(const void* devPtr) const
+    {
+        return (const T_*)(hRes + ((const unsigned char*)devPtr - (const unsigned char*)desc.nom));
+    }
+
+    // host tail of PRMPPIController::getControl (prmppi_controller.cu:268-346); the
+    // candidate choice and the safety decision were taken on the device.
+    void finish(float* outAction, dr_prmppi_info* info)
+    {
+        const float* nom = at<float>(desc.nom);
+        const float* rob = at<float>(desc.rob);
+        const float* mins = at<float>(desc.minCosts);
+        const float* nu = at<float>(desc.nu);
+        const float* full = at<float>(desc.candFull);
+        const int* dec = at<int>(desc.decision);
+        const int* stats = at<int>(desc.stats);
+        resetNom = dec[0] != 0;
+        useNomPlan = dec[1] != 0;
+        hNom.assign(nom, nom + (size_t)T * 2);
+        hRob.assign(rob, rob + (size_t)T * 2);
+        const float* first = useNomPlan ? nom : rob;
+        outAction[0] = first[0];
+        outAction[1] = first[1];
+        for (int w = 0; w < 3; w++)
+        {
+            // adaptTemperature (prmppi_controller.cu:328-342)
+            float& invTemp = lambda[w];
+            if (nu[w] > cfg.max_nu * (float)K && invTemp > 0.01f)
+                invTemp *= 0.9f;
+            else if (nu[w] < cfg.min_nu * (float)K && invTemp < 100.0f)
+                invTemp *= 1.2f;
+        }
+        step++;
+        if (info)
+        {
+            info->use_nom_plan = useNomPlan;
+            info->reset_nom = resetNom;
+            float c1 = 0.0f, c2 = 0.0f;
+            for (int p = 0; p < P; p++)
+            {
+                c1 += full[p];
+                c2 += full[P + p];
+            }
+            info->cand_cost[0] = c1 / (float)P;
+            info->cand_cost[1] = c2 / (float)P;
+            for (int w = 0; w < 3; w++)
+            {
+                info->min_costs[w] = mins[w];
+                info->nu[w] = nu[w];
+                info->inv_temperature[w] = lambda[w];
+            }
+            info->nonfinite_costs = stats[0];
+        }
+    }
+};
+
+struct dr_prmppi_batch
+{
+    std::vector<dr_prmppi*> hs;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    int nopp = 0, nth = 0, maxT = 0, maxP = 0;
+    PrDev* dDesc = nullptr;
+    PrIn* dIn = nullptr;
+    PrIn* hIn = nullptr;
+    Tile *dRoll = nullptr, *dWa = nullptr;
+    int nRoll = 0, nWa = 0;
+    size_t rollSmem = 0;
+    bool useGraph = true;
+    bool profiling = false;
+    Timer timer;
+    int runs = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graphExec = nullptr;
+
+    LaunchArgs args(const Tile* tiles, int n, const PrIn* in) const
+    {
+        LaunchArgs a;
+        a.stream = stream;
+        a.pr = dDesc;
+        a.prIn = in;
+        a.tiles = tiles;
+        a.nTiles = n;
+        return a;
+    }
+
+    int launchAll(const PrIn* in, bool profile, Timer* timer)
+    {
+        const int n = (int)hs.size();
+        if (profile)
+        {
+            timer->begin();
+            timer->mark("prologue", stream);
+        }
+        CK(launchPrPrologue(args(nullptr, 0, in), n));
+        if (profile)
+            timer->mark("rollout", stream);
+        CK(launchPrRollout(args(dRoll, nRoll, in), nopp, nth, rollSmem));
+        if (profile)
+            timer->mark("weighted", stream);
+        CK(launchPrReduce(args(dWa, nWa, in)));
+        if (profile)
+            timer->mark("candidates", stream);
+        CK(launchPrCandidates(args(nullptr, 0, in), nopp, nth, n, maxT, 0));
+        if (profile)
+        {
+            timer->mark("end", stream);
+            timer->end();
+        }
+        return DR_OK;
+    }
+
+    int copyResults()
+    {
+        for (auto* h : hs)
+            CK(cudaMemcpyAsync(h->hRes, h->desc.nom, h->desc.resBytes, cudaMemcpyDeviceToHost, stream));
+        return DR_OK;
+    }
+
+    int enqueue(bool profile)
+    {
+        const int n = (int)hs.size();
+        if (profile || !useGraph || runs == 0)
+        {
+            CK(cudaMemcpyAsync(dIn, hIn, sizeof(PrIn) * n, cudaMemcpyHostToDevice, stream));
+            int rc = launchAll(dIn, profile, &timer);
+            if (rc)
+                return rc;
+            rc = copyResults();
+            runs++;
+            return rc;
+        }
+        if (!graphExec)
+        {
+            CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            cudaMemcpyAsync(dIn, hIn, sizeof(PrIn) * n, cudaMemcpyHostToDevice, stream);
+            int rc = launchAll(dIn, false, nullptr);
+            if (rc == DR_OK)
+                rc = copyResults();
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(stream, &g);
+            if (rc)
+                return rc;
+            CK(e);
+            graph = g;
+            CK(cudaGraphInstantiate(&graphExec, graph, 0));
+        }
+        CK(cudaGraphLaunch(graphExec, stream));
+        runs++;
+        return DR_OK;
+    }
+
+    int step(const dr_sim_state* states, const float* beliefs, int stride, float* actions, dr_prmppi_info* infos)
+    {
+        const int n = (int)hs.size();
+        CK(cudaSetDevice(device));
+        for (int i = 0; i < n; i++)
+            hIn[i] = hs[i]->input(states[i], beliefs + (size_t)i * stride);
+        bool profile = profiling;
+        int rc = enqueue(profile);
+        if (rc)
+            return rc;
+        CK(cudaStreamSynchronize(stream));
+        for (int i = 0; i < n; i++)
+            hs[i]->finish(actions + 2 * i, infos ? infos + i : nullptr);
+        return DR_OK;
+    }
+
+    void release()
+    {
+        if (graphExec)
+            cudaGraphExecDestroy(graphExec);
+        if (graph)
+            cudaGraphDestroy(graph);
+        graphExec = nullptr;
+        graph = nullptr;
+        cudaFree(dDesc);
+        cudaFree(dIn);
+        cudaFree(dRoll);
+        cudaFree(dWa);
+        if (hIn)
+            cudaFreeHost(hIn);
+        if (ownStream && stream)
+            cudaStreamDestroy(stream);
+    }
+};
+
+namespace
+{
+
+int buildPrBatch(dr_prmppi* const* hs, int n, cudaStream_t stream, bool ownStream, dr_prmppi_batch** out)
+{
+    if (n <= 0 || !hs)
+        return fail(DR_ERR_INVALID_ARG, "empty batch");
+    auto b = std::make_unique<dr_prmppi_batch>();
+    b->hs.assign(hs, hs + n);
+    b->device = hs[0]->device;
+    b->nopp = hs[0]->nopp;
+    b->nth = hs[0]->nth;
+    for (int i = 0; i < n; i++)
+        if (!hs[i] || hs[i]->device != b->device || hs[i]->nopp != b->nopp || hs[i]->nth != b->nth)
+            return fail(DR_ERR_INVALID_ARG, "a batch needs controllers on one device with equal n_opp and n_theta");
+    CK(cudaSetDevice(b->device));
+    b->stream = stream;
+    b->ownStream = ownStream;
+    std::vector<PrDev> descs;
+    std::vector<Tile> roll, wa;
+    for (int i = 0; i < n; i++)
+    {
+        dr_prmppi* h = hs[i];
+        descs.push_back(h->desc);
+        const int spb = prRolloutSamplesPerBlock() / h->P;
+        for (int nr = 0; nr < 2; nr++)
+            for (int s0 = 0; s0 < h->K; s0 += spb)
+                roll.push_back(Tile{i, s0, std::min(spb, h->K - s0), nr});
+        for (int w = 0; w < 3 * h->T; w++)
+            wa.push_back(Tile{i, w, 0, 0});
+        b->maxT = std::max(b->maxT, h->T);
+        b->maxP = std::max(b->maxP, h->P);
+        b->rollSmem = std::max(b->rollSmem, prRolloutSmem(h->T));
+    }
+    b->nRoll = (int)roll.size();
+    b->nWa = (int)wa.size();
+    CK(cudaMalloc(&b->dDesc, sizeof(PrDev) * n));
+    CK(cudaMemcpy(b->dDesc, descs.data(), sizeof(PrDev) * n, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&b->dIn, sizeof(PrIn) * n));
+    CK(cudaMallocHost(&b->hIn, sizeof(PrIn) * n));
+    CK(cudaMalloc(&b->dRoll, sizeof(Tile) * roll.size()));
+    CK(cudaMemcpy(b->dRoll, roll.data(), sizeof(Tile) * roll.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&b->dWa, sizeof(Tile) * wa.size()));
+    CK(cudaMemcpy(b->dWa, wa.data(), sizeof(Tile) * wa.size(), cudaMemcpyHostToDevice));
+    *out = b.release();
+    return DR_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
+                     dr_prmppi** out)
+{
+    if (!out)
+        return fail(DR_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = checkEnv(env);
+    if (rc)
+        return rc;
+    if (!cfg)
+        return fail(DR_ERR_INVALID_ARG, "cfg is NULL");
+    if (cfg->n_samples < 1 || cfg->n_samples > (1 << 22))
+        return fail(DR_ERR_INVALID_ARG, "n_samples must be in [1, 2^22]");
+    if (cfg->n_timesteps < 2 || cfg->n_timesteps > DR_MAX_T)
+        return fail(DR_ERR_INVALID_ARG, "n_timesteps must be in [2, 256]");
+    if (cfg->P < 1 || cfg->P > 32)
+        return fail(DR_ERR_INVALID_ARG, "P must be in [1, 32]");
+    for (int i = 0; i < 3; i++)
+        if (!(cfg->inv_temperature > 0.0f))
+            return fail(DR_ERR_INVALID_ARG, "inv_temperature must be positive");
+    if (!prSupported(env->n_opp, env->n_theta))
+        return fail(DR_ERR_UNSUPPORTED, "(n_opp, n_theta) combination not compiled in");
+    rc = selectDevice(device);
+    if (rc)
+        return rc;
+    auto h = std::make_unique<dr_prmppi>();
+    h->device = device;
+    h->env = *env;
+    h->env.p_grid = h->env.dp_grid = h->env.t_grid = h->env.kappa_grid = nullptr;
+    h->cfg = *cfg;
+    if (h->cfg.min_nu == 0.0f && h->cfg.max_nu == 0.0f)
+    {
+        h->cfg.min_nu = 0.0005f; // controllers.h:135-136
+        h->cfg.max_nu = 0.001f;
+    }
+    h->seed = seed;
+    h->nth = env->n_theta;
+    h->nopp = env->n_opp;
+    h->K = cfg->n_samples;
+    h->T = cfg->n_timesteps;
+    h->P = cfg->P;
+    for (int i = 0; i < 3; i++)
+        h->lambda[i] = cfg->inv_temperature; // prmppi_controller.cu:39
+    const int K = h->K, T = h->T, P = h->P;
+    PrDev& D = h->desc;
+    D.env = toEnvParams(*env);
+    D.cfg.K = K;
+    D.cfg.T = T;
+    D.cfg.P = P;
+    D.cfg.nth = h->nth;
+    D.cfg.nopp = h->nopp;
+    float s0 = cfg->sampling_noise_dim[0], s1 = cfg->sampling_noise_dim[1];
+    if (s0 == 0.0f && s1 == 0.0f)
+        s0 = s1 = cfg->sampling_noise;
+    D.cfg.sigma0 = s0;
+    D.cfg.sigma1 = s1;
+    D.cfg.collDistFactor = cfg->coll_dist_factor;
+    D.cfg.boundaryCost = cfg->boundary_cost;
+    D.cfg.boundaryThresholdFactor = cfg->boundary_threshold_factor;
+    D.cfg.winCost = cfg->win_cost;
+    D.cfg.oppWinCost = cfg->opp_win_cost;
+    D.cfg.finalAdvWeight = cfg->final_adv_weight;
+    D.cfg.finalOppAdvWeight = cfg->final_opp_adv_weight;
+    D.cfg.safetyWeight = cfg->safety_weight;
+    D.cfg.k0 = (uint32_t)seed;
+    D.cfg.k1 = (uint32_t)(seed >> 32);
+
+    float *grids, *costNom, *costRob, *avg, *robWork;
+    unsigned* counter;
+    Arena& A = h->arena;
+    A.add(grids, GRID_FLOATS * 4);
+    A.add(costNom, (size_t)P * K * 2 * 4);
+    A.add(costRob, (size_t)P * K * 2 * 4);
+    A.add(avg, (size_t)2 * K * 2 * 4);
+    A.add(robWork, a16((size_t)T * 2 * 4));
+    A.add(counter, 16);
+    const size_t tb = a16((size_t)T * 2 * 4);
+    size_t oNom = 0, oRob = tb, oC1 = 2 * tb, oC2 = 3 * tb, oMin = 4 * tb, oNu = oMin + 16, oFull = oNu + 16, oSafe = oFull + a16((size_t)2 * P * 4),
+           oTh = oSafe + a16((size_t)2 * P * 4), oDec = oTh + a16((size_t)P * 4), oStats = oDec + 16, resBytes = oStats + 16;
+    unsigned char* res;
+    A.add(res, resBytes);
+    CK(A.alloc());
+    D.grids = grids;
+    D.costNom = costNom;
+    D.costRob = costRob;
+    D.avg = avg;
+    D.robWork = robWork;
+    D.nomWork = nullptr;
+    D.counter = counter;
+    D.nom = (float*)(res + oNom);
+    D.rob = (float*)(res + oRob);
+    D.cand1 = (float*)(res + oC1);
+    D.cand2 = (float*)(res + oC2);
+    D.minCosts = (float*)(res + oMin);
+    D.nu = (float*)(res + oNu);
+    D.candFull = (float*)(res + oFull);
+    D.candSafe = (float*)(res + oSafe);
+    D.thetas = (int*)(res + oTh);
+    D.decision = (int*)(res + oDec);
+    D.stats = (int*)(res + oStats);
+    D.resBytes = resBytes;
+    std::vector<float> g = packGrids(*env);
+    CK(cudaMemcpy(grids, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    h->hNom.assign((size_t)T * 2, 0.0f);
+    if (nominal)
+        std::memcpy(h->hNom.data(), nominal, h->hNom.size() * 4);
+    h->hRob = h->hNom;
+    CK(cudaMemcpy(D.nom, h->hNom.data(), h->hNom.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(D.rob, h->hRob.data(), h->hRob.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMallocHost(&h->hRes, resBytes));
+    cudaStream_t s = (cudaStream_t)stream;
+    bool own = false;
+    if (!s)
+    {
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        own = true;
+    }
+    h->stream = s;
+    h->ownStream = own;
+    dr_prmppi* raw = h.get();
+    rc = buildPrBatch(&raw, 1, s, false, &h->self);
+    if (rc)
+        return rc;
+    *out = h.release();
+    return DR_OK;
+}
+
+int dr_prmppi_destroy(dr_prmppi* h)
+{
+    if (!h)
+        return DR_OK;
+    cudaSetDevice(h->device);
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    if (h->self)
+    {
+        h->self->release();
+        delete h->self;
+    }
+    h->arena.release();
+    if (h->hRes)
+        cudaFreeHost(h->hRes);
+    if (h->ownStream && h->stream)
+        cudaStreamDestroy(h->stream);
+    delete h;
+    return DR_OK;
+}
+
+int dr_prmppi_step(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* out_action, dr_prmppi_info* info)
+{
+    if (!h || !state || !belief || !out_action)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->step(state, belief, h->nth, out_action, info);
+}
+
+int dr_prmppi_get_nominals(const dr_prmppi* h, float* nom, float* rob, size_t n)
+{
+    if (!h || n < h->hNom.size())
+        return fail(DR_ERR_INVALID_ARG, "output too small");
+    if (nom)
+        std::memcpy(nom, h->hNom.data(), h->hNom.size() * 4);
+    if (rob)
+        std::memcpy(rob, h->hRob.data(), h->hRob.size() * 4);
+    return DR_OK;
+}
+
+uint64_t dr_prmppi_get_step(const dr_prmppi* h)
+{
+    return h ? h->step : 0;
+}
+
+int dr_prmppi_io_bytes(const dr_prmppi* h, size_t* h2d, size_t* d2h)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    if (h2d)
+        *h2d = sizeof(PrIn);
+    if (d2h)
+        *d2h = h->desc.resBytes;
+    return DR_OK;
+}
+
+int dr_prmppi_set_step(dr_prmppi* h, uint64_t step)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    h->step = step;
+    return DR_OK;
+}
+
+int dr_prmppi_set_profiling(dr_prmppi* h, int on)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    h->self->profiling = on != 0;
+    h->self->timer.reset();
+    return DR_OK;
+}
+
+int dr_prmppi_get_kernel_times(dr_prmppi* h, const char** names, float* ms, int n, int* count)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    return kernelTimes(h->self->timer, names, ms, n, count);
+}
+
+int dr_prmppi_batch_create(dr_prmppi* const* hs, int n, void* stream, dr_prmppi_batch** out)
+{
+    if (!out)
+        return fail(DR_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (n <= 0 || !hs || !hs[0])
+        return fail(DR_ERR_INVALID_ARG, "empty batch");
+    CK(cudaSetDevice(hs[0]->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    bool own = false;
+    if (!s)
+    {
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        own = true;
+    }
+    return buildPrBatch(hs, n, s, own, out);
+}
+
+int dr_prmppi_batch_destroy(dr_prmppi_batch* b)
+{
+    if (!b)
+        return DR_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    b->release();
+    delete b;
+    return DR_OK;
+}
+
+int dr_prmppi_batch_step(dr_prmppi_batch* b, const dr_sim_state* states, const float* beliefs, float* out_actions, dr_prmppi_info* infos)
+{
+    if (!b || !states || !beliefs || !out_actions)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return b->step(states, beliefs, DR_MAX_THETA, out_actions, infos);
+}
+
+int dr_prmppi_batch_step_dev(dr_prmppi_batch* b, const dr_sim_state* states_dev, const float* beliefs_dev)
+{
+    if (!b || !states_dev || !beliefs_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    CK(cudaSetDevice(b->device));
+    const int n = (int)b->hs.size();
+    std::vector<float> zero(DR_MAX_THETA, 0.0f);
+    for (int i = 0; i < n; i++)
+        b->hIn[i] = b->hs[i]->input(dr_sim_state{}, zero.data());
+    CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(PrIn) * n, cudaMemcpyHostToDevice, b->stream));
+    for (int i = 0; i < n; i++)
+    {
+        CK(cudaMemcpyAsync(&b->dIn[i].state, states_dev + i, sizeof(dr_sim_state), cudaMemcpyDeviceToDevice, b->stream));
+        CK(cudaMemcpyAsync(&b->dIn[i].belief, beliefs_dev + (size_t)i * DR_MAX_THETA, DR_MAX_THETA * 4, cudaMemcpyDeviceToDevice, b->stream));
+    }
+    return b->launchAll(b->dIn, b->profiling, &b->timer);
+}
+
+int dr_prmppi_debug_noise(dr_prmppi* h, const float* belief, float* noise, size_t n, int32_t* thetas)
+{
+    size_t need = (size_t)h->T * h->K * 2;
+    if (!h || !belief || (noise && n < need))
+        return fail(DR_ERR_INVALID_ARG, "bad argument");
+    CK(cudaSetDevice(h->device));
+    dr_prmppi_batch* b = h->self;
+    b->hIn[0] = h->input(dr_sim_state{}, belief);
+    CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(PrIn), cudaMemcpyHostToDevice, h->stream));
+    if (noise)
+    {
+        float* d = nullptr;
+        CK(cudaMalloc(&d, need * 4));
+        cudaError_t e = launchPrNoise(b->args(nullptr, 0, b->dIn), need / 2, d);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(noise, d, need * 4, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(h->stream);
+        cudaFree(d);
+        CK(e);
+    }
+    if (thetas)
+    {
+        // theta draw of the prologue, on a scratch copy of the nominals
+        std::vector<float> nom(h->hNom.size()), rob(h->hRob.size());
+        CK(cudaMemcpyAsync(nom.data(), h->desc.nom, nom.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(rob.data(), h->desc.rob, rob.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(launchPrPrologue(b->args(nullptr, 0, b->dIn), 1));
+        CK(cudaMemcpyAsync(thetas, h->desc.thetas, h->P * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaMemcpy(h->desc.nom, nom.data(), nom.size() * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->desc.rob, rob.data(), rob.size() * 4, cudaMemcpyHostToDevice));
+    }
+    return DR_OK;
+}
+
+int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* cost_nom, float* cost_rob)
+{
+    if (!h || !state || !belief)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    CK(cudaSetDevice(h->device));
+    dr_prmppi_batch* b = h->self;
+    std::vector<float> nom(h->hNom.size()), rob(h->hRob.size());
+    CK(cudaMemcpyAsync(nom.data(), h->desc.nom, nom.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(rob.data(), h->desc.rob, rob.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+    b->hIn[0] = h->input(*state, belief);
+    CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(PrIn), cudaMemcpyHostToDevice, h->stream));
+    CK(launchPrPrologue(b->args(nullptr, 0, b->dIn), 1));
+    CK(launchPrRollout(b->args(b->dRoll, b->nRoll, b->dIn), h->nopp, h->nth, b->rollSmem));
+    size_t nb = (size_t)h->P * h->K * 2 * 4;
+    if (cost_nom)
+        CK(cudaMemcpyAsync(cost_nom, h->desc.costNom, nb, cudaMemcpyDeviceToHost, h->stream));
+    if (cost_rob)
+        CK(cudaMemcpyAsync(cost_rob, h->desc.costRob, nb, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    // restore the unshifted nominals: the next step shifts them itself
+    CK(cudaMemcpy(h->desc.nom, nom.data(), nom.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->desc.rob, rob.data(), rob.size() * 4, cudaMemcpyHostToDevice));
+    return DR_OK;
+}
+
+} // extern "C"
+
+// ---- device environment step -------------------------------------------------------------------
+
+template <int NOPP, int NTH>
+__global__ void env_step_kernel(EnvParams E, const float* __restrict__ grids, int trueTheta, float a0, float a1, dr_sim_state* st, float* belief,
+                                int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term)
+{
+    __shared__ float sg[GRID_FLOATS];
+    for (int i = threadIdx.x; i < GRID_FLOATS; i += blockDim.x)
+        sg[i] = grids[i];
+    __syncthreads();
+    if (threadIdx.x != 0)
+        return;
+    constexpr int NA = NOPP + 1;
+    DState<NA> s;
+    for (int a = 0; a < NA; a++)
+    {
+        s.pos[2 * a] = st->pos[2 * a];
+        s.pos[2 * a + 1] = st->pos[2 * a + 1];
+        s.vel[2 * a] = st->vel[2 * a];
+        s.vel[2 * a + 1] = st->vel[2 * a + 1];
+        s.S[a] = st->S[a];
+        s.lat[a] = st->lat_dist[a];
+        s.laps[a] = st->laps[a];
+    }
+    BState<NTH> bs;
+    for (int i = 0; i < NTH; i++)
+        bs.belief[i] = belief[i];
+    bs.predTheta = 0;
+    bs.branchingTime = -1;
+    const Track tr{sg + GRID_P, sg + GRID_T, sg + GRID_K};
+    EnvNoise rng(k0, k1, 0u, 0u, step, S_ENV_STEP);
+    rng.begin_step(0);
+    bool branched = false;
+    StepOut o;
+    if (updateBelief)
+        o = envStep<NOPP, NTH, true, false, false, true>(0, trueTheta, tr, E, a0, a1, s, bs, branched, 2.0f, rng);
+    else
+        o = envStep<NOPP, NTH, false, false, false, false>(0, trueTheta, tr, E, a0, a1, s, bs, branched, 2.0f, rng);
+    for (int a = 0; a < NA; a++)
+    {
+        st->pos[2 * a] = s.pos[2 * a];
+        st->pos[2 * a + 1] = s.pos[2 * a + 1];
+        st->vel[2 * a] = s.vel[2 * a];
+        st->vel[2 * a + 1] = s.vel[2 * a + 1];
+        st->S[a] = s.S[a];
+        st->lat_dist[a] = s.lat[a];
+        st->laps[a] = s.laps[a];
+    }
+    for (int i = 0; i < NTH; i++)
+        belief[i] = bs.belief[i];
+    *term = o.term;
+}
+
+extern "C" int dr_env_step(const dr_env_config* env, int true_theta, const float* action, dr_sim_state* state, float* belief, int update_belief,
+                           uint64_t seed, uint64_t step, int* term)
+{
+    int rc = checkEnv(env);
+    if (rc)
+        return rc;
+    if (!action || !state || !belief || true_theta < 0 || true_theta >= env->n_theta)
+        return fail(DR_ERR_INVALID_ARG, "bad argument");
+    if (!prSupported(env->n_opp, env->n_theta))
+        return fail(DR_ERR_UNSUPPORTED, "(n_opp, n_theta) combination not compiled in");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::vector<float> g = packGrids(*env);
+    EnvParams E = toEnvParams(*env);
+    float* dg = nullptr;
+    dr_sim_state* ds = nullptr;
+    float* db = nullptr;
+    int* dt = nullptr;
+    cudaError_t e = cudaMalloc(&dg, GRID_FLOATS * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&ds, sizeof(dr_sim_state));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&db, DR_MAX_THETA * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dt, 4);
+    if (e == cudaSuccess)
+    {
+        cudaMemcpy(dg, g.data(), GRID_FLOATS * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(ds, state, sizeof(dr_sim_state), cudaMemcpyHostToDevice);
+        cudaMemcpy(db, belief, env->n_theta * 4, cudaMemcpyHostToDevice);
+        uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+        switch (env->n_opp * 16 + env->n_theta)
+        {
+        case 17: env_step_kernel<1, 1><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
+        case 18: env_step_kernel<1, 2><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
+        case 20: env_step_kernel<1, 4><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
+        case 24: env_step_kernel<1, 8><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
+        case 34: env_step_kernel<2, 2><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
+        default: break;
+        }
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpy(state, ds, sizeof(dr_sim_state), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(belief, db, env->n_theta * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && term)
+            e = cudaMemcpy(term, dt, 4, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(dg);
+    cudaFree(ds);
+    cudaFree(db);
+    cudaFree(dt);
+    CK(e);
+    return DR_OK;
+}
+
+extern "C" int dr_prmppi_batch_set_profiling(dr_prmppi_batch* b, int on)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    b->profiling = on != 0;
+    b->timer.reset();
+    return DR_OK;
+}
+
+extern "C" int dr_prmppi_batch_get_kernel_times(dr_prmppi_batch* b, const char** names, float* ms, int n, int* count)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    CK(cudaSetDevice(b->device));
+    return kernelTimes(b->timer, names, ms, n, count);
+}

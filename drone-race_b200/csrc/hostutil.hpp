@@ -1,0 +1,310 @@
+// Host utilities shared by the C ABI translation units: error reporting, a device
+// arena, conversion of the C-ABI configuration to the device layout, event timing.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/drmppi.h"
+#include "instance.cuh"
+
+namespace dr
+{
+
+std::string& lastError();
+
+inline int fail(int code, const std::string& msg)
+{
+    lastError() = msg;
+    return code;
+}
+
+#define CK(call)                                                                                                                                    \
+    do                                                                                                                                              \
+    {                                                                                                                                               \
+        cudaError_t e_ = (call);                                                                                                                    \
+        if (e_ != cudaSuccess)                                                                                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? DR_ERR_OOM : DR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+    } while (0)
+
+inline size_t a16(size_t x)
+{
+    return (x + 15) & ~(size_t)15;
+}
+inline size_t a256(size_t x)
+{
+    return (x + 255) & ~(size_t)255;
+}
+
+// Bump allocator over one cudaMalloc; every block is 256-byte aligned.
+struct Arena
+{
+    std::vector<std::pair<void**, size_t>> req;
+    void* base = nullptr;
+    size_t total = 0;
+    template <typename T> void add(T*& p, size_t bytes)
+    {
+        req.push_back({(void**)&p, bytes});
+    }
+    cudaError_t alloc()
+    {
+        size_t off = 0;
+        for (auto& r : req)
+            off = a256(off) + a256(std::max<size_t>(r.second, 16));
+        total = off;
+        cudaError_t e = cudaMalloc(&base, total);
+        if (e != cudaSuccess)
+            return e;
+        cudaMemset(base, 0, total);
+        off = 0;
+        for (auto& r : req)
+        {
+            off = a256(off);
+            *r.first = (char*)base + off;
+            off += a256(std::max<size_t>(r.second, 16));
+        }
+        return cudaSuccess;
+    }
+    void release()
+    {
+        if (base)
+            cudaFree(base);
+        base = nullptr;
+    }
+};
+
+inline EnvParams toEnvParams(const dr_env_config& c)
+{
+    EnvParams e{};
+    e.dt = c.dt;
+    e.droneRadius = c.drone_radius;
+    e.posNoise = c.pos_noise_level;
+    e.speedNoise = c.speed_noise_level;
+    e.actionNoiseLevel = c.action_noise_level;
+    for (int a = 0; a < 4; a++)
+    {
+        e.maxSpeed[a] = c.max_speed[a];
+        e.maxAccel[a] = c.max_accel[a];
+    }
+    e.trackWidth = c.track_width;
+    e.nWinLaps = c.n_win_laps;
+    e.kP = c.kP;
+    e.kV = c.kV;
+    e.maxOppLatDistFact = c.max_opp_lat_dist_fact;
+    e.trackLength = c.track_length;
+    for (int th = 0; th < 8; th++)
+        for (int o = 0; o < 3; o++)
+        {
+            e.s1[th][o] = c.opp_configs[th].s1[o];
+            e.s2[th][o] = c.opp_configs[th].s2[o];
+            e.s3[th][o] = c.opp_configs[th].s3[o];
+            e.speedScale[th][o] = c.opp_configs[th].speed_scale[o];
+            e.actionNoise[th][o] = c.opp_configs[th].action_noise[o];
+        }
+    return e;
+}
+
+// p[513][2] | t[513][2] | kappa[513] with the wrap-around sample appended.
+inline std::vector<float> packGrids(const dr_env_config& c)
+{
+    std::vector<float> g(GRID_FLOATS, 0.0f);
+    for (int i = 0; i <= NTS; i++)
+    {
+        int k = i % NTS;
+        g[GRID_P + i * 2] = c.p_grid[k * 2];
+        g[GRID_P + i * 2 + 1] = c.p_grid[k * 2 + 1];
+        g[GRID_T + i * 2] = c.t_grid[k * 2];
+        g[GRID_T + i * 2 + 1] = c.t_grid[k * 2 + 1];
+        g[GRID_K + i] = c.kappa_grid[k];
+    }
+    return g;
+}
+
+inline int checkEnv(const dr_env_config* env)
+{
+    if (!env)
+        return fail(DR_ERR_INVALID_ARG, "env is NULL");
+    if (env->n_opp < 1 || env->n_opp > DR_MAX_OPP || env->n_theta < 1 || env->n_theta > DR_MAX_THETA)
+        return fail(DR_ERR_INVALID_ARG, "n_opp must be in [1,3] and n_theta in [1,8]");
+    if (!env->p_grid || !env->t_grid || !env->kappa_grid)
+        return fail(DR_ERR_INVALID_ARG, "track grids must be given");
+    if (!(env->track_length > 0.0f) || !std::isfinite(env->track_length) || !(env->dt > 0.0f))
+        return fail(DR_ERR_INVALID_ARG, "track_length and dt must be positive and finite");
+    for (int i = 0; i < NTS; i++)
+        if (!std::isfinite(env->p_grid[2 * i]) || !std::isfinite(env->p_grid[2 * i + 1]) || !std::isfinite(env->t_grid[2 * i]) ||
+            !std::isfinite(env->t_grid[2 * i + 1]) || !std::isfinite(env->kappa_grid[i]))
+            return fail(DR_ERR_INVALID_ARG, "track grids must be finite");
+    return DR_OK;
+}
+
+inline int selectDevice(int device)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+        return fail(DR_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= n)
+        return fail(DR_ERR_INVALID_ARG, "device index out of range");
+    CK(cudaSetDevice(device));
+    return DR_OK;
+}
+
+// buildSplineMatrix (src/mppi_controller.cu:56-141): natural cubic spline basis evaluated
+// at t = 0..T-1, Thomas algorithm, endpoint hold, float arithmetic.
+inline std::vector<float> splineMatrix(int T, int M, const int* knots)
+{
+    std::vector<float> B((size_t)T * M, 0.0f);
+    std::vector<int> tau(knots, knots + M);
+    std::vector<float> h(M > 1 ? M - 1 : 0);
+    for (int j = 0; j < M - 1; j++)
+        h[j] = float(tau[j + 1] - tau[j]);
+    for (int basis = 0; basis < M; basis++)
+    {
+        std::vector<float> y(M, 0.0f);
+        y[basis] = 1.0f;
+        std::vector<float> m(M, 0.0f);
+        if (M > 2)
+        {
+            const int N = M - 2;
+            std::vector<float> a(N), b(N), c(N), d(N);
+            for (int i = 0; i < N; ++i)
+            {
+                const int j = i + 1;
+                a[i] = h[j - 1];
+                b[i] = 2.0f * (h[j - 1] + h[j]);
+                c[i] = h[j];
+                d[i] = 6.0f * ((y[j + 1] - y[j]) / h[j] - (y[j] - y[j - 1]) / h[j - 1]);
+            }
+            for (int i = 1; i < N; ++i)
+            {
+                float w = a[i] / b[i - 1];
+                b[i] -= w * c[i - 1];
+                d[i] -= w * d[i - 1];
+            }
+            std::vector<float> x(N);
+            x[N - 1] = d[N - 1] / b[N - 1];
+            for (int i = N - 2; i >= 0; --i)
+                x[i] = (d[i] - c[i] * x[i + 1]) / b[i];
+            for (int i = 0; i < N; ++i)
+                m[i + 1] = x[i];
+        }
+        int seg = 0;
+        for (int t = 0; t < T; ++t)
+        {
+            float val = 0.0f;
+            if (t <= tau.front())
+                val = y.front();
+            else if (t >= tau.back())
+                val = y.back();
+            else
+            {
+                while (!(tau[seg] <= t && t <= tau[seg + 1]))
+                    ++seg;
+                const float x0 = float(tau[seg]);
+                const float x1 = float(tau[seg + 1]);
+                const float hh = x1 - x0;
+                const float A = (x1 - t) / hh;
+                const float BB = (t - x0) / hh;
+                val = m[seg] * (A * A * A - A) * (hh * hh) / 6.0f + m[seg + 1] * (BB * BB * BB - BB) * (hh * hh) / 6.0f + y[seg] * A + y[seg + 1] * BB;
+            }
+            B[(size_t)t * M + basis] = val;
+        }
+    }
+    return B;
+}
+
+inline int findConfidentHost(const float* belief, int nth, float threshold)
+{
+    for (int th = 0; th < nth; th++)
+        if (belief[th] > threshold)
+            return th + 1;
+    return 0;
+}
+
+// Per-kernel device times from CUDA events recorded on the launching stream between
+// the kernels of each step; averages over all steps recorded since reset().
+struct Timer
+{
+    static constexpr int MAXM = 8;
+    std::vector<std::string> names;
+    std::vector<cudaEvent_t> ev;
+    int steps = 0, cur = 0, nm = 0;
+    std::vector<float> ms; // averages, filled by collect()
+    void reset()
+    {
+        names.clear();
+        ms.clear();
+        steps = cur = nm = 0;
+    }
+    void begin()
+    {
+        cur = 0;
+    }
+    void mark(const char* name, cudaStream_t s)
+    {
+        size_t idx = (size_t)steps * MAXM + cur;
+        while (ev.size() <= idx)
+        {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            ev.push_back(e);
+        }
+        cudaEventRecord(ev[idx], s);
+        if (steps == 0)
+            names.push_back(name);
+        cur++;
+    }
+    void end()
+    {
+        if (steps == 0)
+            nm = cur;
+        steps++;
+    }
+    void collect()
+    {
+        ms.assign(nm > 0 ? nm - 1 : 0, 0.0f);
+        if (steps == 0 || nm < 2)
+            return;
+        cudaEventSynchronize(ev[(size_t)(steps - 1) * MAXM + nm - 1]);
+        for (int j = 0; j + 1 < nm; j++)
+        {
+            double sum = 0.0;
+            for (int s = 0; s < steps; s++)
+            {
+                float x = 0.0f;
+                cudaEventElapsedTime(&x, ev[(size_t)s * MAXM + j], ev[(size_t)s * MAXM + j + 1]);
+                sum += x;
+            }
+            ms[j] = (float)(sum / steps);
+        }
+    }
+    ~Timer()
+    {
+        for (auto e : ev)
+            cudaEventDestroy(e);
+    }
+};
+
+
+// Averages of the recorded steps; names point into the timer and stay valid until reset.
+inline int kernelTimes(Timer& t, const char** names, float* ms, int n, int* count)
+{
+    t.collect();
+    int c = (int)t.ms.size();
+    if (count)
+        *count = c;
+    for (int i = 0; i < c && i < n; i++)
+    {
+        if (names)
+            names[i] = t.names[i].c_str();
+        if (ms)
+            ms[i] = t.ms[i];
+    }
+    return DR_OK;
+}
+
+} // namespace dr

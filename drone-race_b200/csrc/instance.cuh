@@ -1,0 +1,111 @@
+// Device-side description of one controller instance (one agent's MPPI or PR-MPPI
+// controller) and of the per-step records exchanged with the host. A batch launch
+// covers several instances; each CTA works on one instance, found through a tile table.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/drmppi.h"
+#include "model.cuh"
+
+namespace dr
+{
+
+struct MppiCfgDev
+{
+    int K, T, M, useSplines, V, H, nth, nopp;
+    int knots[DR_MAX_KNOTS];
+    float sigma0, sigma1, minConf;
+    MppiCostW w;
+    uint32_t k0, k1; // Philox key (seed)
+};
+
+// Per-step input of an MPPI instance (one H2D copy per step for the whole batch).
+struct MppiIn
+{
+    dr_sim_state state;
+    float belief[DR_MAX_THETA];
+    float lambda;      // inv_temperature of this step
+    uint32_t step;     // Philox counter word
+    int pendBranch;    // branch to shift (previous step's chosen branch) or -1
+    int pendUseNew;    // previous step used the new plan
+};
+
+// Device buffers of an MPPI instance. `res` is the start of the contiguous result
+// block copied to the host after each step:
+//   fail[2][T] u32 | dense[nbp][T][2] | prevDense[nbp][T][2] | nu[nbp] | minCosts[nbp][M] | stats[4] i32
+struct MppiDev
+{
+    EnvParams env;
+    MppiCfgDev cfg;
+    const float* grids;  // GRID_FLOATS, 16-byte aligned
+    const float* B;      // [T][M] (spline mode)
+    float* knots;        // [nbp][M][2] optimised sequence (dense mode: M == T)
+    float* costsTrue;    // [nth][K]
+    int* binfo;          // [nth][K] predTheta << 16 | (branchTime & 0xffff)
+    float* costs;        // [nbp][K]
+    unsigned* counter;   // completion counter of the update kernel
+    // result block
+    unsigned* fail;      // [2][T]: 0 = new plan, 1 = previous plan
+    float* dense;        // [nbp][T][2]
+    float* prevDense;    // [nbp][T][2]
+    float* nu;           // [nbp]
+    float* minCosts;     // [nbp][M]
+    int* stats;          // [0] non-finite costs, [1] timeouts
+    size_t resBytes;
+};
+
+struct PrCfgDev
+{
+    int K, T, P, nth, nopp;
+    float sigma0, sigma1;
+    float collDistFactor, boundaryCost, boundaryThresholdFactor, winCost, oppWinCost, finalAdvWeight, finalOppAdvWeight, safetyWeight;
+    uint32_t k0, k1;
+};
+
+struct PrIn
+{
+    dr_sim_state state;
+    float belief[DR_MAX_THETA];
+    float lambda[3];
+    uint32_t step;
+    int pad;
+};
+
+// result block: nom[T][2] | rob[T][2] | cand1[T][2] | cand2[T][2] | minCosts[3] | nu[3] |
+//               candFull[2][P] | candSafe[2][P] | thetas[P] | decision[4] | stats[4]
+struct PrDev
+{
+    EnvParams env;
+    PrCfgDev cfg;
+    const float* grids;
+    float* costNom;   // [P][K][2]
+    float* costRob;   // [P][K][2]
+    float* avg;       // [2][K][2] per-sample averaged (full, safe) for nom / rob
+    float* nomWork;   // [T][2] shifted nominal used this step
+    float* robWork;   // [T][2]
+    unsigned* counter;
+    // result block
+    float* nom;       // [T][2] chosen nominal after the step
+    float* rob;       // [T][2] new robust nominal
+    float* cand1;     // [T][2]
+    float* cand2;     // [T][2]
+    float* minCosts;  // [3]
+    float* nu;        // [3]
+    float* candFull;  // [2][P]
+    float* candSafe;  // [2][P] safety of each candidate on the re-check stream
+    int* thetas;      // [P]
+    int* decision;    // [0] resetNom, [1] useNomPlan
+    int* stats;
+    size_t resBytes;
+};
+
+struct Tile
+{
+    int inst;
+    int s0;
+    int count;
+    int aux;
+};
+
+} // namespace dr

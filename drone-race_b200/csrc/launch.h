@@ -1,0 +1,44 @@
+// Host-side launch wrappers of the kernels (implemented in mppi_kernels.cu and
+// prmppi_kernels.cu).
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "instance.cuh"
+
+namespace dr
+{
+
+struct LaunchArgs
+{
+    cudaStream_t stream = nullptr;
+    const MppiDev* mppi = nullptr;
+    const MppiIn* mppiIn = nullptr;
+    const PrDev* pr = nullptr;
+    const PrIn* prIn = nullptr;
+    const Tile* tiles = nullptr;
+    int nTiles = 0;
+};
+
+bool mppiSupported(int nopp, int nth);
+int rolloutSamplesPerBlock(int nth);
+size_t mppiRolloutSmem(int nth, int T, int M, bool spl);
+size_t mppiVerifySmem(int nth, int T);
+cudaError_t launchMppiPrologue(const LaunchArgs& a, int nInst, size_t smem);
+cudaError_t launchMppiRollout(const LaunchArgs& a, int nopp, int nth, bool spl, size_t smem);
+cudaError_t launchMppiUpdate(const LaunchArgs& a, int nth);
+cudaError_t launchMppiAggregate(const LaunchArgs& a, int nth, int K);
+cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem, int* dbgFailTime, int* dbgTheta);
+cudaError_t launchMppiNoise(const LaunchArgs& a, size_t n, float* out);
+
+bool prSupported(int nopp, int nth);
+int prRolloutSamplesPerBlock();
+size_t prRolloutSmem(int T);
+cudaError_t launchPrPrologue(const LaunchArgs& a, int nInst);
+cudaError_t launchPrRollout(const LaunchArgs& a, int nopp, int nth, size_t smem);
+cudaError_t launchPrReduce(const LaunchArgs& a);
+cudaError_t launchPrCandidates(const LaunchArgs& a, int nopp, int nth, int nInst, int maxP, size_t smem);
+cudaError_t launchPrNoise(const LaunchArgs& a, size_t n, float* out);
+
+} // namespace dr

@@ -1,0 +1,692 @@
+// Device model of the StratRace environment: dynamics, opponent policy, belief update
+// and costs, as evaluated inside every rollout step.
+//
+// Semantics follow the reference (include/environments/env_stratrace.h:33-894,
+// include/costs.cuh:7-86, include/state.h:93-228) expression by expression, so that
+// on identical inputs the FP32 results agree with the reference kernels. The work is
+// organised for the GPU: the track quantities of each agent at the start of a step
+// (unit tangent, curvature, ds/dt, centre point) are computed once and shared by
+// every opponent-hypothesis evaluation and by the arc-length update, where the
+// reference recomputes them per call; the hypothesis-independent part of the opponent
+// policy is likewise evaluated once per step. The track grids live in shared memory.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#include "philox.cuh"
+
+namespace dr
+{
+
+constexpr int NTS = 512;       // N_TRACK_SAMPLES (env_stratrace_defs.h:11)
+constexpr int WIN = 10;        // WINDOW_SIZE (env_stratrace_defs.h:40)
+constexpr float DECAY = 0.97f; // include/config.h:30
+constexpr float MIN_COEFF = 0.01f; // MIN_COEFF_THRESHOLD, include/config.h:29
+constexpr int GRID_FLOATS = 2568;  // p[513][2] + t[513][2] + kappa[513], padded to 16 bytes
+constexpr int GRID_P = 0, GRID_T = 1026, GRID_K = 2052;
+
+enum Term
+{
+    TERM_NONE = 0,
+    TERM_LOSE = 1,
+    TERM_WIN = 2,
+    TERM_OPP_WIN = 3
+};
+
+// Environment parameters (EnvironmentConfig minus the grid pointers).
+struct EnvParams
+{
+    float dt, droneRadius, posNoise, speedNoise, actionNoiseLevel;
+    float maxSpeed[4], maxAccel[4];
+    float trackWidth;
+    int nWinLaps;
+    float kP, kV, maxOppLatDistFact, trackLength;
+    float s1[8][3], s2[8][3], s3[8][3], speedScale[8][3], actionNoise[8][3];
+};
+
+template <int NA> struct DState
+{
+    float pos[2 * NA];
+    float vel[2 * NA];
+    float S[NA];
+    float lat[NA];
+    int laps[NA];
+};
+
+template <int NTH> struct BState
+{
+    float belief[NTH];
+    int predTheta;
+    int branchingTime;
+};
+
+struct Track
+{
+    const float* p; // [513][2]
+    const float* t; // [513][2]
+    const float* k; // [513]
+};
+
+// ---- track sampling (env_stratrace.h:44-85) ------------------------------------------
+
+__device__ __forceinline__ void sampleTrack2(const float* __restrict__ arr, float s, float L, float& o0, float& o1)
+{
+    s /= L;
+    s = s - floorf(s);
+    float idx_f = s * NTS;
+    int idx0 = (int)idx_f;
+    int idx1 = (idx0 + 1) % NTS;
+    float t = idx_f - idx0;
+    o0 = (1.0f - t) * arr[idx0 * 2 + 0] + t * arr[idx1 * 2 + 0];
+    o1 = (1.0f - t) * arr[idx0 * 2 + 1] + t * arr[idx1 * 2 + 1];
+}
+
+__device__ __forceinline__ float sampleTrack1(const float* __restrict__ arr, float s, float L)
+{
+    s /= L;
+    s = s - floorf(s);
+    float idx_f = s * NTS;
+    int idx0 = (int)idx_f;
+    int idx1 = (idx0 + 1) % NTS;
+    float t = idx_f - idx0;
+    return (1.0f - t) * arr[idx0] + t * arr[idx1];
+}
+
+__device__ __forceinline__ float sqNorm(float x, float y)
+{
+    return x * x + y * y;
+}
+
+__device__ __forceinline__ void normalizedSpeed(const Track& tr, float s, float L, float& o0, float& o1)
+{
+    sampleTrack2(tr.t, s, L, o0, o1);
+    float invNorm = 1.0f / sqrtf(sqNorm(o0, o1));
+    o0 *= invNorm;
+    o1 *= invNorm;
+}
+
+// fastProjectOnTrack<false> (env_stratrace.h:88-162): returns S, writes latDist.
+__device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float px, float py, float prevS, float& latDist)
+{
+    prevS /= L;
+    prevS = prevS - floorf(prevS);
+    int idxPrev = (int)(prevS * NTS);
+    const float* __restrict__ P = tr.p;
+    int bestInd = (idxPrev - WIN + NTS) % NTS;
+    float bestSqDist;
+    {
+        float sq = 0.f;
+        float d0 = P[bestInd * 2] - px;
+        sq += d0 * d0;
+        float d1 = P[bestInd * 2 + 1] - py;
+        sq += d1 * d1;
+        bestSqDist = sq;
+    }
+#pragma unroll 4
+    for (int offset = NTS - WIN + 1; offset <= NTS + WIN; offset++)
+    {
+        int i = (idxPrev + offset) % NTS;
+        float sq = 0.f;
+        float d0 = P[i * 2] - px;
+        sq += d0 * d0;
+        float d1 = P[i * 2 + 1] - py;
+        sq += d1 * d1;
+        if (sq < bestSqDist)
+        {
+            bestSqDist = sq;
+            bestInd = i;
+        }
+    }
+    float bestSegSqDist = INFINITY;
+    float bestS = 0.0f;
+    float closestX = 0.0f, closestY = 0.0f;
+#pragma unroll
+    for (int seg = -1; seg <= 0; ++seg)
+    {
+        int a = (bestInd + seg + NTS) % NTS;
+        int b = (a + 1) % NTS;
+        float ax = P[2 * a], ay = P[2 * a + 1];
+        float abx = P[2 * b] - ax;
+        float aby = P[2 * b + 1] - ay;
+        float sqAB = sqNorm(abx, aby);
+        float t = 0.0f;
+        if (sqAB > 1e-12f) // the reference compares with the double 1e-12; for floats the two tests agree
+        {
+            t = ((px - ax) * abx + (py - ay) * aby) / sqAB;
+            t = fmaxf(0.0f, fminf(t, 1.0f));
+        }
+        float projx = ax + t * abx;
+        float projy = ay + t * aby;
+        float sqDist = sqNorm(px - projx, py - projy);
+        if (sqDist < bestSegSqDist)
+        {
+            bestSegSqDist = sqDist;
+            bestS = ((float)a + t) / NTS * L;
+            closestX = projx;
+            closestY = projy;
+        }
+    }
+    float tg0, tg1;
+    sampleTrack2(tr.t, bestS, L, tg0, tg1);
+    float cross = -tg1 * (px - closestX) + tg0 * (py - closestY);
+    latDist = copysignf(sqrtf(bestSegSqDist), cross);
+    return bestS;
+}
+
+// ---- per-step agent quantities -------------------------------------------------------
+
+template <int NA> struct AgentGeo
+{
+    float tn0[NA], tn1[NA]; // unit tangent at S[a]
+    float kap[NA];          // curvature at S[a]
+    float sdot[NA];         // computeSdot(a) (env_stratrace.h:302-315)
+};
+
+template <int NA> __device__ __forceinline__ void agentGeometry(const Track& tr, const EnvParams& E, const DState<NA>& s, AgentGeo<NA>& g)
+{
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+    {
+        normalizedSpeed(tr, s.S[a], E.trackLength, g.tn0[a], g.tn1[a]);
+        g.kap[a] = sampleTrack1(tr.k, s.S[a], E.trackLength);
+        float metric = 1 - g.kap[a] * s.lat[a];
+        if (fabsf(metric) < 1e-12f)
+            metric = copysignf(1e-12f, metric);
+        g.sdot[a] = (g.tn0[a] * s.vel[2 * a] + g.tn1[a] * s.vel[2 * a + 1]) / metric;
+    }
+}
+
+// Hypothesis-independent part of the opponent policy for opponent iOpp
+// (env_stratrace.h:318-461 and 611-706).
+struct OppCommon
+{
+    // computeOppTargetLatDist, k = 0 (behind) and 1 (ahead)
+    int j[2];
+    float deltaS[2], deltaE[2], latJ[2], sdotJ[2], blockTol[2], oppLong[2];
+    bool shouldBlock[2], fasterThanJ[2];
+    float sdot_i, maxLatDis;
+    // computeOpponentAction
+    float tang0, tang1, norm0, norm1, kappa, e_n, v_t, v_n, e_n_max, metric_actual, a_centripetal, a_lat_max, distPos, distNeg, maxAccel;
+    bool brakePos, brakeNeg;
+};
+
+template <int NOPP>
+__device__ __forceinline__ void oppCommon(int iOpp, const Track& tr, const EnvParams& E, const DState<NOPP + 1>& s, const AgentGeo<NOPP + 1>& g,
+                                          OppCommon& c)
+{
+    const float L = E.trackLength;
+    int iAhead = 0;
+    float deltaSAhead = s.S[0] - s.S[iOpp];
+    if (deltaSAhead < 0.0f)
+        deltaSAhead += L;
+#pragma unroll
+    for (int j = 1; j <= NOPP; j++)
+        if (j != iOpp)
+        {
+            float deltaS = s.S[j] - s.S[iOpp];
+            if (deltaS < 0.0f)
+                deltaS += L;
+            if (deltaS < deltaSAhead)
+            {
+                deltaSAhead = deltaS;
+                iAhead = j;
+            }
+        }
+    int iBehind = 0;
+    float deltaSBehind = s.S[0] - s.S[iOpp];
+    if (deltaSBehind > 0.0f)
+        deltaSBehind -= L;
+#pragma unroll
+    for (int j = 1; j <= NOPP; j++)
+        if (j != iOpp)
+        {
+            float deltaS = s.S[j] - s.S[iOpp];
+            if (deltaS > 0.0f)
+                deltaS -= L;
+            if (deltaS > deltaSBehind)
+            {
+                deltaSBehind = deltaS;
+                iBehind = j;
+            }
+        }
+    c.sdot_i = g.sdot[iOpp];
+#pragma unroll
+    for (int k = 0; k <= 1; k++)
+    {
+        int j = k ? iAhead : iBehind;
+        float deltaS = k ? deltaSAhead : deltaSBehind;
+        // runtime agent index j -> select from the unrolled arrays
+        float latJ = s.lat[0], S_unused = 0.f, tj0 = g.tn0[0], tj1 = g.tn1[0], sdj = g.sdot[0], vj0 = s.vel[0], vj1 = s.vel[1], msj = E.maxSpeed[0];
+#pragma unroll
+        for (int a = 1; a <= NOPP; a++)
+            if (a == j)
+            {
+                latJ = s.lat[a];
+                tj0 = g.tn0[a];
+                tj1 = g.tn1[a];
+                sdj = g.sdot[a];
+                vj0 = s.vel[2 * a];
+                vj1 = s.vel[2 * a + 1];
+                msj = E.maxSpeed[a];
+            }
+        (void)S_unused;
+        c.j[k] = j;
+        c.deltaS[k] = deltaS;
+        c.deltaE[k] = latJ - s.lat[iOpp];
+        c.latJ[k] = latJ;
+        c.sdotJ[k] = sdj;
+        c.blockTol[k] = msj * 0.3f;
+        c.shouldBlock[k] = (deltaS < 0.0f) && (deltaS > -L * 0.25f) && (sdj + c.blockTol[k] > c.sdot_i);
+        c.fasterThanJ[k] = c.sdot_i > sdj;
+        c.oppLong[k] = vj0 * tj0 + vj1 * tj1;
+    }
+    c.maxLatDis = E.trackWidth - E.droneRadius * E.maxOppLatDistFact;
+
+    c.maxAccel = E.maxAccel[iOpp];
+    float pc0, pc1;
+    sampleTrack2(tr.p, s.S[iOpp], L, pc0, pc1);
+    c.tang0 = g.tn0[iOpp];
+    c.tang1 = g.tn1[iOpp];
+    c.kappa = g.kap[iOpp];
+    c.norm0 = -c.tang1;
+    c.norm1 = c.tang0;
+    float pos0 = s.pos[iOpp * 2], pos1 = s.pos[iOpp * 2 + 1];
+    float vel0 = s.vel[iOpp * 2], vel1 = s.vel[iOpp * 2 + 1];
+    c.e_n = (pos0 - pc0) * c.norm0 + (pos1 - pc1) * c.norm1;
+    c.v_t = vel0 * c.tang0 + vel1 * c.tang1;
+    c.v_n = vel0 * c.norm0 + vel1 * c.norm1;
+    c.e_n_max = E.trackWidth - E.droneRadius * 1.2f;
+    float metric_actual = 1.0f - c.kappa * c.e_n;
+    if (fabsf(metric_actual) < 1e-6f)
+        metric_actual = copysignf(1e-6f, metric_actual);
+    c.metric_actual = metric_actual;
+    c.a_centripetal = c.v_t * c.v_t * c.kappa / metric_actual;
+    c.a_lat_max = fmaxf(c.maxAccel - fabsf(c.a_centripetal), c.maxAccel * 0.2f);
+    c.distPos = fmaxf(c.e_n_max - c.e_n, 0.001f);
+    c.distNeg = fmaxf(c.e_n_max + c.e_n, 0.001f);
+    c.brakePos = c.v_n > 0.0f && c.v_n * c.v_n > 1.8f * c.a_lat_max * c.distPos;
+    c.brakeNeg = c.v_n < 0.0f && c.v_n * c.v_n > 1.8f * c.a_lat_max * c.distNeg;
+}
+
+// Hypothesis-dependent part: target lateral offset / speed goal and the resulting
+// acceleration of opponent iOpp under hypothesis th.
+__device__ __forceinline__ void oppAction(int iOpp, int th, const EnvParams& E, const OppCommon& c, float& out0, float& out1)
+{
+    const float s1 = E.s1[th][iOpp - 1], s2 = E.s2[th][iOpp - 1], s3 = E.s3[th][iOpp - 1];
+    float latDis = 0.0f;
+    float baseSpeed = E.speedScale[th][iOpp - 1] * E.maxSpeed[iOpp];
+    float speedGoal = baseSpeed;
+#pragma unroll
+    for (int k = 0; k <= 1; k++)
+    {
+        float deltaS = c.deltaS[k];
+        float deltaE = c.deltaE[k];
+        bool shouldOvertake = c.fasterThanJ[k] && (fabsf(deltaE) < s1);
+        float factor = expf(-s2 * deltaS * deltaS);
+        if (c.shouldBlock[k])
+        {
+            float blockTerm = c.latJ[k] * (1 - expf(-s3 * (c.sdotJ[k] + c.blockTol[k] - c.sdot_i))) * factor;
+            latDis += blockTerm;
+        }
+        if (shouldOvertake)
+        {
+            float overtakeTerm = (c.latJ[k] - copysignf(s1, deltaE)) * factor;
+            latDis += overtakeTerm;
+            float oppLongSpeed = c.oppLong[k];
+            if (deltaS < 3 * E.droneRadius)
+                speedGoal = fminf(speedGoal, 0.7f * oppLongSpeed);
+            else if (deltaS < 6 * E.droneRadius && s1 > 1e-6f) // double 1e-6 in the reference; same test for floats
+            {
+                float latFactor = fabsf(deltaE) / s1;
+                speedGoal = fminf(speedGoal, latFactor * oppLongSpeed + (1.0f - latFactor) * baseSpeed);
+            }
+        }
+    }
+    float latDisRaw = fmaxf(-c.maxLatDis, fminf(c.maxLatDis, latDis));
+
+    const float maxAccel = c.maxAccel, a_lat_max = c.a_lat_max, v_n = c.v_n, dt = E.dt;
+    float latDisC = fmaxf(-c.e_n_max, fminf(c.e_n_max, latDisRaw));
+    float e_error = latDisC - c.e_n;
+    float a_n_cmd;
+    if (c.brakePos)
+        a_n_cmd = -a_lat_max;
+    else if (c.brakeNeg)
+        a_n_cmd = a_lat_max;
+    else if (fabsf(e_error) < 0.02f)
+    {
+        float kp = a_lat_max / 0.02f;
+        a_n_cmd = kp * e_error - 2.0f * sqrtf(kp) * v_n;
+        a_n_cmd = fmaxf(-a_lat_max, fminf(a_lat_max, a_n_cmd));
+    }
+    else
+    {
+        float stopping_dist = v_n * v_n / (2.0f * a_lat_max);
+        bool v_toward = (e_error > 0.0f && v_n > 0.0f) || (e_error < 0.0f && v_n < 0.0f);
+        bool decel_phase = v_toward && stopping_dist >= fabsf(e_error) * 0.95f;
+        a_n_cmd = (e_error > 0.0f) ? a_lat_max : -a_lat_max;
+        if (decel_phase)
+            a_n_cmd = -a_n_cmd;
+        float v_n_next = v_n + a_n_cmd * dt;
+        if (v_n_next > 0.0f)
+        {
+            float v_safe = sqrtf(2.0f * a_lat_max * c.distPos);
+            if (v_n_next > v_safe)
+                a_n_cmd = (v_safe - v_n) / dt;
+        }
+        else
+        {
+            float v_safe = sqrtf(2.0f * a_lat_max * c.distNeg);
+            if (-v_n_next > v_safe)
+                a_n_cmd = (-v_safe - v_n) / dt;
+        }
+    }
+    float a_n_total = fmaxf(-maxAccel, fminf(maxAccel, a_n_cmd + c.a_centripetal));
+    float a_t_max = sqrtf(fmaxf(maxAccel * maxAccel - a_n_total * a_n_total, 0.0f));
+    float kappa = c.kappa;
+    float kappa_eff = kappa / (1.0f - kappa * latDisC + 1e-6f);
+    float pathSpeed = fminf(speedGoal, sqrtf(maxAccel / fmaxf(fabsf(kappa_eff), 1e-12f)));
+    if (fabsf(a_n_cmd) > a_lat_max * 0.5f)
+        pathSpeed *= fmaxf(0.4f, 1.5f - fabsf(a_n_cmd) / a_lat_max);
+    float a_t_cmd = E.kV * (pathSpeed - c.v_t) - v_n * kappa * c.v_t / c.metric_actual;
+    a_t_cmd = fmaxf(-a_t_max, fminf(a_t_max, a_t_cmd));
+    out0 = a_t_cmd * c.tang0 + a_n_total * c.norm0;
+    out1 = a_t_cmd * c.tang1 + a_n_total * c.norm1;
+}
+
+// findConfident (state.h:93-115) for one parameter factor.
+template <int NTH> __device__ __forceinline__ int findConfident(const float (&belief)[NTH], float threshold)
+{
+    int pt = 0;
+#pragma unroll
+    for (int th = NTH - 1; th >= 0; th--)
+        if (belief[th] > threshold)
+            pt = th + 1;
+    return pt;
+}
+
+struct StepOut
+{
+    int term;
+    float bdRaw;  // trackBoundaryDist without the opponent-win shortcut
+    bool oppWon;  // isOppWinner
+    bool winner;  // isWinner
+};
+
+// environmentStep (env_stratrace.h:711-894).
+//   UPD: shouldUpdateBelief, BR: considerBranching, LOSE: loseOnOppWin,
+//   ALLTH: evaluate the opponent policy under every hypothesis (needed by the belief
+//   update) or only under the true one (the result is the same when UPD is false).
+template <int NOPP, int NTH, bool UPD, bool BR, bool LOSE, bool ALLTH>
+__device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr, const EnvParams& E, float ego0, float ego1, DState<NOPP + 1>& s,
+                                           BState<NTH>& bs, bool& branched, float minConf, EnvNoise& rng)
+{
+    constexpr int NA = NOPP + 1;
+    float prevS[NA];
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+        prevS[a] = s.S[a];
+
+    AgentGeo<NA> g;
+    agentGeometry<NA>(tr, E, s, g);
+
+    float act0[NA], act1[NA];
+    act0[0] = ego0;
+    act1[0] = ego1;
+    float nom0[ALLTH ? NTH : 1][NOPP], nom1[ALLTH ? NTH : 1][NOPP];
+#pragma unroll
+    for (int o = 1; o <= NOPP; o++)
+    {
+        OppCommon c;
+        oppCommon<NOPP>(o, tr, E, s, g, c);
+        float u0 = 0.f, u1 = 0.f;
+        if constexpr (ALLTH)
+        {
+#pragma unroll
+            for (int th = 0; th < NTH; th++)
+            {
+                oppAction(o, th, E, c, nom0[th][o - 1], nom1[th][o - 1]);
+                if (th == trueTheta)
+                {
+                    u0 = nom0[th][o - 1];
+                    u1 = nom1[th][o - 1];
+                }
+            }
+        }
+        else
+        {
+            oppAction(o, trueTheta, E, c, nom0[0][o - 1], nom1[0][o - 1]);
+            u0 = nom0[0][o - 1];
+            u1 = nom1[0][o - 1];
+        }
+        float an = E.actionNoise[trueTheta][o - 1];
+        if (an != 0.0f)
+        {
+            u0 += an * rng.next();
+            u1 += an * rng.next();
+        }
+        act0[o] = u0;
+        act1[o] = u1;
+    }
+    // 2. clamp + action noise
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+    {
+        float sq = 0.0f;
+        sq += act0[a] * act0[a];
+        sq += act1[a] * act1[a];
+        float factor = 1.0f;
+        float maxSq = E.maxAccel[a] * E.maxAccel[a];
+        if (sq > maxSq)
+            factor = E.maxAccel[a] / sqrtf(sq);
+        act0[a] *= factor;
+        if (E.actionNoiseLevel != 0.0f)
+            act0[a] += rng.next() * E.actionNoiseLevel;
+        act1[a] *= factor;
+        if (E.actionNoiseLevel != 0.0f)
+            act1[a] += rng.next() * E.actionNoiseLevel;
+    }
+    // 3. position
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+    {
+        s.pos[2 * a] += E.dt * s.vel[2 * a];
+        s.pos[2 * a + 1] += E.dt * s.vel[2 * a + 1];
+    }
+    // 4. arc length (ds/dt of the pre-step state)
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+        s.S[a] += E.dt * g.sdot[a];
+    // 5. velocity
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+    {
+        s.vel[2 * a] += E.dt * act0[a];
+        s.vel[2 * a + 1] += E.dt * act1[a];
+    }
+    // 6. speed cap
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+    {
+        float sqSpd = sqNorm(s.vel[2 * a], s.vel[2 * a + 1]);
+        if (sqSpd > E.maxSpeed[a] * E.maxSpeed[a])
+        {
+            float sc = E.maxSpeed[a] / sqrtf(sqSpd);
+            s.vel[2 * a] *= sc;
+            s.vel[2 * a + 1] *= sc;
+        }
+    }
+    // 7. state noise
+    if (E.posNoise != 0.0f || E.speedNoise != 0.0f)
+    {
+#pragma unroll
+        for (int a = 0; a < NA; a++)
+#pragma unroll
+            for (int d = 0; d < 2; d++)
+            {
+                if (E.posNoise != 0.0f)
+                    s.pos[a * 2 + d] += rng.next() * E.posNoise;
+                if (E.speedNoise != 0.0f)
+                    s.vel[a * 2 + d] += rng.next() * E.speedNoise;
+            }
+    }
+    // 8. projection
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+        s.S[a] = projectOnTrack(tr, E.trackLength, s.pos[2 * a], s.pos[2 * a + 1], s.S[a], s.lat[a]);
+    // 9. laps
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+    {
+        if (s.S[a] < prevS[a] - E.trackLength * 0.5f)
+            s.laps[a]++;
+        if (s.S[a] > prevS[a] + E.trackLength * 0.5f)
+            s.laps[a]--;
+    }
+    // 10. belief update (env_stratrace.h:166-222)
+    if constexpr (UPD)
+    {
+        float sum = 0.0f;
+        const float sigmaEnv = 0.2f;
+#pragma unroll
+        for (int th = 0; th < NTH; th++)
+        {
+            float logLikelihood = 0.0f;
+#pragma unroll
+            for (int o = 0; o < NOPP; o++)
+            {
+                float n0 = nom0[th][o], n1 = nom1[th][o];
+                float sqAccel = 0.0f;
+                sqAccel += n0 * n0;
+                sqAccel += n1 * n1;
+                float scale = 1.0f;
+                if (sqAccel > E.maxAccel[o + 1] * E.maxAccel[o + 1])
+                    scale = E.maxAccel[o + 1] / sqrtf(sqAccel);
+                float sqDist = 0.0f;
+                float dx0 = act0[o + 1] - n0 * scale;
+                sqDist += dx0 * dx0;
+                float dx1 = act1[o + 1] - n1 * scale;
+                sqDist += dx1 * dx1;
+                float an = E.actionNoise[th][o];
+                float sqSigma = sigmaEnv * sigmaEnv + an * an;
+                logLikelihood += -0.5f * sqDist / sqSigma - (float)2 * 0.5f * logf(2.0f * M_PIf32) - (float)2 * 0.5f * logf(sqSigma);
+            }
+            bs.belief[th] *= expf(logLikelihood);
+            sum += bs.belief[th];
+        }
+        if (sum < 1e-20f)
+        {
+            float uniform = 1.0f / NTH;
+#pragma unroll
+            for (int th = 0; th < NTH; ++th)
+                bs.belief[th] = uniform;
+        }
+        else
+        {
+#pragma unroll
+            for (int th = 0; th < NTH; th++)
+                bs.belief[th] /= sum;
+        }
+    }
+    if constexpr (BR)
+    {
+        int np = findConfident<NTH>(bs.belief, minConf);
+        if (bs.predTheta == 0 && np != 0)
+        {
+            bs.predTheta = np;
+            bs.branchingTime = t + 1;
+            branched = true;
+        }
+    }
+    // terminal checks (trackBoundaryDist / isOutside / isWinner, env_stratrace.h:226-274)
+    StepOut r;
+    bool oppWon = false;
+#pragma unroll
+    for (int o = 1; o <= NOPP; o++)
+        if (s.laps[o] >= E.nWinLaps)
+            oppWon = true;
+    float minSq = INFINITY;
+#pragma unroll
+    for (int o = 1; o <= NOPP; o++)
+        minSq = fminf(minSq, sqNorm(s.pos[2 * o] - s.pos[0], s.pos[2 * o + 1] - s.pos[1]));
+    float bdRaw = fminf(sqrtf(minSq) - E.droneRadius, E.trackWidth - fabsf(s.lat[0]));
+    bool winner = s.laps[0] >= E.nWinLaps;
+#pragma unroll
+    for (int o = 1; o <= NOPP; o++)
+        if (fabsf(s.lat[o]) > E.trackWidth - E.droneRadius)
+            winner = true;
+    float bdTerm = (LOSE && oppWon) ? -1.0f : bdRaw;
+    int term = TERM_NONE;
+    if (bdTerm < E.droneRadius)
+        term = TERM_LOSE;
+    else if (winner)
+        term = TERM_WIN;
+    else if (!LOSE && (oppWon ? -1.0f : bdRaw) < E.droneRadius)
+        term = TERM_OPP_WIN;
+    r.term = term;
+    r.bdRaw = bdRaw;
+    r.oppWon = oppWon;
+    r.winner = winner;
+    return r;
+}
+
+struct MppiCostW
+{
+    float collDistFactor, boundaryCost, boundaryThresholdFactor, outsideCost, winCost, oppWinCost, finalAdvWeight, finalOppAdvWeight;
+};
+
+// stateCost (costs.cuh:7-28) from the step's boundary distance.
+__device__ __forceinline__ float stateCost(const StepOut& o, const EnvParams& E, const MppiCostW& w)
+{
+    float cost = 0.0f;
+    float bd = o.bdRaw;
+    float danger = w.boundaryThresholdFactor * E.droneRadius;
+    if (bd < danger)
+        cost += w.boundaryCost * powf(bd / E.droneRadius, 2.0f);
+    if (bd < E.droneRadius * w.collDistFactor)
+        cost += w.outsideCost;
+    if (o.oppWon)
+        cost += w.oppWinCost;
+    if (o.winner)
+        cost -= w.winCost;
+    return cost;
+}
+
+// PRMPPIstateCost (costs.cuh:44-63).
+__device__ __forceinline__ float prStateCost(const StepOut& o, const EnvParams& E, float boundaryThresholdFactor, float boundaryCost, float winCost,
+                                             float oppWinCost)
+{
+    float cost = 0.0f;
+    float bd = o.oppWon ? -1.0f : o.bdRaw;
+    float danger = boundaryThresholdFactor * E.droneRadius;
+    if (bd < danger)
+        cost += boundaryCost * powf(bd / E.droneRadius, 2.0f);
+    if (o.winner)
+        cost -= winCost;
+    if (o.oppWon)
+        cost += oppWinCost;
+    return cost;
+}
+
+// PRMPPIsafetyCost (costs.cuh:78-86).
+__device__ __forceinline__ float prSafetyCost(const StepOut& o, const EnvParams& E, float collDistFactor)
+{
+    return E.droneRadius * collDistFactor - o.bdRaw;
+}
+
+// finalCost / PRMPPIfinalCost (costs.cuh:31-39, 66-74).
+template <int NOPP> __device__ __forceinline__ float finalCost(const DState<NOPP + 1>& s, const EnvParams& E, float finalAdvWeight, float finalOppAdvWeight)
+{
+    float cost = -finalAdvWeight * (s.S[0] / E.trackLength + s.laps[0]);
+    if (finalOppAdvWeight != 0.0f)
+    {
+        float mx = -INFINITY;
+#pragma unroll
+        for (int o = 1; o <= NOPP; o++)
+            mx = fmaxf(mx, s.S[o] / E.trackLength + s.laps[o]);
+        cost += finalOppAdvWeight * mx;
+    }
+    return cost;
+}
+
+} // namespace dr

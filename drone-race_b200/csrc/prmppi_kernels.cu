@@ -1,0 +1,489 @@
+// PR-MPPI control-step kernels (reference: src/prmppi_kernels.cu; host sequence
+// src/prmppi_controller.cu:142-349).
+//
+//   pr_prologue    shifts both nominals by one step (prmppi_controller.cu:163-175) and
+//                  draws the P hypotheses from the belief (PRMPPIsampleThetaValues,
+//                  prmppi_kernels.cu:23-51).
+//   pr_rollout     one thread per (nominal/robust, sample, hypothesis): rollout of
+//                  nominal + Philox perturbation under theta_p with running and safety cost
+//                  (PRMPPIfullRolloutKernel, :55-130); the hypotheses of a sample sit in
+//                  neighbouring threads, so the per-sample average over p and the safety
+//                  indicator (PRMPPIcostAvgKernel, :134-166) are done in the epilogue.
+//   pr_weighted    per (which, t): minimum of the averaged cost (PRMPPIcomputeMinCosts-
+//                  Kernel, :169-199), exponential weights and the weighted average of the
+//                  absolute perturbed controls (PRMPPIWeightedAverageKernel, :204-282),
+//                  with the perturbation regenerated and the sums in the reference's order.
+//   pr_candidates  full cost of both candidates under every theta_p (PRMPPIcompute-
+//                  CandidateCostKernel, :285-347) and, speculatively for both, the safety
+//                  re-check of the one that will be chosen (PRMPPIcomputeSafeCostKernel,
+//                  :350-393); then the choice itself (prmppi_controller.cu:232-304) so
+//                  that the host needs one synchronisation per step.
+#include "common.cuh"
+#include "instance.cuh"
+#include "launch.h"
+
+namespace dr
+{
+
+constexpr int PRB = 128;
+constexpr int PUB = 256;
+
+__host__ __device__ __forceinline__ size_t pa16(size_t x)
+{
+    return (x + 15) & ~(size_t)15;
+}
+
+__device__ __forceinline__ void copyEnvP(EnvParams* dst, const EnvParams* src)
+{
+    const int n = (int)(sizeof(EnvParams) / 4);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        ((float*)dst)[i] = ((const float*)src)[i];
+}
+
+template <int NA> __device__ __forceinline__ void loadState(DState<NA>& st, const dr_sim_state& s)
+{
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+    {
+        st.pos[2 * a] = s.pos[2 * a];
+        st.pos[2 * a + 1] = s.pos[2 * a + 1];
+        st.vel[2 * a] = s.vel[2 * a];
+        st.vel[2 * a + 1] = s.vel[2 * a + 1];
+        st.S[a] = s.S[a];
+        st.lat[a] = s.lat_dist[a];
+        st.laps[a] = s.laps[a];
+    }
+}
+
+__global__ void __launch_bounds__(256) pr_prologue(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, int nInst)
+{
+    __shared__ float sh[2 * DR_MAX_T * 2];
+    const int inst = blockIdx.x;
+    if (inst >= nInst)
+        return;
+    const PrDev& D = insts[inst];
+    const PrIn& I = in[inst];
+    const int T = D.cfg.T, P = D.cfg.P, nth = D.cfg.nth;
+    for (int i = threadIdx.x; i < T * 2; i += blockDim.x)
+    {
+        sh[i] = D.nom[i];
+        sh[T * 2 + i] = D.rob[i];
+    }
+    if (threadIdx.x < 4)
+        D.stats[threadIdx.x] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < T * 2; i += blockDim.x)
+    {
+        int t = i >> 1, d = i & 1;
+        D.nom[i] = (t < T - 1) ? sh[(t + 1) * 2 + d] : 0.0f;
+        D.rob[i] = (t < T - 1) ? sh[T * 2 + (t + 1) * 2 + d] : 0.0f;
+    }
+    for (int p = threadIdx.x; p < P; p += blockDim.x)
+    {
+        float u = uniform_from_word(draw(D.cfg.k0, D.cfg.k1, (uint32_t)p, 0u, I.step, S_PR_THETA, 0).x);
+        float accum = 0.0f;
+        int theta = nth - 1;
+        for (int i = 0; i < nth; i++)
+        {
+            accum += I.belief[i];
+            if (u <= accum)
+            {
+                theta = i;
+                break;
+            }
+        }
+        D.thetas[p] = theta;
+    }
+}
+
+struct PrRollSmem
+{
+    size_t env, grids, nom, red, total;
+};
+
+__host__ __device__ inline PrRollSmem prLayout(int T)
+{
+    auto a16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    PrRollSmem L;
+    size_t off = 16;
+    L.env = off;
+    off = a16(off + sizeof(EnvParams));
+    L.grids = off;
+    off = a16(off + GRID_FLOATS * 4);
+    L.nom = off;
+    off = a16(off + (size_t)T * 2 * 4);
+    L.red = off;
+    off = a16(off + (size_t)PRB * 2 * 4);
+    L.total = off;
+    return L;
+}
+
+// tile: inst, s0 (first sample), count (samples), aux (0 nominal / 1 robust)
+template <int NOPP, int NTH>
+__global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, const Tile* __restrict__ tiles)
+{
+    constexpr int NA = NOPP + 1;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    const Tile tile = tiles[blockIdx.x];
+    const PrDev& D = insts[tile.inst];
+    const PrIn& I = in[tile.inst];
+    const int K = D.cfg.K, T = D.cfg.T, P = D.cfg.P;
+    const int robust = tile.aux;
+    const PrRollSmem L = prLayout(T);
+    uint64_t* bar = (uint64_t*)smraw;
+    EnvParams* sE = (EnvParams*)(smraw + L.env);
+    float* sGrid = (float*)(smraw + L.grids);
+    float* sNom = (float*)(smraw + L.nom);
+    float* red = (float*)(smraw + L.red);
+    const uint32_t nomBytes = (uint32_t)pa16((size_t)T * 2 * 4);
+    if (threadIdx.x == 0)
+    {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, GRID_FLOATS * 4 + nomBytes);
+        bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
+        bulk_g2s(sNom, robust ? D.rob : D.nom, nomBytes, bar);
+    }
+    copyEnvP(sE, &D.env);
+    __syncthreads();
+    if (!__syncthreads_and(mbar_wait(bar, 0)))
+    {
+        if (threadIdx.x == 0)
+            atomicAdd(&D.stats[1], 1);
+        return;
+    }
+    const EnvParams& E = *sE;
+    const Track tr{sGrid + GRID_P, sGrid + GRID_T, sGrid + GRID_K};
+    const int spb = PRB / P;
+    const int sl = threadIdx.x / P, p = threadIdx.x % P;
+    const int s = tile.s0 + sl;
+    const bool valid = sl < spb && sl < tile.count;
+    float running = 0.0f, safe = -INFINITY;
+    if (valid)
+    {
+        const int theta = D.thetas[p];
+        DState<NA> st;
+        loadState<NA>(st, I.state);
+        BState<NTH> bs{};
+        const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+        EnvNoise rng(k0, k1, (uint32_t)s, ((((uint32_t)robust << 8) | (uint32_t)p) << 16), step, S_PR_ROLL_ENV);
+        float decay = 1.0f;
+        bool stop = false;
+        for (int t = 0; t < T && !stop; t++)
+        {
+            rng.begin_step((uint32_t)t);
+            U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)t, step, S_PR_EPS, 0);
+            float ego0 = sNom[t * 2] + D.cfg.sigma0 * normal_from_word(r.x);
+            float ego1 = sNom[t * 2 + 1] + D.cfg.sigma1 * normal_from_word(r.y);
+            bool branched = false;
+            StepOut o = envStep<NOPP, NTH, false, false, true, false>(t, theta, tr, E, ego0, ego1, st, bs, branched, 0.0f, rng);
+            stop = (o.term != TERM_NONE);
+            running += decay * prStateCost(o, E, D.cfg.boundaryThresholdFactor, D.cfg.boundaryCost, D.cfg.winCost, D.cfg.oppWinCost);
+            safe = fmaxf(safe, prSafetyCost(o, E, D.cfg.collDistFactor));
+            decay *= DECAY;
+        }
+        running += finalCost<NOPP>(st, E, D.cfg.finalAdvWeight, D.cfg.finalOppAdvWeight);
+        float* out = robust ? D.costRob : D.costNom;
+        out[((size_t)p * K + s) * 2 + 0] = running;
+        out[((size_t)p * K + s) * 2 + 1] = safe;
+    }
+    red[threadIdx.x * 2] = running;
+    red[threadIdx.x * 2 + 1] = safe;
+    __syncthreads();
+    // PRMPPIcostAvgKernel (prmppi_kernels.cu:134-166)
+    if (valid && p == 0)
+    {
+        float avg = 0.0f, maxSafe = -INFINITY;
+        for (int q = 0; q < P; q++)
+        {
+            avg += red[(sl * P + q) * 2];
+            maxSafe = fmaxf(maxSafe, red[(sl * P + q) * 2 + 1]);
+        }
+        avg /= (float)P;
+        float full = avg + ((maxSafe > 0.0f) ? D.cfg.safetyWeight : 0.0f);
+        D.avg[((size_t)robust * K + s) * 2 + 0] = full;
+        D.avg[((size_t)robust * K + s) * 2 + 1] = maxSafe;
+        if (!isfinite(full))
+            atomicAdd(&D.stats[0], 1);
+    }
+}
+
+// block per (inst, which, t); tile.s0 = which * T + t
+__global__ void __launch_bounds__(PUB) pr_weighted(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, const Tile* __restrict__ tiles)
+{
+    __shared__ float sA[PUB], sB[PUB], sC[PUB];
+    __shared__ float sMin[PUB / 32];
+    const Tile tile = tiles[blockIdx.x];
+    const PrDev& D = insts[tile.inst];
+    const PrIn& I = in[tile.inst];
+    const int K = D.cfg.K, T = D.cfg.T;
+    const int which = tile.s0 / T, t = tile.s0 % T;
+    const int tid = threadIdx.x;
+    // which 0: nominal + full cost; 1: robust + full cost; 2: robust + safety cost
+    const float* arr = D.avg + (size_t)(which == 0 ? 0 : K) * 2 + (which == 2 ? 1 : 0);
+    const float* nominal = which == 0 ? D.nom : D.rob;
+    float mn = INFINITY;
+    for (int s = tid; s < K; s += PUB)
+        mn = fminf(mn, arr[(size_t)s * 2]);
+    mn = warp_min(mn);
+    if ((tid & 31) == 0)
+        sMin[tid >> 5] = mn;
+    __syncthreads();
+    float minCost = sMin[0];
+#pragma unroll
+    for (int w = 1; w < PUB / 32; w++)
+        minCost = fminf(minCost, sMin[w]);
+    const float invTemp = I.lambda[which];
+    const float nom0 = nominal[t * 2], nom1 = nominal[t * 2 + 1];
+    const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+    float num0 = 0.0f, num1 = 0.0f, den = 0.0f;
+    for (int s = tid; s < K; s += PUB)
+    {
+        float cost = arr[(size_t)s * 2];
+        float w = expf(-(cost - minCost) / invTemp);
+        U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)t, step, S_PR_EPS, 0);
+        float u0 = nom0 + D.cfg.sigma0 * normal_from_word(r.x);
+        float u1 = nom1 + D.cfg.sigma1 * normal_from_word(r.y);
+        num0 += w * u0;
+        num1 += w * u1;
+        den += w;
+    }
+    sA[tid] = num0;
+    sB[tid] = num1;
+    sC[tid] = den;
+    __syncthreads();
+#pragma unroll
+    for (int stride = PUB / 2; stride >= 32; stride >>= 1)
+    {
+        if (tid < stride)
+        {
+            sA[tid] += sA[tid + stride];
+            sB[tid] += sB[tid + stride];
+            sC[tid] += sC[tid + stride];
+        }
+        __syncthreads();
+    }
+    if (tid < 32)
+    {
+        float a0 = sA[tid], a1 = sB[tid], dd = sC[tid];
+#pragma unroll
+        for (int stride = 16; stride > 0; stride >>= 1)
+        {
+            a0 += __shfl_down_sync(0xffffffffu, a0, stride);
+            a1 += __shfl_down_sync(0xffffffffu, a1, stride);
+            dd += __shfl_down_sync(0xffffffffu, dd, stride);
+        }
+        if (tid == 0)
+        {
+            float* out = which == 0 ? D.cand1 : (which == 1 ? D.cand2 : D.robWork);
+            out[t * 2] = (dd > 1e-30f) ? a0 / dd : nom0;
+            out[t * 2 + 1] = (dd > 1e-30f) ? a1 / dd : nom1;
+            if (t == 0)
+            {
+                D.nu[which] = dd;
+                D.minCosts[which] = minCost;
+            }
+        }
+    }
+}
+
+// one block per instance: threads (kind, cand, p), kind 0 = full cost, 1 = safety re-check
+template <int NOPP, int NTH>
+__global__ void __launch_bounds__(PRB) pr_candidates(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, int nInst)
+{
+    constexpr int NA = NOPP + 1;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ int sChosen;
+    const int inst = blockIdx.x;
+    if (inst >= nInst)
+        return;
+    const PrDev& D = insts[inst];
+    const PrIn& I = in[inst];
+    const int T = D.cfg.T, P = D.cfg.P;
+    uint64_t* bar = (uint64_t*)smraw;
+    EnvParams* sE = (EnvParams*)(smraw + 16);
+    const size_t offG = pa16(16 + sizeof(EnvParams));
+    float* sGrid = (float*)(smraw + offG);
+    float* sC1 = (float*)(smraw + offG + GRID_FLOATS * 4);
+    const uint32_t cb = (uint32_t)pa16((size_t)T * 2 * 4);
+    float* sC2 = (float*)((unsigned char*)sC1 + cb);
+    if (threadIdx.x == 0)
+    {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, GRID_FLOATS * 4 + 2 * cb);
+        bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
+        bulk_g2s(sC1, D.cand1, cb, bar);
+        bulk_g2s(sC2, D.cand2, cb, bar);
+    }
+    copyEnvP(sE, &D.env);
+    __syncthreads();
+    if (!__syncthreads_and(mbar_wait(bar, 0)))
+    {
+        if (threadIdx.x == 0)
+            atomicAdd(&D.stats[1], 1);
+        return;
+    }
+    const EnvParams& E = *sE;
+    const Track tr{sGrid + GRID_P, sGrid + GRID_T, sGrid + GRID_K};
+    const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+    for (int task = threadIdx.x; task < 4 * P; task += blockDim.x)
+    {
+        const int kind = task / (2 * P);
+        const int tid = task % (2 * P);
+        const int second = tid >= P;
+        const int p = second ? tid - P : tid;
+        const float* nominal = second ? sC2 : sC1;
+        const int theta = D.thetas[p];
+        DState<NA> st;
+        loadState<NA>(st, I.state);
+        BState<NTH> bs{};
+        EnvNoise rng(k0, k1, (uint32_t)p, (uint32_t)second << 16, step, kind ? S_PR_SAFE_ENV : S_PR_CAND_ENV);
+        float cost = 0.0f, safeCost = -INFINITY, decay = 1.0f;
+        bool stop = false;
+        for (int t = 0; t < T && !stop; ++t)
+        {
+            rng.begin_step((uint32_t)t);
+            bool branched = false;
+            StepOut o = envStep<NOPP, NTH, false, false, true, false>(t, theta, tr, E, nominal[t * 2], nominal[t * 2 + 1], st, bs, branched, 0.0f, rng);
+            stop = (o.term != TERM_NONE);
+            cost += decay * prStateCost(o, E, D.cfg.boundaryThresholdFactor, D.cfg.boundaryCost, D.cfg.winCost, D.cfg.oppWinCost);
+            decay *= DECAY;
+            safeCost = fmaxf(safeCost, prSafetyCost(o, E, D.cfg.collDistFactor));
+        }
+        cost += finalCost<NOPP>(st, E, D.cfg.finalAdvWeight, D.cfg.finalOppAdvWeight);
+        if (safeCost > 0.0f)
+            cost += D.cfg.safetyWeight;
+        if (kind == 0)
+            D.candFull[tid] = cost;
+        else
+            D.candSafe[tid] = safeCost;
+    }
+    __syncthreads();
+    // candidate choice (prmppi_controller.cu:236-256) and safety decision (:264-275)
+    if (threadIdx.x == 0)
+    {
+        float c1 = 0.0f, c2 = 0.0f;
+        for (int p = 0; p < P; ++p)
+        {
+            c1 += D.candFull[p];
+            c2 += D.candFull[P + p];
+        }
+        c1 /= (float)P;
+        c2 /= (float)P;
+        D.decision[0] = c2 < c1;          // resetNom
+        int chosen = (c1 <= c2) ? 0 : 1;
+        int useNom = 1;
+        for (int p = 0; p < P; p++)
+            if (D.candSafe[chosen * P + p] > 0.0f)
+            {
+                useNom = 0;
+                break;
+            }
+        D.decision[1] = useNom;
+        D.decision[2] = chosen;
+        sChosen = chosen;
+    }
+    __syncthreads();
+    const float* ch = sChosen ? sC2 : sC1;
+    for (int i = threadIdx.x; i < T * 2; i += blockDim.x)
+    {
+        D.nom[i] = ch[i];
+        D.rob[i] = D.robWork[i];
+    }
+}
+
+// perturbation of the next step, reference layout noise[T][K][2] (test hook)
+__global__ void pr_noise(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, float* __restrict__ out)
+{
+    const PrDev& D = insts[0];
+    const int K = D.cfg.K, T = D.cfg.T;
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)T * K)
+        return;
+    int s = (int)(i % K), t = (int)(i / K);
+    U4 r = draw(D.cfg.k0, D.cfg.k1, (uint32_t)s, (uint32_t)t, in[0].step, S_PR_EPS, 0);
+    out[i * 2] = D.cfg.sigma0 * normal_from_word(r.x);
+    out[i * 2 + 1] = D.cfg.sigma1 * normal_from_word(r.y);
+}
+
+bool prSupported(int nopp, int nth)
+{
+    int key = nopp * 16 + nth;
+    return key == 17 || key == 18 || key == 20 || key == 24 || key == 34;
+}
+
+int prRolloutSamplesPerBlock()
+{
+    return PRB;
+}
+
+size_t prRolloutSmem(int T)
+{
+    return prLayout(T).total;
+}
+
+static size_t prCandSmem(int T)
+{
+    return pa16(16 + sizeof(EnvParams)) + GRID_FLOATS * 4 + 2 * pa16((size_t)T * 2 * 4);
+}
+
+cudaError_t launchPrPrologue(const LaunchArgs& a, int nInst)
+{
+    pr_prologue<<<nInst, 256, 0, a.stream>>>(a.pr, a.prIn, nInst);
+    return cudaGetLastError();
+}
+
+template <int NOPP, int NTH> static cudaError_t prRollT(const LaunchArgs& a, size_t smem)
+{
+    auto k = pr_rollout<NOPP, NTH>;
+    ensureSmem(k, smem);
+    k<<<a.nTiles, PRB, smem, a.stream>>>(a.pr, a.prIn, a.tiles);
+    return cudaGetLastError();
+}
+
+template <int NOPP, int NTH> static cudaError_t prCandT(const LaunchArgs& a, int nInst, int T)
+{
+    auto k = pr_candidates<NOPP, NTH>;
+    size_t smem = prCandSmem(T);
+    ensureSmem(k, smem);
+    k<<<nInst, PRB, smem, a.stream>>>(a.pr, a.prIn, nInst);
+    return cudaGetLastError();
+}
+
+#define DR_PR_DISPATCH(NOPP_, NTH_, CALL)                                                                                                            \
+    switch (NOPP_ * 16 + NTH_)                                                                                                                       \
+    {                                                                                                                                                \
+    case 1 * 16 + 1: return CALL(1, 1);                                                                                                             \
+    case 1 * 16 + 2: return CALL(1, 2);                                                                                                             \
+    case 1 * 16 + 4: return CALL(1, 4);                                                                                                             \
+    case 1 * 16 + 8: return CALL(1, 8);                                                                                                             \
+    case 2 * 16 + 2: return CALL(2, 2);                                                                                                             \
+    default: return cudaErrorInvalidValue;                                                                                                           \
+    }
+
+cudaError_t launchPrRollout(const LaunchArgs& a, int nopp, int nth, size_t smem)
+{
+#define CALL(P_, Q_) prRollT<P_, Q_>(a, smem)
+    DR_PR_DISPATCH(nopp, nth, CALL)
+#undef CALL
+}
+
+cudaError_t launchPrReduce(const LaunchArgs& a)
+{
+    pr_weighted<<<a.nTiles, PUB, 0, a.stream>>>(a.pr, a.prIn, a.tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t launchPrCandidates(const LaunchArgs& a, int nopp, int nth, int nInst, int maxT, size_t)
+{
+#define CALL(P_, Q_) prCandT<P_, Q_>(a, nInst, maxT)
+    DR_PR_DISPATCH(nopp, nth, CALL)
+#undef CALL
+}
+
+cudaError_t launchPrNoise(const LaunchArgs& a, size_t n, float* out)
+{
+    pr_noise<<<(unsigned)((n + 255) / 256), 256, 0, a.stream>>>(a.pr, a.prIn, out);
+    return cudaGetLastError();
+}
+
+} // namespace dr

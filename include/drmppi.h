@@ -1,0 +1,310 @@
+/*
+ * drmppi.h — C ABI of the B200-native MPPI / PR-MPPI control step for the
+ * drone-race StratRace environment.
+ *
+ * This is the drop-in boundary for the reference's controller layer:
+ *   class Controller { virtual void getControl(const SimState&, float* outAction) = 0; ... }
+ *   (reference: include/controllers.h:12-21), with the two concrete controllers
+ *   MPPIController  (include/controllers.h:23-111, src/mppi_controller.cu:15-514) and
+ *   PRMPPIController (include/controllers.h:114-179, src/prmppi_controller.cu:14-349).
+ *
+ * Every entry point returns an int status (DR_OK == 0) and never throws. Pointers are
+ * host pointers unless a name ends in `_dev`. Nothing here takes a torch type.
+ *
+ * Compile-time sizes of the reference (N_OPP, N_TRUE_MODELS, USE_SPLINES, ...) are
+ * runtime fields here; supported combinations are listed in dr_supported().
+ * The model has one parameter factor (reference N_MODEL_FACTORS = 1,
+ * include/environments/env_stratrace_defs.h:17), so the number of branch plans is
+ * n_theta + 1 (reference N_BRANCH_PLANS = BRANCH_SIZE(0)).
+ */
+#ifndef DRMPPI_H
+#define DRMPPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DR_ABI_VERSION 1
+
+#define DR_DIM 2             /* reference EnvStratRace::DIM == ACTION_DIM (env_stratrace_defs.h:9,15) */
+#define DR_MAX_OPP 3         /* reference N_OPP (compile-time 1, env_stratrace_defs.h:10) */
+#define DR_MAX_AGENTS 4      /* N_OPP + 1 */
+#define DR_MAX_THETA 8       /* reference N_TRUE_MODELS (compile-time 2) */
+#define DR_MAX_KNOTS 64      /* reference MAX_N_KNOTS = 60 (include/config.h:27) */
+#define DR_MAX_T 256         /* longest horizon accepted (dense mode: nKnots = nTimesteps) */
+#define DR_N_TRACK_SAMPLES 512 /* reference N_TRACK_SAMPLES (env_stratrace_defs.h:11) */
+
+/* Status codes. */
+enum dr_status
+{
+    DR_OK = 0,
+    DR_ERR_INVALID_ARG = 1,  /* bad pointer, size or config value (reference throws std::runtime_error) */
+    DR_ERR_UNSUPPORTED = 2,  /* (n_opp, n_theta) combination not compiled in */
+    DR_ERR_CUDA = 3,         /* a CUDA runtime call failed; dr_last_error() has the text */
+    DR_ERR_OOM = 4,          /* device allocation failed */
+    DR_ERR_NO_DEVICE = 5,    /* no usable CUDA device */
+    DR_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up */
+    DR_ERR_STATE = 7,        /* call out of order (e.g. engine not set) */
+};
+
+/* Per-hypothesis opponent policy parameters (reference OppConfig,
+ * env_stratrace_defs.h:42-50). Arrays are indexed by opponent 0..n_opp-1. */
+typedef struct dr_opp_config
+{
+    float s1[DR_MAX_OPP];
+    float s2[DR_MAX_OPP];
+    float s3[DR_MAX_OPP];
+    float speed_scale[DR_MAX_OPP];
+    float action_noise[DR_MAX_OPP];
+} dr_opp_config;
+
+/* Environment (reference EnvironmentConfig, env_stratrace_defs.h:53-86; wire order of
+ * src/environments/env_stratrace.cpp:135-226). Agent 0 is the controlled (ego) agent.
+ * The four track grids are HOST pointers to DR_N_TRACK_SAMPLES samples each
+ * ([512][2] for p/dp/t, [512] for kappa); they are copied at create time. */
+typedef struct dr_env_config
+{
+    int32_t n_opp;   /* 1..DR_MAX_OPP */
+    int32_t n_theta; /* 1..DR_MAX_THETA */
+    float arena_min[DR_DIM];
+    float arena_max[DR_DIM];
+    float dt;
+    int32_t send_states;
+    float drone_radius;
+    float pos_noise_level;
+    float speed_noise_level;
+    float action_noise_level;
+    float max_speed[DR_MAX_AGENTS];
+    float max_accel[DR_MAX_AGENTS];
+    float track_width;
+    int32_t n_win_laps;
+    float init_belief[DR_MAX_THETA];
+    dr_opp_config opp_configs[DR_MAX_THETA];
+    float kP;
+    float kV;
+    float max_opp_lat_dist_fact;
+    float track_length;
+    const float* p_grid;
+    const float* dp_grid;
+    const float* t_grid;
+    const float* kappa_grid;
+} dr_env_config;
+
+/* Simulation state (reference SimState, env_stratrace_defs.h:88-96). Only the first
+ * n_opp + 1 agents are used. */
+typedef struct dr_sim_state
+{
+    float pos[DR_MAX_AGENTS * DR_DIM];
+    float vel[DR_MAX_AGENTS * DR_DIM];
+    float S[DR_MAX_AGENTS];
+    float lat_dist[DR_MAX_AGENTS];
+    int32_t laps[DR_MAX_AGENTS];
+} dr_sim_state;
+
+/* MPPI configuration (reference MPPIConfig, include/config.h:116-154; wire order of
+ * src/config.cpp:5-53). Fields after max_verif_eps are extensions. */
+typedef struct dr_mppi_config
+{
+    int32_t n_samples;
+    int32_t n_timesteps;
+    int32_t n_knots;                /* spline mode: M knots; dense mode: ignored (M = T) */
+    int32_t knots[DR_MAX_KNOTS];    /* tau_i, strictly increasing, tau_{M-1} <= T-2 */
+    int32_t use_splines;            /* reference compile-time USE_SPLINES (include/config.h:25) */
+    float inv_temperature;          /* used as a temperature: w = exp(-(c-min)/inv_temperature) */
+    float sampling_noise;           /* stddev of the control perturbation */
+    float gate_traversal_margin;    /* carried for wire compatibility; unused by the model */
+    float coll_dist_factor;
+    float boundary_cost;
+    float boundary_threshold_factor;
+    float outside_cost;
+    float win_cost;
+    float opp_win_cost;
+    float final_adv_weight;
+    float final_opp_adv_weight;
+    float min_confidence;
+    int32_t n_verif_samples;
+    float beta;
+    int32_t verif_horizon;          /* must be <= n_timesteps */
+    float max_verif_eps;
+    /* extensions (not in the reference; defaults keep reference behaviour) */
+    float sampling_noise_dim[DR_DIM]; /* per-dimension stddev; 0 => use sampling_noise */
+    float min_nu;                   /* reference MPPIController::min_nu = 0.0005 (controllers.h:47) */
+    float max_nu;                   /* reference MPPIController::max_nu = 0.001 (controllers.h:48) */
+    int32_t verify;                 /* 1 (reference) = run plan verification; 0 = always use the new plan */
+} dr_mppi_config;
+
+/* PR-MPPI configuration (reference PRMPPIConfig, include/config.h:157-192; wire order
+ * of src/config.cpp:55-84). */
+typedef struct dr_prmppi_config
+{
+    int32_t n_samples;
+    int32_t n_timesteps;
+    float inv_temperature;
+    float sampling_noise;
+    float gate_traversal_margin;
+    float coll_dist_factor;
+    float boundary_cost;
+    float boundary_threshold_factor;
+    float win_cost;
+    float opp_win_cost;
+    float final_adv_weight;
+    float final_opp_adv_weight;
+    float safety_weight;
+    float min_safe_dist;
+    float delta;
+    int32_t P;                      /* number of sampled hypotheses */
+    /* extensions */
+    float sampling_noise_dim[DR_DIM];
+    float min_nu;
+    float max_nu;
+} dr_prmppi_config;
+
+/* Per-step outputs of an MPPI controller; mirrors the public fields the reference
+ * engine reads (src/engine.cpp:75-117). */
+typedef struct dr_mppi_info
+{
+    uint32_t fail_count_total;   /* sum of the chosen plan's failCount (engine.cpp:77) */
+    int32_t use_new_plan;
+    double epsilon;
+    double epsilon_partial;
+    double certified_loss;
+    int32_t branch_idx;          /* branch whose first action was sent */
+    float min_cost;              /* minCosts[branch_idx][0] */
+    float nu;                    /* nu[branch_idx] */
+    float inv_temperature;       /* temperature after this step's adaptation */
+    int32_t nonfinite_costs;     /* number of samples whose cost was not finite */
+    int32_t verif_timeouts;      /* always 0 unless a bounded wait gave up */
+} dr_mppi_info;
+
+/* Per-step outputs of a PR-MPPI controller (src/engine.cpp:171-212). */
+typedef struct dr_prmppi_info
+{
+    int32_t use_nom_plan;
+    int32_t reset_nom;
+    float cand_cost[2];          /* averaged full cost of cand1 / cand2 */
+    float min_costs[3];          /* nom_full, rob_full, rob_safe */
+    float nu[3];
+    float inv_temperature[3];    /* after this step's adaptation */
+    int32_t nonfinite_costs;
+} dr_prmppi_info;
+
+typedef struct dr_mppi dr_mppi;
+typedef struct dr_prmppi dr_prmppi;
+typedef struct dr_mppi_batch dr_mppi_batch;
+typedef struct dr_prmppi_batch dr_prmppi_batch;
+
+/* ---- library ------------------------------------------------------------------ */
+int dr_abi_version(void);
+/* 1 if (n_opp, n_theta) is compiled in. */
+int dr_supported(int n_opp, int n_theta);
+/* Text of the last error on this thread ("" if none). */
+const char* dr_last_error(void);
+const char* dr_status_string(int status);
+
+/* ---- MPPI controller (reference MPPIController) --------------------------------- */
+/* nominal: n_theta+1 branch plans x n_timesteps x DR_DIM, or NULL for zeros
+ * (controllers.h:26-29; mppi_controller.cu:25-34). stream: cudaStream_t or NULL for a
+ * stream owned by the controller. */
+int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
+                   dr_mppi** out);
+int dr_mppi_destroy(dr_mppi* h);
+/* One control step (reference MPPIController::getControl, mppi_controller.cu:250-466).
+ * belief: n_theta floats. out_action: DR_DIM floats. info may be NULL. Blocks until done. */
+int dr_mppi_step(dr_mppi* h, const dr_sim_state* state, const float* belief, float* out_action, dr_mppi_info* info);
+/* Host mirror of the dense nominal (reference h_nominal, (n_theta+1) x T x DR_DIM). */
+int dr_mppi_get_nominal(const dr_mppi* h, float* out, size_t n);
+/* Spline knots currently on the device ((n_theta+1) x M x DR_DIM; dense mode: x T). */
+int dr_mppi_get_knots(dr_mppi* h, float* out, size_t n);
+/* failCount arrays of the last step (n_timesteps each): new plan, previous plan, chosen. */
+int dr_mppi_get_fail_counts(const dr_mppi* h, uint32_t* fc_new, uint32_t* fc_old, uint32_t* fc_chosen, size_t n);
+float dr_mppi_get_temperature(const dr_mppi* h);
+int dr_mppi_set_temperature(dr_mppi* h, float inv_temperature);
+/* Control-step counter (it keys the Philox streams); settable for deterministic replay. */
+uint64_t dr_mppi_get_step(const dr_mppi* h);
+/* Bytes copied host->device and device->host by one dr_mppi_step of this controller. */
+int dr_mppi_io_bytes(const dr_mppi* h, size_t* h2d, size_t* d2h);
+int dr_mppi_set_step(dr_mppi* h, uint64_t step);
+/* Per-kernel device time (ms) of the last step, measured with CUDA events on the
+ * controller's stream when profiling is on. names/ms arrays of capacity n. */
+int dr_mppi_set_profiling(dr_mppi* h, int on);
+/* Average per-kernel ms over the steps recorded since profiling was switched on. */
+int dr_mppi_get_kernel_times(dr_mppi* h, const char** names, float* ms, int n, int* count);
+
+/* Batched step: n controllers on one device advanced by one launch sequence
+ * (all agents x samples in one grid). states: n; beliefs: n x DR_MAX_THETA;
+ * out_actions: n x DR_DIM; infos: n or NULL. */
+int dr_mppi_batch_create(dr_mppi* const* hs, int n, void* stream, dr_mppi_batch** out);
+int dr_mppi_batch_destroy(dr_mppi_batch* b);
+int dr_mppi_batch_step(dr_mppi_batch* b, const dr_sim_state* states, const float* beliefs, float* out_actions, dr_mppi_info* infos);
+/* Device-resident variant for throughput measurement: states/beliefs already on the
+ * device (n records), results stay on the device; no host synchronisation. */
+int dr_mppi_batch_step_dev(dr_mppi_batch* b, const dr_sim_state* states_dev, const float* beliefs_dev);
+int dr_mppi_batch_set_graph(dr_mppi_batch* b, int use_graph);
+/* Per-kernel device time of the batch's steps (CUDA events on its stream), averaged
+ * over the steps recorded since profiling was switched on (also for *_step_dev). */
+int dr_mppi_batch_set_profiling(dr_mppi_batch* b, int on);
+int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** names, float* ms, int n, int* count);
+
+/* ---- MPPI test hooks (component parity against the reference kernels) ----------- */
+/* Control perturbation the next step will draw, in the reference layout
+ * noise[(n_theta+1)][M][K][DR_DIM] (kernels.cu:28). */
+int dr_mppi_debug_noise(dr_mppi* h, float* noise, size_t n);
+/* Rollout of the next step on the current knots/nominal (kernels.cu:34-171): costsTrue
+ * [n_theta][K], branchUsed/branchTime [n_theta][K], costs [n_theta+1][K] (kernels.cu:175-217). */
+int dr_mppi_debug_rollout(dr_mppi* h, const dr_sim_state* state, const float* belief, float* costs_true, int32_t* branch_used,
+                          int32_t* branch_time, float* costs);
+/* Update only (kernels.cu:221-456) on the given rollout outputs: replaces the device knots
+ * (spline mode) or dense nominal and writes the new dense nominal, minCosts
+ * [(n_theta+1)][M] and nu [(n_theta+1)]. Uses the same noise as the next step. */
+int dr_mppi_debug_update(dr_mppi* h, const float* belief, const float* costs_true, const int32_t* branch_used, const int32_t* branch_time,
+                         float* dense_nominal, float* min_costs, float* nu);
+/* Verification of a dense plan ((n_theta+1) x T x DR_DIM) from `state`: failCount[T]
+ * (kernels.cu:488-551). plan selects the Philox stream (0 new, 1 previous).
+ * fail_time (optional, V entries): per-sample failure time or -1. thetas (optional): V. */
+int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* belief, const float* dense_plan, int plan,
+                         uint32_t* fail_count, int32_t* fail_time, int32_t* thetas);
+
+/* ---- PR-MPPI controller (reference PRMPPIController) ---------------------------- */
+/* nominal: n_timesteps x DR_DIM or NULL (prmppi_controller.cu:24-37). */
+int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
+                     dr_prmppi** out);
+int dr_prmppi_destroy(dr_prmppi* h);
+/* One control step (prmppi_controller.cu:142-349). */
+int dr_prmppi_step(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* out_action, dr_prmppi_info* info);
+/* Host mirrors h_nom_nominal / h_rob_nominal (T x DR_DIM each). */
+int dr_prmppi_get_nominals(const dr_prmppi* h, float* nom, float* rob, size_t n);
+uint64_t dr_prmppi_get_step(const dr_prmppi* h);
+int dr_prmppi_io_bytes(const dr_prmppi* h, size_t* h2d, size_t* d2h);
+int dr_prmppi_set_step(dr_prmppi* h, uint64_t step);
+int dr_prmppi_set_profiling(dr_prmppi* h, int on);
+int dr_prmppi_get_kernel_times(dr_prmppi* h, const char** names, float* ms, int n, int* count);
+int dr_prmppi_batch_create(dr_prmppi* const* hs, int n, void* stream, dr_prmppi_batch** out);
+int dr_prmppi_batch_destroy(dr_prmppi_batch* b);
+int dr_prmppi_batch_step(dr_prmppi_batch* b, const dr_sim_state* states, const float* beliefs, float* out_actions, dr_prmppi_info* infos);
+int dr_prmppi_batch_step_dev(dr_prmppi_batch* b, const dr_sim_state* states_dev, const float* beliefs_dev);
+int dr_prmppi_batch_set_profiling(dr_prmppi_batch* b, int on);
+int dr_prmppi_batch_get_kernel_times(dr_prmppi_batch* b, const char** names, float* ms, int n, int* count);
+
+/* ---- PR-MPPI test hooks ---------------------------------------------------------- */
+/* noise[T][K][DR_DIM] (prmppi_kernels.cu:17) and thetas[P] (prmppi_kernels.cu:23-51) of the next step. */
+int dr_prmppi_debug_noise(dr_prmppi* h, const float* belief, float* noise, size_t n, int32_t* thetas);
+/* Rollout of the next step (prmppi_kernels.cu:55-130): cost_nom/cost_rob [P][K][2]
+ * (running cost, safety cost), before averaging. The nominals are the shifted ones. */
+int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* cost_nom, float* cost_rob);
+
+/* ---- environment step on the device (reference engine dynStep, engine.cpp:286-312) */
+/* Advances `state` in place by one true-dynamics step for the ego action, with the
+ * given true hypothesis; updates belief (n_theta) in place. Returns the terminal type
+ * (0 none, 1 lose, 2 win, 3 opponent win) in *term. Noise is drawn from the Philox
+ * stream (seed, step). */
+int dr_env_step(const dr_env_config* env, int true_theta, const float* action, dr_sim_state* state, float* belief, int update_belief,
+                uint64_t seed, uint64_t step, int* term);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRMPPI_H */
