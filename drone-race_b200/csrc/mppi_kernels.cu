@@ -245,8 +245,8 @@ __global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ i
                     for (int m = 0; m < M; m++)
                     {
                         U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)(b * M + m), step, S_MPPI_EPS, 0);
-                        float e0 = sig0 * normal_from_word(r.x);
-                        float e1 = sig1 * normal_from_word(r.y);
+                        float e0 = scaled_normal(sig0, r.x);
+                        float e1 = scaled_normal(sig1, r.y);
                         vbuf[(m * 2 + 0) * RB + threadIdx.x] = sKn[(b * M + m) * 2 + 0] + e0;
                         vbuf[(m * 2 + 1) * RB + threadIdx.x] = sKn[(b * M + m) * 2 + 1] + e1;
                     }
@@ -265,8 +265,8 @@ __global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ i
             else
             {
                 U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)(b * T + local), step, S_MPPI_EPS, 0);
-                float e0 = sig0 * normal_from_word(r.x);
-                float e1 = sig1 * normal_from_word(r.y);
+                float e0 = scaled_normal(sig0, r.x);
+                float e1 = scaled_normal(sig1, r.y);
                 ego0 = sKn[(b * T + local) * 2 + 0] + e0;
                 ego1 = sKn[(b * T + local) * 2 + 1] + e1;
             }
@@ -454,8 +454,8 @@ template <int NTH> __global__ void __launch_bounds__(UB) mppi_update(const MppiD
                 float cost = costs[s];
                 float w = expf(-(cost - minC) / lambda);
                 U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)(b * M + k), step, S_MPPI_EPS, 0);
-                float eps0 = D.cfg.sigma0 * normal_from_word(r.x);
-                float eps1 = D.cfg.sigma1 * normal_from_word(r.y);
+                float eps0 = scaled_normal(D.cfg.sigma0, r.x);
+                float eps1 = scaled_normal(D.cfg.sigma1, r.y);
                 num0 += w * coeff * eps0;
                 num1 += w * coeff * eps1;
                 den += w * coeff;
@@ -673,8 +673,8 @@ __global__ void mppi_noise(const MppiDev* __restrict__ insts, const MppiIn* __re
     int s = (int)(i % K);
     int bk = (int)(i / K);
     U4 r = draw(D.cfg.k0, D.cfg.k1, (uint32_t)s, (uint32_t)bk, in[0].step, S_MPPI_EPS, 0);
-    out[i * 2] = D.cfg.sigma0 * normal_from_word(r.x);
-    out[i * 2 + 1] = D.cfg.sigma1 * normal_from_word(r.y);
+    out[i * 2] = scaled_normal(D.cfg.sigma0, r.x);
+    out[i * 2 + 1] = scaled_normal(D.cfg.sigma1, r.y);
 }
 
 // ---------------------------------------------------------------------------------------

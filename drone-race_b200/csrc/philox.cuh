@@ -140,6 +140,14 @@ __device__ __forceinline__ float normal_from_word(uint32_t w)
     return normal_from_uniform(uniform_from_word(w));
 }
 
+// A perturbation entry sigma * N(0,1), rounded on its own (the reference stores the
+// perturbation tensor and adds it to the nominal afterwards; letting the compiler fuse
+// the product into that addition would change the last bit).
+__device__ __forceinline__ float scaled_normal(float sigma, uint32_t w)
+{
+    return __fmul_rn(sigma, normal_from_word(w));
+}
+
 // Sequential normal source for the environment noise of one rollout step.
 struct EnvNoise
 {

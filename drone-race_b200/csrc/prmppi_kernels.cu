@@ -172,8 +172,8 @@ __global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ inst
         {
             rng.begin_step((uint32_t)t);
             U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)t, step, S_PR_EPS, 0);
-            float ego0 = sNom[t * 2] + D.cfg.sigma0 * normal_from_word(r.x);
-            float ego1 = sNom[t * 2 + 1] + D.cfg.sigma1 * normal_from_word(r.y);
+            float ego0 = sNom[t * 2] + scaled_normal(D.cfg.sigma0, r.x);
+            float ego1 = sNom[t * 2 + 1] + scaled_normal(D.cfg.sigma1, r.y);
             bool branched = false;
             StepOut o = envStep<NOPP, NTH, false, false, true, false>(t, theta, tr, E, ego0, ego1, st, bs, branched, 0.0f, rng);
             stop = (o.term != TERM_NONE);
@@ -241,8 +241,8 @@ __global__ void __launch_bounds__(PUB) pr_weighted(const PrDev* __restrict__ ins
         float cost = arr[(size_t)s * 2];
         float w = expf(-(cost - minCost) / invTemp);
         U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)t, step, S_PR_EPS, 0);
-        float u0 = nom0 + D.cfg.sigma0 * normal_from_word(r.x);
-        float u1 = nom1 + D.cfg.sigma1 * normal_from_word(r.y);
+        float u0 = nom0 + scaled_normal(D.cfg.sigma0, r.x);
+        float u1 = nom1 + scaled_normal(D.cfg.sigma1, r.y);
         num0 += w * u0;
         num1 += w * u1;
         den += w;
@@ -401,8 +401,8 @@ __global__ void pr_noise(const PrDev* __restrict__ insts, const PrIn* __restrict
         return;
     int s = (int)(i % K), t = (int)(i / K);
     U4 r = draw(D.cfg.k0, D.cfg.k1, (uint32_t)s, (uint32_t)t, in[0].step, S_PR_EPS, 0);
-    out[i * 2] = D.cfg.sigma0 * normal_from_word(r.x);
-    out[i * 2 + 1] = D.cfg.sigma1 * normal_from_word(r.y);
+    out[i * 2] = scaled_normal(D.cfg.sigma0, r.x);
+    out[i * 2 + 1] = scaled_normal(D.cfg.sigma1, r.y);
 }
 
 bool prSupported(int nopp, int nth)

@@ -19,6 +19,18 @@
 namespace orc
 {
 
+using std::copysign;
+using std::exp;
+using std::fabs;
+using std::floor;
+using std::fmax;
+using std::fmin;
+using std::isfinite;
+using std::isinf;
+using std::log;
+using std::pow;
+using std::sqrt;
+
 constexpr int DIM = 2;
 constexpr int NTS = DR_N_TRACK_SAMPLES;
 constexpr int WINDOW_SIZE = 10; // env_stratrace_defs.h:40
@@ -35,7 +47,7 @@ enum Term
 
 template <typename R> inline R rsqrt_div(R x)
 {
-    return R(1) / std::sqrt(x);
+    return R(1) / sqrt(x);
 }
 
 // Environment parameters converted to R, plus the track grids padded with one
@@ -217,7 +229,7 @@ template <typename R> inline R sqNorm(R x, R y) // :33-36
 template <typename R> inline void sampleTrackArray2(const R* arr, R s, R* out, R L)
 {
     s /= L;
-    s = s - std::floor(s);
+    s = s - floor(s);
     R idx_f = s * NTS;
     int idx0 = (int)idx_f;
     int idx1 = (idx0 + 1) % NTS;
@@ -230,7 +242,7 @@ template <typename R> inline void sampleTrackArray2(const R* arr, R s, R* out, R
 template <typename R> inline R sampleTrackArray1(const R* arr, R s, R L)
 {
     s /= L;
-    s = s - std::floor(s);
+    s = s - floor(s);
     R idx_f = s * NTS;
     int idx0 = (int)idx_f;
     int idx1 = (idx0 + 1) % NTS;
@@ -242,7 +254,7 @@ template <typename R> inline R sampleTrackArray1(const R* arr, R s, R L)
 template <typename R> inline void sampleNormalizedSpeed(const R* t_grid, R s, R* out, R L)
 {
     sampleTrackArray2(t_grid, s, out, L);
-    R invNorm = R(1) / std::sqrt(sqNorm(out[0], out[1]));
+    R invNorm = R(1) / sqrt(sqNorm(out[0], out[1]));
     out[0] *= invNorm;
     out[1] *= invNorm;
 }
@@ -260,7 +272,7 @@ template <typename R> inline R sqDistToSample(const R* p_grid, int i, const R* p
 template <typename R> inline R fastProjectOnTrack(const Env<R>& env, const R* pos, R prevS, R& latDist)
 {
     prevS /= env.trackLength;
-    prevS = prevS - std::floor(prevS);
+    prevS = prevS - floor(prevS);
     int idxPrev = (int)(prevS * NTS);
 
     int bestInd = (idxPrev - WINDOW_SIZE + NTS) % NTS;
@@ -291,7 +303,7 @@ template <typename R> inline R fastProjectOnTrack(const Env<R>& env, const R* po
         if ((double)sqAB > 1e-12) // float compared with a double literal, as in the reference
         {
             t = ((pos[0] - P[2 * a]) * abx + (pos[1] - P[2 * a + 1]) * aby) / sqAB;
-            t = std::fmax(R(0), std::fmin(t, R(1)));
+            t = fmax(R(0), fmin(t, R(1)));
         }
         R projx = P[2 * a] + t * abx;
         R projy = P[2 * a + 1] + t * aby;
@@ -307,7 +319,7 @@ template <typename R> inline R fastProjectOnTrack(const Env<R>& env, const R* po
     R tang[2];
     sampleTrackArray2(env.t.data(), bestS, tang, env.trackLength);
     R cross = -tang[1] * (pos[0] - closestX) + tang[0] * (pos[1] - closestY);
-    latDist = std::copysign(std::sqrt(bestSegSqDist), cross);
+    latDist = copysign(sqrt(bestSegSqDist), cross);
     return bestS;
 }
 
@@ -329,7 +341,7 @@ template <typename R> inline void updateBelief(const Env<R>& env, R* belief, con
                 sqAccel += nom[d] * nom[d];
             R scale = R(1);
             if (sqAccel > env.maxAccel[o + 1] * env.maxAccel[o + 1])
-                scale = env.maxAccel[o + 1] / std::sqrt(sqAccel);
+                scale = env.maxAccel[o + 1] / sqrt(sqAccel);
             R sqDist = R(0);
             for (int d = 0; d < DIM; d++)
             {
@@ -338,9 +350,9 @@ template <typename R> inline void updateBelief(const Env<R>& env, R* belief, con
             }
             R an = env.actionNoise[th][o];
             R sqSigma = sigmaEnv * sigmaEnv + an * an;
-            logLikelihood += R(-0.5) * sqDist / sqSigma - (R)DIM * R(0.5) * std::log(R(2) * pi) - (R)DIM * R(0.5) * std::log(sqSigma);
+            logLikelihood += R(-0.5) * sqDist / sqSigma - (R)DIM * R(0.5) * log(R(2) * pi) - (R)DIM * R(0.5) * log(sqSigma);
         }
-        belief[th] *= std::exp(logLikelihood);
+        belief[th] *= exp(logLikelihood);
         sum += belief[th];
     }
     if (sum < R(1e-20))
@@ -365,8 +377,8 @@ template <typename R> inline R trackBoundaryDist(const State<R>& s, const Env<R>
                 return R(-1);
     R minSq = INFINITY;
     for (int o = 1; o <= env.nopp; o++)
-        minSq = std::fmin(minSq, sqNorm(s.pos[2 * o] - s.pos[0], s.pos[2 * o + 1] - s.pos[1]));
-    return std::fmin(std::sqrt(minSq) - env.droneRadius, env.trackWidth - std::fabs(s.lat[0]));
+        minSq = fmin(minSq, sqNorm(s.pos[2 * o] - s.pos[0], s.pos[2 * o + 1] - s.pos[1]));
+    return fmin(sqrt(minSq) - env.droneRadius, env.trackWidth - fabs(s.lat[0]));
 }
 
 template <typename R> inline bool isOutside(const State<R>& s, const Env<R>& env, R radius, bool loseOnOppWin) // :246-250
@@ -379,7 +391,7 @@ template <typename R> inline bool isWinner(const State<R>& s, const Env<R>& env)
     if (s.laps[0] >= env.nWinLaps)
         return true;
     for (int o = 1; o <= env.nopp; o++)
-        if (std::fabs(s.lat[o]) > env.trackWidth - env.droneRadius)
+        if (fabs(s.lat[o]) > env.trackWidth - env.droneRadius)
             return true;
     return false;
 }
@@ -401,7 +413,7 @@ template <typename R> inline R getOppAdvance(const State<R>& s, const Env<R>& en
 {
     R mx = -INFINITY;
     for (int o = 1; o <= env.nopp; o++)
-        mx = std::fmax(mx, getAnyAdvance(s, env, o));
+        mx = fmax(mx, getAnyAdvance(s, env, o));
     return mx;
 }
 
@@ -412,8 +424,8 @@ template <typename R> inline R computeSdot(int i, const State<R>& s, const Env<R
     sampleNormalizedSpeed(env.t.data(), s.S[i], tang_i, env.trackLength);
     R kappa_current = sampleTrackArray1(env.kappa.data(), s.S[i], env.trackLength);
     R metric = 1 - kappa_current * s.lat[i];
-    if (std::fabs(metric) < R(1e-12))
-        metric = std::copysign(R(1e-12), metric);
+    if (fabs(metric) < R(1e-12))
+        metric = copysign(R(1e-12), metric);
     return (tang_i[0] * s.vel[2 * i] + tang_i[1] * s.vel[2 * i + 1]) / metric;
 }
 
@@ -472,29 +484,29 @@ template <typename R> inline R computeOppTargetLatDist(int iOpp, const State<R>&
         R sdot_j = computeSdot(j, s, env);
         R blockTolerance = env.maxSpeed[j] * R(0.3);
         bool shouldBlock = (deltaS < R(0)) && (deltaS > -env.trackLength * R(0.25)) && (sdot_j + blockTolerance > sdot_i);
-        bool shouldOvertake = (sdot_i > sdot_j) && (std::fabs(deltaE) < s1);
-        R factor = std::exp(-s2 * deltaS * deltaS);
+        bool shouldOvertake = (sdot_i > sdot_j) && (fabs(deltaE) < s1);
+        R factor = exp(-s2 * deltaS * deltaS);
         if (shouldBlock)
         {
-            R blockTerm = s.lat[j] * (1 - std::exp(-s3 * (sdot_j + blockTolerance - sdot_i))) * factor;
+            R blockTerm = s.lat[j] * (1 - exp(-s3 * (sdot_j + blockTolerance - sdot_i))) * factor;
             latDis += blockTerm;
         }
         if (shouldOvertake)
         {
-            R overtakeTerm = (s.lat[j] - std::copysign(s1, deltaE)) * factor;
+            R overtakeTerm = (s.lat[j] - copysign(s1, deltaE)) * factor;
             latDis += overtakeTerm;
             R oppLongSpeed = s.vel[2 * j] * tang_j[0] + s.vel[2 * j + 1] * tang_j[1];
             if (deltaS < 3 * env.droneRadius)
-                speedGoal = std::fmin(speedGoal, R(0.7) * oppLongSpeed);
+                speedGoal = fmin(speedGoal, R(0.7) * oppLongSpeed);
             else if (deltaS < 6 * env.droneRadius && (double)s1 > 1e-6) // double literal, as in the reference
             {
-                R latFactor = std::fabs(deltaE) / s1;
-                speedGoal = std::fmin(speedGoal, latFactor * oppLongSpeed + (R(1) - latFactor) * baseSpeed);
+                R latFactor = fabs(deltaE) / s1;
+                speedGoal = fmin(speedGoal, latFactor * oppLongSpeed + (R(1) - latFactor) * baseSpeed);
             }
         }
     }
     R maxLatDis = env.trackWidth - env.droneRadius * env.maxOppLatDistFact;
-    latDis = std::fmax(-maxLatDis, std::fmin(maxLatDis, latDis));
+    latDis = fmax(-maxLatDis, fmin(maxLatDis, latDis));
     speedGoalOut = speedGoal;
     return latDis;
 }
@@ -523,57 +535,57 @@ template <typename R> inline void computeOpponentAction(int iOpp, const State<R>
 
     R e_n_max = env.trackWidth - env.droneRadius * R(1.2);
     R metric_actual = R(1) - kappa * e_n;
-    if (std::fabs(metric_actual) < R(1e-6))
-        metric_actual = std::copysign(R(1e-6), metric_actual);
+    if (fabs(metric_actual) < R(1e-6))
+        metric_actual = copysign(R(1e-6), metric_actual);
     R a_centripetal = v_t * v_t * kappa / metric_actual;
-    R a_lat_max = std::fmax(maxAccel - std::fabs(a_centripetal), maxAccel * R(0.2));
+    R a_lat_max = fmax(maxAccel - fabs(a_centripetal), maxAccel * R(0.2));
 
-    R latDis = std::fmax(-e_n_max, std::fmin(e_n_max, latDisRaw));
+    R latDis = fmax(-e_n_max, fmin(e_n_max, latDisRaw));
     R e_error = latDis - e_n;
-    R dist_to_pos_wall = std::fmax(e_n_max - e_n, R(0.001));
-    R dist_to_neg_wall = std::fmax(e_n_max + e_n, R(0.001));
+    R dist_to_pos_wall = fmax(e_n_max - e_n, R(0.001));
+    R dist_to_neg_wall = fmax(e_n_max + e_n, R(0.001));
 
     R a_n_cmd;
     if (v_n > R(0) && v_n * v_n > R(1.8) * a_lat_max * dist_to_pos_wall)
         a_n_cmd = -a_lat_max;
     else if (v_n < R(0) && v_n * v_n > R(1.8) * a_lat_max * dist_to_neg_wall)
         a_n_cmd = a_lat_max;
-    else if (std::fabs(e_error) < R(0.02))
+    else if (fabs(e_error) < R(0.02))
     {
         R kp = a_lat_max / R(0.02);
-        a_n_cmd = kp * e_error - R(2) * std::sqrt(kp) * v_n;
-        a_n_cmd = std::fmax(-a_lat_max, std::fmin(a_lat_max, a_n_cmd));
+        a_n_cmd = kp * e_error - R(2) * sqrt(kp) * v_n;
+        a_n_cmd = fmax(-a_lat_max, fmin(a_lat_max, a_n_cmd));
     }
     else
     {
         R stopping_dist = v_n * v_n / (R(2) * a_lat_max);
         bool v_toward = (e_error > R(0) && v_n > R(0)) || (e_error < R(0) && v_n < R(0));
-        bool decel_phase = v_toward && stopping_dist >= std::fabs(e_error) * R(0.95);
+        bool decel_phase = v_toward && stopping_dist >= fabs(e_error) * R(0.95);
         a_n_cmd = (e_error > R(0)) ? a_lat_max : -a_lat_max;
         if (decel_phase)
             a_n_cmd = -a_n_cmd;
         R v_n_next = v_n + a_n_cmd * dt;
         if (v_n_next > R(0))
         {
-            R v_safe = std::sqrt(R(2) * a_lat_max * dist_to_pos_wall);
+            R v_safe = sqrt(R(2) * a_lat_max * dist_to_pos_wall);
             if (v_n_next > v_safe)
                 a_n_cmd = (v_safe - v_n) / dt;
         }
         else
         {
-            R v_safe = std::sqrt(R(2) * a_lat_max * dist_to_neg_wall);
+            R v_safe = sqrt(R(2) * a_lat_max * dist_to_neg_wall);
             if (-v_n_next > v_safe)
                 a_n_cmd = (-v_safe - v_n) / dt;
         }
     }
-    R a_n_total = std::fmax(-maxAccel, std::fmin(maxAccel, a_n_cmd + a_centripetal));
-    R a_t_max = std::sqrt(std::fmax(maxAccel * maxAccel - a_n_total * a_n_total, R(0)));
+    R a_n_total = fmax(-maxAccel, fmin(maxAccel, a_n_cmd + a_centripetal));
+    R a_t_max = sqrt(fmax(maxAccel * maxAccel - a_n_total * a_n_total, R(0)));
     R kappa_eff = kappa / (R(1) - kappa * latDis + R(1e-6));
-    R pathSpeed = std::fmin(speedGoal, std::sqrt(maxAccel / std::fmax(std::fabs(kappa_eff), R(1e-12))));
-    if (std::fabs(a_n_cmd) > a_lat_max * R(0.5))
-        pathSpeed *= std::fmax(R(0.4), R(1.5) - std::fabs(a_n_cmd) / a_lat_max);
+    R pathSpeed = fmin(speedGoal, sqrt(maxAccel / fmax(fabs(kappa_eff), R(1e-12))));
+    if (fabs(a_n_cmd) > a_lat_max * R(0.5))
+        pathSpeed *= fmax(R(0.4), R(1.5) - fabs(a_n_cmd) / a_lat_max);
     R a_t_cmd = env.kV * (pathSpeed - v_t) - v_n * kappa * v_t / metric_actual;
-    a_t_cmd = std::fmax(-a_t_max, std::fmin(a_t_max, a_t_cmd));
+    a_t_cmd = fmax(-a_t_max, fmin(a_t_max, a_t_cmd));
     out[0] = a_t_cmd * tang[0] + a_n_total * norm[0];
     out[1] = a_t_cmd * tang[1] + a_n_total * norm[1];
 }
@@ -623,7 +635,7 @@ inline int environmentStep(int t, int trueTheta, const Env<R>& env, const R* ego
         R factor = R(1);
         R maxSq = env.maxAccel[a] * env.maxAccel[a];
         if (sq > maxSq)
-            factor = env.maxAccel[a] / std::sqrt(sq);
+            factor = env.maxAccel[a] / sqrt(sq);
         for (int d = 0; d < DIM; d++)
         {
             R& v = actions[a * DIM + d];
@@ -648,7 +660,7 @@ inline int environmentStep(int t, int trueTheta, const Env<R>& env, const R* ego
         R sqSpd = sqNorm(s.vel[2 * a], s.vel[2 * a + 1]);
         if (sqSpd > env.maxSpeed[a] * env.maxSpeed[a])
         {
-            R sc = env.maxSpeed[a] / std::sqrt(sqSpd);
+            R sc = env.maxSpeed[a] / sqrt(sqSpd);
             for (int d = 0; d < DIM; d++)
                 s.vel[a * DIM + d] *= sc;
         }
@@ -709,7 +721,7 @@ template <typename R> struct PrCosts
 
 template <typename R> inline R powi2(R x)
 {
-    return std::pow(x, R(2));
+    return pow(x, R(2));
 }
 
 // stateCost, costs.cuh:7-28

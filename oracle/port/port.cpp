@@ -169,7 +169,7 @@ void mppiUpdate(const dr_env_config& ec, const dr_mppi_config& mc, const float* 
                 if (!branchCompatibleWithModel(b, th))
                     continue;
                 R c = costsTrue[th * K + s];
-                if (!std::isfinite(c))
+                if (!isfinite(c))
                     continue;
                 R w = belief[th];
                 num += w * c;
@@ -217,14 +217,14 @@ void mppiUpdate(const dr_env_config& ec, const dr_mppi_config& mc, const float* 
                 for (int i = 0; i < NT; i++)
                     pnum[i] = pden[i] = R(0);
                 R minC = minCosts[b * M + k];
-                if (!std::isinf(minC))
+                if (!isinf(minC))
                     for (int s = 0; s < K; s++)
                     {
                         R coeff = sampleCoeff(mc, nth, belief, b, k, s, K, branchUsed, branchTime);
                         if (coeff > (R)MIN_COEFF_THRESHOLD)
                         {
                             R cost = costs[b * K + s];
-                            R w = std::exp(-(cost - minC) / lambda);
+                            R w = exp(-(cost - minC) / lambda);
                             R eps = noise[((size_t)(b * M + k) * K + s) * DIM + d];
                             int slot = blockorder ? (s % NT) : 0;
                             pnum[slot] += w * coeff * eps;
@@ -269,7 +269,7 @@ void mppiUpdate(const dr_env_config& ec, const dr_mppi_config& mc, const float* 
         R maxSq = maxAccel * maxAccel;
         if (sq > maxSq)
         {
-            R scale = maxAccel / std::sqrt(sq);
+            R scale = maxAccel / sqrt(sq);
             for (int d = 0; d < DIM; d++)
                 knots[v * DIM + d] *= scale;
         }
@@ -398,7 +398,7 @@ void prRollout(const dr_env_config& ec, const dr_prmppi_config& pc, const dr_sim
             int term = environmentStep(t, theta, env, ego, flags, st, bs, branched, R(0), rng);
             stop = (term != TERM_NONE);
             running += decay * prStateCost(st, env, cc);
-            safe = std::fmax(safe, prSafetyCost(st, env, cc));
+            safe = fmax(safe, prSafetyCost(st, env, cc));
             decay *= (R)DECAY;
         }
         running += finalCost(st, env, cc.finalAdvWeight, cc.finalOppAdvWeight);
@@ -433,7 +433,7 @@ void prUpdate(const dr_prmppi_config& pc, double* costNomIO, double* costRobIO, 
             {
                 size_t off = ((size_t)p * K + s) * 2;
                 avg += c[off];
-                maxSafe = std::fmax(maxSafe, c[off + 1]);
+                maxSafe = fmax(maxSafe, c[off + 1]);
             }
             avg /= (R)P;
             c[s * 2] = avg + ((maxSafe > R(0)) ? sw : R(0));
@@ -451,7 +451,7 @@ void prUpdate(const dr_prmppi_config& pc, double* costNomIO, double* costRobIO, 
         const R* arr = which == 0 ? cn.data() : (which == 1 ? cr.data() : cr.data() + 1);
         R v = INFINITY;
         for (int i = 0; i < K; i++)
-            v = std::fmin(v, arr[i * 2]);
+            v = fmin(v, arr[i * 2]);
         minCosts[which] = v;
         minCostsOut[which] = (double)v;
     }
@@ -472,7 +472,7 @@ void prUpdate(const dr_prmppi_config& pc, double* costNomIO, double* costRobIO, 
                 for (int i = 0; i < K; i++)
                 {
                     R cost = arr[2 * i];
-                    R w = std::exp(-(cost - minCosts[which]) / lambda);
+                    R w = exp(-(cost - minCosts[which]) / lambda);
                     R u = nomv + (R)noise[((size_t)t * K + i) * DIM + d];
                     int slot = blockorder ? (i % NT) : 0;
                     pnum[slot] += w * u;
@@ -525,7 +525,7 @@ void prCandidates(const dr_env_config& ec, const dr_prmppi_config& pc, const dr_
             stop = (term != TERM_NONE);
             cost += decay * prStateCost(st, env, cc);
             decay *= (R)DECAY;
-            safe = std::fmax(safe, prSafetyCost(st, env, cc));
+            safe = fmax(safe, prSafetyCost(st, env, cc));
         }
         cost += finalCost(st, env, cc.finalAdvWeight, cc.finalOppAdvWeight);
         if (safe > R(0))

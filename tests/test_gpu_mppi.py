@@ -51,9 +51,14 @@ def test_rollout_matches_reference_kernel(gpu, spl):
     nominal = random_nominal(sc, rng)
     ctl = mppi_ctl(sc, nominal=nominal)
     belief = sc.belief()
+    if spl:
+        # one full step first, so that the knots are no longer the initial zeros
+        ctl.engine = object()
+        ctl.getControl(sc.state)
     noise = _dev_noise(ctl, sc)
-    kn = ctl.knots()
     ct, bu, bt, costs = _dev_rollout(ctl, sc, belief)
+    kn = ctl.knots()  # the (shifted) knots the rollout used
+    assert np.abs(kn).max() > 0
     rct = np.zeros_like(ct)
     rbu = np.zeros_like(bu)
     rbt = np.zeros_like(bt)
