@@ -6,4 +6,4 @@ track preprocessing (track), configuration presets (scenarios), the controller
 classes mirroring the reference's include/controllers.h (controllers) and the
 reference's wire protocol (protocol).
 """
-from . import abi, controllers, scenarios, track  # noqa: F401
+from . import abi, controllers, protocol, scenarios, track  # noqa: F401

@@ -930,3 +930,15 @@ extern "C" int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** nam
     CK(cudaSetDevice(b->device));
     return kernelTimes(b->timer, names, ms, n, count);
 }
+
+extern "C" int dr_spline_matrix(int T, int M, const int32_t* knots, float* out)
+{
+    if (T < 2 || M < 2 || M > DR_MAX_KNOTS || !knots || !out)
+        return fail(DR_ERR_INVALID_ARG, "bad spline size or NULL pointer");
+    for (int i = 0; i < M; i++)
+        if (knots[i] < 0 || knots[i] >= T || (i > 0 && knots[i] <= knots[i - 1]))
+            return fail(DR_ERR_INVALID_ARG, "knots must be strictly increasing inside [0, T)");
+    std::vector<float> B = splineMatrix(T, M, knots);
+    std::memcpy(out, B.data(), B.size() * sizeof(float));
+    return DR_OK;
+}

@@ -208,6 +208,10 @@ struct OppCommon
     float sdot_i, maxLatDis;
     // computeOpponentAction
     float tang0, tang1, norm0, norm1, kappa, e_n, v_t, v_n, e_n_max, metric_actual, a_centripetal, a_lat_max, distPos, distNeg, maxAccel;
+    // maxAccel^2 rounded on its own: the reference evaluates the policy under every
+    // hypothesis, so this hypothesis-independent product is shared and never fused into
+    // maxAccel^2 - a_n^2 (env_stratrace.h:691); fusing it would change the last bit
+    float maxAccelSq;
     bool brakePos, brakeNeg;
 };
 
@@ -284,6 +288,7 @@ __device__ __forceinline__ void oppCommon(int iOpp, const Track& tr, const EnvPa
     c.maxLatDis = E.trackWidth - E.droneRadius * E.maxOppLatDistFact;
 
     c.maxAccel = E.maxAccel[iOpp];
+    c.maxAccelSq = __fmul_rn(c.maxAccel, c.maxAccel);
     float pc0, pc1;
     sampleTrack2(tr.p, s.S[iOpp], L, pc0, pc1);
     c.tang0 = g.tn0[iOpp];
@@ -382,7 +387,7 @@ __device__ __forceinline__ void oppAction(int iOpp, int th, const EnvParams& E, 
         }
     }
     float a_n_total = fmaxf(-maxAccel, fminf(maxAccel, a_n_cmd + c.a_centripetal));
-    float a_t_max = sqrtf(fmaxf(maxAccel * maxAccel - a_n_total * a_n_total, 0.0f));
+    float a_t_max = sqrtf(fmaxf(c.maxAccelSq - a_n_total * a_n_total, 0.0f));
     float kappa = c.kappa;
     float kappa_eff = kappa / (1.0f - kappa * latDisC + 1e-6f);
     float pathSpeed = fminf(speedGoal, sqrtf(maxAccel / fmaxf(fabsf(kappa_eff), 1e-12f)));

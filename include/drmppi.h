@@ -295,6 +295,10 @@ int dr_prmppi_debug_noise(dr_prmppi* h, const float* belief, float* noise, size_
  * (running cost, safety cost), before averaging. The nominals are the shifted ones. */
 int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* cost_nom, float* cost_rob);
 
+/* Natural-cubic-spline basis B (T x M, row-major) of the knots tau_0..tau_{M-1}: the
+ * reference's MPPIController::buildSplineMatrix (src/mppi_controller.cu:56-141). */
+int dr_spline_matrix(int T, int M, const int32_t* knots, float* out);
+
 /* ---- environment step on the device (reference engine dynStep, engine.cpp:286-312) */
 /* Advances `state` in place by one true-dynamics step for the ego action, with the
  * given true hypothesis; updates belief (n_theta) in place. Returns the terminal type

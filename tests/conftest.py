@@ -43,6 +43,8 @@ def _ensure_oracle():
     ref_src = Path(os.environ.get("DR_REFERENCE", "/root/reference"))
     if ref_src.exists() and not all(O.ref_available(v) for v in ("nth2_spline", "nth2_dense", "nth8_spline")):
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "-j4", "ref"], check=True)
+    if ref_src.exists() and not (O.REF_DIR / "libengine_dropin.so").exists() and drb.abi.LIB_PATH.exists():
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "engine"], check=True)
 
 
 _ensure_oracle()

@@ -64,9 +64,15 @@ def test_pr_rollout_matches_reference_kernel(gpu, nth):
     rc = O.ref(variant).refc_pr_rollout(C.byref(sc.env), C.byref(c), C.byref(sc.state), O._f(shifted), O._f(shifted), O._f(noise), O._i(th), 9,
                                         O._f(rcn), O._f(rcr))
     assert rc == 0
-    for a, b in ((cn, rcn), (cr, rcr)):
+    for name, a, b in (("nom", cn, rcn), ("rob", cr, rcr)):
         mism = ~((a == b) | (np.isnan(a) & np.isnan(b)))
-        assert mism.sum() == 0, f"{mism.sum()} of {a.size} differ"
+        if mism.any():
+            idx = np.argwhere(mism)
+            rel = np.abs(a - b) / np.maximum(1.0, np.abs(b))
+            print(f"{name}: {mism.sum()} differ; per p {mism.any(axis=2).sum(axis=1)}; thetas {th}; samples {np.unique(idx[:, 1])[:20]}")
+            for p, s, k in idx[:6]:
+                print(f"  p={p} s={s} k={k} mine={a[p, s, k]!r} ref={b[p, s, k]!r} rel={rel[p, s, k]:.2e}")
+        assert mism.sum() == 0, f"{name}: {mism.sum()} of {a.size} differ"
 
 
 def test_pr_steps_match_oracle(gpu):

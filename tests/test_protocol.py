@@ -1,0 +1,74 @@
+"""Wire protocol: the configuration headers that the reference's Python front-end
+packs (golden frames from its BytePacker, tests/golden/wire_*.bin) decode into the
+same configurations this package builds, and re-encode to the same bytes; malformed
+frames are rejected like the reference's C++ Reader does."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import drb
+
+P = drb.protocol if hasattr(drb, "protocol") else None
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(scope="module")
+def proto():
+    import drone_race_b200.protocol as p
+
+    return p
+
+
+@pytest.mark.parametrize("name,use_pr,spl", [("mppi_spline", False, True), ("mppi_dense", False, False), ("prmppi", True, True)])
+def test_reference_frames_round_trip(proto, name, use_pr, spl):
+    frames = proto.split_frames((GOLD / f"wire_{name}.bin").read_bytes())
+    env_f, cont_f, state_f = frames
+    hdr = proto.unpack_env(env_f)
+    cont = proto.unpack_controller(cont_f)
+    st = proto.unpack_state(state_f, hdr.env.n_opp)
+    assert proto.pack_env(hdr.env, hdr.grids, hdr.seed, hdr.true_theta) == env_f
+    assert proto.pack_controller(cont) == cont_f
+    assert proto.pack_state(st, hdr.env.n_opp) == state_f
+    # the same configuration as this package's restatement of stratRaceEnv
+    sc = drb.scenarios.strat_race(use_pr=use_pr, use_splines=spl)
+    mine = sc.prmppi if use_pr else sc.mppi
+    # stratRaceEnv leaves the verification fields at the dataclass defaults (mainGate
+    # changes them afterwards, main.py:1021-1025) and sends nKnots = 6 in dense mode
+    skip = {"sampling_noise_dim", "min_nu", "max_nu", "verify", "knots", "n_verif_samples", "beta", "verif_horizon", "max_verif_eps"}
+    if not spl:
+        skip.add("n_knots")
+    for fname, _ in type(cont)._fields_:
+        if fname in skip:
+            continue
+        a, b = getattr(cont, fname), getattr(mine, fname)
+        assert a == pytest.approx(b, rel=1e-6), fname
+    assert hdr.env.n_theta == sc.env.n_theta and hdr.env.n_opp == sc.env.n_opp
+    for fname in ("dt", "drone_radius", "track_width", "kP", "kV", "max_opp_lat_dist_fact", "track_length"):
+        assert getattr(hdr.env, fname) == pytest.approx(getattr(sc.env, fname), rel=1e-6), fname
+    np.testing.assert_array_equal(hdr.grids.p_grid, sc.grids.p_grid)
+    np.testing.assert_array_equal(hdr.grids.kappa_grid, sc.grids.kappa_grid)
+    for a in range(2):
+        assert st.S[a] == pytest.approx(sc.state.S[a], rel=1e-6)
+
+
+def test_malformed_frames_are_rejected(proto):
+    env_f, cont_f, state_f = proto.split_frames((GOLD / "wire_mppi_spline.bin").read_bytes())
+    with pytest.raises(proto.ProtocolError, match="underflow"):
+        proto.unpack_env(env_f[:-3])
+    with pytest.raises(proto.ProtocolError, match="not fully parsed"):
+        proto.unpack_controller(cont_f + b"\0\0\0\0")
+    bad = bytearray(cont_f)
+    bad[0:4] = (7).to_bytes(4, "little")
+    with pytest.raises(proto.ProtocolError, match="Expected header"):
+        proto.unpack_controller(bytes(bad))
+    bad = bytearray(cont_f)
+    bad[4:8] = (5).to_bytes(4, "little")
+    with pytest.raises(proto.ProtocolError, match="invalid controller kind"):
+        proto.unpack_controller(bytes(bad))
+    bad = bytearray(env_f)
+    bad[4:8] = (0).to_bytes(4, "little")  # ENV_DRONERACE
+    with pytest.raises(proto.ProtocolError, match="kind mismatch"):
+        proto.unpack_env(bytes(bad))
