@@ -132,13 +132,14 @@ def _dist():
     return world, rank, local
 
 
-def _max_over_ranks(x: float, world: int) -> float:
+def _max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """Max of a per-rank time over all ranks (the multi-GPU timing rule)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -158,9 +158,13 @@ struct dr_mppi_batch
     MppiDev* dDesc = nullptr;
     MppiIn* dIn = nullptr;
     MppiIn* hIn = nullptr;
-    Tile *dRoll = nullptr, *dUpd = nullptr, *dVer = nullptr;
-    int nRoll = 0, nUpd = 0, nVer = 0;
+    Tile *dRoll = nullptr, *dUpd = nullptr, *dVer = nullptr, *dVerNew = nullptr, *dVerOld = nullptr;
+    int nRoll = 0, nUpd = 0, nVer = 0, nVerNew = 0, nVerOld = 0;
     size_t rollSmem = 0, verSmem = 0, proSmem = 0;
+    bool overlap = true;                 // previous-plan verification on sideStream
+    cudaStream_t sideStream = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    Timer timerSide;
     bool useGraph = true;
     bool profiling = false;
     Timer timer;
@@ -190,23 +194,51 @@ struct dr_mppi_batch
             timer->mark("prologue", stream);
         }
         CK(launchMppiPrologue(args(nullptr, 0, in), n, proSmem));
+        // The previous plan's verification needs only the prologue's shifted plan, so it
+        // runs on a second stream while the rollout (a few warps per SM) and the update
+        // run on the first; the new plan's verification follows the update.
+        const bool side = verify && overlap && nVerOld > 0;
+        if (side)
+        {
+            CK(cudaEventRecord(evFork, stream));
+            CK(cudaStreamWaitEvent(sideStream, evFork, 0));
+            if (profile)
+            {
+                timerSide.begin();
+                timerSide.mark("verify_old", sideStream);
+            }
+            LaunchArgs a = args(dVerOld, nVerOld, in);
+            a.stream = sideStream;
+            CK(launchMppiVerify(a, nopp, nth, verSmem, nullptr, nullptr));
+            if (profile)
+            {
+                timerSide.mark("end", sideStream);
+                timerSide.end();
+            }
+            CK(cudaEventRecord(evJoin, sideStream));
+        }
         if (profile)
             timer->mark("rollout", stream);
         CK(launchMppiRollout(args(dRoll, nRoll, in), nopp, nth, spl, rollSmem));
         if (profile)
             timer->mark("update", stream);
         CK(launchMppiUpdate(args(dUpd, nUpd, in), nth));
-        if (verify && nVer > 0)
+        if (verify && nVerNew > 0)
         {
             if (profile)
-                timer->mark("verify", stream);
-            CK(launchMppiVerify(args(dVer, nVer, in), nopp, nth, verSmem, nullptr, nullptr));
+                timer->mark(side ? "verify_new" : "verify", stream);
+            if (side)
+                CK(launchMppiVerify(args(dVerNew, nVerNew, in), nopp, nth, verSmem, nullptr, nullptr));
+            else
+                CK(launchMppiVerify(args(dVer, nVer, in), nopp, nth, verSmem, nullptr, nullptr));
         }
         if (profile)
         {
             timer->mark("end", stream);
             timer->end();
         }
+        if (side)
+            CK(cudaStreamWaitEvent(stream, evJoin, 0));
         return DR_OK;
     }
 
@@ -282,6 +314,15 @@ struct dr_mppi_batch
         cudaFree(dVer);
         if (hIn)
             cudaFreeHost(hIn);
+        if (sideStream)
+        {
+            cudaStreamSynchronize(sideStream);
+            cudaStreamDestroy(sideStream);
+        }
+        if (evFork)
+            cudaEventDestroy(evFork);
+        if (evJoin)
+            cudaEventDestroy(evJoin);
         if (ownStream && stream)
             cudaStreamDestroy(stream);
     }
@@ -309,7 +350,7 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     b->stream = stream;
     b->ownStream = ownStream;
     std::vector<MppiDev> descs;
-    std::vector<Tile> roll, upd, ver;
+    std::vector<Tile> roll, upd, ver, verOld;
     const int spb = rolloutSamplesPerBlock(b->nth);
     int maxT = 0, maxM = 0, maxNbpT = 0;
     for (int i = 0; i < n; i++)
@@ -323,11 +364,15 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
         if (b->verify)
             for (int plan = 0; plan < 2; plan++)
                 for (int v0 = 0; v0 < h->V; v0 += 128)
-                    ver.push_back(Tile{i, v0, std::min(128, h->V - v0), plan});
+                    (plan == 0 ? ver : verOld).push_back(Tile{i, v0, std::min(128, h->V - v0), plan});
         maxT = std::max(maxT, h->T);
         maxM = std::max(maxM, h->M);
         maxNbpT = std::max(maxNbpT, h->nbp * h->T);
     }
+    // tile table: new-plan tiles first, then previous-plan tiles
+    b->nVerNew = (int)ver.size();
+    b->nVerOld = (int)verOld.size();
+    ver.insert(ver.end(), verOld.begin(), verOld.end());
     for (int i = 0; i < n; i++)
     {
         b->rollSmem = std::max(b->rollSmem, mppiRolloutSmem(b->nth, hs[i]->T, hs[i]->M, b->spl));
@@ -350,6 +395,11 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     CK(cudaMalloc(&b->dVer, sizeof(Tile) * std::max<size_t>(ver.size(), 1)));
     if (!ver.empty())
         CK(cudaMemcpy(b->dVer, ver.data(), sizeof(Tile) * ver.size(), cudaMemcpyHostToDevice));
+    b->dVerNew = b->dVer;
+    b->dVerOld = b->dVer + b->nVerNew;
+    CK(cudaStreamCreateWithFlags(&b->sideStream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&b->evFork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&b->evJoin, cudaEventDisableTiming));
     *out = b.release();
     return DR_OK;
 }
@@ -661,6 +711,7 @@ int dr_mppi_set_profiling(dr_mppi* h, int on)
         return fail(DR_ERR_INVALID_ARG, "NULL handle");
     h->self->profiling = on != 0;
     h->self->timer.reset();
+    h->self->timerSide.reset();
     return DR_OK;
 }
 
@@ -668,7 +719,7 @@ int dr_mppi_get_kernel_times(dr_mppi* h, const char** names, float* ms, int n, i
 {
     if (!h)
         return fail(DR_ERR_INVALID_ARG, "NULL handle");
-    return kernelTimes(h->self->timer, names, ms, n, count);
+    return kernelTimes(h->self->timer, names, ms, n, count, &h->self->timerSide);
 }
 
 int dr_mppi_batch_create(dr_mppi* const* hs, int n, void* stream, dr_mppi_batch** out)
@@ -920,6 +971,7 @@ extern "C" int dr_mppi_batch_set_profiling(dr_mppi_batch* b, int on)
         return fail(DR_ERR_INVALID_ARG, "NULL batch");
     b->profiling = on != 0;
     b->timer.reset();
+    b->timerSide.reset();
     return DR_OK;
 }
 
@@ -928,7 +980,22 @@ extern "C" int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** nam
     if (!b)
         return fail(DR_ERR_INVALID_ARG, "NULL batch");
     CK(cudaSetDevice(b->device));
-    return kernelTimes(b->timer, names, ms, n, count);
+    return kernelTimes(b->timer, names, ms, n, count, &b->timerSide);
+}
+
+extern "C" int dr_mppi_batch_set_overlap(dr_mppi_batch* b, int on)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    if (b->graphExec)
+    {
+        cudaGraphExecDestroy(b->graphExec);
+        cudaGraphDestroy(b->graph);
+        b->graphExec = nullptr;
+        b->graph = nullptr;
+    }
+    b->overlap = on != 0;
+    return DR_OK;
 }
 
 extern "C" int dr_spline_matrix(int T, int M, const int32_t* knots, float* out)

@@ -290,20 +290,29 @@ struct Timer
 };
 
 
-// Averages of the recorded steps; names point into the timer and stay valid until reset.
-inline int kernelTimes(Timer& t, const char** names, float* ms, int n, int* count)
+// Averages of the recorded steps of a main-stream timer and, optionally, a side-stream
+// timer; names point into the timers and stay valid until reset.
+inline int kernelTimes(Timer& t, const char** names, float* ms, int n, int* count, Timer* side = nullptr)
 {
     t.collect();
-    int c = (int)t.ms.size();
+    if (side)
+        side->collect();
+    int c = 0;
+    for (Timer* tm : {&t, side})
+    {
+        if (!tm)
+            continue;
+        for (size_t i = 0; i < tm->ms.size(); i++, c++)
+            if (c < n)
+            {
+                if (names)
+                    names[c] = tm->names[i].c_str();
+                if (ms)
+                    ms[c] = tm->ms[i];
+            }
+    }
     if (count)
         *count = c;
-    for (int i = 0; i < c && i < n; i++)
-    {
-        if (names)
-            names[i] = t.names[i].c_str();
-        if (ms)
-            ms[i] = t.ms[i];
-    }
     return DR_OK;
 }
 

@@ -280,7 +280,8 @@ __device__ __forceinline__ void oppCommon(int iOpp, const Track& tr, const EnvPa
         c.deltaE[k] = latJ - s.lat[iOpp];
         c.latJ[k] = latJ;
         c.sdotJ[k] = sdj;
-        c.blockTol[k] = msj * 0.3f;
+        // loop-invariant in the reference (hoisted, rounded on its own before the additions)
+        c.blockTol[k] = __fmul_rn(msj, 0.3f);
         c.shouldBlock[k] = (deltaS < 0.0f) && (deltaS > -L * 0.25f) && (sdj + c.blockTol[k] > c.sdot_i);
         c.fasterThanJ[k] = c.sdot_i > sdj;
         c.oppLong[k] = vj0 * tj0 + vj1 * tj1;
@@ -674,9 +675,23 @@ __device__ __forceinline__ float prStateCost(const StepOut& o, const EnvParams& 
 }
 
 // PRMPPIsafetyCost (costs.cuh:78-86).
-__device__ __forceinline__ float prSafetyCost(const StepOut& o, const EnvParams& E, float collDistFactor)
+// droneRadius * collDistFactor - bd with one rounding: in the reference both factors
+// are kernel parameters used in place, and the product is fused into the subtraction
+// (measured against PRMPPIfullRolloutKernel); computing the product once before the
+// loop here would otherwise round it separately.
+struct SafetyMargin
 {
-    return E.droneRadius * collDistFactor - o.bdRaw;
+    float r, cdf;
+};
+
+__device__ __forceinline__ SafetyMargin safetyMargin(const EnvParams& E, float collDistFactor)
+{
+    return SafetyMargin{E.droneRadius, collDistFactor};
+}
+
+__device__ __forceinline__ float prSafetyCost(const StepOut& o, SafetyMargin m)
+{
+    return __fmaf_rn(m.r, m.cdf, -o.bdRaw);
 }
 
 // finalCost / PRMPPIfinalCost (costs.cuh:31-39, 66-74).

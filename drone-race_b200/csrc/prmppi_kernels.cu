@@ -168,6 +168,7 @@ __global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ inst
         EnvNoise rng(k0, k1, (uint32_t)s, ((((uint32_t)robust << 8) | (uint32_t)p) << 16), step, S_PR_ROLL_ENV);
         float decay = 1.0f;
         bool stop = false;
+        const SafetyMargin margin = safetyMargin(E, D.cfg.collDistFactor);
         for (int t = 0; t < T && !stop; t++)
         {
             rng.begin_step((uint32_t)t);
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ inst
             StepOut o = envStep<NOPP, NTH, false, false, true, false>(t, theta, tr, E, ego0, ego1, st, bs, branched, 0.0f, rng);
             stop = (o.term != TERM_NONE);
             running += decay * prStateCost(o, E, D.cfg.boundaryThresholdFactor, D.cfg.boundaryCost, D.cfg.winCost, D.cfg.oppWinCost);
-            safe = fmaxf(safe, prSafetyCost(o, E, D.cfg.collDistFactor));
+            safe = fmaxf(safe, prSafetyCost(o, margin));
             decay *= DECAY;
         }
         running += finalCost<NOPP>(st, E, D.cfg.finalAdvWeight, D.cfg.finalOppAdvWeight);
@@ -338,6 +339,7 @@ __global__ void __launch_bounds__(PRB) pr_candidates(const PrDev* __restrict__ i
         BState<NTH> bs{};
         EnvNoise rng(k0, k1, (uint32_t)p, (uint32_t)second << 16, step, kind ? S_PR_SAFE_ENV : S_PR_CAND_ENV);
         float cost = 0.0f, safeCost = -INFINITY, decay = 1.0f;
+        const SafetyMargin margin = safetyMargin(E, D.cfg.collDistFactor);
         bool stop = false;
         for (int t = 0; t < T && !stop; ++t)
         {
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(PRB) pr_candidates(const PrDev* __restrict__ i
             stop = (o.term != TERM_NONE);
             cost += decay * prStateCost(o, E, D.cfg.boundaryThresholdFactor, D.cfg.boundaryCost, D.cfg.winCost, D.cfg.oppWinCost);
             decay *= DECAY;
-            safeCost = fmaxf(safeCost, prSafetyCost(o, E, D.cfg.collDistFactor));
+            safeCost = fmaxf(safeCost, prSafetyCost(o, margin));
         }
         cost += finalCost<NOPP>(st, E, D.cfg.finalAdvWeight, D.cfg.finalOppAdvWeight);
         if (safeCost > 0.0f)

@@ -246,6 +246,9 @@ int dr_mppi_batch_set_graph(dr_mppi_batch* b, int use_graph);
 /* Per-kernel device time of the batch's steps (CUDA events on its stream), averaged
  * over the steps recorded since profiling was switched on (also for *_step_dev). */
 int dr_mppi_batch_set_profiling(dr_mppi_batch* b, int on);
+/* 1 (default): the previous plan's verification runs on a second stream concurrently
+ * with the rollout and the update; 0: everything in order on the batch's stream. */
+int dr_mppi_batch_set_overlap(dr_mppi_batch* b, int on);
 int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** names, float* ms, int n, int* count);
 
 /* ---- MPPI test hooks (component parity against the reference kernels) ----------- */
