@@ -232,6 +232,8 @@ _PROTOS = {
     "dr_prmppi_batch_step_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "dr_prmppi_debug_noise": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_size_t, C.POINTER(C.c_int32)]),
     "dr_prmppi_debug_rollout": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "dr_mppi_rollout_costs_noalloc": (C.c_int, [C.POINTER(dr_env_config), C.POINTER(dr_mppi_config), C.c_uint64, C.c_uint64, C.POINTER(dr_sim_state),
+                                                C.POINTER(C.c_float), C.c_void_p, C.c_void_p, C.c_void_p]),
     "dr_spline_matrix": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "dr_env_step": (C.c_int, [C.POINTER(dr_env_config), C.c_int, C.POINTER(C.c_float), C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_int)]),
 }

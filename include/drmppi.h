@@ -298,6 +298,25 @@ int dr_prmppi_debug_noise(dr_prmppi* h, const float* belief, float* noise, size_
  * (running cost, safety cost), before averaging. The nominals are the shifted ones. */
 int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* cost_nom, float* cost_rob);
 
+/* ---- allocation-free rollout ------------------------------------------------------
+ * No counterpart in the reference: an entry point for callers that cannot call
+ * cudaMalloc (code where the device allocator is off limits, e.g. a real-time control
+ * loop or a memory-pool owner that forbids allocation, or a host framework that hands
+ * the library only buffers it owns). It runs the same fused rollout + per-branch cost
+ * aggregation as dr_mppi_debug_rollout, for the controls knots_dev and the Philox
+ * stream (seed, step), and writes costs_dev ((n_theta+1) x n_samples, device memory).
+ * knots_dev: (n_theta+1) x M x DR_DIM floats on the device, M = n_knots (spline mode)
+ * or n_timesteps (dense mode). Allocates nothing: its scratch is one static device
+ * array of DR_NOALLOC_SCRATCH_BYTES per GPU, held until the process exits; a problem
+ * that does not fit (roughly 8 x n_theta x n_samples bytes plus the track and the
+ * controls) is rejected with DR_ERR_INVALID_ARG. All calls share that array: calls
+ * whose GPU work overlaps race on it. The first call on a device looks the array up
+ * (cudaGetSymbolAddress) with that device current, so make it before any stream
+ * capture. Returns after the work on `stream` (NULL: legacy default) has completed. */
+#define DR_NOALLOC_SCRATCH_BYTES (4u << 20)
+int dr_mppi_rollout_costs_noalloc(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t seed, uint64_t step, const dr_sim_state* state,
+                                  const float* belief, const float* knots_dev, float* costs_dev, void* stream);
+
 /* Natural-cubic-spline basis B (T x M, row-major) of the knots tau_0..tau_{M-1}: the
  * reference's MPPIController::buildSplineMatrix (src/mppi_controller.cu:56-141). */
 int dr_spline_matrix(int T, int M, const int32_t* knots, float* out);
