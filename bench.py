@@ -219,6 +219,8 @@ def run_ours(args) -> None:
     stream = torch.cuda.Stream()  # non-default stream: the batch captures a CUDA graph on it
     ctls = [ctl_mod.MPPIController(s.env, s.mppi, s.seed, device=local, stream=stream.cuda_stream) for s in scs]
     batch = ctl_mod.MPPIBatch(ctls, stream=stream.cuda_stream)
+    if args.no_overlap:
+        batch.set_overlap(False)
     n = len(ctls)
     states = [s.state for s in scs]
     beliefs = np.stack([s.belief() for s in scs])
@@ -373,6 +375,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e, no CPU baseline): for profiler runs")
+    ap.add_argument("--no-overlap", action="store_true", help="run the previous plan's verification after the rollout instead of beside it")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

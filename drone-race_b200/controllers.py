@@ -229,6 +229,9 @@ class MPPIBatch:
     def set_graph(self, on: bool) -> None:
         check(lib().dr_mppi_batch_set_graph(self._b, int(on)), "dr_mppi_batch_set_graph")
 
+    def set_overlap(self, on: bool) -> None:
+        check(lib().dr_mppi_batch_set_overlap(self._b, int(on)), "dr_mppi_batch_set_overlap")
+
     def step_dev(self, states_dev_ptr: int, beliefs_dev_ptr: int) -> None:
         check(lib().dr_mppi_batch_step_dev(self._b, C.c_void_p(states_dev_ptr), C.c_void_p(beliefs_dev_ptr)), "dr_mppi_batch_step_dev")
 

@@ -202,6 +202,7 @@ def test_graph_replay_equals_eager(gpu):
     Bc = [drb.controllers.MPPIController(s.env, s.mppi, s.seed) for s in scs]
     ba, bb = drb.controllers.MPPIBatch(A), drb.controllers.MPPIBatch(Bc)
     bb.set_graph(False)
+    bb.set_overlap(False)  # eager, in-order reference for the graph-replayed, overlapped batch
     beliefs = np.stack([s.belief() for s in scs])
     for k in range(4):
         x = ba.step([s.state for s in scs], beliefs)
