@@ -16,7 +16,9 @@ scaling, no data-path collective); timing is the max over ranks.
 
 --impl reference times the reference's own CPU implementation of the path (its model
 functions compiled from the reference sources, oracle/_ref, OpenMP over all host
-threads) on a bounded sample of the same workload.
+threads) on a bounded sample of the same workload. When a GPU is present it also
+reports, as an extra field, the reference's own CUDA path (its kernels and its
+MPPIController::getControl compiled from the reference sources) on the same workload.
 """
 from __future__ import annotations
 
@@ -51,6 +53,11 @@ VERIF_H = 40
 # (the reference evaluates 1323 ops per step as written; 652 / 571 are distinct).
 FLOPS_PER_ROLLOUT_STEP = 652.0    # MPPI rollout step (belief update over 2 hypotheses)
 FLOPS_PER_VERIFY_STEP = 571.0     # verification step (noise-free ego plan)
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture
+# of each kernel on this workload (--quick, 3 steps); the grids, plans and tile tables are
+# L2-resident after the first launch, so DRAM traffic is a few hundred KB per launch.
+TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 271616.0, "rollout": 140288.0}
 
 
 def _package():
@@ -151,9 +158,11 @@ def _barrier(world: int):
         dist.barrier()
 
 
-def cpu_baseline_reference(scs, target_s: float = 12.0) -> dict:
+def cpu_baseline_reference(scs, target_s: float = 10.0, max_reps: int = 100000, k_s: int = 4096, v_s: int = 32768) -> dict:
     """The reference's CPU path (its model functions from oracle/_ref, OpenMP) on a bounded
-    sample of one agent's control step, scaled to the 4-agent control step."""
+    sample of one agent's control step, scaled to the 4-agent control step. The sample
+    controls agent 0 from its start state with an all-zero plan (the plan only steers the
+    ego drone; 40 steps of coasting stay on this track, so no sample ends early)."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as O
 
@@ -168,7 +177,6 @@ def cpu_baseline_reference(scs, target_s: float = 12.0) -> dict:
     c = sc.mppi
     belief = sc.belief()
     # sample: k_s rollout samples and v_s verification samples
-    k_s, v_s = 256, 2048
     c_small = type(c).from_buffer_copy(c)
     c_small.n_samples = k_s
     c_small.n_verif_samples = v_s
@@ -193,7 +201,7 @@ def cpu_baseline_reference(scs, target_s: float = 12.0) -> dict:
         t_roll += b - a
         t_ver += e - b
         reps += 1
-        if e - t0 > target_s or reps >= 50:
+        if e - t0 > target_s or reps >= max_reps:
             break
     sc.mppi = c
     t_roll /= reps
@@ -278,16 +286,40 @@ def run_ours(args) -> None:
         d2h += b.value
 
     # ---- roofline of the dominant kernel --------------------------------------------------
-    dom = max(kt, key=kt.get) if kt else None
+    # With the previous-plan verification beside the rollout, the two verification launches
+    # share the SMs with each other and with the rollout, so their event durations are not
+    # per-kernel times. A short pass after the timed region, with the verification of both
+    # plans in one launch on the main stream, measures the kernels one at a time.
+    kt_serial, serial_steps = kt, args.steps
+    if not args.no_overlap:
+        batch.set_overlap(False)
+        serial_steps = max(10, min(50, args.steps))
+        for _ in range(3):
+            batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+        torch.cuda.synchronize()
+        batch.set_profiling(True)
+        for _ in range(serial_steps):
+            batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+        torch.cuda.synchronize()
+        kt_serial = batch.kernel_times()
+        batch.set_profiling(False)
+        batch.set_overlap(True)
     units = {"rollout": AGENTS * K * N_THETA * H, "verify": AGENTS * 2 * V * VERIF_H}
     flops_unit = {"rollout": FLOPS_PER_ROLLOUT_STEP, "verify": FLOPS_PER_VERIFY_STEP}
-    roof = None
+    dom = max(kt_serial, key=kt_serial.get) if kt_serial else None
+    roof = roof_step = None
     if dom in units and clk.get("sm_mhz"):
-        achieved = units[dom] * flops_unit[dom] / (kt[dom] / 1e3) / 1e12
         peak = 2 * 128 * 148 * clk["sm_mhz"] * 1e6 / 1e12
-        roof = {"bound": "fp32", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+        achieved = units[dom] * flops_unit[dom] / (kt_serial[dom] / 1e3) / 1e12
+        roof = {"bound": "fp32", "kernel": f"mppi_verify ({dom})" if dom == "verify" else f"mppi_{dom}", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH.get(dom),
                 "peak_source": "FP32 FMA rate of 148 SMs x 128 lanes at the median SM clock sampled during the timed region (MEASURED_PEAKS.json has no FP32 figure)",
-                "units_per_launch": units[dom], "flops_per_unit": flops_unit[dom], "kernel_ms": kt[dom]}
+                "units_per_launch": units[dom], "flops_per_unit": flops_unit[dom], "kernel_ms": kt_serial[dom],
+                "measured": f"CUDA events around each launch on its stream, {serial_steps} steps with both plans verified in one launch"}
+        step_flops = sum(units[k] * flops_unit[k] for k in units)
+        ach_step = step_flops / (ms_per_step / 1e3) / 1e12
+        roof_step = {"bound": "fp32", "achieved": ach_step, "peak": peak, "unit": "TFLOP/s", "frac": ach_step / peak,
+                     "scope": "all FP32 work of one control step (rollout + both verifications) / device step time of the timed region"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.quick:
@@ -316,8 +348,9 @@ def run_ours(args) -> None:
         "kernel_ms": kt,
         "e2e": None if args.quick else {"value": world * args.steps / e2e_s, "unit": "control steps/s", "h2d_bytes_per_step": h2d,
                                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s / args.steps * 1e3},
-        "gpu_launches": (4 if ctls[0].mppiConfig.verify else 3) * args.steps,
+        "gpu_launches": len(kt) * args.steps,
         "roofline": roof,
+        "roofline_step": roof_step,
         "cpu_baseline": cpu,
         "clocks": clk,
     }
@@ -332,6 +365,39 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def reference_cuda_timing(scs, warmup: int = 3, steps: int = 20) -> dict | None:
+    """The reference's own CUDA path on this GPU (oracle/_ref, compiled from the reference
+    sources for sm_100a, N_OPP 1, N_TRUE_MODELS 2, dense controls), 4 controllers on the
+    benchmark track: (i) its kernel sequence of one MPPI update per agent (noise, rollout,
+    aggregation, masked min, weighted average, clamp; CUDA events), (ii) its full
+    MPPIController::getControl per agent, verification of both plans included (wall time
+    with the device synchronised). None without a GPU or without the compiled reference."""
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return None
+    except Exception:
+        return None
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O
+
+    drb = _package()
+    O.set_abi(drb.abi)
+    variant = O.ref_variant_name(N_THETA, False)
+    if not O.ref_available(variant):
+        return None
+    sc = scs[0]
+    out = (C.c_double * 2)()
+    rc = O.ref(variant).refc_mppi_time(C.byref(sc.env), C.byref(sc.mppi), C.byref(sc.state), AGENTS, warmup, steps, out)
+    if rc != 0:
+        return {"error": f"reference CUDA timing failed with status {rc}"}
+    return {"kernels_ms_per_step": out[0], "getcontrol_ms_per_step": out[1], "control_steps_per_s": 1e3 / out[1],
+            "kernels_only_steps_per_s": 1e3 / out[0], "steps": steps, "warmup": warmup,
+            "what": "reference CUDA kernels built from its sources: (i) noise+rollout+aggregate+min+weighted average+clamp per agent, "
+                    "CUDA events; (ii) MPPIController::getControl per agent incl. verification, wall clock"}
+
+
 def run_reference(args) -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -341,7 +407,7 @@ def run_reference(args) -> None:
     steps_ms = []
     base = None
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline_reference(scs, target_s=min(20.0, 120.0 / max(1, args.warmup + args.steps)))
+        r = cpu_baseline_reference(scs, target_s=min(20.0, 120.0 / max(1, args.warmup + args.steps)), max_reps=1)
         if i >= args.warmup:
             steps_ms.append(r["ms_per_control_step"])
         base = r
@@ -365,6 +431,7 @@ def run_reference(args) -> None:
                    "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "control_steps/s", "cores": base["cores"], "kind": base["kind"], "sample": base["sample"]},
         "e2e": {"value": value, "unit": "control steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda": None if args.no_reference_cuda else reference_cuda_timing(scs),
     }
     print(json.dumps(line), flush=True)
 
@@ -378,6 +445,7 @@ def main():
     ap.add_argument("--no-overlap", action="store_true", help="run the previous plan's verification after the rollout instead of beside it")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

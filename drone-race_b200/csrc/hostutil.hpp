@@ -113,11 +113,15 @@ inline EnvParams toEnvParams(const dr_env_config& c)
 inline std::vector<float> packGrids(const dr_env_config& c)
 {
     std::vector<float> g(GRID_FLOATS, 0.0f);
+    for (int i = -GRID_PAD; i < NTS + GRID_PAD; i++)
+    {
+        int k = (i + NTS) % NTS;
+        g[GRID_P + i * 2] = c.p_grid[k * 2];
+        g[GRID_P + i * 2 + 1] = c.p_grid[k * 2 + 1];
+    }
     for (int i = 0; i <= NTS; i++)
     {
         int k = i % NTS;
-        g[GRID_P + i * 2] = c.p_grid[k * 2];
-        g[GRID_P + i * 2 + 1] = c.p_grid[k * 2 + 1];
         g[GRID_T + i * 2] = c.t_grid[k * 2];
         g[GRID_T + i * 2 + 1] = c.t_grid[k * 2 + 1];
         g[GRID_K + i] = c.kappa_grid[k];

@@ -23,8 +23,13 @@ constexpr int NTS = 512;       // N_TRACK_SAMPLES (env_stratrace_defs.h:11)
 constexpr int WIN = 10;        // WINDOW_SIZE (env_stratrace_defs.h:40)
 constexpr float DECAY = 0.97f; // include/config.h:30
 constexpr float MIN_COEFF = 0.01f; // MIN_COEFF_THRESHOLD, include/config.h:29
-constexpr int GRID_FLOATS = 2568;  // p[513][2] + t[513][2] + kappa[513], padded to 16 bytes
-constexpr int GRID_P = 0, GRID_T = 1026, GRID_K = 2052;
+// Track grids in one buffer: the centreline p with GRID_PAD wrapped samples on each
+// side (p[j] for j in [-16, 528), so the projection window needs no modulo), the unit
+// tangent t[513] and the curvature kappa[513] (sample 512 = sample 0); 16-byte multiple.
+constexpr int GRID_PAD = 16;
+constexpr int GRID_FLOATS = 2628;
+constexpr int GRID_P = GRID_PAD * 2, GRID_T = (NTS + 2 * GRID_PAD) * 2, GRID_K = GRID_T + (NTS + 1) * 2;
+static_assert(GRID_K + NTS + 1 <= GRID_FLOATS && GRID_FLOATS % 4 == 0 && GRID_PAD > WIN + 1, "grid layout");
 
 enum Term
 {
@@ -113,42 +118,48 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
     prevS = prevS - floorf(prevS);
     int idxPrev = (int)(prevS * NTS);
     const float* __restrict__ P = tr.p;
-    int bestInd = (idxPrev - WIN + NTS) % NTS;
+    // window idxPrev-10 .. idxPrev+10 in the reference's order (first minimum wins),
+    // indexed into the padded grid instead of modulo 512
+    const float2* __restrict__ P2 = reinterpret_cast<const float2*>(P);
+    int bestJ = idxPrev - WIN;
     float bestSqDist;
     {
+        float2 q = P2[bestJ];
         float sq = 0.f;
-        float d0 = P[bestInd * 2] - px;
+        float d0 = q.x - px;
         sq += d0 * d0;
-        float d1 = P[bestInd * 2 + 1] - py;
+        float d1 = q.y - py;
         sq += d1 * d1;
         bestSqDist = sq;
     }
 #pragma unroll 4
-    for (int offset = NTS - WIN + 1; offset <= NTS + WIN; offset++)
+    for (int j = idxPrev - WIN + 1; j <= idxPrev + WIN; j++)
     {
-        int i = (idxPrev + offset) % NTS;
+        float2 q = P2[j];
         float sq = 0.f;
-        float d0 = P[i * 2] - px;
+        float d0 = q.x - px;
         sq += d0 * d0;
-        float d1 = P[i * 2 + 1] - py;
+        float d1 = q.y - py;
         sq += d1 * d1;
         if (sq < bestSqDist)
         {
             bestSqDist = sq;
-            bestInd = i;
+            bestJ = j;
         }
     }
+    const int bestInd = (bestJ + NTS) % NTS;
     float bestSegSqDist = INFINITY;
     float bestS = 0.0f;
     float closestX = 0.0f, closestY = 0.0f;
 #pragma unroll
     for (int seg = -1; seg <= 0; ++seg)
     {
-        int a = (bestInd + seg + NTS) % NTS;
-        int b = (a + 1) % NTS;
-        float ax = P[2 * a], ay = P[2 * a + 1];
-        float abx = P[2 * b] - ax;
-        float aby = P[2 * b + 1] - ay;
+        const int aj = bestInd + seg;  // -1 .. 511; the padded grid holds p[-1] and p[512]
+        const int a = aj < 0 ? aj + NTS : aj;
+        const float2 qa = P2[aj], qb = P2[aj + 1];
+        float ax = qa.x, ay = qa.y;
+        float abx = qb.x - ax;
+        float aby = qb.y - ay;
         float sqAB = sqNorm(abx, aby);
         float t = 0.0f;
         if (sqAB > 1e-12f) // the reference compares with the double 1e-12; for floats the two tests agree

@@ -29,6 +29,12 @@ namespace dr
 {
 
 constexpr int RB = 128; // rollout / verification block size
+// Verification blocks per SM that the register allocation is sized for (128 threads a
+// block): 5 -> 96 registers a thread, no spills; 7 -> 72 registers, 36 bytes spilled.
+// Measured on the 4 x 2^17 x 40 verification: 3.29 ms at 5, 3.22 at 6, 3.15 at 7, 3.16 at 8.
+#ifndef VERIFY_MIN_BLOCKS
+#define VERIFY_MIN_BLOCKS 7
+#endif
 constexpr int UB = 256; // update block size (the reference's reduction width)
 
 __device__ __forceinline__ int packInfo(int pt, int bt)
@@ -550,7 +556,7 @@ template <int NTH> __global__ void __launch_bounds__(UB) mppi_update(const MppiD
 // verification
 // ---------------------------------------------------------------------------------------
 template <int NOPP, int NTH>
-__global__ void __launch_bounds__(RB) mppi_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(RB, VERIFY_MIN_BLOCKS) mppi_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
                                                   int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
 {
     constexpr int NA = NOPP + 1;

@@ -149,6 +149,22 @@ __device__ __forceinline__ float scaled_normal(float sigma, uint32_t w)
 }
 
 // Sequential normal source for the environment noise of one rollout step.
+// Out-of-line copies for the environment-step noise. An environment step has up to 14
+// noise sites (opponent action noise, action noise per agent and axis, position and
+// velocity noise); most are switched off in a given configuration but all are compiled.
+// Inlining a Philox block and the inverse CDF at each of them multiplies the size of the
+// step's code, and the instruction-cache misses that follow cost more than two calls.
+// The arithmetic is the same either way (every operation is rounded explicitly).
+static __device__ __noinline__ U4 draw_ool(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t step, uint32_t stream, uint32_t sub)
+{
+    return draw(k0, k1, c0, c1, step, stream, sub);
+}
+
+static __device__ __noinline__ float normal_from_word_ool(uint32_t w)
+{
+    return normal_from_word(w);
+}
+
 struct EnvNoise
 {
     uint32_t k0, k1, c0, c1base, step, stream, t;
@@ -166,10 +182,10 @@ struct EnvNoise
     __device__ __forceinline__ float next()
     {
         if ((j & 3) == 0)
-            cur = draw(k0, k1, c0, c1base | t, step, stream, (uint32_t)(j >> 2));
+            cur = draw_ool(k0, k1, c0, c1base | t, step, stream, (uint32_t)(j >> 2));
         uint32_t w = (j & 3) == 0 ? cur.x : (j & 3) == 1 ? cur.y : (j & 3) == 2 ? cur.z : cur.w;
         j++;
-        return normal_from_word(w);
+        return normal_from_word_ool(w);
     }
 };
 
