@@ -55,9 +55,10 @@ FLOPS_PER_ROLLOUT_STEP = 652.0    # MPPI rollout step (belief update over 2 hypo
 FLOPS_PER_VERIFY_STEP = 571.0     # verification step (noise-free ego plan)
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture
-# of each kernel on this workload (--quick, 3 steps); the grids, plans and tile tables are
-# L2-resident after the first launch, so DRAM traffic is a few hundred KB per launch.
-TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 271616.0, "rollout": 140288.0}
+# of each kernel on this workload (--quick --no-overlap, 3 steps); grids, plans and tile
+# tables stay in L2, so DRAM traffic is spilled registers and first-touch reads, about a
+# megabyte per launch.
+TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 1365504.0, "rollout": 140288.0}
 
 
 def _package():
@@ -162,7 +163,8 @@ def cpu_baseline_reference(scs, target_s: float = 10.0, max_reps: int = 100000, 
     """The reference's CPU path (its model functions from oracle/_ref, OpenMP) on a bounded
     sample of one agent's control step, scaled to the 4-agent control step. The sample
     controls agent 0 from its start state with an all-zero plan (the plan only steers the
-    ego drone; 40 steps of coasting stay on this track, so no sample ends early)."""
+    ego drone; none of its verification samples fails within the 40 steps, so the sample
+    does the full horizon of work)."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as O
 

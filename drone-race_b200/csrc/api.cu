@@ -363,8 +363,8 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
             upd.push_back(Tile{i, bk, 0, 0});
         if (b->verify)
             for (int plan = 0; plan < 2; plan++)
-                for (int v0 = 0; v0 < h->V; v0 += 128)
-                    (plan == 0 ? ver : verOld).push_back(Tile{i, v0, std::min(128, h->V - v0), plan});
+                for (int v0 = 0; v0 < h->V; v0 += VERIFY_TILE)
+                    (plan == 0 ? ver : verOld).push_back(Tile{i, v0, std::min(VERIFY_TILE, h->V - v0), plan});
         maxT = std::max(maxT, h->T);
         maxM = std::max(maxM, h->M);
         maxNbpT = std::max(maxNbpT, h->nbp * h->T);
@@ -901,8 +901,8 @@ int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* bel
     MppiIn* dIn = nullptr;
     Tile* dT = nullptr;
     std::vector<Tile> tiles;
-    for (int v0 = 0; v0 < V; v0 += 128)
-        tiles.push_back(Tile{0, v0, std::min(128, V - v0), plan});
+    for (int v0 = 0; v0 < V; v0 += VERIFY_TILE)
+        tiles.push_back(Tile{0, v0, std::min(VERIFY_TILE, V - v0), plan});
     size_t planBytes = a16((size_t)h->nbp * T * 2 * 4);
     cudaError_t e = cudaMalloc(&dPlan, planBytes);
     if (e == cudaSuccess)

@@ -21,6 +21,11 @@ struct LaunchArgs
     int nTiles = 0;
 };
 
+// Samples per verification CTA (one thread each). The CTA's warps step through the
+// horizon together (a barrier per step), so the warps sharing an SM sub-partition fetch
+// the same instructions; 512 threads, two CTAs per SM.
+constexpr int VERIFY_TILE = 512;
+
 bool mppiSupported(int nopp, int nth);
 int rolloutSamplesPerBlock(int nth);
 size_t mppiRolloutSmem(int nth, int T, int M, bool spl);

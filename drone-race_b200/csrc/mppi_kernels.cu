@@ -29,12 +29,19 @@ namespace dr
 {
 
 constexpr int RB = 128; // rollout / verification block size
-// Verification blocks per SM that the register allocation is sized for (128 threads a
-// block): 5 -> 96 registers a thread, no spills; 7 -> 72 registers, 36 bytes spilled.
-// Measured on the 4 x 2^17 x 40 verification: 3.29 ms at 5, 3.22 at 6, 3.15 at 7, 3.16 at 8.
+// Verification CTAs per SM that the register allocation is sized for (VERIFY_TILE = 512
+// threads a CTA: 2 -> 64 registers a thread). Measured on the 4 x 2^17 x 40 verification
+// (B200, 1965 MHz): 128-thread CTAs without the per-step barrier 3.14 ms (72 registers);
+// 128 with the barrier 3.05; 256 x 3 CTAs 2.90; 512 x 2 2.73; 1024 x 1 2.74.
+// The larger models (two opponents, or eight hypotheses) spill heavily at 64 registers
+// and get one CTA per SM instead.
 #ifndef VERIFY_MIN_BLOCKS
-#define VERIFY_MIN_BLOCKS 7
+#define VERIFY_MIN_BLOCKS 2
 #endif
+template <int NOPP, int NTH> constexpr int verifyMinBlocks()
+{
+    return (NOPP == 1 && NTH <= 4) ? VERIFY_MIN_BLOCKS : 1;
+}
 constexpr int UB = 256; // update block size (the reference's reduction width)
 
 __device__ __forceinline__ int packInfo(int pt, int bt)
@@ -556,7 +563,7 @@ template <int NTH> __global__ void __launch_bounds__(UB) mppi_update(const MppiD
 // verification
 // ---------------------------------------------------------------------------------------
 template <int NOPP, int NTH>
-__global__ void __launch_bounds__(RB, VERIFY_MIN_BLOCKS) mppi_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) mppi_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
                                                   int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
 {
     constexpr int NA = NOPP + 1;
@@ -594,7 +601,7 @@ __global__ void __launch_bounds__(RB, VERIFY_MIN_BLOCKS) mppi_verify(const MppiD
     const EnvParams& E = *sE;
     const Track tr{sGrid + GRID_P, sGrid + GRID_T, sGrid + GRID_K};
     const int v = tile.s0 + threadIdx.x;
-    if (threadIdx.x < tile.count)
+    bool active = threadIdx.x < tile.count; // idle lanes of a partial tile still take the barriers
     {
         const float minConf = D.cfg.minConf;
         DState<NA> st;
@@ -634,10 +641,16 @@ __global__ void __launch_bounds__(RB, VERIFY_MIN_BLOCKS) mppi_verify(const MppiD
             }
         }
         EnvNoise rng(k0, k1, (uint32_t)v, (uint32_t)plan << 16, step, S_VERIF_ENV);
-        int tOrigin = 0, t = 0;
+        int tOrigin = 0, t = 0, tEnd = H;
         bool failed = false;
         for (; t < H; t++)
         {
+            // every thread of the CTA takes this barrier once per step (H is uniform); it
+            // keeps the warps on the same step and ends the loop once all samples are done
+            if (!__syncthreads_or(active))
+                break;
+            if (!active)
+                continue;
             rng.begin_step((uint32_t)t);
             int local = t - tOrigin;
             int b = bs.predTheta;
@@ -649,17 +662,24 @@ __global__ void __launch_bounds__(RB, VERIFY_MIN_BLOCKS) mppi_verify(const MppiD
             if (o.term == TERM_LOSE)
             {
                 failed = true;
-                break;
+                active = false;
+                tEnd = t;
             }
             else if (o.term == TERM_WIN || o.term == TERM_OPP_WIN)
-                break;
+            {
+                active = false;
+                tEnd = t;
+            }
         }
         if (failed)
-            atomicAdd(&hist[t], 1u);
-        if (dbgFailTime)
-            dbgFailTime[v] = failed ? t : -1;
-        if (dbgTheta)
-            dbgTheta[v] = theta;
+            atomicAdd(&hist[tEnd], 1u);
+        if (threadIdx.x < tile.count)
+        {
+            if (dbgFailTime)
+                dbgFailTime[v] = failed ? tEnd : -1;
+            if (dbgTheta)
+                dbgTheta[v] = theta;
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < T; i += blockDim.x)
@@ -717,7 +737,7 @@ template <int NOPP, int NTH> static cudaError_t launchVerifyT(const LaunchArgs& 
 {
     auto k = mppi_verify<NOPP, NTH>;
     ensureSmem(k, smem);
-    k<<<a.nTiles, RB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, ft, th);
+    k<<<a.nTiles, VERIFY_TILE, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, ft, th);
     return cudaGetLastError();
 }
 
