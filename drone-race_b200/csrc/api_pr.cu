@@ -611,13 +611,20 @@ int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float
 // ---- device environment step -------------------------------------------------------------------
 
 template <int NOPP, int NTH>
-__global__ void env_step_kernel(EnvParams E, const float* __restrict__ grids, int trueTheta, float a0, float a1, dr_sim_state* st, float* belief,
+__global__ void env_step_kernel(EnvParams Eh, const float* __restrict__ grids, int trueTheta, float a0, float a1, dr_sim_state* st, float* belief,
                                 int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term)
 {
     __shared__ float sg[GRID_FLOATS];
+    __shared__ EnvParams sE;
     for (int i = threadIdx.x; i < GRID_FLOATS; i += blockDim.x)
         sg[i] = grids[i];
+    if (threadIdx.x == 0)
+    {
+        sE = Eh;
+        envDeviceTerms(sE, Eh, 0, 1);
+    }
     __syncthreads();
+    const EnvParams& E = sE;
     if (threadIdx.x != 0)
         return;
     constexpr int NA = NOPP + 1;
@@ -632,6 +639,7 @@ __global__ void env_step_kernel(EnvParams E, const float* __restrict__ grids, in
         s.lat[a] = st->lat_dist[a];
         s.laps[a] = st->laps[a];
     }
+    s.locate(E.trackLength);
     BState<NTH> bs;
     for (int i = 0; i < NTH; i++)
         bs.belief[i] = belief[i];

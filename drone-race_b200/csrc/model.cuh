@@ -12,6 +12,7 @@
 #pragma once
 
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 
 #include "philox.cuh"
@@ -48,7 +49,46 @@ struct EnvParams
     int nWinLaps;
     float kP, kV, maxOppLatDistFact, trackLength;
     float s1[8][3], s2[8][3], s3[8][3], speedScale[8][3], actionNoise[8][3];
+    // Filled on the device by envDeviceTerms (never copied from the host):
+    // logf(0.2^2 + actionNoise^2), the per-hypothesis constant of the belief update's
+    // log-likelihood (env_stratrace.h:199-203), evaluated once per launch instead of
+    // once per step with the same device logf.
+    float logSqSigma[8][3];
 };
+
+constexpr int ENV_HOST_WORDS = (int)(offsetof(EnvParams, logSqSigma) / 4);
+constexpr float BELIEF_SIGMA_ENV = 0.2f; // sigmaEnv of updateBelief (env_stratrace.h:170)
+
+__device__ __forceinline__ float beliefSqSigma(float an)
+{
+    return BELIEF_SIGMA_ENV * BELIEF_SIGMA_ENV + an * an;
+}
+
+// Device-computed terms of EnvParams from the host-filled fields of `src`; thread `tid`
+// of `n` fills its share of `dst`.
+__device__ __forceinline__ void envDeviceTerms(EnvParams& dst, const EnvParams& src, int tid, int n)
+{
+    for (int i = tid; i < 8 * 3; i += n)
+        dst.logSqSigma[i / 3][i % 3] = logf(beliefSqSigma(src.actionNoise[i / 3][i % 3]));
+}
+
+// Position on the sampled track (sampleTrackArray, env_stratrace.h:53-67, split into its
+// index computation and its interpolation): sample index below s and the weight of the
+// next sample.
+struct TrackPos
+{
+    int i0;
+    float w;
+};
+
+__device__ __forceinline__ TrackPos trackPos(float s, float L)
+{
+    s /= L;
+    s = s - floorf(s);
+    float idx_f = s * NTS;
+    int idx0 = (int)idx_f;
+    return TrackPos{idx0, idx_f - idx0};
+}
 
 template <int NA> struct DState
 {
@@ -57,6 +97,16 @@ template <int NA> struct DState
     float S[NA];
     float lat[NA];
     int laps[NA];
+    // trackPos(S[a]): computed by the projection that produced S[a] (or by locate() for a
+    // loaded state) and reused by the next step's track lookups at the same S[a]
+    TrackPos tp[NA];
+
+    __device__ __forceinline__ void locate(float L)
+    {
+#pragma unroll
+        for (int a = 0; a < NA; a++)
+            tp[a] = trackPos(S[a], L);
+    }
 };
 
 template <int NTH> struct BState
@@ -75,26 +125,20 @@ struct Track
 
 // ---- track sampling (env_stratrace.h:44-85) ------------------------------------------
 
-__device__ __forceinline__ void sampleTrack2(const float* __restrict__ arr, float s, float L, float& o0, float& o1)
+__device__ __forceinline__ void sampleAt2(const float* __restrict__ arr, TrackPos q, float& o0, float& o1)
 {
-    s /= L;
-    s = s - floorf(s);
-    float idx_f = s * NTS;
-    int idx0 = (int)idx_f;
-    int idx1 = (idx0 + 1) % NTS;
-    float t = idx_f - idx0;
+    const int idx0 = q.i0;
+    const int idx1 = (idx0 + 1) % NTS;
+    const float t = q.w;
     o0 = (1.0f - t) * arr[idx0 * 2 + 0] + t * arr[idx1 * 2 + 0];
     o1 = (1.0f - t) * arr[idx0 * 2 + 1] + t * arr[idx1 * 2 + 1];
 }
 
-__device__ __forceinline__ float sampleTrack1(const float* __restrict__ arr, float s, float L)
+__device__ __forceinline__ float sampleAt1(const float* __restrict__ arr, TrackPos q)
 {
-    s /= L;
-    s = s - floorf(s);
-    float idx_f = s * NTS;
-    int idx0 = (int)idx_f;
-    int idx1 = (idx0 + 1) % NTS;
-    float t = idx_f - idx0;
+    const int idx0 = q.i0;
+    const int idx1 = (idx0 + 1) % NTS;
+    const float t = q.w;
     return (1.0f - t) * arr[idx0] + t * arr[idx1];
 }
 
@@ -103,16 +147,17 @@ __device__ __forceinline__ float sqNorm(float x, float y)
     return x * x + y * y;
 }
 
-__device__ __forceinline__ void normalizedSpeed(const Track& tr, float s, float L, float& o0, float& o1)
+__device__ __forceinline__ void normalizedSpeed(const Track& tr, TrackPos q, float& o0, float& o1)
 {
-    sampleTrack2(tr.t, s, L, o0, o1);
+    sampleAt2(tr.t, q, o0, o1);
     float invNorm = 1.0f / sqrtf(sqNorm(o0, o1));
     o0 *= invNorm;
     o1 *= invNorm;
 }
 
-// fastProjectOnTrack<false> (env_stratrace.h:88-162): returns S, writes latDist.
-__device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float px, float py, float prevS, float& latDist)
+// fastProjectOnTrack<false> (env_stratrace.h:88-162): returns S, writes latDist and the
+// track position of S.
+__device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float px, float py, float prevS, float& latDist, TrackPos& tpS)
 {
     prevS /= L;
     prevS = prevS - floorf(prevS);
@@ -179,7 +224,8 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
         }
     }
     float tg0, tg1;
-    sampleTrack2(tr.t, bestS, L, tg0, tg1);
+    tpS = trackPos(bestS, L);
+    sampleAt2(tr.t, tpS, tg0, tg1);
     float cross = -tg1 * (px - closestX) + tg0 * (py - closestY);
     latDist = copysignf(sqrtf(bestSegSqDist), cross);
     return bestS;
@@ -199,8 +245,8 @@ template <int NA> __device__ __forceinline__ void agentGeometry(const Track& tr,
 #pragma unroll
     for (int a = 0; a < NA; a++)
     {
-        normalizedSpeed(tr, s.S[a], E.trackLength, g.tn0[a], g.tn1[a]);
-        g.kap[a] = sampleTrack1(tr.k, s.S[a], E.trackLength);
+        normalizedSpeed(tr, s.tp[a], g.tn0[a], g.tn1[a]);
+        g.kap[a] = sampleAt1(tr.k, s.tp[a]);
         float metric = 1 - g.kap[a] * s.lat[a];
         if (fabsf(metric) < 1e-12f)
             metric = copysignf(1e-12f, metric);
@@ -302,7 +348,7 @@ __device__ __forceinline__ void oppCommon(int iOpp, const Track& tr, const EnvPa
     c.maxAccel = E.maxAccel[iOpp];
     c.maxAccelSq = __fmul_rn(c.maxAccel, c.maxAccel);
     float pc0, pc1;
-    sampleTrack2(tr.p, s.S[iOpp], L, pc0, pc1);
+    sampleAt2(tr.p, s.tp[iOpp], pc0, pc1);
     c.tang0 = g.tn0[iOpp];
     c.tang1 = g.tn1[iOpp];
     c.kappa = g.kap[iOpp];
@@ -340,6 +386,8 @@ __device__ __forceinline__ void oppAction(int iOpp, int th, const EnvParams& E, 
         float deltaS = c.deltaS[k];
         float deltaE = c.deltaE[k];
         bool shouldOvertake = c.fasterThanJ[k] && (fabsf(deltaE) < s1);
+        if (!c.shouldBlock[k] && !shouldOvertake)
+            continue; // neither term uses the proximity factor
         float factor = expf(-s2 * deltaS * deltaS);
         if (c.shouldBlock[k])
         {
@@ -550,7 +598,7 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     // 8. projection
 #pragma unroll
     for (int a = 0; a < NA; a++)
-        s.S[a] = projectOnTrack(tr, E.trackLength, s.pos[2 * a], s.pos[2 * a + 1], s.S[a], s.lat[a]);
+        s.S[a] = projectOnTrack(tr, E.trackLength, s.pos[2 * a], s.pos[2 * a + 1], s.S[a], s.lat[a], s.tp[a]);
     // 9. laps
 #pragma unroll
     for (int a = 0; a < NA; a++)
@@ -564,7 +612,6 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     if constexpr (UPD)
     {
         float sum = 0.0f;
-        const float sigmaEnv = 0.2f;
 #pragma unroll
         for (int th = 0; th < NTH; th++)
         {
@@ -585,8 +632,8 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
                 float dx1 = act1[o + 1] - n1 * scale;
                 sqDist += dx1 * dx1;
                 float an = E.actionNoise[th][o];
-                float sqSigma = sigmaEnv * sigmaEnv + an * an;
-                logLikelihood += -0.5f * sqDist / sqSigma - (float)2 * 0.5f * logf(2.0f * M_PIf32) - (float)2 * 0.5f * logf(sqSigma);
+                float sqSigma = beliefSqSigma(an);
+                logLikelihood += -0.5f * sqDist / sqSigma - (float)2 * 0.5f * logf(2.0f * M_PIf32) - (float)2 * 0.5f * E.logSqSigma[th][o];
             }
             bs.belief[th] *= expf(logLikelihood);
             sum += bs.belief[th];

@@ -57,11 +57,13 @@ __device__ __forceinline__ int infoTime(int v)
     return (int)(short)(v & 0xffff);
 }
 
+// Copies the host-filled part of EnvParams to shared memory and computes the
+// device-filled part; the caller's next __syncthreads publishes both.
 __device__ __forceinline__ void copyEnv(EnvParams* dst, const EnvParams* src)
 {
-    const int n = (int)(sizeof(EnvParams) / 4);
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    for (int i = threadIdx.x; i < ENV_HOST_WORDS; i += blockDim.x)
         ((float*)dst)[i] = ((const float*)src)[i];
+    envDeviceTerms(*dst, *src, threadIdx.x, blockDim.x);
 }
 
 __host__ __device__ __forceinline__ size_t align16(size_t x)
@@ -232,6 +234,7 @@ __global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ i
             st.lat[a] = I.state.lat_dist[a];
             st.laps[a] = I.state.laps[a];
         }
+        st.locate(E.trackLength);
         BState<NTH> bs;
 #pragma unroll
         for (int i = 0; i < NTH; i++)
@@ -616,6 +619,7 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
             st.lat[a] = I.state.lat_dist[a];
             st.laps[a] = I.state.laps[a];
         }
+        st.locate(E.trackLength);
         BState<NTH> bs;
 #pragma unroll
         for (int i = 0; i < NTH; i++)

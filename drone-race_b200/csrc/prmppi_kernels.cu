@@ -33,11 +33,13 @@ __host__ __device__ __forceinline__ size_t pa16(size_t x)
     return (x + 15) & ~(size_t)15;
 }
 
+// Copies the host-filled part of EnvParams to shared memory and computes the
+// device-filled part; the caller's next __syncthreads publishes both.
 __device__ __forceinline__ void copyEnvP(EnvParams* dst, const EnvParams* src)
 {
-    const int n = (int)(sizeof(EnvParams) / 4);
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    for (int i = threadIdx.x; i < ENV_HOST_WORDS; i += blockDim.x)
         ((float*)dst)[i] = ((const float*)src)[i];
+    envDeviceTerms(*dst, *src, threadIdx.x, blockDim.x);
 }
 
 template <int NA> __device__ __forceinline__ void loadState(DState<NA>& st, const dr_sim_state& s)
@@ -163,6 +165,7 @@ __global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ inst
         const int theta = D.thetas[p];
         DState<NA> st;
         loadState<NA>(st, I.state);
+        st.locate(E.trackLength);
         BState<NTH> bs{};
         const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
         EnvNoise rng(k0, k1, (uint32_t)s, ((((uint32_t)robust << 8) | (uint32_t)p) << 16), step, S_PR_ROLL_ENV);
@@ -336,6 +339,7 @@ __global__ void __launch_bounds__(PRB) pr_candidates(const PrDev* __restrict__ i
         const int theta = D.thetas[p];
         DState<NA> st;
         loadState<NA>(st, I.state);
+        st.locate(E.trackLength);
         BState<NTH> bs{};
         EnvNoise rng(k0, k1, (uint32_t)p, (uint32_t)second << 16, step, kind ? S_PR_SAFE_ENV : S_PR_CAND_ENV);
         float cost = 0.0f, safeCost = -INFINITY, decay = 1.0f;
