@@ -58,7 +58,7 @@ FLOPS_PER_VERIFY_STEP = 571.0     # verification step (noise-free ego plan)
 # of each kernel on this workload (--quick --no-overlap, 3 steps); grids, plans and tile
 # tables stay in L2, so DRAM traffic is spilled registers and first-touch reads, about a
 # megabyte per launch.
-TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 1365504.0, "rollout": 140288.0}
+TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 1365504.0, "rollout": 145152.0}
 
 
 def _package():

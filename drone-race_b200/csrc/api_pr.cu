@@ -645,7 +645,7 @@ __global__ void env_step_kernel(EnvParams Eh, const float* __restrict__ grids, i
         bs.belief[i] = belief[i];
     bs.predTheta = 0;
     bs.branchingTime = -1;
-    const Track tr{sg + GRID_P, sg + GRID_T, sg + GRID_K};
+    const Track tr = trackIn(sg);
     EnvNoise rng(k0, k1, 0u, 0u, step, S_ENV_STEP);
     rng.begin_step(0);
     bool branched = false;

@@ -118,6 +118,8 @@ inline std::vector<float> packGrids(const dr_env_config& c)
         int k = (i + NTS) % NTS;
         g[GRID_P + i * 2] = c.p_grid[k * 2];
         g[GRID_P + i * 2 + 1] = c.p_grid[k * 2 + 1];
+        g[GRID_PX + i] = c.p_grid[k * 2];
+        g[GRID_PY + i] = c.p_grid[k * 2 + 1];
     }
     for (int i = 0; i <= NTS; i++)
     {

@@ -24,13 +24,18 @@ constexpr int NTS = 512;       // N_TRACK_SAMPLES (env_stratrace_defs.h:11)
 constexpr int WIN = 10;        // WINDOW_SIZE (env_stratrace_defs.h:40)
 constexpr float DECAY = 0.97f; // include/config.h:30
 constexpr float MIN_COEFF = 0.01f; // MIN_COEFF_THRESHOLD, include/config.h:29
-// Track grids in one buffer: the centreline p with GRID_PAD wrapped samples on each
-// side (p[j] for j in [-16, 528), so the projection window needs no modulo), the unit
-// tangent t[513] and the curvature kappa[513] (sample 512 = sample 0); 16-byte multiple.
+// Track grids in one buffer (offsets in floats, each of a sample index 0):
+//   p      centreline points, interleaved (x, y), with GRID_PAD wrapped samples on each
+//          side (p[j] for j in [-16, 528)), so that the projection window needs no modulo;
+//   t      unit tangent [513][2] and kappa curvature [513] (sample 512 = sample 0);
+//   px, py the padded centreline again as separate x and y rows (8-byte aligned at even
+//          indices), read two samples at a time by the projection window.
 constexpr int GRID_PAD = 16;
-constexpr int GRID_FLOATS = 2628;
-constexpr int GRID_P = GRID_PAD * 2, GRID_T = (NTS + 2 * GRID_PAD) * 2, GRID_K = GRID_T + (NTS + 1) * 2;
-static_assert(GRID_K + NTS + 1 <= GRID_FLOATS && GRID_FLOATS % 4 == 0 && GRID_PAD > WIN + 1, "grid layout");
+constexpr int GRID_ROW = NTS + 2 * GRID_PAD; // padded centreline samples
+constexpr int GRID_P = GRID_PAD * 2, GRID_T = GRID_ROW * 2, GRID_K = GRID_T + (NTS + 1) * 2;
+constexpr int GRID_PX = GRID_K + NTS + 1 + 1 + GRID_PAD, GRID_PY = GRID_PX + GRID_ROW;
+constexpr int GRID_FLOATS = GRID_PY - GRID_PAD + GRID_ROW;
+static_assert(GRID_FLOATS % 4 == 0 && GRID_PX % 2 == 0 && GRID_PY % 2 == 0 && GRID_PAD > WIN + 1, "grid layout");
 
 enum Term
 {
@@ -118,10 +123,17 @@ template <int NTH> struct BState
 
 struct Track
 {
-    const float* p; // [513][2]
-    const float* t; // [513][2]
-    const float* k; // [513]
+    const float* p;  // [-16, 528)[2]
+    const float* t;  // [513][2]
+    const float* k;  // [513]
+    const float* px; // [-16, 528)
+    const float* py; // [-16, 528)
 };
+
+__device__ __forceinline__ Track trackIn(const float* grids)
+{
+    return Track{grids + GRID_P, grids + GRID_T, grids + GRID_K, grids + GRID_PX, grids + GRID_PY};
+}
 
 // ---- track sampling (env_stratrace.h:44-85) ------------------------------------------
 
@@ -163,34 +175,56 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
     prevS = prevS - floorf(prevS);
     int idxPrev = (int)(prevS * NTS);
     const float* __restrict__ P = tr.p;
-    // window idxPrev-10 .. idxPrev+10 in the reference's order (first minimum wins),
-    // indexed into the padded grid instead of modulo 512
     const float2* __restrict__ P2 = reinterpret_cast<const float2*>(P);
-    int bestJ = idxPrev - WIN;
-    float bestSqDist;
+    // Window idxPrev-10 .. idxPrev+10, first minimum of the squared distance wins (the
+    // reference scans it in increasing index order with a strict '<'). Samples are taken
+    // in pairs of consecutive indices from the separate x / y rows with packed FP32x2
+    // arithmetic (each lane rounds exactly like the scalar sub, mul and fma), then the
+    // one sample left over; the window of 21 has 10 pairs starting at an even index and
+    // one single sample, either its first (odd start) or its last (even start).
+    const int j0 = idxPrev - WIN;
+    const int jp = (j0 + 1) & ~1;
+    const int js = (j0 & 1) ? j0 : j0 + 2 * WIN;
+    const uint64_t* __restrict__ PX2 = reinterpret_cast<const uint64_t*>(tr.px);
+    const uint64_t* __restrict__ PY2 = reinterpret_cast<const uint64_t*>(tr.py);
+    uint64_t pxx, pyy;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(pxx) : "f"(px));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(pyy) : "f"(py));
+    float bestSqDist = INFINITY;
+    int bestJ = j0;
+#pragma unroll 5
+    for (int q = 0; q < WIN; q++)
     {
-        float2 q = P2[bestJ];
-        float sq = 0.f;
-        float d0 = q.x - px;
-        sq += d0 * d0;
-        float d1 = q.y - py;
-        sq += d1 * d1;
-        bestSqDist = sq;
-    }
-#pragma unroll 4
-    for (int j = idxPrev - WIN + 1; j <= idxPrev + WIN; j++)
-    {
-        float2 q = P2[j];
-        float sq = 0.f;
-        float d0 = q.x - px;
-        sq += d0 * d0;
-        float d1 = q.y - py;
-        sq += d1 * d1;
-        if (sq < bestSqDist)
+        const int j = jp + 2 * q;
+        float sqA, sqB;
+        asm("{\n\t.reg .b64 d0, d1, s;\n\t"
+            "sub.rn.f32x2 d0, %2, %4;\n\t"
+            "sub.rn.f32x2 d1, %3, %5;\n\t"
+            "mul.rn.f32x2 s, d0, d0;\n\t"
+            "fma.rn.f32x2 s, d1, d1, s;\n\t"
+            "mov.b64 {%0, %1}, s;\n\t}"
+            : "=f"(sqA), "=f"(sqB)
+            : "l"(PX2[j >> 1]), "l"(PY2[j >> 1]), "l"(pxx), "l"(pyy));
+        if (sqA < bestSqDist)
         {
-            bestSqDist = sq;
+            bestSqDist = sqA;
             bestJ = j;
         }
+        if (sqB < bestSqDist)
+        {
+            bestSqDist = sqB;
+            bestJ = j + 1;
+        }
+    }
+    {
+        float2 qs = P2[js];
+        float sq = 0.f;
+        float d0 = qs.x - px;
+        sq += d0 * d0;
+        float d1 = qs.y - py;
+        sq += d1 * d1;
+        if (sq < bestSqDist || (sq == bestSqDist && js < bestJ))
+            bestJ = js;
     }
     const int bestInd = (bestJ + NTS) % NTS;
     float bestSegSqDist = INFINITY;
@@ -527,8 +561,9 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
         float an = E.actionNoise[trueTheta][o - 1];
         if (an != 0.0f)
         {
-            u0 += an * rng.next();
-            u1 += an * rng.next();
+            const float2 nn = rng.next2(); // the stream's next two words, as next() twice
+            u0 += an * nn.x;
+            u1 += an * nn.y;
         }
         act0[o] = u0;
         act1[o] = u1;

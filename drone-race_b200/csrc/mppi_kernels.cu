@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ i
         return;
     }
     const EnvParams& E = *sE;
-    const Track tr{sGrid + GRID_P, sGrid + GRID_T, sGrid + GRID_K};
+    const Track tr = trackIn(sGrid);
 
     const int th = threadIdx.x % NTH;
     const int sl = threadIdx.x / NTH;
@@ -602,7 +602,7 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
         return;
     }
     const EnvParams& E = *sE;
-    const Track tr{sGrid + GRID_P, sGrid + GRID_T, sGrid + GRID_K};
+    const Track tr = trackIn(sGrid);
     const int v = tile.s0 + threadIdx.x;
     bool active = threadIdx.x < tile.count; // idle lanes of a partial tile still take the barriers
     {

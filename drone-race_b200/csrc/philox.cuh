@@ -165,6 +165,11 @@ static __device__ __noinline__ float normal_from_word_ool(uint32_t w)
     return normal_from_word(w);
 }
 
+static __device__ __noinline__ float2 normal_pair_ool(uint32_t w0, uint32_t w1)
+{
+    return make_float2(normal_from_word(w0), normal_from_word(w1));
+}
+
 struct EnvNoise
 {
     uint32_t k0, k1, c0, c1base, step, stream, t;
@@ -186,6 +191,18 @@ struct EnvNoise
         uint32_t w = (j & 3) == 0 ? cur.x : (j & 3) == 1 ? cur.y : (j & 3) == 2 ? cur.z : cur.w;
         j++;
         return normal_from_word_ool(w);
+    }
+    // The next two normals (words j and j+1 of the stream; j is even, so both come from
+    // the same Philox block). The block is drawn inline: this is the one noise site that
+    // runs every step in the default configuration (opponent action noise).
+    __device__ __forceinline__ float2 next2()
+    {
+        if ((j & 3) == 0)
+            cur = draw(k0, k1, c0, c1base | t, step, stream, (uint32_t)(j >> 2));
+        const bool lo = (j & 3) == 0;
+        const uint32_t w0 = lo ? cur.x : cur.z, w1 = lo ? cur.y : cur.w;
+        j += 2;
+        return normal_pair_ool(w0, w1);
     }
 };
 

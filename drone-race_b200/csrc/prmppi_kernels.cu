@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ inst
         return;
     }
     const EnvParams& E = *sE;
-    const Track tr{sGrid + GRID_P, sGrid + GRID_T, sGrid + GRID_K};
+    const Track tr = trackIn(sGrid);
     const int spb = PRB / P;
     const int sl = threadIdx.x / P, p = threadIdx.x % P;
     const int s = tile.s0 + sl;
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(PRB) pr_candidates(const PrDev* __restrict__ i
         return;
     }
     const EnvParams& E = *sE;
-    const Track tr{sGrid + GRID_P, sGrid + GRID_T, sGrid + GRID_K};
+    const Track tr = trackIn(sGrid);
     const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
     for (int task = threadIdx.x; task < 4 * P; task += blockDim.x)
     {
