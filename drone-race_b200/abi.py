@@ -1,8 +1,9 @@
 """ctypes mirror of include/drmppi.h (the C ABI of the control step).
 
 The structures follow the reference's configuration structs field by field
-(include/environments/env_stratrace_defs.h:42-96, include/config.h:116-192), with the
-compile-time sizes of the reference turned into runtime counts.
+(include/environments/env_stratrace_defs.h:42-96, include/config.h:116-192, and for the
+gate race include/environments/env_dronerace_defs.h:44-103), with the compile-time
+sizes of the reference turned into runtime counts.
 """
 from __future__ import annotations
 
@@ -161,6 +162,66 @@ class dr_prmppi_info(C.Structure):
     ]
 
 
+# ---- gate race (reference EnvDroneRace, include/environments/env_dronerace_defs.h) ----
+DR_GATE_AGENTS = 2
+DR_GATE_RACELINES = 2
+DR_GATE_MAX_GATES = 16
+DR_GATE_MAX_OBSTACLES = 4
+
+
+class dr_pid_config(C.Structure):
+    _fields_ = [
+        ("kp", C.c_float),
+        ("kd", C.c_float),
+        ("repulsion_factor", C.c_float),
+        ("repulsion_power", C.c_float),
+        ("repulsion_dist_fact", C.c_float),
+        ("raceline_index", C.c_int32),
+        ("action_noise", C.c_float),
+    ]
+
+
+class dr_gate_env_config(C.Structure):
+    _fields_ = [
+        ("n_theta", C.c_int32),
+        ("arena_min", C.c_float * DR_DIM),
+        ("arena_max", C.c_float * DR_DIM),
+        ("dt", C.c_float),
+        ("send_states", C.c_int32),
+        ("drone_radius", C.c_float),
+        ("pos_noise_level", C.c_float),
+        ("speed_noise_level", C.c_float),
+        ("action_noise_level", C.c_float),
+        ("max_speed", C.c_float * DR_GATE_AGENTS),
+        ("max_accel", C.c_float * DR_GATE_AGENTS),
+        ("n_win_laps", C.c_int32),
+        ("target_distance", C.c_float),
+        ("n_gates", C.c_int32),
+        ("gate_centers", C.c_float * (DR_GATE_MAX_GATES * DR_DIM)),
+        ("gate_vectors", C.c_float * (DR_GATE_MAX_GATES * DR_DIM)),
+        ("gate_radius", C.c_float * DR_GATE_MAX_GATES),
+        ("n_obstacles", C.c_int32),
+        ("obstacles", C.c_float * (DR_GATE_MAX_OBSTACLES * DR_DIM * 2)),
+        ("n_round_obstacles", C.c_int32),
+        ("round_obs_centers", C.c_float * (DR_GATE_MAX_OBSTACLES * DR_DIM)),
+        ("round_obs_radius", C.c_float * DR_GATE_MAX_OBSTACLES),
+        ("track_points", C.POINTER(C.c_float)),
+        ("init_belief", C.c_float * DR_MAX_THETA),
+        ("opp_pid", dr_pid_config * DR_MAX_THETA),
+        ("i_mppi", C.c_int32),
+    ]
+
+
+class dr_gate_state(C.Structure):
+    _fields_ = [
+        ("pos", C.c_float * (DR_GATE_AGENTS * DR_DIM)),
+        ("vel", C.c_float * (DR_GATE_AGENTS * DR_DIM)),
+        ("S", C.c_float * (DR_GATE_AGENTS * DR_GATE_RACELINES)),
+        ("laps", C.c_int32 * DR_GATE_AGENTS),
+        ("gates", C.c_int32 * DR_GATE_AGENTS),
+    ]
+
+
 def fptr(a: np.ndarray) -> C.POINTER(C.c_float):
     assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(C.POINTER(C.c_float))
@@ -236,6 +297,12 @@ _PROTOS = {
                                                 C.POINTER(C.c_float), C.c_void_p, C.c_void_p, C.c_void_p]),
     "dr_spline_matrix": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "dr_env_step": (C.c_int, [C.POINTER(dr_env_config), C.c_int, C.POINTER(C.c_float), C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_int)]),
+    "dr_gate_mppi_create": (C.c_int, [C.POINTER(dr_gate_env_config), C.POINTER(dr_mppi_config), C.c_uint64, C.POINTER(C.c_float), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "dr_gate_mppi_step": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_mppi_info)]),
+    "dr_gate_mppi_batch_step": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_mppi_info)]),
+    "dr_gate_mppi_debug_rollout": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    "dr_gate_mppi_debug_verify": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "dr_gate_env_step": (C.c_int, [C.POINTER(dr_gate_env_config), C.c_int, C.POINTER(C.c_float), C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_int)]),
 }
 
 EXPORTED = sorted(_PROTOS)

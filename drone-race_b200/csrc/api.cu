@@ -8,6 +8,7 @@
 #include <memory>
 #include <numeric>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -35,6 +36,7 @@ std::string& lastError()
 // ============================================================================================
 struct dr_mppi
 {
+    int envKind = 0; // 0 strategic race, 1 gate race
     int device = 0;
     cudaStream_t stream = nullptr;
     bool ownStream = false;
@@ -61,13 +63,26 @@ struct dr_mppi
     {
         MppiIn in{};
         in.state = s;
+        fillInput(in, belief);
+        return in;
+    }
+
+    MppiIn input(const dr_gate_state& s, const float* belief) const
+    {
+        MppiIn in{};
+        in.gstate = s;
+        fillInput(in, belief);
+        return in;
+    }
+
+    void fillInput(MppiIn& in, const float* belief) const
+    {
         for (int i = 0; i < DR_MAX_THETA; i++)
             in.belief[i] = i < nth ? belief[i] : 0.0f;
         in.lambda = lambda;
         in.step = (uint32_t)step;
         in.pendBranch = pendBranch;
         in.pendUseNew = pendUseNew;
-        return in;
     }
 
     // host tail of MPPIController::getControl (mppi_controller.cu:363-456)
@@ -150,6 +165,7 @@ struct dr_mppi
 struct dr_mppi_batch
 {
     std::vector<dr_mppi*> hs;
+    int envKind = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool ownStream = false;
@@ -184,6 +200,16 @@ struct dr_mppi_batch
         return a;
     }
 
+    cudaError_t launchRollout(const LaunchArgs& a) const
+    {
+        return envKind ? launchGateRollout(a, nth, spl, rollSmem) : launchMppiRollout(a, nopp, nth, spl, rollSmem);
+    }
+
+    cudaError_t launchVerify(const LaunchArgs& a) const
+    {
+        return envKind ? launchGateVerify(a, nth, verSmem, nullptr, nullptr) : launchMppiVerify(a, nopp, nth, verSmem, nullptr, nullptr);
+    }
+
     // kernels of one control step, reading inputs from `in` (device)
     int launchAll(const MppiIn* in, bool profile, Timer* timer)
     {
@@ -209,7 +235,7 @@ struct dr_mppi_batch
             }
             LaunchArgs a = args(dVerOld, nVerOld, in);
             a.stream = sideStream;
-            CK(launchMppiVerify(a, nopp, nth, verSmem, nullptr, nullptr));
+            CK(launchVerify(a));
             if (profile)
             {
                 timerSide.mark("end", sideStream);
@@ -219,7 +245,7 @@ struct dr_mppi_batch
         }
         if (profile)
             timer->mark("rollout", stream);
-        CK(launchMppiRollout(args(dRoll, nRoll, in), nopp, nth, spl, rollSmem));
+        CK(launchRollout(args(dRoll, nRoll, in)));
         if (profile)
             timer->mark("update", stream);
         CK(launchMppiUpdate(args(dUpd, nUpd, in), nth));
@@ -228,9 +254,9 @@ struct dr_mppi_batch
             if (profile)
                 timer->mark(side ? "verify_new" : "verify", stream);
             if (side)
-                CK(launchMppiVerify(args(dVerNew, nVerNew, in), nopp, nth, verSmem, nullptr, nullptr));
+                CK(launchVerify(args(dVerNew, nVerNew, in)));
             else
-                CK(launchMppiVerify(args(dVer, nVer, in), nopp, nth, verSmem, nullptr, nullptr));
+                CK(launchVerify(args(dVer, nVer, in)));
         }
         if (profile)
         {
@@ -283,9 +309,12 @@ struct dr_mppi_batch
         return DR_OK;
     }
 
-    int step(const dr_sim_state* states, const float* beliefs, int beliefStride, float* actions, dr_mppi_info* infos)
+    template <class St> int step(const St* states, const float* beliefs, int beliefStride, float* actions, dr_mppi_info* infos)
     {
         const int n = (int)hs.size();
+        if (envKind != (std::is_same<St, dr_gate_state>::value ? 1 : 0))
+            return fail(DR_ERR_INVALID_ARG, envKind ? "gate-race controllers: step them with the dr_gate_* functions"
+                                                    : "strategic-race controllers: step them with dr_mppi_step / dr_mppi_batch_step");
         CK(cudaSetDevice(device));
         for (int i = 0; i < n; i++)
             hIn[i] = hs[i]->input(states[i], beliefs + (size_t)i * beliefStride);
@@ -342,16 +371,17 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     b->nth = hs[0]->nth;
     b->spl = hs[0]->spl;
     b->verify = hs[0]->cfg.verify != 0;
+    b->envKind = hs[0]->envKind;
     for (int i = 0; i < n; i++)
         if (!hs[i] || hs[i]->device != b->device || hs[i]->nopp != b->nopp || hs[i]->nth != b->nth || hs[i]->spl != b->spl ||
-            (hs[i]->cfg.verify != 0) != b->verify)
-            return fail(DR_ERR_INVALID_ARG, "a batch needs controllers on one device with equal n_opp, n_theta, use_splines and verify");
+            (hs[i]->cfg.verify != 0) != b->verify || hs[i]->envKind != b->envKind)
+            return fail(DR_ERR_INVALID_ARG, "a batch needs controllers on one device with equal environment kind, n_opp, n_theta, use_splines and verify");
     CK(cudaSetDevice(b->device));
     b->stream = stream;
     b->ownStream = ownStream;
     std::vector<MppiDev> descs;
     std::vector<Tile> roll, upd, ver, verOld;
-    const int spb = rolloutSamplesPerBlock(b->nth);
+    const int spb = b->envKind ? gateRolloutSamplesPerBlock(b->nth) : rolloutSamplesPerBlock(b->nth);
     int maxT = 0, maxM = 0, maxNbpT = 0;
     for (int i = 0; i < n; i++)
     {
@@ -375,8 +405,8 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     ver.insert(ver.end(), verOld.begin(), verOld.end());
     for (int i = 0; i < n; i++)
     {
-        b->rollSmem = std::max(b->rollSmem, mppiRolloutSmem(b->nth, hs[i]->T, hs[i]->M, b->spl));
-        b->verSmem = std::max(b->verSmem, mppiVerifySmem(b->nth, hs[i]->T));
+        b->rollSmem = std::max(b->rollSmem, b->envKind ? gateRolloutSmem(b->nth, hs[i]->T, hs[i]->M, b->spl) : mppiRolloutSmem(b->nth, hs[i]->T, hs[i]->M, b->spl));
+        b->verSmem = std::max(b->verSmem, b->envKind ? gateVerifySmem(b->nth, hs[i]->T) : mppiVerifySmem(b->nth, hs[i]->T));
     }
     b->proSmem = ((size_t)maxNbpT * 2 + (size_t)maxM * 2) * 4;
     if (b->rollSmem > 227 * 1024)
@@ -473,28 +503,47 @@ const char* dr_status_string(int s)
     }
 }
 
-int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream, dr_mppi** out)
+} // extern "C"
+
+// MPPIController construction for either environment: the strategic race (env) or the
+// gate race (genv); exactly one of the two is given.
+static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, const dr_mppi_config* cfg, uint64_t seed, const float* nominal,
+                      int device, void* stream, dr_mppi** out)
 {
     if (!out)
         return fail(DR_ERR_INVALID_ARG, "out is NULL");
     *out = nullptr;
-    int rc = checkEnv(env);
+    int rc = env ? checkEnv(env) : checkGateEnv(genv);
     if (rc)
         return rc;
-    rc = checkMppiCfg(env, cfg);
+    if (env)
+        rc = checkMppiCfg(env, cfg);
+    else
+    {
+        dr_env_config probe{};
+        probe.n_opp = 1;
+        probe.n_theta = genv->n_theta;
+        rc = checkMppiCfg(&probe, cfg);
+        if (!rc && !gateSupported(genv->n_theta))
+            rc = fail(DR_ERR_UNSUPPORTED, "n_theta not compiled in for the gate race");
+    }
     if (rc)
         return rc;
     rc = selectDevice(device);
     if (rc)
         return rc;
     auto h = std::make_unique<dr_mppi>();
+    h->envKind = env ? 0 : 1;
     h->device = device;
-    h->env = *env;
-    h->env.p_grid = h->env.dp_grid = h->env.t_grid = h->env.kappa_grid = nullptr;
+    if (env)
+    {
+        h->env = *env;
+        h->env.p_grid = h->env.dp_grid = h->env.t_grid = h->env.kappa_grid = nullptr;
+    }
     h->cfg = *cfg;
     h->seed = seed;
-    h->nth = env->n_theta;
-    h->nopp = env->n_opp;
+    h->nth = env ? env->n_theta : genv->n_theta;
+    h->nopp = env ? env->n_opp : 1;
     h->K = cfg->n_samples;
     h->T = cfg->n_timesteps;
     h->spl = cfg->use_splines != 0;
@@ -508,7 +557,10 @@ int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t
     h->lambda = cfg->inv_temperature;
     const int K = h->K, T = h->T, M = h->M, nbp = h->nbp, nth = h->nth;
     MppiDev& D = h->desc;
-    D.env = toEnvParams(*env);
+    if (env)
+        D.env = toEnvParams(*env);
+    else
+        D.env.maxAccel[0] = genv->max_accel[genv->i_mppi]; // Env::getMaxAccel, the update's clamp (mppi_controller.cu:345)
     D.cfg.K = K;
     D.cfg.T = T;
     D.cfg.M = M;
@@ -525,6 +577,7 @@ int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t
     D.cfg.sigma0 = s0;
     D.cfg.sigma1 = s1;
     D.cfg.minConf = cfg->min_confidence;
+    D.cfg.gateMargin = cfg->gate_traversal_margin;
     D.cfg.w = MppiCostW{cfg->coll_dist_factor, cfg->boundary_cost, cfg->boundary_threshold_factor, cfg->outside_cost,
                         cfg->win_cost,         cfg->opp_win_cost,  cfg->final_adv_weight,          cfg->final_opp_adv_weight};
     D.cfg.k0 = (uint32_t)seed;
@@ -540,7 +593,15 @@ int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t
     int *binfo, *stats;
     unsigned *counter, *failc;
     Arena& A = h->arena;
-    A.add(grids, GRID_FLOATS * 4);
+    GateParams* gp = nullptr;
+    float* gtrack = nullptr;
+    if (env)
+        A.add(grids, GRID_FLOATS * 4);
+    else
+    {
+        A.add(gp, a16(sizeof(GateParams)));
+        A.add(gtrack, GATE_TRACK_FLOATS * 4);
+    }
     A.add(B, a16((size_t)T * M * 4));
     A.add(knots, a16((size_t)nbp * M * 2 * 4));
     A.add(costsTrue, (size_t)nth * K * 4);
@@ -559,7 +620,9 @@ int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t
     nu = (float*)(res + oNu);
     minCosts = (float*)(res + oMin);
     stats = (int*)(res + oStats);
-    D.grids = grids;
+    D.grids = env ? grids : nullptr;
+    D.gate = gp;
+    D.gtrack = gtrack;
     D.B = B;
     D.knots = knots;
     D.costsTrue = costsTrue;
@@ -573,8 +636,18 @@ int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t
     D.minCosts = minCosts;
     D.stats = stats;
     D.resBytes = resBytes;
-    std::vector<float> g = packGrids(*env);
-    CK(cudaMemcpy(grids, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    if (env)
+    {
+        std::vector<float> g = packGrids(*env);
+        CK(cudaMemcpy(grids, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    }
+    else
+    {
+        GateParams hp = toGateParams(*genv);
+        CK(cudaMemcpy(gp, &hp, sizeof(GateParams), cudaMemcpyHostToDevice));
+        std::vector<float> t = packGateTrack(*genv);
+        CK(cudaMemcpy(gtrack, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+    }
     if (h->spl)
     {
         std::vector<float> Bm = splineMatrix(T, M, h->cfg.knots);
@@ -608,6 +681,23 @@ int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t
     return DR_OK;
 }
 
+extern "C" {
+
+int dr_mppi_create(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream, dr_mppi** out)
+{
+    if (!env)
+        return fail(DR_ERR_INVALID_ARG, "env is NULL");
+    return createMppi(env, nullptr, cfg, seed, nominal, device, stream, out);
+}
+
+int dr_gate_mppi_create(const dr_gate_env_config* env, const dr_mppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
+                        dr_mppi** out)
+{
+    if (!env)
+        return fail(DR_ERR_INVALID_ARG, "env is NULL");
+    return createMppi(nullptr, env, cfg, seed, nominal, device, stream, out);
+}
+
 int dr_mppi_destroy(dr_mppi* h)
 {
     if (!h)
@@ -630,6 +720,13 @@ int dr_mppi_destroy(dr_mppi* h)
 }
 
 int dr_mppi_step(dr_mppi* h, const dr_sim_state* state, const float* belief, float* out_action, dr_mppi_info* info)
+{
+    if (!h || !state || !belief || !out_action)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->step(state, belief, h->nth, out_action, info);
+}
+
+int dr_gate_mppi_step(dr_mppi* h, const dr_gate_state* state, const float* belief, float* out_action, dr_mppi_info* info)
 {
     if (!h || !state || !belief || !out_action)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
@@ -758,6 +855,13 @@ int dr_mppi_batch_step(dr_mppi_batch* b, const dr_sim_state* states, const float
     return b->step(states, beliefs, DR_MAX_THETA, out_actions, infos);
 }
 
+int dr_gate_mppi_batch_step(dr_mppi_batch* b, const dr_gate_state* states, const float* beliefs, float* out_actions, dr_mppi_info* infos)
+{
+    if (!b || !states || !beliefs || !out_actions)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return b->step(states, beliefs, DR_MAX_THETA, out_actions, infos);
+}
+
 int dr_mppi_batch_set_graph(dr_mppi_batch* b, int use_graph)
 {
     if (!b)
@@ -780,11 +884,13 @@ int dr_mppi_batch_step_dev(dr_mppi_batch* b, const dr_sim_state* states_dev, con
         MppiIn tmp = b->hs[i]->input(dr_sim_state{}, std::vector<float>(DR_MAX_THETA, 0.0f).data());
         b->hIn[i] = tmp;
     }
+    // a gate-race batch takes dr_gate_state records
+    const size_t stBytes = b->envKind ? sizeof(dr_gate_state) : sizeof(dr_sim_state);
     // host part of the record (temperature, step, pending shift), then state and belief device-to-device
     CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(MppiIn) * n, cudaMemcpyHostToDevice, b->stream));
     for (int i = 0; i < n; i++)
     {
-        CK(cudaMemcpyAsync(&b->dIn[i].state, states_dev + i, sizeof(dr_sim_state), cudaMemcpyDeviceToDevice, b->stream));
+        CK(cudaMemcpyAsync(&b->dIn[i].state, (const unsigned char*)states_dev + i * stBytes, stBytes, cudaMemcpyDeviceToDevice, b->stream));
         CK(cudaMemcpyAsync(&b->dIn[i].belief, beliefs_dev + (size_t)i * DR_MAX_THETA, DR_MAX_THETA * 4, cudaMemcpyDeviceToDevice, b->stream));
     }
     return b->launchAll(b->dIn, b->profiling, &b->timer);
@@ -814,7 +920,8 @@ int dr_mppi_debug_noise(dr_mppi* h, float* noise, size_t n)
     return DR_OK;
 }
 
-static int applyPending(dr_mppi* h, const dr_sim_state* state, const float* belief)
+extern "C++" {
+template <class St> static int applyPending(dr_mppi* h, const St* state, const float* belief)
 {
     dr_mppi_batch* b = h->self;
     b->hIn[0] = h->input(*state, belief);
@@ -826,18 +933,22 @@ static int applyPending(dr_mppi* h, const dr_sim_state* state, const float* beli
     CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(MppiIn), cudaMemcpyHostToDevice, h->stream));
     return DR_OK;
 }
+} // extern "C++"
 
-int dr_mppi_debug_rollout(dr_mppi* h, const dr_sim_state* state, const float* belief, float* costs_true, int32_t* branch_used, int32_t* branch_time,
-                          float* costs)
+extern "C++" {
+template <class St>
+static int debugRollout(dr_mppi* h, const St* state, const float* belief, float* costs_true, int32_t* branch_used, int32_t* branch_time, float* costs)
 {
     if (!h || !state || !belief)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->envKind != (std::is_same<St, dr_gate_state>::value ? 1 : 0))
+        return fail(DR_ERR_INVALID_ARG, "state type does not match the controller's environment");
     CK(cudaSetDevice(h->device));
     int rc = applyPending(h, state, belief);
     if (rc)
         return rc;
     dr_mppi_batch* b = h->self;
-    CK(launchMppiRollout(b->args(b->dRoll, b->nRoll, b->dIn), h->nopp, h->nth, h->spl, b->rollSmem));
+    CK(b->launchRollout(b->args(b->dRoll, b->nRoll, b->dIn)));
     const size_t nk = (size_t)h->nth * h->K;
     std::vector<int> info(nk);
     if (costs_true)
@@ -854,6 +965,19 @@ int dr_mppi_debug_rollout(dr_mppi* h, const dr_sim_state* state, const float* be
             branch_time[i] = (int)(short)(info[i] & 0xffff);
     }
     return DR_OK;
+}
+} // extern "C++"
+
+int dr_mppi_debug_rollout(dr_mppi* h, const dr_sim_state* state, const float* belief, float* costs_true, int32_t* branch_used, int32_t* branch_time,
+                          float* costs)
+{
+    return debugRollout(h, state, belief, costs_true, branch_used, branch_time, costs);
+}
+
+int dr_gate_mppi_debug_rollout(dr_mppi* h, const dr_gate_state* state, const float* belief, float* costs_true, int32_t* branch_used,
+                               int32_t* branch_time, float* costs)
+{
+    return debugRollout(h, state, belief, costs_true, branch_used, branch_time, costs);
 }
 
 int dr_mppi_debug_update(dr_mppi* h, const float* belief, const float* costs_true, const int32_t* branch_used, const int32_t* branch_time,
@@ -885,11 +1009,15 @@ int dr_mppi_debug_update(dr_mppi* h, const float* belief, const float* costs_tru
     return DR_OK;
 }
 
-int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* belief, const float* dense_plan, int plan, uint32_t* fail_count,
-                         int32_t* fail_time, int32_t* thetas)
+extern "C++" {
+template <class St>
+static int debugVerify(dr_mppi* h, const St* state, const float* belief, const float* dense_plan, int plan, uint32_t* fail_count, int32_t* fail_time,
+                       int32_t* thetas)
 {
     if (!h || !state || !belief || !dense_plan || plan < 0 || plan > 1 || h->V <= 0)
         return fail(DR_ERR_INVALID_ARG, "bad argument (verification disabled?)");
+    if (h->envKind != (std::is_same<St, dr_gate_state>::value ? 1 : 0))
+        return fail(DR_ERR_INVALID_ARG, "state type does not match the controller's environment");
     CK(cudaSetDevice(h->device));
     const int V = h->V, T = h->T;
     // a private copy of the instance with its own plan and histogram buffers
@@ -938,7 +1066,8 @@ int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* bel
         a.mppiIn = dIn;
         a.tiles = dT;
         a.nTiles = (int)tiles.size();
-        e = launchMppiVerify(a, h->nopp, h->nth, mppiVerifySmem(h->nth, T), dFt, dTh);
+        e = h->envKind ? launchGateVerify(a, h->nth, gateVerifySmem(h->nth, T), dFt, dTh)
+                       : launchMppiVerify(a, h->nopp, h->nth, mppiVerifySmem(h->nth, T), dFt, dTh);
         std::vector<unsigned> fc(2 * T);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(fc.data(), dFail, 2 * T * 4, cudaMemcpyDeviceToHost, h->stream);
@@ -961,6 +1090,19 @@ int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* bel
     cudaFree(dT);
     CK(e);
     return DR_OK;
+}
+} // extern "C++"
+
+int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* belief, const float* dense_plan, int plan, uint32_t* fail_count,
+                         int32_t* fail_time, int32_t* thetas)
+{
+    return debugVerify(h, state, belief, dense_plan, plan, fail_count, fail_time, thetas);
+}
+
+int dr_gate_mppi_debug_verify(dr_mppi* h, const dr_gate_state* state, const float* belief, const float* dense_plan, int plan, uint32_t* fail_count,
+                              int32_t* fail_time, int32_t* thetas)
+{
+    return debugVerify(h, state, belief, dense_plan, plan, fail_count, fail_time, thetas);
 }
 
 } // extern "C"

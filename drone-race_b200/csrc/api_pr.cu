@@ -725,6 +725,60 @@ extern "C" int dr_env_step(const dr_env_config* env, int true_theta, const float
     return DR_OK;
 }
 
+extern "C" int dr_gate_env_step(const dr_gate_env_config* env, int true_theta, const float* action, dr_gate_state* state, float* belief,
+                                int update_belief, uint64_t seed, uint64_t step, int* term)
+{
+    int rc = checkGateEnv(env);
+    if (rc)
+        return rc;
+    if (!action || !state || !belief || true_theta < 0 || true_theta >= env->n_theta)
+        return fail(DR_ERR_INVALID_ARG, "bad argument");
+    if (!gateSupported(env->n_theta))
+        return fail(DR_ERR_UNSUPPORTED, "n_theta not compiled in for the gate race");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    GateParams hp = toGateParams(*env);
+    std::vector<float> tr = packGateTrack(*env);
+    GateParams* dgp = nullptr;
+    float* dtr = nullptr;
+    dr_gate_state* ds = nullptr;
+    float* db = nullptr;
+    int* dt = nullptr;
+    cudaError_t e = cudaMalloc(&dgp, sizeof(GateParams));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dtr, tr.size() * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&ds, sizeof(dr_gate_state));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&db, DR_MAX_THETA * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dt, 4);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dgp, &hp, sizeof(GateParams), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dtr, tr.data(), tr.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ds, state, sizeof(dr_gate_state), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(db, belief, env->n_theta * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = launchGateEnvStep(nullptr, env->n_theta, dgp, dtr, true_theta, action[0], action[1], ds, db, update_belief, (uint32_t)seed,
+                              (uint32_t)(seed >> 32), (uint32_t)step, dt);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(state, ds, sizeof(dr_gate_state), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(belief, db, env->n_theta * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && term)
+        e = cudaMemcpy(term, dt, 4, cudaMemcpyDeviceToHost);
+    cudaFree(dgp);
+    cudaFree(dtr);
+    cudaFree(ds);
+    cudaFree(db);
+    cudaFree(dt);
+    CK(e);
+    return DR_OK;
+}
+
 extern "C" int dr_prmppi_batch_set_profiling(dr_prmppi_batch* b, int on)
 {
     if (!b)

@@ -1,0 +1,473 @@
+// MPPI kernels of the gate race (the reference's kernels.cu compiled with
+// USE_ENV_DRONERACE): the rollout with per-branch cost aggregation and the plan
+// verification, built like mppi_rollout / mppi_verify (one thread per (sample,
+// hypothesis), resp. per verification sample; state in registers; racelines in shared
+// memory, staged by a bulk copy; gate parameters copied to shared memory; perturbations
+// from Philox) on the model of gate_model.cuh. The prologue and the update kernels of
+// mppi_kernels.cu serve both environments (they see only costs, bookkeeping and plans).
+#include <cstdio>
+
+#include "common.cuh"
+#include "gate_model.cuh"
+#include "instance.cuh"
+#include "launch.h"
+
+namespace dr
+{
+
+namespace
+{
+
+constexpr int GRB = 128; // rollout block size
+
+__host__ __device__ __forceinline__ size_t ga16(size_t x)
+{
+    return (x + 15) & ~(size_t)15;
+}
+
+__device__ __forceinline__ int gPackInfo(int pt, int bt)
+{
+    return (pt << 16) | (bt & 0xffff);
+}
+
+__device__ __forceinline__ void copyGate(GateParams* dst, const GateParams* src)
+{
+    for (int i = threadIdx.x; i < GATE_HOST_WORDS; i += blockDim.x)
+        ((float*)dst)[i] = ((const float*)src)[i];
+    gateDeviceTerms(*dst, *src, threadIdx.x, blockDim.x);
+}
+
+struct GateSmem
+{
+    size_t gp, track, knots, B, vbuf, red, total;
+};
+
+__host__ __device__ inline GateSmem gateRolloutLayout(int nbp, int T, int M, bool spl)
+{
+    GateSmem L;
+    size_t off = 16; // mbarrier
+    L.gp = off;
+    off = ga16(off + sizeof(GateParams));
+    L.track = off;
+    off = ga16(off + GATE_TRACK_FLOATS * 4);
+    L.knots = off;
+    off = ga16(off + (size_t)nbp * M * 2 * 4);
+    L.B = off;
+    if (spl)
+        off = ga16(off + (size_t)T * M * 4);
+    L.vbuf = off;
+    if (spl)
+        off = ga16(off + (size_t)M * 2 * GRB * 4);
+    L.red = off;
+    off = ga16(off + GRB * 4);
+    L.total = off;
+    return L;
+}
+
+} // namespace
+
+// fullRolloutKernel (kernels.cu:34-171) + aggregateBranchCostsKernel (175-217) on the
+// gate race: environmentStep<true, true, false> (kernels.cu:141-143).
+template <int NTH, bool SPL>
+__global__ void __launch_bounds__(GRB) gate_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles)
+{
+    constexpr int NBP = NTH + 1;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    const Tile tile = tiles[blockIdx.x];
+    const MppiDev& D = insts[tile.inst];
+    const MppiIn& I = in[tile.inst];
+    const int K = D.cfg.K, T = D.cfg.T, M = D.cfg.M;
+    const GateSmem L = gateRolloutLayout(NBP, T, M, SPL);
+    uint64_t* bar = (uint64_t*)smraw;
+    GateParams* sG = (GateParams*)(smraw + L.gp);
+    float* sTrack = (float*)(smraw + L.track);
+    float* sKn = (float*)(smraw + L.knots);
+    float* sB = (float*)(smraw + L.B);
+    float* vbuf = (float*)(smraw + L.vbuf);
+    float* red = (float*)(smraw + L.red);
+    const uint32_t knBytes = (uint32_t)ga16((size_t)NBP * M * 2 * 4);
+    const uint32_t bBytes = SPL ? (uint32_t)ga16((size_t)T * M * 4) : 0u;
+    if (threadIdx.x == 0)
+    {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, GATE_TRACK_FLOATS * 4 + knBytes + bBytes);
+        bulk_g2s(sTrack, D.gtrack, GATE_TRACK_FLOATS * 4, bar);
+        bulk_g2s(sKn, D.knots, knBytes, bar);
+        if (SPL)
+            bulk_g2s(sB, D.B, bBytes, bar);
+    }
+    copyGate(sG, D.gate);
+    __syncthreads();
+    if (!__syncthreads_and(mbar_wait(bar, 0)))
+    {
+        if (threadIdx.x == 0)
+            atomicAdd(&D.stats[1], 1);
+        return;
+    }
+    const GateParams& G = *sG;
+    const int th = threadIdx.x % NTH;
+    const int sl = threadIdx.x / NTH;
+    const int s = tile.s0 + sl;
+    const bool valid = sl < tile.count;
+    const float minConf = D.cfg.minConf;
+    const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+    const float sig0 = D.cfg.sigma0, sig1 = D.cfg.sigma1;
+    const float gateMargin = D.cfg.gateMargin;
+
+    float belief0[NTH];
+#pragma unroll
+    for (int i = 0; i < NTH; i++)
+        belief0[i] = I.belief[i];
+    const int pt0 = findConfident<NTH>(belief0, minConf);
+    const int bt0 = pt0 == 0 ? -1 : 0;
+    const bool compatible = (pt0 == 0 || pt0 == th + 1);
+
+    float cost = INFINITY;
+    int pt = pt0, bt = bt0;
+    if (valid && compatible)
+    {
+        GState st;
+        loadGState(st, I.gstate);
+        BState<NTH> bs;
+#pragma unroll
+        for (int i = 0; i < NTH; i++)
+            bs.belief[i] = belief0[i];
+        bs.predTheta = pt0;
+        bs.branchingTime = bt0;
+        cost = 0.0f;
+        bool stop = false;
+        float decay = 1.0f;
+        int tOrigin = 0;
+        EnvNoise rng(k0, k1, (uint32_t)s, (uint32_t)th << 16, step, S_MPPI_ROLL_ENV);
+        int curB = -1;
+        for (int t = 0; t < T && !stop; t++)
+        {
+            rng.begin_step((uint32_t)t);
+            const int local = t - tOrigin;
+            const int b = bs.predTheta;
+            float ego0, ego1;
+            if constexpr (SPL)
+            {
+                if (b != curB)
+                {
+                    for (int m = 0; m < M; m++)
+                    {
+                        U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)(b * M + m), step, S_MPPI_EPS, 0);
+                        float e0 = scaled_normal(sig0, r.x);
+                        float e1 = scaled_normal(sig1, r.y);
+                        vbuf[(m * 2 + 0) * GRB + threadIdx.x] = sKn[(b * M + m) * 2 + 0] + e0;
+                        vbuf[(m * 2 + 1) * GRB + threadIdx.x] = sKn[(b * M + m) * 2 + 1] + e1;
+                    }
+                    curB = b;
+                }
+                const float* Brow = sB + local * M;
+                float sum = 0.0f;
+                for (int m = 0; m < M; m++)
+                    sum += Brow[m] * vbuf[(m * 2 + 0) * GRB + threadIdx.x];
+                ego0 = sum;
+                sum = 0.0f;
+                for (int m = 0; m < M; m++)
+                    sum += Brow[m] * vbuf[(m * 2 + 1) * GRB + threadIdx.x];
+                ego1 = sum;
+            }
+            else
+            {
+                U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)(b * T + local), step, S_MPPI_EPS, 0);
+                float e0 = scaled_normal(sig0, r.x);
+                float e1 = scaled_normal(sig1, r.y);
+                ego0 = sKn[(b * T + local) * 2 + 0] + e0;
+                ego1 = sKn[(b * T + local) * 2 + 1] + e1;
+            }
+            bool branched = false;
+            StepOut o = gateStep<NTH, true, true, false, true>(t, th, sTrack, G, ego0, ego1, st, bs, branched, minConf, rng, gateMargin);
+            if (branched)
+                tOrigin = t + 1;
+            stop = (o.term != TERM_NONE);
+            cost += gateStateCost(o, G, D.cfg.w) * decay;
+            decay *= DECAY;
+        }
+        cost += gateFinalCost(st, G, D.cfg.w.finalAdvWeight, D.cfg.w.finalOppAdvWeight);
+        pt = bs.predTheta;
+        bt = bs.branchingTime;
+    }
+    if (valid)
+    {
+        D.costsTrue[th * K + s] = cost;
+        D.binfo[th * K + s] = gPackInfo(pt, bt);
+        if (compatible && !isfinite(cost))
+            atomicAdd(&D.stats[0], 1);
+    }
+    red[threadIdx.x] = cost;
+    __syncthreads();
+    // aggregateBranchCostsKernel (kernels.cu:175-217): costs[b][s] = E_belief[cost | b]
+    if (valid)
+    {
+        const float* c = red + sl * NTH;
+        if (th == 0)
+        {
+            float num = 0.0f, den = 0.0f;
+#pragma unroll
+            for (int m = 0; m < NTH; m++)
+            {
+                float cv = c[m];
+                if (!isfinite(cv))
+                    continue;
+                float w = belief0[m];
+                num += w * cv;
+                den += w;
+            }
+            D.costs[s] = (den > 1e-30f) ? (num / den) : INFINITY;
+        }
+        {
+            float num = 0.0f, den = 0.0f;
+            float cv = c[th];
+            if (isfinite(cv))
+            {
+                float w = belief0[th];
+                num += w * cv;
+                den += w;
+            }
+            D.costs[(size_t)(th + 1) * K + s] = (den > 1e-30f) ? (num / den) : INFINITY;
+        }
+    }
+}
+
+// verifyNominalFailureKernel (kernels.cu:488-551) on the gate race:
+// environmentStep<true, true, false, false>; one thread per sample, both plans in one
+// grid, the CTA's warps in step (a barrier per step) as in mppi_verify.
+template <int NTH>
+__global__ void __launch_bounds__(VERIFY_TILE, 1) gate_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
+                                                             int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
+{
+    constexpr int NBP = NTH + 1;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    const Tile tile = tiles[blockIdx.x];
+    const MppiDev& D = insts[tile.inst];
+    const MppiIn& I = in[tile.inst];
+    const int T = D.cfg.T, H = D.cfg.H;
+    const int plan = tile.aux;
+    uint64_t* bar = (uint64_t*)smraw;
+    GateParams* sG = (GateParams*)(smraw + 16);
+    const size_t offT = ga16(16 + sizeof(GateParams));
+    float* sTrack = (float*)(smraw + offT);
+    float* sPlan = (float*)(smraw + offT + GATE_TRACK_FLOATS * 4);
+    const uint32_t planBytes = (uint32_t)ga16((size_t)NBP * T * 2 * 4);
+    unsigned* hist = (unsigned*)(smraw + offT + GATE_TRACK_FLOATS * 4 + planBytes);
+    if (threadIdx.x == 0)
+    {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, GATE_TRACK_FLOATS * 4 + planBytes);
+        bulk_g2s(sTrack, D.gtrack, GATE_TRACK_FLOATS * 4, bar);
+        bulk_g2s(sPlan, plan == 0 ? D.dense : D.prevDense, planBytes, bar);
+    }
+    copyGate(sG, D.gate);
+    for (int i = threadIdx.x; i < T; i += blockDim.x)
+        hist[i] = 0u;
+    __syncthreads();
+    if (!__syncthreads_and(mbar_wait(bar, 0)))
+    {
+        if (threadIdx.x == 0)
+            atomicAdd(&D.stats[1], 1);
+        return;
+    }
+    const GateParams& G = *sG;
+    const int v = tile.s0 + threadIdx.x;
+    bool active = threadIdx.x < tile.count; // idle lanes of a partial tile still take the barriers
+    {
+        const float minConf = D.cfg.minConf;
+        const float gateMargin = D.cfg.gateMargin;
+        GState st;
+        loadGState(st, I.gstate);
+        BState<NTH> bs;
+#pragma unroll
+        for (int i = 0; i < NTH; i++)
+            bs.belief[i] = I.belief[i];
+        bs.predTheta = findConfident<NTH>(bs.belief, minConf);
+        bs.branchingTime = bs.predTheta == 0 ? -1 : 0;
+        // sampleModelFromBelief (state.h:118-131) on a Philox uniform
+        const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+        float u = uniform_from_word(draw(k0, k1, (uint32_t)v, (uint32_t)plan, step, S_VERIF_THETA, 0).x);
+        int theta = NTH - 1;
+        {
+            float cdf = 0.0f;
+            bool found = false;
+#pragma unroll
+            for (int kk = 0; kk < NTH; kk++)
+            {
+                cdf += bs.belief[kk];
+                if (!found && u <= cdf)
+                {
+                    theta = kk;
+                    found = true;
+                }
+            }
+        }
+        EnvNoise rng(k0, k1, (uint32_t)v, (uint32_t)plan << 16, step, S_VERIF_ENV);
+        int tOrigin = 0, tEnd = H;
+        bool failed = false;
+        for (int t = 0; t < H; t++)
+        {
+            // every thread takes this barrier once per step (H is uniform); it ends the
+            // loop once all samples of the CTA are done
+            if (!__syncthreads_or(active))
+                break;
+            if (!active)
+                continue;
+            rng.begin_step((uint32_t)t);
+            int local = t - tOrigin;
+            int b = bs.predTheta;
+            float e0 = sPlan[(b * T + local) * 2], e1 = sPlan[(b * T + local) * 2 + 1];
+            bool branched = false;
+            StepOut o = gateStep<NTH, true, true, false, false>(t, theta, sTrack, G, e0, e1, st, bs, branched, minConf, rng, gateMargin);
+            if (branched)
+                tOrigin = t + 1;
+            if (o.term == TERM_LOSE)
+            {
+                failed = true;
+                active = false;
+                tEnd = t;
+            }
+            else if (o.term == TERM_WIN || o.term == TERM_OPP_WIN)
+            {
+                active = false;
+                tEnd = t;
+            }
+        }
+        if (failed)
+            atomicAdd(&hist[tEnd], 1u);
+        if (threadIdx.x < tile.count)
+        {
+            if (dbgFailTime)
+                dbgFailTime[v] = failed ? tEnd : -1;
+            if (dbgTheta)
+                dbgTheta[v] = theta;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < T; i += blockDim.x)
+        if (hist[i])
+            atomicAdd(&D.fail[plan * T + i], hist[i]);
+}
+
+// One true-dynamics step (environmentStep with noise, as the engine's dynStep).
+template <int NTH>
+__global__ void gate_env_step_kernel(const GateParams* __restrict__ gp, const float* __restrict__ track, int trueTheta, float a0, float a1,
+                                     dr_gate_state* st, float* belief, int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term)
+{
+    __shared__ GateParams sG;
+    if (threadIdx.x == 0)
+    {
+        sG = *gp;
+        gateDeviceTerms(sG, *gp, 0, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x != 0)
+        return;
+    GState s;
+    loadGState(s, *st);
+    BState<NTH> bs;
+    for (int i = 0; i < NTH; i++)
+        bs.belief[i] = belief[i];
+    bs.predTheta = 0;
+    bs.branchingTime = -1;
+    EnvNoise rng(k0, k1, 0u, 0u, step, S_ENV_STEP);
+    rng.begin_step(0);
+    bool branched = false;
+    StepOut o;
+    if (updateBelief)
+        o = gateStep<NTH, true, false, false, true>(0, trueTheta, track, sG, a0, a1, s, bs, branched, 2.0f, rng, 0.0f);
+    else
+        o = gateStep<NTH, false, false, false, true>(0, trueTheta, track, sG, a0, a1, s, bs, branched, 2.0f, rng, 0.0f);
+    storeGState(*st, s);
+    for (int i = 0; i < NTH; i++)
+        belief[i] = bs.belief[i];
+    *term = o.term;
+}
+
+// ---------------------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------------------
+bool gateSupported(int nth)
+{
+    return nth == 1 || nth == 2 || nth == 4 || nth == 8;
+}
+
+size_t gateRolloutSmem(int nth, int T, int M, bool spl)
+{
+    return gateRolloutLayout(nth + 1, T, M, spl).total;
+}
+
+size_t gateVerifySmem(int nth, int T)
+{
+    return ga16(16 + sizeof(GateParams)) + GATE_TRACK_FLOATS * 4 + ga16((size_t)(nth + 1) * T * 2 * 4) + (size_t)T * 4;
+}
+
+int gateRolloutSamplesPerBlock(int nth)
+{
+    return GRB / nth;
+}
+
+template <int NTH> static cudaError_t launchGateRolloutT(const LaunchArgs& a, bool spl, size_t smem)
+{
+    if (spl)
+    {
+        auto k = gate_rollout<NTH, true>;
+        ensureSmem(k, smem);
+        k<<<a.nTiles, GRB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles);
+    }
+    else
+    {
+        auto k = gate_rollout<NTH, false>;
+        ensureSmem(k, smem);
+        k<<<a.nTiles, GRB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles);
+    }
+    return cudaGetLastError();
+}
+
+template <int NTH> static cudaError_t launchGateVerifyT(const LaunchArgs& a, size_t smem, int* ft, int* th)
+{
+    auto k = gate_verify<NTH>;
+    ensureSmem(k, smem);
+    k<<<a.nTiles, VERIFY_TILE, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, ft, th);
+    return cudaGetLastError();
+}
+
+cudaError_t launchGateRollout(const LaunchArgs& a, int nth, bool spl, size_t smem)
+{
+    switch (nth)
+    {
+    case 1: return launchGateRolloutT<1>(a, spl, smem);
+    case 2: return launchGateRolloutT<2>(a, spl, smem);
+    case 4: return launchGateRolloutT<4>(a, spl, smem);
+    case 8: return launchGateRolloutT<8>(a, spl, smem);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launchGateVerify(const LaunchArgs& a, int nth, size_t smem, int* dbgFailTime, int* dbgTheta)
+{
+    switch (nth)
+    {
+    case 1: return launchGateVerifyT<1>(a, smem, dbgFailTime, dbgTheta);
+    case 2: return launchGateVerifyT<2>(a, smem, dbgFailTime, dbgTheta);
+    case 4: return launchGateVerifyT<4>(a, smem, dbgFailTime, dbgTheta);
+    case 8: return launchGateVerifyT<8>(a, smem, dbgFailTime, dbgTheta);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launchGateEnvStep(cudaStream_t stream, int nth, const GateParams* gp, const float* track, int trueTheta, float a0, float a1,
+                              dr_gate_state* st, float* belief, int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term)
+{
+    switch (nth)
+    {
+    case 1: gate_env_step_kernel<1><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term); break;
+    case 2: gate_env_step_kernel<2><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term); break;
+    case 4: gate_env_step_kernel<4><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term); break;
+    case 8: gate_env_step_kernel<8><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+} // namespace dr

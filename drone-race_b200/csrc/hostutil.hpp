@@ -148,6 +148,97 @@ inline int checkEnv(const dr_env_config* env)
     return DR_OK;
 }
 
+// Gate race: validation of the C-ABI config (the reference checks the same counts
+// against its compile-time sizes when it unpacks them, env_dronerace.cpp:156-219).
+inline int checkGateEnv(const dr_gate_env_config* env)
+{
+    if (!env)
+        return fail(DR_ERR_INVALID_ARG, "env is NULL");
+    if (env->n_theta < 1 || env->n_theta > DR_MAX_THETA)
+        return fail(DR_ERR_INVALID_ARG, "n_theta must be in [1,8]");
+    if (env->n_gates < 1 || env->n_gates > DR_GATE_MAX_GATES)
+        return fail(DR_ERR_INVALID_ARG, "n_gates must be in [1,16]");
+    if (env->n_obstacles < 0 || env->n_obstacles > DR_GATE_MAX_OBSTACLES || env->n_round_obstacles < 0 ||
+        env->n_round_obstacles > DR_GATE_MAX_OBSTACLES)
+        return fail(DR_ERR_INVALID_ARG, "obstacle counts must be in [0,4]");
+    if (env->i_mppi < 0 || env->i_mppi >= DR_GATE_AGENTS)
+        return fail(DR_ERR_INVALID_ARG, "i_mppi must be 0 or 1");
+    if (!env->track_points)
+        return fail(DR_ERR_INVALID_ARG, "track_points must be given");
+    if (!(env->dt > 0.0f) || !std::isfinite(env->dt))
+        return fail(DR_ERR_INVALID_ARG, "dt must be positive and finite");
+    for (int th = 0; th < env->n_theta; th++)
+        if (env->opp_pid[th].raceline_index < 0 || env->opp_pid[th].raceline_index >= DR_GATE_RACELINES)
+            return fail(DR_ERR_INVALID_ARG, "raceline_index must be 0 or 1");
+    for (int i = 0; i < DR_GATE_RACELINES * NTS * 2; i++)
+        if (!std::isfinite(env->track_points[i]))
+            return fail(DR_ERR_INVALID_ARG, "track points must be finite");
+    return DR_OK;
+}
+
+inline GateParams toGateParams(const dr_gate_env_config& c)
+{
+    GateParams g{};
+    for (int d = 0; d < 2; d++)
+    {
+        g.arenaMin[d] = c.arena_min[d];
+        g.arenaMax[d] = c.arena_max[d];
+    }
+    g.dt = c.dt;
+    g.droneRadius = c.drone_radius;
+    g.posNoise = c.pos_noise_level;
+    g.speedNoise = c.speed_noise_level;
+    g.actionNoiseLevel = c.action_noise_level;
+    for (int a = 0; a < G_NA; a++)
+    {
+        g.maxSpeed[a] = c.max_speed[a];
+        g.maxAccel[a] = c.max_accel[a];
+    }
+    g.nWinLaps = c.n_win_laps;
+    g.targetDistance = c.target_distance;
+    g.nGates = c.n_gates;
+    g.nObs = c.n_obstacles;
+    g.nRound = c.n_round_obstacles;
+    g.iMppi = c.i_mppi;
+    for (int i = 0; i < G_MAXG * 2; i++)
+    {
+        g.gateCenters[i] = c.gate_centers[i];
+        g.gateVectors[i] = c.gate_vectors[i];
+    }
+    for (int i = 0; i < G_MAXG; i++)
+        g.gateRadius[i] = c.gate_radius[i];
+    for (int i = 0; i < G_MAXO * 4; i++)
+        g.obstacles[i] = c.obstacles[i];
+    for (int i = 0; i < G_MAXO * 2; i++)
+        g.roundCenters[i] = c.round_obs_centers[i];
+    for (int i = 0; i < G_MAXO; i++)
+        g.roundRadius[i] = c.round_obs_radius[i];
+    for (int th = 0; th < DR_MAX_THETA; th++)
+    {
+        const dr_pid_config& p = c.opp_pid[th];
+        g.pidKp[th] = p.kp;
+        g.pidKd[th] = p.kd;
+        g.pidRepF[th] = p.repulsion_factor;
+        g.pidRepP[th] = p.repulsion_power;
+        g.pidRepD[th] = p.repulsion_dist_fact;
+        g.pidRaceline[th] = p.raceline_index;
+        g.pidNoise[th] = p.action_noise;
+    }
+    return g;
+}
+
+// racelines plus the sample the reference reads when s wraps to exactly 1.0f
+inline std::vector<float> packGateTrack(const dr_gate_env_config& c)
+{
+    std::vector<float> t(GATE_TRACK_FLOATS, 0.0f);
+    const size_t n = (size_t)G_NR * NTS * 2;
+    for (size_t i = 0; i < n; i++)
+        t[i] = c.track_points[i];
+    t[n] = c.track_points[(size_t)(G_NR - 1) * NTS * 2];
+    t[n + 1] = c.track_points[(size_t)(G_NR - 1) * NTS * 2 + 1];
+    return t;
+}
+
 inline int selectDevice(int device)
 {
     int n = 0;

@@ -6,6 +6,7 @@
 #include <cstdint>
 
 #include "../../include/drmppi.h"
+#include "gate_model.cuh"
 #include "model.cuh"
 
 namespace dr
@@ -16,6 +17,7 @@ struct MppiCfgDev
     int K, T, M, useSplines, V, H, nth, nopp;
     int knots[DR_MAX_KNOTS];
     float sigma0, sigma1, minConf;
+    float gateMargin; // gateTraversalMargin (gate race)
     MppiCostW w;
     uint32_t k0, k1; // Philox key (seed)
 };
@@ -23,7 +25,11 @@ struct MppiCfgDev
 // Per-step input of an MPPI instance (one H2D copy per step for the whole batch).
 struct MppiIn
 {
-    dr_sim_state state;
+    union
+    {
+        dr_sim_state state;   // strategic race
+        dr_gate_state gstate; // gate race
+    };
     float belief[DR_MAX_THETA];
     float lambda;      // inv_temperature of this step
     uint32_t step;     // Philox counter word
@@ -36,9 +42,11 @@ struct MppiIn
 //   fail[2][T] u32 | dense[nbp][T][2] | prevDense[nbp][T][2] | nu[nbp] | minCosts[nbp][M] | stats[4] i32
 struct MppiDev
 {
-    EnvParams env;
+    EnvParams env;       // strategic race (for the gate race only maxAccel[0], the ego's, is set)
     MppiCfgDev cfg;
-    const float* grids;  // GRID_FLOATS, 16-byte aligned
+    const float* grids;  // GRID_FLOATS, 16-byte aligned (strategic race)
+    const GateParams* gate; // gate race: parameters and racelines (GATE_TRACK_FLOATS), else null
+    const float* gtrack;
     const float* B;      // [T][M] (spline mode)
     float* knots;        // [nbp][M][2] optimised sequence (dense mode: M == T)
     float* costsTrue;    // [nth][K]

@@ -276,3 +276,151 @@ def robust_race(agent: int = 0, seed: int = 0, K: int = 2048, T: int = 64, P: in
     sc = Scenario(env=env, grids=grids, state=st, seed=seed * 1000 + agent, name="robust_race")
     sc.prmppi = make_prmppi(K=K, T=T, P=P, inv_temperature=1.0, sampling_noise=1.0)
     return sc
+
+
+# ==== gate race (the reference's EnvDroneRace) ==========================================
+
+@dataclass
+class GateScenario:
+    """A gate-race environment (C-ABI struct) with the racelines it points to."""
+
+    env: abi.dr_gate_env_config
+    track: np.ndarray  # (DR_GATE_RACELINES, 512, 2) float32, referenced by env.track_points
+    state: abi.dr_gate_state
+    mppi: abi.dr_mppi_config | None = None
+    true_theta: int = 0
+    seed: int = 42
+    name: str = ""
+
+    @property
+    def n_theta(self) -> int:
+        return int(self.env.n_theta)
+
+    def belief(self) -> np.ndarray:
+        return np.array(self.env.init_belief[: self.n_theta], dtype=np.float32)
+
+
+def pid_config(kp: float = 5.0, kd: float = 20.0, repulsion_factor: float = 0.0, repulsion_power: float = 2.0, repulsion_dist_fact: float = 10.0,
+               raceline_index: int = 0, action_noise: float = 0.0) -> abi.dr_pid_config:
+    """PIDConfig (env_dronerace_defs.h:44-56); defaults of python-src/main.py:65-66."""
+    p = abi.dr_pid_config()
+    p.kp, p.kd = kp, kd
+    p.repulsion_factor, p.repulsion_power, p.repulsion_dist_fact = repulsion_factor, repulsion_power, repulsion_dist_fact
+    p.raceline_index = raceline_index
+    p.action_noise = action_noise
+    return p
+
+
+def ellipse_racelines(a: float = 15.0, b: float = 10.0, offsets=(-0.6, 0.6), n: int = abi.DR_N_TRACK_SAMPLES) -> np.ndarray:
+    """Racelines parallel to an a x b ellipse (semi-axes), offset along its outward
+    normal, sampled at n equal parameter steps counter-clockwise: (len(offsets), n, 2)."""
+    u = np.arange(n) * (2 * np.pi / n)
+    c = np.stack([a * np.cos(u), b * np.sin(u)], axis=1)
+    t = np.stack([-a * np.sin(u), b * np.cos(u)], axis=1)
+    t /= np.linalg.norm(t, axis=1, keepdims=True)
+    nrm = np.stack([t[:, 1], -t[:, 0]], axis=1)  # outward for a counter-clockwise loop
+    return np.stack([c + o * nrm for o in offsets]).astype(np.float32)
+
+
+def ellipse_gates(n_gates: int, a: float = 15.0, b: float = 10.0, radius: float = 1.5, seed: int | None = None):
+    """n_gates gates on an a x b ellipse, facing along the race direction (counter-
+    clockwise), at equal parameter steps (uniform random angles, sorted, when seeded)."""
+    if seed is None:
+        u = np.arange(n_gates) * (2 * np.pi / n_gates)
+    else:
+        u = np.sort(np.random.default_rng(seed).uniform(0, 2 * np.pi, n_gates))
+    centers = np.stack([a * np.cos(u), b * np.sin(u)], axis=1)
+    vec = np.stack([-a * np.sin(u), b * np.cos(u)], axis=1)
+    vec /= np.linalg.norm(vec, axis=1, keepdims=True)
+    return centers.astype(np.float32), vec.astype(np.float32), np.full(n_gates, radius, np.float32)
+
+
+def make_gate_env(track: np.ndarray, centers, vectors, radius, pids: list, *, dt: float, drone_radius: float, max_speed, max_accel,
+                  target_distance: float = 0.05, n_win_laps: int = 1, init_belief=None, i_mppi: int = 0, arena_margin: float = 3.0,
+                  pos_noise: float = 0.0, speed_noise: float = 0.0, action_noise: float = 0.0, round_obstacles=(), rect_obstacles=()) -> abi.dr_gate_env_config:
+    """EnvironmentConfig of the gate race (env_dronerace_defs.h:60-93)."""
+    e = abi.dr_gate_env_config()
+    n_theta = len(pids)
+    e.n_theta = n_theta
+    lo = track.reshape(-1, 2).min(axis=0) - arena_margin
+    hi = track.reshape(-1, 2).max(axis=0) + arena_margin
+    for d in range(2):
+        e.arena_min[d] = float(lo[d])
+        e.arena_max[d] = float(hi[d])
+    e.dt = dt
+    e.send_states = 1
+    e.drone_radius = drone_radius
+    e.pos_noise_level, e.speed_noise_level, e.action_noise_level = pos_noise, speed_noise, action_noise
+    for a in range(2):
+        e.max_speed[a] = float(max_speed[a])
+        e.max_accel[a] = float(max_accel[a])
+    e.n_win_laps = n_win_laps
+    e.target_distance = target_distance
+    e.n_gates = len(centers)
+    for g in range(len(centers)):
+        for d in range(2):
+            e.gate_centers[2 * g + d] = float(centers[g][d])
+            e.gate_vectors[2 * g + d] = float(vectors[g][d])
+        e.gate_radius[g] = float(radius[g])
+    e.n_round_obstacles = len(round_obstacles)
+    for i, (cx, cy, rr) in enumerate(round_obstacles):
+        e.round_obs_centers[2 * i], e.round_obs_centers[2 * i + 1], e.round_obs_radius[i] = cx, cy, rr
+    e.n_obstacles = len(rect_obstacles)
+    for i, box in enumerate(rect_obstacles):
+        for j in range(4):
+            e.obstacles[4 * i + j] = float(box[j])
+    e.track_points = abi.fptr(track)
+    if init_belief is None:
+        init_belief = np.full(n_theta, 1.0 / n_theta)
+    for th in range(n_theta):
+        e.init_belief[th] = float(np.float32(init_belief[th]))
+        e.opp_pid[th] = pids[th]
+    e.i_mppi = i_mppi
+    return e
+
+
+def gate_state(track: np.ndarray, start_u: list[float], i_mppi: int, gates: list[int], speed: float = 0.0) -> abi.dr_gate_state:
+    """Both agents on raceline 0 at the given fractions of a lap, moving along it at
+    `speed`; each opponent's S on every raceline is its fraction of a lap, the ego's is
+    -1 (untracked, as env_dronerace.cpp:96-97 loads it)."""
+    s = abi.dr_gate_state()
+    n = track.shape[1]
+    for a in range(2):
+        i = int(round(start_u[a] * n)) % n
+        p = track[0, i]
+        q = track[0, (i + 1) % n] - track[0, i - 1]
+        q = q / np.linalg.norm(q)
+        s.pos[2 * a], s.pos[2 * a + 1] = float(p[0]), float(p[1])
+        s.vel[2 * a], s.vel[2 * a + 1] = float(speed * q[0]), float(speed * q[1])
+        for r in range(abi.DR_GATE_RACELINES):
+            s.S[a * abi.DR_GATE_RACELINES + r] = -1.0 if a == i_mppi else float(np.float32(i / n))
+        s.laps[a] = 0
+        s.gates[a] = gates[a]
+    return s
+
+
+def gate_race(agent: int = 0, seed: int = 0, K: int = 4096, T: int = 64, use_splines: bool = False, n_verif: int = 2**17, n_gates: int = 2,
+              action_noise: float = 0.5, i_mppi: int = 0) -> GateScenario:
+    """Gate race on a 30 x 20 m ellipse: n_gates gates of radius 1.5 m facing the race
+    direction, two racelines 0.6 m inside and outside the ellipse, one PID opponent whose
+    hypotheses follow either raceline (kp 5, kd 20, python-src/main.py:65-66), drone
+    radius 0.5, dt 0.02; the MPPI settings of tinyGateEnv (main.py:140-189). The agents
+    start a metre or two apart just past a gate (the opponent ahead), so a lap is the
+    whole loop; `agent` shifts the start around the loop."""
+    track = ellipse_racelines()
+    centers, vectors, radius = ellipse_gates(n_gates)
+    pids = [pid_config(raceline_index=0, action_noise=action_noise), pid_config(raceline_index=1, action_noise=action_noise)]
+    env = make_gate_env(track, centers, vectors, radius, pids, dt=0.02, drone_radius=0.5, max_speed=[6.0, 4.0], max_accel=[6.0, 6.0],
+                        target_distance=0.05, i_mppi=i_mppi)
+    shift = 0.37 * agent
+    ego_u, opp_u = (0.01 + shift) % 1.0, (0.035 + shift) % 1.0
+    # gates[a]: last gate passed; the next one is the first gate ahead of the start
+    next_gate = int(np.searchsorted(np.arange(n_gates) / n_gates, (ego_u + 1e-9) % 1.0)) % n_gates
+    last = (next_gate - 1) % n_gates
+    start = [ego_u, opp_u] if i_mppi == 0 else [opp_u, ego_u]
+    st = gate_state(track, start, i_mppi, [last, last], speed=2.0)
+    sc = GateScenario(env=env, track=track, state=st, seed=seed * 1000 + agent, name="gate_race")
+    sc.mppi = make_mppi(K=K, T=T, use_splines=use_splines, M=min(10, max(2, (T - 2) // 2)), inv_temperature=10.0, sampling_noise=2.0,
+                        coll_dist_factor=1.1, final_adv_weight=200.0, boundary_cost=0.0, boundary_threshold_factor=1.7, outside_cost=1e6, win_cost=1e6,
+                        opp_win_cost=1e5, n_verif_samples=n_verif, verif_horizon=min(40, T), gate_traversal_margin=0.9)
+    return sc

@@ -329,6 +329,96 @@ int dr_spline_matrix(int T, int M, const int32_t* knots, float* out);
 int dr_env_step(const dr_env_config* env, int true_theta, const float* action, dr_sim_state* state, float* belief, int update_belief,
                 uint64_t seed, uint64_t step, int* term);
 
+/* ==== gate race (the reference's EnvDroneRace, include/environments/env_dronerace.h) ====
+ * Two agents (the MPPI ego at index i_mppi, one PID opponent), gates crossed in order,
+ * laps counted at the last gate, PID opponents following racelines. The reference fixes
+ * N_GATES, N_RACELINES and the obstacle counts at compile time (env_dronerace_defs.h:
+ * 2 gates, 2 racelines, no obstacles); here gates and obstacles are runtime counts up to
+ * the maxima below, the racelines stay 2. */
+#define DR_GATE_AGENTS 2        /* reference EnvDroneRace::N_AGENTS (env_dronerace_defs.h:8) */
+#define DR_GATE_RACELINES 2     /* reference N_RACELINES (env_dronerace_defs.h:17); fixed */
+#define DR_GATE_MAX_GATES 16
+#define DR_GATE_MAX_OBSTACLES 4 /* rectangle and round obstacles each */
+
+/* Opponent PID controller (reference PIDConfig, env_dronerace_defs.h:44-56; wire order of
+ * env_dronerace.cpp:104-121). */
+typedef struct dr_pid_config
+{
+    float kp;
+    float kd;
+    float repulsion_factor;
+    float repulsion_power;
+    float repulsion_dist_fact;
+    int32_t raceline_index;
+    float action_noise;
+} dr_pid_config;
+
+/* Gate-race environment (reference EnvDroneRace::EnvironmentConfig,
+ * env_dronerace_defs.h:60-93). track_points is a HOST pointer to
+ * DR_GATE_RACELINES x DR_N_TRACK_SAMPLES x 2 floats (the racelines, one after the other). */
+typedef struct dr_gate_env_config
+{
+    int32_t n_theta;            /* PID hypotheses (reference N_TRUE_MODELS) */
+    float arena_min[DR_DIM];
+    float arena_max[DR_DIM];
+    float dt;
+    int32_t send_states;
+    float drone_radius;
+    float pos_noise_level;
+    float speed_noise_level;
+    float action_noise_level;
+    float max_speed[DR_GATE_AGENTS];
+    float max_accel[DR_GATE_AGENTS];
+    int32_t n_win_laps;
+    float target_distance;      /* PID look-ahead along the raceline (fraction of a lap) */
+    int32_t n_gates;
+    float gate_centers[DR_GATE_MAX_GATES * DR_DIM];
+    float gate_vectors[DR_GATE_MAX_GATES * DR_DIM];
+    float gate_radius[DR_GATE_MAX_GATES];
+    int32_t n_obstacles;        /* rectangles [xmin, ymin, xmax, ymax] */
+    float obstacles[DR_GATE_MAX_OBSTACLES * DR_DIM * 2];
+    int32_t n_round_obstacles;
+    float round_obs_centers[DR_GATE_MAX_OBSTACLES * DR_DIM];
+    float round_obs_radius[DR_GATE_MAX_OBSTACLES];
+    const float* track_points;  /* host, [DR_GATE_RACELINES][DR_N_TRACK_SAMPLES][2] */
+    float init_belief[DR_MAX_THETA];
+    dr_pid_config opp_pid[DR_MAX_THETA];
+    int32_t i_mppi;             /* index of the ego agent (0 or 1) */
+} dr_gate_env_config;
+
+/* Gate-race state (reference EnvDroneRace::SimState, env_dronerace_defs.h:95-103).
+ * S[agent * DR_GATE_RACELINES + r] is the arc-length fraction on raceline r; a negative
+ * S of an agent means "not tracked" (the reference sets the ego's to -1 on load,
+ * env_dronerace.cpp:96-97, and never projects it). */
+typedef struct dr_gate_state
+{
+    float pos[DR_GATE_AGENTS * DR_DIM];
+    float vel[DR_GATE_AGENTS * DR_DIM];
+    float S[DR_GATE_AGENTS * DR_GATE_RACELINES];
+    int32_t laps[DR_GATE_AGENTS];
+    int32_t gates[DR_GATE_AGENTS];
+} dr_gate_state;
+
+/* An MPPI controller on the gate race (the reference's MPPIController compiled with
+ * USE_ENV_DRONERACE). The handle is a dr_mppi: destroy, nominals, knots, fail counts,
+ * temperature, profiling and batching work as for the strategic race; a batch holds
+ * controllers of one environment kind (for a gate-race batch, dr_mppi_batch_step_dev
+ * takes dr_gate_state records). Step it with dr_gate_mppi_step. */
+int dr_gate_mppi_create(const dr_gate_env_config* env, const dr_mppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
+                        dr_mppi** out);
+/* MPPIController::getControl (src/mppi_controller.cu:250-466) on the gate race. */
+int dr_gate_mppi_step(dr_mppi* h, const dr_gate_state* state, const float* belief, float* out_action, dr_mppi_info* info);
+int dr_gate_mppi_batch_step(dr_mppi_batch* b, const dr_gate_state* states, const float* beliefs, float* out_actions, dr_mppi_info* infos);
+/* Test hooks, as dr_mppi_debug_rollout / dr_mppi_debug_verify (same outputs). */
+int dr_gate_mppi_debug_rollout(dr_mppi* h, const dr_gate_state* state, const float* belief, float* costs_true, int32_t* branch_used,
+                               int32_t* branch_time, float* costs);
+int dr_gate_mppi_debug_verify(dr_mppi* h, const dr_gate_state* state, const float* belief, const float* dense_plan, int plan,
+                              uint32_t* fail_counts, int32_t* fail_time, int32_t* theta);
+/* One gate-race environment step on the device (environmentStep, env_dronerace.h:
+ * 546-680, with noise on, as the engine's dynStep), like dr_env_step. */
+int dr_gate_env_step(const dr_gate_env_config* env, int true_theta, const float* action, dr_gate_state* state, float* belief, int update_belief,
+                     uint64_t seed, uint64_t step, int* term);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,7 @@ def port() -> C.CDLL:
         P = C.POINTER
         f, d, i, u = P(C.c_float), P(C.c_double), P(C.c_int32), P(C.c_uint32)
         E, M, PR, S = P(a.dr_env_config), P(a.dr_mppi_config), P(a.dr_prmppi_config), P(a.dr_sim_state)
+        GE, GS = P(a.dr_gate_env_config), P(a.dr_gate_state)
         u64 = C.c_uint64
         protos = {
             "orc_mppi_noise": (None, [u64, u64, C.c_int, C.c_int, C.c_int, f, f]),
@@ -77,6 +78,12 @@ def port() -> C.CDLL:
             "orc_pr_candidates": (C.c_int, [C.c_int, E, PR, S, d, d, i, u64, u64, C.c_int, d, d]),
             "orc_env_step": (C.c_int, [C.c_int, E, C.c_int, f, S, f, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, u64, u64, C.c_int]),
             "orc_costs": (None, [E, M, PR, S, f]),
+            "orc_gate_rollout": (C.c_int, [C.c_int, GE, M, GS, f, f, f, f, u64, u64, d, i, i]),
+            "orc_gate_update": (C.c_int, [C.c_int, GE, M, f, d, i, i, f, f, d, d, d, d, d, C.c_int]),
+            "orc_gate_verify": (C.c_int, [C.c_int, GE, M, GS, f, d, u64, u64, C.c_int, u, i, i]),
+            "orc_gate_env_step": (C.c_int, [C.c_int, GE, C.c_int, f, GS, f, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_int, C.c_int, u64, u64,
+                                            C.c_int]),
+            "orc_gate_costs": (None, [GE, M, GS, f]),
         }
         for n, (r, args) in protos.items():
             fn = getattr(L, n)
@@ -93,6 +100,11 @@ def ref_variant_name(n_theta: int, use_splines: bool) -> str:
     return f"nth{n_theta}_{'spline' if use_splines else 'dense'}"
 
 
+def gate_variant_name(use_splines: bool) -> str:
+    """The reference compiled for the gate race (EnvDroneRace, N_TRUE_MODELS = 2)."""
+    return f"gate_{'spline' if use_splines else 'dense'}"
+
+
 def ref_available(variant: str) -> bool:
     return (REF_DIR / f"libref_{variant}.so").exists()
 
@@ -104,6 +116,8 @@ def ref(variant: str) -> C.CDLL:
         P = C.POINTER
         f, d, i, u = P(C.c_float), P(C.c_double), P(C.c_int32), P(C.c_uint32)
         E, M, PR, S = P(a.dr_env_config), P(a.dr_mppi_config), P(a.dr_prmppi_config), P(a.dr_sim_state)
+        if variant.startswith("gate_"):  # the same entry points on the gate race's structs
+            E, S = P(a.dr_gate_env_config), P(a.dr_gate_state)
         u64, I = C.c_uint64, C.c_int
         protos = {
             "ref_n_theta": (I, []),
@@ -154,6 +168,39 @@ def _i(a):
 
 def _u(a):
     return _types().uptr(a)
+
+
+def _gate(sc) -> bool:
+    """A gate-race scenario (its env is a dr_gate_env_config)."""
+    return isinstance(sc.env, _types().dr_gate_env_config)
+
+
+def gate_env_step(sc, true_theta, action, state, belief, update_belief=True, consider_branching=False, min_confidence=2.0, add_margin=False,
+                  gate_margin=0.0, lose_on_opp_win=True, apply_noise=True, step=0, t=0, prec=32, impl="port"):
+    """One gate-race environmentStep on a copy of `state`; returns (term, state', belief')."""
+    a = _types()
+    st = a.dr_gate_state.from_buffer_copy(state)
+    bel = np.zeros(a.DR_MAX_THETA, np.float32)
+    bel[: sc.n_theta] = belief
+    act = np.ascontiguousarray(action, np.float32)
+    if impl == "port":
+        term = port().orc_gate_env_step(prec, C.byref(sc.env), true_theta, _f(act), C.byref(st), _f(bel), int(update_belief), int(consider_branching),
+                                        min_confidence, int(add_margin), gate_margin, int(lose_on_opp_win), int(apply_noise), sc.seed, step, t)
+    else:
+        term = ref(impl).refh_env_step(C.byref(sc.env), true_theta, _f(act), C.byref(st), _f(bel), int(update_belief), int(consider_branching),
+                                       min_confidence, int(lose_on_opp_win), int(apply_noise), sc.seed, step, t)
+    return term, st, bel[: sc.n_theta].copy()
+
+
+def gate_costs(sc, state, impl="port") -> np.ndarray:
+    """(stateCost, finalCost) of a gate-race state."""
+    out = np.zeros(4, np.float32)
+    if impl == "port":
+        port().orc_gate_costs(C.byref(sc.env), C.byref(sc.mppi), C.byref(state), _f(out))
+        return out[:2]
+    pc = _types().dr_prmppi_config()
+    ref(impl).refh_costs(C.byref(sc.env), C.byref(sc.mppi), C.byref(pc), C.byref(state), _f(out))
+    return np.array([out[0], out[3]], np.float32)
 
 
 def nbp(sc) -> int:
@@ -211,8 +258,8 @@ def mppi_rollout(sc, belief, nominal, noise, B, step, prec=32, impl="port", nthr
     noise = np.ascontiguousarray(noise, np.float32)
     Bm = np.ascontiguousarray(B if B is not None else np.zeros(1), np.float32)
     if impl == "port":
-        rc = port().orc_mppi_rollout(prec, C.byref(sc.env), C.byref(c), C.byref(sc.state), _f(belief), _f(nominal), _f(noise), _f(Bm), sc.seed, step,
-                                     _d(ct), _i(bu), _i(bt))
+        fn = port().orc_gate_rollout if _gate(sc) else port().orc_mppi_rollout
+        rc = fn(prec, C.byref(sc.env), C.byref(c), C.byref(sc.state), _f(belief), _f(nominal), _f(noise), _f(Bm), sc.seed, step, _d(ct), _i(bu), _i(bt))
     else:
         rc = ref(impl).refh_mppi_rollout(C.byref(sc.env), C.byref(c), C.byref(sc.state), _f(belief), _f(nominal), _f(noise), _f(Bm), sc.seed, step,
                                          _d(ct), _i(bu), _i(bt), nthreads or os.cpu_count())
@@ -232,8 +279,9 @@ def mppi_update(sc, belief, ct, bu, bt, noise, B, knots, prec=32, impl="port", b
         mins = np.zeros((n, M), np.float64)
         nu = np.zeros(n, np.float64)
         costs = np.zeros((n, K), np.float64)
-        port().orc_mppi_update(prec, C.byref(sc.env), C.byref(c), _f(belief), _d(np.ascontiguousarray(ct, np.float64)), _i(bu), _i(bt),
-                               _f(np.ascontiguousarray(noise, np.float32)), _f(Bm), _d(kn), _d(dense), _d(mins), _d(nu), _d(costs), blockorder)
+        fn = port().orc_gate_update if _gate(sc) else port().orc_mppi_update
+        fn(prec, C.byref(sc.env), C.byref(c), _f(belief), _d(np.ascontiguousarray(ct, np.float64)), _i(bu), _i(bt), _f(np.ascontiguousarray(noise, np.float32)),
+           _f(Bm), _d(kn), _d(dense), _d(mins), _d(nu), _d(costs), blockorder)
     else:
         kn = np.ascontiguousarray(knots, np.float32).copy()
         dense = np.zeros((n, T, 2), np.float32)
@@ -254,8 +302,9 @@ def mppi_verify(sc, belief, plan, step, plan_id, prec=32, impl="port", nthreads=
     belief = np.ascontiguousarray(belief, np.float32)
     if impl == "port":
         th = np.zeros(c.n_verif_samples, np.int32)
-        port().orc_mppi_verify(prec, C.byref(sc.env), C.byref(c), C.byref(sc.state), _f(belief), _d(np.ascontiguousarray(plan, np.float64)), sc.seed,
-                               step, plan_id, _u(fc), _i(ft), _i(th))
+        fn = port().orc_gate_verify if _gate(sc) else port().orc_mppi_verify
+        fn(prec, C.byref(sc.env), C.byref(c), C.byref(sc.state), _f(belief), _d(np.ascontiguousarray(plan, np.float64)), sc.seed, step, plan_id, _u(fc),
+           _i(ft), _i(th))
         return fc, ft, th
     rc = ref(impl).refh_mppi_verify(C.byref(sc.env), C.byref(c), C.byref(sc.state), _f(belief), _f(np.ascontiguousarray(plan, np.float32)), sc.seed,
                                     step, plan_id, _u(fc), _i(ft), nthreads or os.cpu_count())

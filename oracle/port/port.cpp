@@ -17,6 +17,7 @@
 
 #include <boost/math/distributions/beta.hpp> // oracle/stubs (boost is absent here)
 
+#include "gate_model.hpp"
 #include "model.hpp"
 
 using namespace orc;
@@ -41,19 +42,19 @@ inline int mk(const dr_mppi_config& c)
     return c.use_splines ? c.n_knots : c.n_timesteps;
 }
 
-// fullRolloutKernel, src/kernels.cu:34-171 (one loop iteration per thread s).
-template <typename R>
-void mppiRollout(const dr_env_config& ec, const dr_mppi_config& mc, const dr_sim_state& s0, const float* belief0, const float* nominal,
-                 const float* noise, const float* B, uint64_t seed, uint64_t step, double* costsTrue, int* branchUsed, int* branchTime)
+// fullRolloutKernel, src/kernels.cu:34-171 (one loop iteration per thread s), for either
+// model: EnvT / StateT are Env / State of model.hpp or of gate_model.hpp, whose
+// environmentStep, stateCost and finalCost are found by argument-dependent lookup.
+template <typename R, typename EnvT, typename StateT, typename FlagsT, typename S0>
+void mppiRolloutT(const EnvT& env, const FlagsT& flags, const dr_mppi_config& mc, const S0& s0, const float* belief0, const float* nominal,
+                  const float* noise, const float* B, uint64_t seed, uint64_t step, double* costsTrue, int* branchUsed, int* branchTime)
 {
-    Env<R> env(ec);
-    const int K = mc.n_samples, T = mc.n_timesteps, M = mk(mc), nth = ec.n_theta;
+    const int K = mc.n_samples, T = mc.n_timesteps, M = mk(mc), nth = env.nth;
     const R minConf = mc.min_confidence;
     MppiCosts<R> cc = mppiCosts<R>(mc);
     R initBelief[DR_MAX_THETA];
     for (int th = 0; th < nth; th++)
         initBelief[th] = belief0[th];
-    const StepFlags flags{true, true, true, true, true};
 
 #pragma omp parallel for schedule(dynamic, 16)
     for (int s = 0; s < K; s++)
@@ -70,7 +71,7 @@ void mppiRollout(const dr_env_config& ec, const dr_mppi_config& mc, const dr_sim
         {
             if (!branchCompatibleWithModel(first.predTheta, th))
                 continue;
-            State<R> st = State<R>::from(s0);
+            StateT st = StateT::from(s0);
             Branch<R> bs = first;
             R cost = R(0);
             bool stop = false;
@@ -121,6 +122,25 @@ void mppiRollout(const dr_env_config& ec, const dr_mppi_config& mc, const dr_sim
     }
 }
 
+template <typename R>
+void mppiRollout(const dr_env_config& ec, const dr_mppi_config& mc, const dr_sim_state& s0, const float* belief0, const float* nominal,
+                 const float* noise, const float* B, uint64_t seed, uint64_t step, double* costsTrue, int* branchUsed, int* branchTime)
+{
+    Env<R> env(ec);
+    const StepFlags flags{true, true, true, true, true};
+    mppiRolloutT<R, Env<R>, State<R>>(env, flags, mc, s0, belief0, nominal, noise, B, seed, step, costsTrue, branchUsed, branchTime);
+}
+
+// the gate race: environmentStep<true, true, false> (kernels.cu:141-143; addMargin off)
+template <typename R>
+void gateRollout(const dr_gate_env_config& ec, const dr_mppi_config& mc, const dr_gate_state& s0, const float* belief0, const float* nominal,
+                 const float* noise, const float* B, uint64_t seed, uint64_t step, double* costsTrue, int* branchUsed, int* branchTime)
+{
+    gate::Env<R> env(ec);
+    const gate::Flags flags{true, true, false, true, true, mc.gate_traversal_margin};
+    mppiRolloutT<R, gate::Env<R>, gate::State<R>>(env, flags, mc, s0, belief0, nominal, noise, B, seed, step, costsTrue, branchUsed, branchTime);
+}
+
 // coefficient of sample s for (branch plan b, knot/timestep k): kernels.cu:252-279
 template <typename R>
 R sampleCoeff(const dr_mppi_config& mc, int nth, const R* belief, int b, int k, int s, int K, const int* branchUsed, const int* branchTime)
@@ -148,11 +168,11 @@ R sampleCoeff(const dr_mppi_config& mc, int nth, const R* belief, int b, int k, 
 // (mppi_controller.cu:299-345). blockorder != 0 sums the weighted average the way a
 // 256-thread block does (strided partials, then a halving tree).
 template <typename R>
-void mppiUpdate(const dr_env_config& ec, const dr_mppi_config& mc, const float* belief0, const double* costsTrueIn, const int* branchUsed,
+void mppiUpdate(int nth, float maxAccelEgo, const dr_mppi_config& mc, const float* belief0, const double* costsTrueIn, const int* branchUsed,
                 const int* branchTime, const float* noise, const float* B, double* knotsIO, double* denseOut, double* minCostsOut, double* nuOut,
                 double* costsOut, int blockorder)
 {
-    const int K = mc.n_samples, T = mc.n_timesteps, M = mk(mc), nth = ec.n_theta, nbp = nth + 1;
+    const int K = mc.n_samples, T = mc.n_timesteps, M = mk(mc), nbp = nth + 1;
     R belief[DR_MAX_THETA];
     for (int th = 0; th < nth; th++)
         belief[th] = belief0[th];
@@ -260,7 +280,7 @@ void mppiUpdate(const dr_env_config& ec, const dr_mppi_config& mc, const float* 
                     dense[(b * T + t) * DIM + d] = sum;
                 }
     // clamp (knots in spline mode, the dense nominal otherwise)
-    const R maxAccel = ec.max_accel[0];
+    const R maxAccel = maxAccelEgo; // Env::getMaxAccel (mppi_controller.cu:345)
     for (int v = 0; v < nbp * M; v++)
     {
         R sq = R(0);
@@ -295,13 +315,12 @@ template <typename R> int sampleModel(const R* belief, int nth, float u)
     return nth - 1;
 }
 
-// verifyNominalFailureKernel, src/kernels.cu:488-551.
-template <typename R>
-void mppiVerify(const dr_env_config& ec, const dr_mppi_config& mc, const dr_sim_state& s0, const float* belief0, const double* plan, uint64_t seed,
-                uint64_t step, int planId, unsigned* failCount, int* failTime, int* thetasOut)
+// verifyNominalFailureKernel, src/kernels.cu:488-551, for either model (as mppiRolloutT).
+template <typename R, typename EnvT, typename StateT, typename FlagsT, typename S0>
+void mppiVerifyT(const EnvT& env, const FlagsT& flags, const dr_mppi_config& mc, const S0& s0, const float* belief0, const double* plan, uint64_t seed,
+                 uint64_t step, int planId, unsigned* failCount, int* failTime, int* thetasOut)
 {
-    Env<R> env(ec);
-    const int V = mc.n_verif_samples, T = mc.n_timesteps, H = mc.verif_horizon, nth = ec.n_theta;
+    const int V = mc.n_verif_samples, T = mc.n_timesteps, H = mc.verif_horizon, nth = env.nth;
     const R minConf = mc.min_confidence;
     R initBelief[DR_MAX_THETA];
     for (int th = 0; th < nth; th++)
@@ -309,13 +328,12 @@ void mppiVerify(const dr_env_config& ec, const dr_mppi_config& mc, const dr_sim_
     std::vector<R> nominal((size_t)(nth + 1) * T * DIM);
     for (size_t i = 0; i < nominal.size(); i++)
         nominal[i] = (R)plan[i];
-    const StepFlags flags{true, true, false, true, true};
     const Key key(seed);
     std::vector<int> ft(V, -1);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int v = 0; v < V; v++)
     {
-        State<R> st = State<R>::from(s0);
+        StateT st = StateT::from(s0);
         Branch<R> bs;
         initBranchState(bs, initBelief, nth, minConf);
         float u = uniform_from_word(draw(key, (uint32_t)v, (uint32_t)planId, step, S_VERIF_THETA, 0).v[0]);
@@ -357,6 +375,25 @@ void mppiVerify(const dr_env_config& ec, const dr_mppi_config& mc, const dr_sim_
         if (failTime)
             failTime[v] = ft[v];
     }
+}
+
+template <typename R>
+void mppiVerify(const dr_env_config& ec, const dr_mppi_config& mc, const dr_sim_state& s0, const float* belief0, const double* plan, uint64_t seed,
+                uint64_t step, int planId, unsigned* failCount, int* failTime, int* thetasOut)
+{
+    Env<R> env(ec);
+    const StepFlags flags{true, true, false, true, true};
+    mppiVerifyT<R, Env<R>, State<R>>(env, flags, mc, s0, belief0, plan, seed, step, planId, failCount, failTime, thetasOut);
+}
+
+// the gate race: environmentStep<true, true, false, false> (kernels.cu:529-531)
+template <typename R>
+void gateVerify(const dr_gate_env_config& ec, const dr_mppi_config& mc, const dr_gate_state& s0, const float* belief0, const double* plan,
+                uint64_t seed, uint64_t step, int planId, unsigned* failCount, int* failTime, int* thetasOut)
+{
+    gate::Env<R> env(ec);
+    const gate::Flags flags{true, true, false, false, true, mc.gate_traversal_margin};
+    mppiVerifyT<R, gate::Env<R>, gate::State<R>>(env, flags, mc, s0, belief0, plan, seed, step, planId, failCount, failTime, thetasOut);
 }
 
 // PRMPPIfullRolloutKernel, src/prmppi_kernels.cu:55-130 (one iteration per (nom/rob, p, s)).
@@ -626,10 +663,88 @@ int orc_mppi_update(int prec, const dr_env_config* ec, const dr_mppi_config* mc,
                     double* costsOut, int blockorder)
 {
     if (prec == 64)
-        mppiUpdate<double>(*ec, *mc, belief, costsTrue, branchUsed, branchTime, noise, B, knotsIO, denseOut, minCosts, nu, costsOut, blockorder);
+        mppiUpdate<double>(ec->n_theta, ec->max_accel[0], *mc, belief, costsTrue, branchUsed, branchTime, noise, B, knotsIO, denseOut, minCosts, nu,
+                           costsOut, blockorder);
     else
-        mppiUpdate<float>(*ec, *mc, belief, costsTrue, branchUsed, branchTime, noise, B, knotsIO, denseOut, minCosts, nu, costsOut, blockorder);
+        mppiUpdate<float>(ec->n_theta, ec->max_accel[0], *mc, belief, costsTrue, branchUsed, branchTime, noise, B, knotsIO, denseOut, minCosts, nu,
+                          costsOut, blockorder);
     return 0;
+}
+
+// ---- gate race ------------------------------------------------------------------------
+
+int orc_gate_rollout(int prec, const dr_gate_env_config* ec, const dr_mppi_config* mc, const dr_gate_state* s0, const float* belief,
+                     const float* nominal, const float* noise, const float* B, uint64_t seed, uint64_t step, double* costsTrue, int* branchUsed,
+                     int* branchTime)
+{
+    if (prec == 64)
+        gateRollout<double>(*ec, *mc, *s0, belief, nominal, noise, B, seed, step, costsTrue, branchUsed, branchTime);
+    else
+        gateRollout<float>(*ec, *mc, *s0, belief, nominal, noise, B, seed, step, costsTrue, branchUsed, branchTime);
+    return 0;
+}
+
+int orc_gate_update(int prec, const dr_gate_env_config* ec, const dr_mppi_config* mc, const float* belief, const double* costsTrue,
+                    const int* branchUsed, const int* branchTime, const float* noise, const float* B, double* knotsIO, double* denseOut,
+                    double* minCosts, double* nu, double* costsOut, int blockorder)
+{
+    const float maxAccel = ec->max_accel[ec->i_mppi];
+    if (prec == 64)
+        mppiUpdate<double>(ec->n_theta, maxAccel, *mc, belief, costsTrue, branchUsed, branchTime, noise, B, knotsIO, denseOut, minCosts, nu, costsOut,
+                           blockorder);
+    else
+        mppiUpdate<float>(ec->n_theta, maxAccel, *mc, belief, costsTrue, branchUsed, branchTime, noise, B, knotsIO, denseOut, minCosts, nu, costsOut,
+                          blockorder);
+    return 0;
+}
+
+int orc_gate_verify(int prec, const dr_gate_env_config* ec, const dr_mppi_config* mc, const dr_gate_state* s0, const float* belief, const double* plan,
+                    uint64_t seed, uint64_t step, int planId, unsigned* failCount, int* failTime, int* thetas)
+{
+    if (prec == 64)
+        gateVerify<double>(*ec, *mc, *s0, belief, plan, seed, step, planId, failCount, failTime, thetas);
+    else
+        gateVerify<float>(*ec, *mc, *s0, belief, plan, seed, step, planId, failCount, failTime, thetas);
+    return 0;
+}
+
+// environmentStep on the gate race (the reference's flags as arguments), for unit tests
+int orc_gate_env_step(int prec, const dr_gate_env_config* ec, int trueTheta, const float* action, dr_gate_state* state, float* belief,
+                      int updateBelief, int considerBranching, float minConfidence, int addMargin, float gateMargin, int loseOnOppWin, int applyNoise,
+                      uint64_t seed, uint64_t step, int t)
+{
+    auto run = [&](auto zero) -> int
+    {
+        using R = decltype(zero);
+        gate::Env<R> env(*ec);
+        gate::State<R> st = gate::State<R>::from(*state);
+        Branch<R> bs;
+        R b0[DR_MAX_THETA];
+        for (int th = 0; th < ec->n_theta; th++)
+            b0[th] = belief[th];
+        initBranchState(bs, b0, ec->n_theta, (R)minConfidence);
+        gate::Flags f{updateBelief != 0, considerBranching != 0, addMargin != 0, loseOnOppWin != 0, applyNoise != 0, gateMargin};
+        EnvNoise rng(seed, 0u, 0u, step, S_ENV_STEP);
+        rng.begin_step(0);
+        R ego[DIM] = {(R)action[0], (R)action[1]};
+        bool branched = false;
+        int term = environmentStep(t, trueTheta, env, ego, f, st, bs, branched, (R)minConfidence, rng);
+        st.to(*state);
+        for (int th = 0; th < ec->n_theta; th++)
+            belief[th] = (float)bs.belief[th];
+        return term;
+    };
+    return prec == 64 ? run(0.0) : run(0.0f);
+}
+
+// stateCost and finalCost of a gate-race state (for unit tests)
+void orc_gate_costs(const dr_gate_env_config* ec, const dr_mppi_config* mc, const dr_gate_state* s, float* out2)
+{
+    gate::Env<float> env(*ec);
+    gate::State<float> st = gate::State<float>::from(*s);
+    MppiCosts<float> m = mppiCosts<float>(*mc);
+    out2[0] = stateCost(st, env, m);
+    out2[1] = finalCost(st, env, m.finalAdvWeight, m.finalOppAdvWeight);
 }
 
 int orc_mppi_verify(int prec, const dr_env_config* ec, const dr_mppi_config* mc, const dr_sim_state* s0, const float* belief, const double* plan,

@@ -32,6 +32,17 @@
 #include "../../include/drmppi.h"
 #include "../port/philox_host.hpp"
 
+// The C-ABI environment and state the exported functions take: the strategic race's
+// (dr_env_config / dr_sim_state), or the gate race's when the reference is compiled with
+// USE_ENV_DRONERACE (dr_gate_env_config / dr_gate_state).
+#ifdef USE_ENV_DRONERACE
+typedef dr_gate_env_config CEnv;
+typedef dr_gate_state CState;
+#else
+typedef dr_env_config CEnv;
+typedef dr_sim_state CState;
+#endif
+
 // RNG whose normals come from the Philox environment-noise stream.
 struct PhiloxRefRNG
 {
@@ -50,6 +61,106 @@ constexpr int NBP = N_BRANCH_PLANS;
 constexpr int NTH = N_TRUE_MODELS;
 constexpr int DIMR = ACTION_DIM;
 
+#ifdef USE_ENV_DRONERACE
+struct HostGrids
+{
+    std::vector<float> track;
+};
+
+// EnvironmentConfig of the gate race (env_dronerace_defs.h:60-93) from the C-ABI struct;
+// the counts the reference fixes at compile time must match.
+bool toRefEnv(const CEnv& c, EnvironmentConfig& e, HostGrids& g)
+{
+    if (c.n_theta != NTH || c.n_gates != Env::N_GATES || c.n_obstacles != Env::N_OBSTACLES || c.n_round_obstacles != Env::N_ROUND_OBSTACLES)
+        return false;
+    for (int d = 0; d < 2; d++)
+    {
+        e.arenaMin[d] = c.arena_min[d];
+        e.arenaMax[d] = c.arena_max[d];
+    }
+    e.dt = c.dt;
+    e.sendStates = c.send_states != 0;
+    e.droneRadius = c.drone_radius;
+    e.posNoiseLevel = c.pos_noise_level;
+    e.speedNoiseLevel = c.speed_noise_level;
+    e.actionNoiseLevel = c.action_noise_level;
+    for (int a = 0; a < Env::N_AGENTS; a++)
+    {
+        e.maxSpeed[a] = c.max_speed[a];
+        e.maxAccel[a] = c.max_accel[a];
+    }
+    e.nWinLaps = c.n_win_laps;
+    e.targetDistance = c.target_distance;
+    for (int i = 0; i < Env::N_GATES * 2; i++)
+    {
+        e.gateCenters[i] = c.gate_centers[i];
+        e.gateVectors[i] = c.gate_vectors[i];
+    }
+    for (int i = 0; i < Env::N_GATES; i++)
+        e.gateRadius[i] = c.gate_radius[i];
+    for (int i = 0; i < Env::N_OBSTACLES * 4; i++)
+        e.obstacles[i] = c.obstacles[i];
+    for (int i = 0; i < Env::N_ROUND_OBSTACLES * 2; i++)
+        e.roundObsCenters[i] = c.round_obs_centers[i];
+    for (int i = 0; i < Env::N_ROUND_OBSTACLES; i++)
+        e.roundObsRadius[i] = c.round_obs_radius[i];
+    for (int th = 0; th < NTH; th++)
+    {
+        e.initBelief[th] = c.init_belief[th];
+        const dr_pid_config& p = c.opp_pid[th];
+        e.oppPid[th].kp = p.kp;
+        e.oppPid[th].kd = p.kd;
+        e.oppPid[th].repulsionFactor = p.repulsion_factor;
+        e.oppPid[th].repulsionPower = p.repulsion_power;
+        e.oppPid[th].repulsionDistFact = p.repulsion_dist_fact;
+        e.oppPid[th].racelineIndex = p.raceline_index;
+        e.oppPid[th].actionNoise = p.action_noise;
+    }
+    e.iMppi = c.i_mppi;
+    // the racelines plus one sample (the last raceline's first) read when s wraps to 1.0f
+    const size_t n = (size_t)Env::N_RACELINES * NTS * 2;
+    g.track.assign(c.track_points, c.track_points + n);
+    g.track.push_back(c.track_points[(size_t)(Env::N_RACELINES - 1) * NTS * 2]);
+    g.track.push_back(c.track_points[(size_t)(Env::N_RACELINES - 1) * NTS * 2 + 1]);
+    e.trackPoints = g.track.data();
+    return true;
+}
+
+SimState toRefState(const CState& s)
+{
+    SimState r;
+    for (int i = 0; i < Env::N_AGENTS * 2; i++)
+    {
+        r.pos[i] = s.pos[i];
+        r.vel[i] = s.vel[i];
+    }
+    for (int i = 0; i < Env::N_AGENTS * Env::N_RACELINES; i++)
+        r.S[i] = s.S[i];
+    for (int a = 0; a < Env::N_AGENTS; a++)
+    {
+        r.laps[a] = s.laps[a];
+        r.gates[a] = s.gates[a];
+    }
+    return r;
+}
+
+void fromRefState(const SimState& r, CState& s)
+{
+    for (int i = 0; i < Env::N_AGENTS * 2; i++)
+    {
+        s.pos[i] = r.pos[i];
+        s.vel[i] = r.vel[i];
+    }
+    for (int i = 0; i < Env::N_AGENTS * Env::N_RACELINES; i++)
+        s.S[i] = r.S[i];
+    for (int a = 0; a < Env::N_AGENTS; a++)
+    {
+        s.laps[a] = r.laps[a];
+        s.gates[a] = r.gates[a];
+    }
+}
+
+#else
 struct HostGrids
 {
     std::vector<float> p, dp, t, kappa;
@@ -57,7 +168,7 @@ struct HostGrids
 
 // EnvironmentConfig (env_stratrace_defs.h:53-86) from the C-ABI struct. Grids are
 // padded with one wrap-around sample (see oracle/port/model.hpp).
-bool toRefEnv(const dr_env_config& c, EnvironmentConfig& e, HostGrids& g)
+bool toRefEnv(const CEnv& c, EnvironmentConfig& e, HostGrids& g)
 {
     if (c.n_opp != Env::N_OPP || c.n_theta != NTH)
         return false;
@@ -117,7 +228,7 @@ bool toRefEnv(const dr_env_config& c, EnvironmentConfig& e, HostGrids& g)
     return true;
 }
 
-SimState toRefState(const dr_sim_state& s)
+SimState toRefState(const CState& s)
 {
     SimState r;
     for (int i = 0; i < Env::N_AGENTS * 2; i++)
@@ -134,7 +245,7 @@ SimState toRefState(const dr_sim_state& s)
     return r;
 }
 
-void fromRefState(const SimState& r, dr_sim_state& s)
+void fromRefState(const SimState& r, CState& s)
 {
     for (int i = 0; i < Env::N_AGENTS * 2; i++)
     {
@@ -148,6 +259,8 @@ void fromRefState(const SimState& r, dr_sim_state& s)
         s.laps[a] = r.laps[a];
     }
 }
+
+#endif
 
 MPPIConfig toRefMppi(const dr_mppi_config& c)
 {
@@ -325,6 +438,20 @@ struct DevBuf
     }
 };
 
+#ifdef USE_ENV_DRONERACE
+// Device copy of the racelines in an EnvironmentConfig.
+struct DevEnv
+{
+    EnvironmentConfig e;
+    DevBuf track;
+    DevEnv(const EnvironmentConfig& host) : e(host), track(((size_t)Env::N_RACELINES * NTS + 1) * 2 * 4)
+    {
+        cudaMemcpy(track.p, host.trackPoints, ((size_t)Env::N_RACELINES * NTS + 1) * 2 * 4, cudaMemcpyHostToDevice);
+        e.trackPoints = track.as<float>();
+    }
+};
+
+#else
 // Device copy of the (padded) track grids in an EnvironmentConfig.
 struct DevEnv
 {
@@ -343,6 +470,8 @@ struct DevEnv
         e.kappa_grid = k.as<float>();
     }
 };
+
+#endif
 
 int cudaStatus()
 {
@@ -389,7 +518,11 @@ int ref_n_theta()
 }
 int ref_n_opp()
 {
+#ifdef USE_ENV_DRONERACE
+    return Env::N_AGENTS - 1;
+#else
     return Env::N_OPP;
+#endif
 }
 int ref_use_splines()
 {
@@ -405,7 +538,7 @@ void ref_sizes(int* out)
 
 // ==== host face ==============================================================================
 
-int refh_mppi_rollout(const dr_env_config* ec, const dr_mppi_config* c, const dr_sim_state* s0, const float* belief, const float* nominal,
+int refh_mppi_rollout(const CEnv* ec, const dr_mppi_config* c, const CState* s0, const float* belief, const float* nominal,
                       const float* noise, const float* B, uint64_t seed, uint64_t step, double* costsTrue, int* branchUsed, int* branchTime,
                       int nthreads)
 {
@@ -424,7 +557,7 @@ int refh_mppi_rollout(const dr_env_config* ec, const dr_mppi_config* c, const dr
 
 // aggregate (kernels.cu:175-217), masked min (221-301), weighted average (307-408,
 // sums in 256-thread block order), interpolation (411-431), clamp (434-456).
-int refh_mppi_update(const dr_env_config* ec, const dr_mppi_config* c, const float* belief, const double* costsTrueIn, const int* branchUsed,
+int refh_mppi_update(const CEnv* ec, const dr_mppi_config* c, const float* belief, const double* costsTrueIn, const int* branchUsed,
                      const int* branchTime, const float* noise, const float* B, float* splineOrDense, float* denseOut, float* minCosts, float* nu,
                      float* costsOut, int nthreads)
 {
@@ -554,7 +687,7 @@ int refh_mppi_update(const dr_env_config* ec, const dr_mppi_config* c, const flo
 
 // verifyNominalFailureKernel (kernels.cu:488-551) with the theta draw and the
 // environment noise from the Philox streams.
-int refh_mppi_verify(const dr_env_config* ec, const dr_mppi_config* c, const dr_sim_state* s0, const float* belief, const float* plan, uint64_t seed,
+int refh_mppi_verify(const CEnv* ec, const dr_mppi_config* c, const CState* s0, const float* belief, const float* plan, uint64_t seed,
                      uint64_t step, int planId, unsigned* failCount, int* failTime, int nthreads)
 {
     EnvironmentConfig envConfig;
@@ -627,7 +760,7 @@ int refh_mppi_verify(const dr_env_config* ec, const dr_mppi_config* c, const dr_
 }
 
 // MPPIController::buildSplineMatrix (src/mppi_controller.cu:56-141), the reference's own code.
-int refh_spline_matrix(const dr_env_config* ec, const dr_mppi_config* c, float* Bout)
+int refh_spline_matrix(const CEnv* ec, const dr_mppi_config* c, float* Bout)
 {
     EnvironmentConfig env;
     HostGrids g;
@@ -651,7 +784,7 @@ double refh_cp_upper(unsigned k, unsigned n, double alpha)
 }
 
 // PRMPPIfullRolloutKernel (prmppi_kernels.cu:55-130).
-int refh_pr_rollout(const dr_env_config* ec, const dr_prmppi_config* c, const dr_sim_state* s0, const float* nom_nominal, const float* rob_nominal,
+int refh_pr_rollout(const CEnv* ec, const dr_prmppi_config* c, const CState* s0, const float* nom_nominal, const float* rob_nominal,
                     const float* noise, const int* thetas, uint64_t seed, uint64_t step, double* cost_nom, double* cost_rob, int nthreads)
 {
     EnvironmentConfig envConfig;
@@ -701,7 +834,7 @@ int refh_pr_rollout(const dr_env_config* ec, const dr_prmppi_config* c, const dr
 
 // PRMPPIcomputeCandidateCostKernel (prmppi_kernels.cu:285-347) and the rollout of
 // PRMPPIcomputeSafeCostKernel (350-393), for both candidates, noise stream `stream`.
-int refh_pr_candidates(const dr_env_config* ec, const dr_prmppi_config* c, const dr_sim_state* s0, const float* cand1, const float* cand2,
+int refh_pr_candidates(const CEnv* ec, const dr_prmppi_config* c, const CState* s0, const float* cand1, const float* cand2,
                        const int* thetas, uint64_t seed, uint64_t step, int stream, double* fullCost, double* safeCostOut)
 {
     EnvironmentConfig envConfig;
@@ -747,7 +880,7 @@ int refh_pr_candidates(const dr_env_config* ec, const dr_prmppi_config* c, const
 }
 
 // One environment step with the reference's own environmentStep (engine.cpp:286-312).
-int refh_env_step(const dr_env_config* ec, int trueTheta, const float* action, dr_sim_state* st, float* belief, int updateBelief, int considerBranching,
+int refh_env_step(const CEnv* ec, int trueTheta, const float* action, CState* st, float* belief, int updateBelief, int considerBranching,
                   float minConfidence, int loseOnOppWin, int applyNoise, uint64_t seed, uint64_t step, int t)
 {
     EnvironmentConfig envConfig;
@@ -782,7 +915,7 @@ int refh_env_step(const dr_env_config* ec, int trueTheta, const float* action, d
     return (int)term;
 }
 
-void refh_costs(const dr_env_config* ec, const dr_mppi_config* c, const dr_prmppi_config* pc, const dr_sim_state* s, float* out4)
+void refh_costs(const CEnv* ec, const dr_mppi_config* c, const dr_prmppi_config* pc, const CState* s, float* out4)
 {
     EnvironmentConfig envConfig;
     HostGrids g;
@@ -808,7 +941,7 @@ int refc_device_count()
 }
 
 // fullRolloutKernel on injected noise (mppi_controller.cu:290-291 launch shape).
-int refc_mppi_rollout(const dr_env_config* ec, const dr_mppi_config* c, const dr_sim_state* s0, const float* belief, const float* nominal,
+int refc_mppi_rollout(const CEnv* ec, const dr_mppi_config* c, const CState* s0, const float* belief, const float* nominal,
                       const float* noise, const float* B, uint64_t seed, float* costsTrue, int* branchUsed, int* branchTime)
 {
     EnvironmentConfig env;
@@ -839,7 +972,7 @@ int refc_mppi_rollout(const dr_env_config* ec, const dr_mppi_config* c, const dr
 
 // aggregate + masked min + weighted average + interpolate + clamp, the reference
 // kernels in the launch order of mppi_controller.cu:299-345.
-int refc_mppi_update(const dr_env_config* ec, const dr_mppi_config* c, const float* belief, const float* costsTrue, const int* branchUsed,
+int refc_mppi_update(const CEnv* ec, const dr_mppi_config* c, const float* belief, const float* costsTrue, const int* branchUsed,
                      const int* branchTime, const float* noise, const float* B, float* splineOrDense, float* denseOut, float* minCosts, float* nu,
                      float* costsOut)
 {
@@ -885,7 +1018,7 @@ int refc_mppi_update(const dr_env_config* ec, const dr_mppi_config* c, const flo
 }
 
 // verifyNominalFailureKernel with its curand streams (statistical comparison only).
-int refc_mppi_verify(const dr_env_config* ec, const dr_mppi_config* c, const dr_sim_state* s0, const float* belief, const float* plan, uint64_t seed,
+int refc_mppi_verify(const CEnv* ec, const dr_mppi_config* c, const CState* s0, const float* belief, const float* plan, uint64_t seed,
                      unsigned* failCount)
 {
     EnvironmentConfig env;
@@ -911,7 +1044,7 @@ int refc_mppi_verify(const dr_env_config* ec, const dr_mppi_config* c, const dr_
 }
 
 // PRMPPIfullRolloutKernel on injected noise and thetas.
-int refc_pr_rollout(const dr_env_config* ec, const dr_prmppi_config* c, const dr_sim_state* s0, const float* nom, const float* rob, const float* noise,
+int refc_pr_rollout(const CEnv* ec, const dr_prmppi_config* c, const CState* s0, const float* nom, const float* rob, const float* noise,
                     const int* thetas, uint64_t seed, float* cost_nom, float* cost_rob)
 {
     EnvironmentConfig env;
@@ -971,7 +1104,7 @@ int refc_pr_update(const dr_prmppi_config* c, float* cost_nom, float* cost_rob, 
 }
 
 // PRMPPIcomputeCandidateCostKernel and PRMPPIcomputeSafeCostKernel (noise-free configs).
-int refc_pr_candidates(const dr_env_config* ec, const dr_prmppi_config* c, const dr_sim_state* s0, const float* cand1, const float* cand2,
+int refc_pr_candidates(const CEnv* ec, const dr_prmppi_config* c, const CState* s0, const float* cand1, const float* cand2,
                        const float* chosen, const int* thetas, uint64_t seed, float* candCosts, float* safeCosts)
 {
     EnvironmentConfig env;
@@ -1004,7 +1137,7 @@ int refc_pr_candidates(const dr_env_config* ec, const dr_prmppi_config* c, const
 //           mppi_controller.cu:282-345, injected initial state, no host copies),
 //  out[1] = full MPPIController::getControl wall ms per step (stdout silenced).
 // nAgents controllers are stepped one after the other per control step.
-int refc_mppi_time(const dr_env_config* ec, const dr_mppi_config* c, const dr_sim_state* s0, int nAgents, int warmup, int steps, double* out)
+int refc_mppi_time(const CEnv* ec, const dr_mppi_config* c, const CState* s0, int nAgents, int warmup, int steps, double* out)
 {
     EnvironmentConfig env;
     HostGrids g;
@@ -1089,7 +1222,7 @@ int refc_mppi_time(const dr_env_config* ec, const dr_mppi_config* c, const dr_si
 }
 
 // Full PRMPPIController::getControl wall ms per control step (nAgents controllers).
-int refc_prmppi_time(const dr_env_config* ec, const dr_prmppi_config* c, const dr_sim_state* s0, int nAgents, int warmup, int steps, double* out)
+int refc_prmppi_time(const CEnv* ec, const dr_prmppi_config* c, const CState* s0, int nAgents, int warmup, int steps, double* out)
 {
     EnvironmentConfig env;
     HostGrids g;
