@@ -14,10 +14,11 @@ from . import abi
 from .abi import check, lib
 
 
-def _state(s) -> abi.dr_sim_state:
-    if isinstance(s, abi.dr_sim_state):
+def _state(s, gate: bool = False):
+    want = abi.dr_gate_state if gate else abi.dr_sim_state
+    if isinstance(s, want):
         return s
-    raise TypeError("state must be a dr_sim_state")
+    raise TypeError(f"state must be a {want.__name__}")
 
 
 class Controller:
@@ -32,9 +33,11 @@ class Controller:
 
 
 class MPPIController(Controller):
-    """MPPIController (include/controllers.h:23-111, src/mppi_controller.cu)."""
+    """MPPIController (include/controllers.h:23-111, src/mppi_controller.cu). `env` is a
+    dr_env_config (the strategic race) or a dr_gate_env_config (the gate race, the
+    reference's controller compiled with USE_ENV_DRONERACE); states match it."""
 
-    def __init__(self, env: abi.dr_env_config, cfg: abi.dr_mppi_config, seed: int, nominal: np.ndarray | None = None, device: int = 0, stream=None):
+    def __init__(self, env, cfg: abi.dr_mppi_config, seed: int, nominal: np.ndarray | None = None, device: int = 0, stream=None):
         super().__init__(env.n_theta, np.array(env.init_belief))
         self.mppiConfig = cfg
         self.n_theta = int(env.n_theta)
@@ -47,7 +50,9 @@ class MPPIController(Controller):
             if nominal.size != self.nbp * self.T * 2:
                 raise ValueError(f"Invalid MPPI construction: expected nominal size {self.nbp * self.T * 2}, got {nominal.size}")
             nom = abi.fptr(nominal)
-        check(lib().dr_mppi_create(C.byref(env), C.byref(cfg), seed, nom, device, C.c_void_p(stream) if stream else None, C.byref(h)), "dr_mppi_create")
+        self.gate = isinstance(env, abi.dr_gate_env_config)
+        create = lib().dr_gate_mppi_create if self.gate else lib().dr_mppi_create
+        check(create(C.byref(env), C.byref(cfg), seed, nom, device, C.c_void_p(stream) if stream else None, C.byref(h)), "dr_mppi_create")
         self._h = h
         self.info = abi.dr_mppi_info()
         self.failCount = np.zeros(self.T, np.uint32)
@@ -75,7 +80,8 @@ class MPPIController(Controller):
         if self.engine is None:
             raise RuntimeError("MPPI: engine not set")
         out = np.zeros(2, np.float32)
-        check(lib().dr_mppi_step(self._h, C.byref(_state(state)), abi.fptr(self.h_belief), abi.fptr(out), C.byref(self.info)), "dr_mppi_step")
+        step = lib().dr_gate_mppi_step if self.gate else lib().dr_mppi_step
+        check(step(self._h, C.byref(_state(state, self.gate)), abi.fptr(self.h_belief), abi.fptr(out), C.byref(self.info)), "dr_mppi_step")
         self._pull()
         return out
 
@@ -219,11 +225,13 @@ class MPPIBatch:
 
     def step(self, states, beliefs: np.ndarray) -> np.ndarray:
         n = len(self.ctls)
-        st = (abi.dr_sim_state * n)(*states)
+        gate = self.ctls[0].gate
+        st = ((abi.dr_gate_state if gate else abi.dr_sim_state) * n)(*states)
         bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
         bel[:, : beliefs.shape[1]] = beliefs
         out = np.zeros((n, 2), np.float32)
-        check(lib().dr_mppi_batch_step(self._b, st, abi.fptr(bel), abi.fptr(out), self.infos), "dr_mppi_batch_step")
+        step = lib().dr_gate_mppi_batch_step if gate else lib().dr_mppi_batch_step
+        check(step(self._b, st, abi.fptr(bel), abi.fptr(out), self.infos), "dr_mppi_batch_step")
         return out
 
     def set_graph(self, on: bool) -> None:
@@ -301,3 +309,17 @@ def env_step(env: abi.dr_env_config, true_theta: int, action, state: abi.dr_sim_
     check(lib().dr_env_step(C.byref(env), true_theta, abi.fptr(a), C.byref(state), abi.fptr(belief), int(update_belief), seed, step, C.byref(term)),
           "dr_env_step")
     return term.value
+
+
+def gate_env_step(env: abi.dr_gate_env_config, true_theta: int, action, state: abi.dr_gate_state, belief: np.ndarray, update_belief: bool, seed: int,
+                  step: int):
+    """One gate-race environment step on the device (dr_gate_env_step); returns
+    (terminal type, new state, new belief)."""
+    st = abi.dr_gate_state.from_buffer_copy(state)
+    bel = np.zeros(abi.DR_MAX_THETA, np.float32)
+    bel[: env.n_theta] = belief
+    act = np.ascontiguousarray(action, np.float32)
+    term = C.c_int()
+    check(lib().dr_gate_env_step(C.byref(env), true_theta, abi.fptr(act), C.byref(st), abi.fptr(bel), int(update_belief), seed, step, C.byref(term)),
+          "dr_gate_env_step")
+    return term.value, st, bel[: env.n_theta].copy()

@@ -9,6 +9,7 @@
                    functions compiled from its sources (oracle/_ref, host build) on small
                    cases with perturbations from the Philox streams.
   * pr_*.npz       the same for PR-MPPI.
+  * gate_*.npz     the same for the gate race (the reference built with USE_ENV_DRONERACE).
   * cp.npz         Clopper-Pearson bounds from scipy.stats.beta.ppf.
 
 Run from the repository root with the reference at /root/reference:
@@ -101,6 +102,29 @@ def gen_mppi(variant: str, spl: bool):
                         plan=plan, fail_count=fc, fail_time=ft)
 
 
+def gen_gate(variant: str, spl: bool):
+    """Gate race (the reference built with USE_ENV_DRONERACE): rollout, update and a
+    verification whose plan drives the ego into the opponent."""
+    from helpers import small_gate, toward_opponent_plan
+
+    sc = small_gate(spl, K=64, T=40, n_verif=256, seed=13, noise=True, agent=1, gap=0.02)
+    rng = np.random.default_rng(9)
+    c = sc.mppi
+    nbp, M = sc.n_theta + 1, O.mk(c)
+    knots = rng.normal(0, 1.0, (nbp, M, 2)).astype(np.float32)
+    belief = np.array([0.4, 0.6], np.float32)
+    noise = O.mppi_noise(sc, 2)
+    B = O.spline_matrix(c) if spl else None
+    ct, bu, bt = O.mppi_rollout(sc, belief, knots, noise, B, 2, impl=variant, nthreads=4)
+    kn, dense, mins, nu, costs = O.mppi_update(sc, belief, ct, bu, bt, noise, B, knots, impl=variant, nthreads=4)
+    plan = toward_opponent_plan(sc)
+    fc, ft, _ = O.mppi_verify(sc, belief, plan, 2, 0, impl=variant, nthreads=4)
+    assert fc.sum() > 0
+    np.savez_compressed(HERE / f"{variant}.npz", knots_in=knots, belief=belief, noise=noise, B=B if spl else np.zeros(1, np.float32), step=2,
+                        seed=sc.seed, costs_true=ct, branch_used=bu, branch_time=bt, knots_out=kn, dense=dense, min_costs=mins, nu=nu, costs=costs,
+                        plan=plan, fail_count=fc, fail_time=ft)
+
+
 def gen_pr(variant: str, nth: int):
     sc = S.strat_race(use_pr=True, K=64, T=24) if nth == 2 else S.robust_race(agent=1, seed=2, K=64, T=24, P=8, n_theta=nth)
     sc.prmppi = S.make_prmppi(K=64, T=24, P=8, inv_temperature=1.0, sampling_noise=1.0) if nth == 2 else sc.prmppi
@@ -132,6 +156,10 @@ def gen_cp():
 
 
 def main():
+    if "--gate" in sys.argv:  # the gate-race fixtures alone
+        gen_gate("gate_spline", True)
+        gen_gate("gate_dense", False)
+        return
     utils, protocol = ref_python()
     gen_tracks(utils)
     gen_wire(utils, protocol)
@@ -140,6 +168,8 @@ def main():
     gen_pr("nth2_spline", 2)
     gen_pr("nth8_spline", 8)
     gen_cp()
+    gen_gate("gate_spline", True)
+    gen_gate("gate_dense", False)
     print("golden fixtures written to", HERE)
 
 

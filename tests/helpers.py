@@ -128,3 +128,27 @@ class OracleMPPI:
         self.pend = (bidx, use_new)
         self.step += 1
         return action, dict(use_new=use_new, cert=cert, fc_new=fc_new, fc_old=fc_old, nu=nu, mins=mins, bidx=bidx)
+
+
+def small_gate(use_splines: bool, K=512, T=40, n_verif=1024, seed=7, noise=True, agent=0, gap=None):
+    """A small gate-race case; noise=False turns off the PID action noise (the reference's
+    kernels draw it from curand). gap (fraction of a lap): put the ego that far behind the
+    opponent on its raceline, both at 2 m/s."""
+    sc = S.gate_race(agent=agent, K=K, T=T, use_splines=use_splines, n_verif=n_verif, action_noise=0.5 if noise else 0.0)
+    sc.seed = seed
+    if gap is not None:
+        n = sc.track.shape[1]
+        opp_u = float(np.float32(sc.state.S[2] if sc.state.S[2] >= 0 else sc.state.S[0]))
+        st = S.gate_state(sc.track, [opp_u - gap, opp_u], 0, list(sc.state.gates), speed=2.0)
+        sc.state = st
+    return sc
+
+
+def toward_opponent_plan(sc, accel=6.0):
+    """A dense plan accelerating the ego straight at the opponent on every branch: many
+    verification samples end in a collision."""
+    st = sc.state
+    me = int(sc.env.i_mppi)
+    d = np.array([st.pos[2 * (1 - me)] - st.pos[2 * me], st.pos[2 * (1 - me) + 1] - st.pos[2 * me + 1]], np.float64)
+    d = d / np.linalg.norm(d) * accel
+    return np.broadcast_to(d, (sc.n_theta + 1, sc.mppi.n_timesteps, 2)).astype(np.float32).copy()
