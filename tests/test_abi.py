@@ -41,7 +41,8 @@ def test_library_exports_every_declared_function():
 def test_struct_layouts_match_c(tmp_path: Path):
     structs = {"dr_opp_config": abi.dr_opp_config, "dr_env_config": abi.dr_env_config, "dr_sim_state": abi.dr_sim_state,
                "dr_mppi_config": abi.dr_mppi_config, "dr_prmppi_config": abi.dr_prmppi_config, "dr_mppi_info": abi.dr_mppi_info,
-               "dr_prmppi_info": abi.dr_prmppi_info}
+               "dr_prmppi_info": abi.dr_prmppi_info, "dr_pid_config": abi.dr_pid_config, "dr_gate_env_config": abi.dr_gate_env_config,
+               "dr_gate_state": abi.dr_gate_state}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for sname, st in structs.items():
         lines.append(f'printf("{sname} size %zu\\n", sizeof({sname}));')
