@@ -316,3 +316,182 @@ def split_frames(blob: bytes) -> list[bytes]:
         out.append(blob[off + 4 : off + 4 + n])
         off += 4 + n
     return out
+
+
+# ---- gate race (the reference's EnvDroneRace) -----------------------------------------
+
+@dataclass
+class GateEnvHeader:
+    env: abi.dr_gate_env_config
+    track: np.ndarray  # (DR_GATE_RACELINES, 512, 2) float32, referenced by env.track_points
+    seed: int
+    true_theta: int
+    model_sizes: list[int]
+
+
+def unpack_gate_env(buf: bytes) -> GateEnvHeader:
+    """EnvDroneRace::unpackEnvConfig (env_dronerace.cpp:124-250), with this build's limits
+    (2 agents, 2 racelines, up to 16 gates and 4 obstacles of each kind) in place of the
+    reference's compile-time sizes."""
+    r = Reader(buf)
+    if (k := r.int32()) != MSG_HEADER:
+        raise ProtocolError(f"Expected header message type for environment config (type {MSG_HEADER}) but got type {k} instead")
+    if (ek := r.int32()) != ENV_DRONERACE:
+        raise ProtocolError(f"Environment kind mismatch: received kind {ek}, but this decoder reads ENV_DRONERACE ({ENV_DRONERACE})")
+    n_factors = r.int32()
+    if n_factors != 1:
+        raise ProtocolError(f"Received config for {n_factors} environment parameters but this build supports one parameter factor")
+    sizes = [int(x) for x in r.array()]
+    n_theta = sizes[0] if sizes else 0
+    if not 1 <= n_theta <= abi.DR_MAX_THETA:
+        raise ProtocolError(f"Received invalid model size {n_theta} (supported: 1..{abi.DR_MAX_THETA})")
+    e = abi.dr_gate_env_config()
+    e.n_theta = n_theta
+    amin, amax = r.array(2), r.array(2)
+    n_agents, dim = r.int32(), r.int32()
+    e.dt = r.float32()
+    e.send_states = r.int32()
+    n_race, n_gates = r.int32(), r.int32()
+    if n_agents != abi.DR_GATE_AGENTS:
+        raise ProtocolError(f"Received config for {n_agents} agents but N_AGENTS is {abi.DR_GATE_AGENTS}")
+    if dim != abi.DR_DIM:
+        raise ProtocolError(f"Received config for dimension {dim} but DIM is {abi.DR_DIM}")
+    if n_race != abi.DR_GATE_RACELINES:
+        raise ProtocolError(f"Received config for {n_race} racelines but N_RACELINES is {abi.DR_GATE_RACELINES}")
+    if not 1 <= n_gates <= abi.DR_GATE_MAX_GATES:
+        raise ProtocolError(f"Received config for {n_gates} gates (supported: 1..{abi.DR_GATE_MAX_GATES})")
+    for d in range(2):
+        e.arena_min[d] = float(amin[d])
+        e.arena_max[d] = float(amax[d])
+    e.drone_radius = r.float32()
+    e.pos_noise_level = r.float32()
+    e.speed_noise_level = r.float32()
+    e.action_noise_level = r.float32()
+    ms, ma = r.array(2), r.array(2)
+    for a in range(2):
+        e.max_speed[a] = float(ms[a])
+        e.max_accel[a] = float(ma[a])
+    nts = r.int32()
+    if nts != abi.DR_N_TRACK_SAMPLES:
+        raise ProtocolError(f"Received config for {nts} track samples but N_TRACK_SAMPLES is {abi.DR_N_TRACK_SAMPLES}")
+    e.n_win_laps = r.int32()
+    e.target_distance = r.float32()
+    e.n_gates = n_gates
+    gc, gv, gr = r.array(2 * n_gates), r.array(2 * n_gates), r.array(n_gates)
+    for i in range(2 * n_gates):
+        e.gate_centers[i] = float(gc[i])
+        e.gate_vectors[i] = float(gv[i])
+    for i in range(n_gates):
+        e.gate_radius[i] = float(gr[i])
+    n_obs = r.int32()
+    if not 0 <= n_obs <= abi.DR_GATE_MAX_OBSTACLES:
+        raise ProtocolError(f"Received config for {n_obs} rect obstacles (supported: 0..{abi.DR_GATE_MAX_OBSTACLES})")
+    obs = r.array(4 * n_obs)
+    e.n_obstacles = n_obs
+    for i in range(4 * n_obs):
+        e.obstacles[i] = float(obs[i])
+    n_round = r.int32()
+    if not 0 <= n_round <= abi.DR_GATE_MAX_OBSTACLES:
+        raise ProtocolError(f"Received config for {n_round} round obstacles (supported: 0..{abi.DR_GATE_MAX_OBSTACLES})")
+    rc, rr = r.array(2 * n_round), r.array(n_round)
+    e.n_round_obstacles = n_round
+    for i in range(2 * n_round):
+        e.round_obs_centers[i] = float(rc[i])
+    for i in range(n_round):
+        e.round_obs_radius[i] = float(rr[i])
+    seed = r.int32()
+    ib = r.array(n_theta)
+    for th in range(n_theta):
+        e.init_belief[th] = float(ib[th])
+    for th in range(n_theta):  # unpackPIDConfig, env_dronerace.cpp:104-121
+        p = e.opp_pid[th]
+        p.kp, p.kd = r.float32(), r.float32()
+        p.repulsion_factor, p.repulsion_power, p.repulsion_dist_fact = r.float32(), r.float32(), r.float32()
+        p.raceline_index = r.int32()
+        p.action_noise = r.float32()
+    e.i_mppi = r.int32()
+    true_theta = r.int32()
+    tp = r.array(abi.DR_GATE_RACELINES * nts * 2)
+    r.finished()
+    track = np.ascontiguousarray(tp.reshape(abi.DR_GATE_RACELINES, nts, 2), np.float32)
+    e.track_points = abi.fptr(track)
+    return GateEnvHeader(e, track, seed, true_theta, sizes)
+
+
+def pack_gate_env(env: abi.dr_gate_env_config, track: np.ndarray, seed: int, true_theta: int) -> bytes:
+    """The environment header as python-src/protocol.py packs a DroneRaceEnvironmentConfig."""
+    w = Writer()
+    w.int32(MSG_HEADER)
+    w.int32(ENV_DRONERACE)
+    w.int32(1)
+    w.array([env.n_theta])
+    w.array(list(env.arena_min))
+    w.array(list(env.arena_max))
+    w.int32(abi.DR_GATE_AGENTS)
+    w.int32(abi.DR_DIM)
+    w.float32(env.dt)
+    w.int32(env.send_states)
+    w.int32(abi.DR_GATE_RACELINES)
+    w.int32(env.n_gates)
+    for v in (env.drone_radius, env.pos_noise_level, env.speed_noise_level, env.action_noise_level):
+        w.float32(v)
+    w.array(list(env.max_speed))
+    w.array(list(env.max_accel))
+    w.int32(abi.DR_N_TRACK_SAMPLES)
+    w.int32(env.n_win_laps)
+    w.float32(env.target_distance)
+    ng = env.n_gates
+    w.array(list(env.gate_centers)[: 2 * ng])
+    w.array(list(env.gate_vectors)[: 2 * ng])
+    w.array(list(env.gate_radius)[:ng])
+    w.int32(env.n_obstacles)
+    w.array(list(env.obstacles)[: 4 * env.n_obstacles])
+    w.int32(env.n_round_obstacles)
+    w.array(list(env.round_obs_centers)[: 2 * env.n_round_obstacles])
+    w.array(list(env.round_obs_radius)[: env.n_round_obstacles])
+    w.int32(seed)
+    w.array(list(env.init_belief)[: env.n_theta])
+    for th in range(env.n_theta):
+        p = env.opp_pid[th]
+        for v in (p.kp, p.kd, p.repulsion_factor, p.repulsion_power, p.repulsion_dist_fact):
+            w.float32(v)
+        w.int32(p.raceline_index)
+        w.float32(p.action_noise)
+    w.int32(env.i_mppi)
+    w.int32(true_theta)
+    w.array(np.asarray(track, np.float32).ravel())
+    return w.bytes()
+
+
+def unpack_gate_state(buf: bytes, i_mppi: int) -> abi.dr_gate_state:
+    """EnvDroneRace::unpackSimState (env_dronerace.cpp:78-100): the ego's arc lengths are
+    reset to -1 (untracked)."""
+    r = Reader(buf)
+    if (k := r.int32()) != MSG_HEADER:
+        raise ProtocolError(f"Expected header message type for environment config (type {MSG_HEADER}) but got type {k} instead")
+    na, nr = abi.DR_GATE_AGENTS, abi.DR_GATE_RACELINES
+    pos, vel, S, laps, gates = r.array(2 * na), r.array(2 * na), r.array(na * nr), r.array(na), r.array(na)
+    r.finished()
+    s = abi.dr_gate_state()
+    for i in range(2 * na):
+        s.pos[i] = float(pos[i])
+        s.vel[i] = float(vel[i])
+    for i in range(na * nr):
+        s.S[i] = float(S[i])
+    for a in range(na):
+        s.laps[a] = int(laps[a])
+        s.gates[a] = int(gates[a])
+    for k in range(nr):
+        s.S[i_mppi * nr + k] = -1.0
+    return s
+
+
+def pack_gate_state(s: abi.dr_gate_state) -> bytes:
+    w = Writer()
+    w.int32(MSG_HEADER)
+    w.array(list(s.pos))
+    w.array(list(s.vel))
+    w.array(list(s.S))
+    w.array(list(s.laps))
+    w.array(list(s.gates))
+    return w.bytes()

@@ -4,7 +4,8 @@
                    StratRaceEnvironmentConfig.__post_init__, imported from the reference
                    sources) for its round track (python-src/main.py:867-868).
   * wire_*.bin     configuration headers packed by the reference's BytePacker
-                   (python-src/protocol.py:13-72) for the stratRaceEnv presets.
+                   (python-src/protocol.py:13-72) for the stratRaceEnv presets and its
+                   tinyGateEnv (wire_gate_mppi.bin).
   * mppi_*.npz     rollout / update / verification outputs of the reference's own model
                    functions compiled from its sources (oracle/_ref, host build) on small
                    cases with perturbations from the Philox streams.
@@ -76,6 +77,25 @@ def gen_wire(utils, protocol):
             for fr in frames:
                 f.write(len(fr).to_bytes(4, "little"))
                 f.write(fr)
+
+
+def gen_wire_gate(utils, protocol):
+    """The same frames for the reference's tinyGateEnv (python-src/main.py:40-220, one
+    round obstacle, spline MPPI)."""
+    sys.path.insert(0, str(REF / "python-src"))
+    import main as ref_main
+
+    env, init, cont, _ = ref_main.tinyGateEnv(roundObs=True, useSplines=True, usePR=False)
+    frames = []
+    for obj in (env, cont, init):
+        p = protocol.BytePacker()
+        p.pushInt(utils.MSG_TYPE.MSG_HEADER)
+        p.pushObj(obj)
+        frames.append(p.toBytes())
+    with open(HERE / "wire_gate_mppi.bin", "wb") as f:
+        for fr in frames:
+            f.write(len(fr).to_bytes(4, "little"))
+            f.write(fr)
 
 
 def gen_mppi(variant: str, spl: bool):
@@ -157,12 +177,15 @@ def gen_cp():
 
 def main():
     if "--gate" in sys.argv:  # the gate-race fixtures alone
+        utils, protocol = ref_python()
+        gen_wire_gate(utils, protocol)
         gen_gate("gate_spline", True)
         gen_gate("gate_dense", False)
         return
     utils, protocol = ref_python()
     gen_tracks(utils)
     gen_wire(utils, protocol)
+    gen_wire_gate(utils, protocol)
     gen_mppi("nth2_spline", True)
     gen_mppi("nth2_dense", False)
     gen_pr("nth2_spline", 2)

@@ -72,3 +72,33 @@ def test_malformed_frames_are_rejected(proto):
     bad[4:8] = (0).to_bytes(4, "little")  # ENV_DRONERACE
     with pytest.raises(proto.ProtocolError, match="kind mismatch"):
         proto.unpack_env(bytes(bad))
+
+
+def test_reference_gate_frames_round_trip(proto):
+    """tinyGateEnv (python-src/main.py:40-220) as the reference's front-end packs it: the
+    gate-race decoder reads every field, the ego's arc lengths load as -1, and the
+    encoders reproduce the bytes."""
+    env_f, cont_f, state_f = proto.split_frames((GOLD / "wire_gate_mppi.bin").read_bytes())
+    hdr = proto.unpack_gate_env(env_f)
+    e = hdr.env
+    assert e.n_theta == 2 and e.n_gates == 2 and e.n_round_obstacles == 1 and e.n_obstacles == 0 and e.i_mppi == 0
+    assert e.opp_pid[0].raceline_index == 0 and e.opp_pid[1].raceline_index == 1
+    assert e.opp_pid[0].kp == pytest.approx(5.0) and e.opp_pid[0].kd == pytest.approx(20.0)
+    assert hdr.track.shape == (2, 512, 2)
+    assert proto.pack_gate_env(e, hdr.track, hdr.seed, hdr.true_theta) == env_f
+    cont = proto.unpack_controller(cont_f)
+    assert proto.pack_controller(cont) == cont_f
+    assert cont.n_knots == 10 and cont.final_adv_weight == pytest.approx(200.0)
+    st = proto.unpack_gate_state(state_f, e.i_mppi)
+    assert st.S[0] == -1.0 and st.S[1] == -1.0 and st.S[2] >= 0
+    st2 = drb.abi.dr_gate_state.from_buffer_copy(st)
+    raw = proto.Reader(state_f)
+    raw.int32()
+    for _ in range(2):
+        raw.array()
+    S = raw.array()
+    for i in range(2):
+        st2.S[i] = float(S[i])
+    assert proto.pack_gate_state(st2) == state_f
+    # the C ABI accepts the decoded configuration
+    assert drb.scenarios.GateScenario(env=e, track=hdr.track, state=st).n_theta == 2
