@@ -54,6 +54,33 @@ VERIF_H = 40
 FLOPS_PER_ROLLOUT_STEP = 652.0    # MPPI rollout step (belief update over 2 hypotheses)
 FLOPS_PER_VERIFY_STEP = 571.0     # verification step (noise-free ego plan)
 
+# --workload gates: the same control step on the gate race (the reference's EnvDroneRace:
+# one PID opponent with 2 hypotheses, 8 gates on a 30 x 20 m ellipse, 2 racelines), FLOPs
+# per step counted the same way on oracle/port/gate_model.hpp (orc_gate_count_ops).
+N_GATES = 8
+GATE_FLOPS_PER_ROLLOUT_STEP = 486.3
+GATE_FLOPS_PER_VERIFY_STEP = 473.4
+WL = {"kind": "strat"}  # the workload of this run (set from --workload)
+
+
+def _flops():
+    if WL["kind"] == "gates":
+        return GATE_FLOPS_PER_ROLLOUT_STEP, GATE_FLOPS_PER_VERIFY_STEP
+    return FLOPS_PER_ROLLOUT_STEP, FLOPS_PER_VERIFY_STEP
+
+
+def _workload_name() -> str:
+    return "gate_mppi_4x4096x64_8gates" if WL["kind"] == "gates" else "mppi_4x4096x64"
+
+
+def _unit() -> str:
+    race = f"gate race, {N_GATES} gates" if WL["kind"] == "gates" else "strategic race"
+    return f"control steps/s (4 agents x K=4096 x H=64 MPPI, verification V=2^17 x 40, all agents advanced once; {race})"
+
+
+def _ref_variant(O) -> str:
+    return "gate8_dense" if WL["kind"] == "gates" else O.ref_variant_name(N_THETA, False)
+
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture
 # of each kernel on this workload (--quick --no-overlap, 3 steps); grids, plans and tile
 # tables stay in L2, so DRAM traffic is spilled registers and first-touch reads, about a
@@ -74,6 +101,8 @@ def _package():
 def workload(rank: int):
     drb = _package()
     S = drb.scenarios
+    if WL["kind"] == "gates":
+        return [S.gate_race(agent=a, seed=rank, K=K, T=H, use_splines=False, n_verif=V, n_gates=N_GATES) for a in range(AGENTS)]
     return [S.circle_race(agent=a, seed=rank, K=K, T=H, use_splines=False, n_theta=N_THETA, n_verif=V) for a in range(AGENTS)]
 
 
@@ -170,7 +199,7 @@ def cpu_baseline_reference(scs, target_s: float = 10.0, max_reps: int = 100000, 
 
     drb = _package()
     O.set_abi(drb.abi)
-    variant = O.ref_variant_name(N_THETA, False)
+    variant = _ref_variant(O)
     kind = "reference"
     if not O.ref_available(variant):
         kind = "port"
@@ -235,7 +264,7 @@ def run_ours(args) -> None:
     states = [s.state for s in scs]
     beliefs = np.stack([s.belief() for s in scs])
     # device-resident inputs
-    st_bytes = bytes((abi.dr_sim_state * n)(*states))
+    st_bytes = bytes((type(states[0]) * n)(*states))
     st_dev = torch.frombuffer(bytearray(st_bytes), dtype=torch.uint8).to("cuda")
     bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
     bel[:, :N_THETA] = beliefs
@@ -307,14 +336,14 @@ def run_ours(args) -> None:
         batch.set_profiling(False)
         batch.set_overlap(True)
     units = {"rollout": AGENTS * K * N_THETA * H, "verify": AGENTS * 2 * V * VERIF_H}
-    flops_unit = {"rollout": FLOPS_PER_ROLLOUT_STEP, "verify": FLOPS_PER_VERIFY_STEP}
+    flops_unit = dict(zip(("rollout", "verify"), _flops()))
     dom = max(kt_serial, key=kt_serial.get) if kt_serial else None
     roof = roof_step = None
     if dom in units and clk.get("sm_mhz"):
         peak = 2 * 128 * 148 * clk["sm_mhz"] * 1e6 / 1e12
         achieved = units[dom] * flops_unit[dom] / (kt_serial[dom] / 1e3) / 1e12
         roof = {"bound": "fp32", "kernel": f"mppi_verify ({dom})" if dom == "verify" else f"mppi_{dom}", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH.get(dom),
+                "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH.get(dom) if WL["kind"] == "strat" else None,
                 "peak_source": "FP32 FMA rate of 148 SMs x 128 lanes at the median SM clock sampled during the timed region (MEASURED_PEAKS.json has no FP32 figure)",
                 "units_per_launch": units[dom], "flops_per_unit": flops_unit[dom], "kernel_ms": kt_serial[dom],
                 "measured": f"CUDA events around each launch on its stream, {serial_steps} steps with both plans verified in one launch"}
@@ -332,7 +361,7 @@ def run_ours(args) -> None:
     line = {
         "metric": "control_steps_per_s",
         "value": value,
-        "unit": "control steps/s (4 agents x K=4096 x H=64 MPPI, verification V=2^17 x 40, all agents advanced once)",
+        "unit": _unit(),
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -342,7 +371,7 @@ def run_ours(args) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded tracks and states; no dataset)",
-        "config": {"workload": "mppi_4x4096x64", "agents": AGENTS, "K": K, "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
+        "config": {"workload": _workload_name(), "agents": AGENTS, "K": K, "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
                    "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": f"replicas x{world}",
                    "l2": "working set per step < L2; steps are dependent control steps of the same controllers"},
         "rollout_steps_per_s": world * rollout_steps * args.steps / (ms / 1e3),
@@ -386,7 +415,7 @@ def reference_cuda_timing(scs, warmup: int = 3, steps: int = 20) -> dict | None:
 
     drb = _package()
     O.set_abi(drb.abi)
-    variant = O.ref_variant_name(N_THETA, False)
+    variant = _ref_variant(O)
     if not O.ref_available(variant):
         return None
     sc = scs[0]
@@ -419,7 +448,7 @@ def run_reference(args) -> None:
         "impl": "reference",
         "metric": "control_steps_per_s",
         "value": value,
-        "unit": "control steps/s (4 agents x K=4096 x H=64 MPPI, verification V=2^17 x 40, all agents advanced once)",
+        "unit": _unit(),
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -429,7 +458,7 @@ def run_reference(args) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded tracks and states; no dataset)",
-        "config": {"workload": "mppi_4x4096x64", "agents": AGENTS, "K": K, "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
+        "config": {"workload": _workload_name(), "agents": AGENTS, "K": K, "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
                    "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "control_steps/s", "cores": base["cores"], "kind": base["kind"], "sample": base["sample"]},
         "e2e": {"value": value, "unit": "control steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -446,9 +475,12 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e, no CPU baseline): for profiler runs")
     ap.add_argument("--no-overlap", action="store_true", help="run the previous plan's verification after the rollout instead of beside it")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="strat", choices=["strat", "gates"],
+                    help="strat: the strategic race (the headline workload); gates: the gate race (EnvDroneRace)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")
     args = ap.parse_args()
+    WL["kind"] = args.workload
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -84,6 +84,8 @@ def port() -> C.CDLL:
             "orc_gate_env_step": (C.c_int, [C.c_int, GE, C.c_int, f, GS, f, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_int, C.c_int, u64, u64,
                                             C.c_int]),
             "orc_gate_costs": (None, [GE, M, GS, f]),
+            "orc_count_ops": (C.c_int, [E, M, S, f, f, f, u64, u64, C.c_int, C.c_int, C.c_int, d]),
+            "orc_gate_count_ops": (C.c_int, [GE, M, GS, f, f, f, u64, u64, C.c_int, C.c_int, C.c_int, d]),
         }
         for n, (r, args) in protos.items():
             fn = getattr(L, n)
@@ -116,7 +118,7 @@ def ref(variant: str) -> C.CDLL:
         P = C.POINTER
         f, d, i, u = P(C.c_float), P(C.c_double), P(C.c_int32), P(C.c_uint32)
         E, M, PR, S = P(a.dr_env_config), P(a.dr_mppi_config), P(a.dr_prmppi_config), P(a.dr_sim_state)
-        if variant.startswith("gate_"):  # the same entry points on the gate race's structs
+        if variant.startswith("gate"):  # the same entry points on the gate race's structs
             E, S = P(a.dr_gate_env_config), P(a.dr_gate_state)
         u64, I = C.c_uint64, C.c_int
         protos = {

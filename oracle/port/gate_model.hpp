@@ -221,17 +221,17 @@ template <typename R> inline int walkMin(const R* tp, int i0, const R* pos, int 
     int bestI = i0;
     bestSq = baseSq;
     int cur = (i0 + delta + NTS) % NTS;
-    R curSq = sqDistToSample(tp, cur, pos);
+    R curSq = gate::sqDistToSample(tp, cur, pos);
     while (curSq < bestSq)
     {
         bestI = cur;
         bestSq = curSq;
         cur = (cur + delta + NTS) % NTS;
-        curSq = sqDistToSample(tp, cur, pos);
+        curSq = gate::sqDistToSample(tp, cur, pos);
     }
     for (int i = 0; i < margin; i++)
     {
-        curSq = sqDistToSample(tp, cur, pos);
+        curSq = gate::sqDistToSample(tp, cur, pos);
         if (curSq < bestSq)
         {
             bestI = cur;
@@ -248,7 +248,7 @@ template <typename R> inline R projectGreedy(const R* tp, const R* pos, R prevS)
     if (prevS < R(0))
         return projectFull(tp, pos);
     int baseI = (int)(prevS * (R)NTS + R(0.5)) % NTS;
-    R baseSq = sqDistToSample(tp, baseI, pos);
+    R baseSq = gate::sqDistToSample(tp, baseI, pos);
     R bSq, fSq;
     int bI = walkMin(tp, baseI, pos, -1, baseSq, bSq);
     int fI = walkMin(tp, baseI, pos, +1, baseSq, fSq);

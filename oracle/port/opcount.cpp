@@ -13,6 +13,7 @@
 #include <unordered_set>
 #include <vector>
 
+#include "gate_model.hpp"
 #include "model.hpp"
 
 namespace orc
@@ -186,13 +187,16 @@ using namespace orc;
 // out[0..8] = add, mul, div, sqrt, exp, log, pow, minmax, cmp; out[9] = environment steps.
 // kind 0: MPPI rollout of `nsamples` samples (dense controls, nominal + noise inputs);
 // kind 1: verification rollouts of `nsamples` samples of the dense plan `nominal`.
-extern "C" int orc_count_ops(const dr_env_config* ec, const dr_mppi_config* mc, const dr_sim_state* s0, const float* belief0, const float* nominal,
-                             const float* noise, uint64_t seed, uint64_t step, int nsamples, int kind, int dedup, double* out)
+// the counting loop for either model (model.hpp / gate_model.hpp, found by argument-
+// dependent lookup); makeFlags(kind) gives the environmentStep flags of the rollout
+// (kind 0) or the verification (kind 1)
+template <typename EnvT, typename StateT, typename S0, typename MakeFlags>
+static int countOps(const EnvT& env, const dr_mppi_config* mc, const S0* s0, const float* belief0, const float* nominal, const float* noise,
+                    uint64_t seed, uint64_t step, int nsamples, int kind, int dedup, double* out, MakeFlags makeFlags)
 {
     CountCtx ctx;
     ctx.dedup = dedup != 0;
-    Env<CF> env(*ec);
-    const int K = mc->n_samples, T = mc->n_timesteps, nth = ec->n_theta;
+    const int K = mc->n_samples, T = mc->n_timesteps, nth = env.nth;
     const CF minConf = mc->min_confidence;
     MppiCosts<CF> cc{mc->coll_dist_factor, mc->boundary_cost, mc->boundary_threshold_factor, mc->outside_cost,
                      mc->win_cost,         mc->opp_win_cost, mc->final_adv_weight,          mc->final_opp_adv_weight};
@@ -229,13 +233,13 @@ extern "C" int orc_count_ops(const dr_env_config* ec, const dr_mppi_config* mc, 
             int theta = kind == 1 ? thetaV : th;
             if (kind == 0 && !branchCompatibleWithModel(first.predTheta, theta))
                 continue;
-            State<CF> st = State<CF>::from(*s0);
+            StateT st = StateT::from(*s0);
             Branch<CF> bs = first;
             CF cost = 0.0, decay = 1.0;
             bool stop = false;
             int tOrigin = 0;
             EnvNoise rng(seed, (uint32_t)s, kind == 0 ? ((uint32_t)theta << 16) : 0u, step, kind == 0 ? S_MPPI_ROLL_ENV : S_VERIF_ENV);
-            const StepFlags flags{true, true, kind == 0, true, true};
+            const auto flags = makeFlags(kind);
             int H = kind == 0 ? T : mc->verif_horizon;
             for (int t = 0; t < H && !stop; t++)
             {
@@ -276,4 +280,22 @@ extern "C" int orc_count_ops(const dr_env_config* ec, const dr_mppi_config* mc, 
     double v[10] = {o.add, o.mul, o.div, o.sqrt_, o.exp_, o.log_, o.pow_, o.minmax, o.cmp, steps};
     std::memcpy(out, v, sizeof(v));
     return 0;
+}
+
+extern "C" int orc_count_ops(const dr_env_config* ec, const dr_mppi_config* mc, const dr_sim_state* s0, const float* belief0, const float* nominal,
+                             const float* noise, uint64_t seed, uint64_t step, int nsamples, int kind, int dedup, double* out)
+{
+    Env<CF> env(*ec);
+    return countOps<Env<CF>, State<CF>>(env, mc, s0, belief0, nominal, noise, seed, step, nsamples, kind, dedup, out,
+                                        [](int k) { return StepFlags{true, true, k == 0, true, true}; });
+}
+
+// the same on the gate race (gate_model.hpp): environmentStep<true, true, false, k == 0>
+extern "C" int orc_gate_count_ops(const dr_gate_env_config* ec, const dr_mppi_config* mc, const dr_gate_state* s0, const float* belief0,
+                                  const float* nominal, const float* noise, uint64_t seed, uint64_t step, int nsamples, int kind, int dedup, double* out)
+{
+    gate::Env<CF> env(*ec);
+    const float margin = mc->gate_traversal_margin;
+    return countOps<gate::Env<CF>, gate::State<CF>>(env, mc, s0, belief0, nominal, noise, seed, step, nsamples, kind, dedup, out,
+                                                    [margin](int k) { return gate::Flags{true, true, false, k == 0, true, margin}; });
 }
