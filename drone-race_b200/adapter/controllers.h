@@ -17,6 +17,14 @@
 
 #include "drmppi.h"
 
+// The C-ABI environment the controllers hold: the strategic race's, or the gate race's
+// when the reference is built with USE_ENV_DRONERACE (include/config.h:17-19).
+#ifdef USE_ENV_DRONERACE
+using DrAdapterEnv = dr_gate_env_config;
+#else
+using DrAdapterEnv = dr_env_config;
+#endif
+
 // forward
 class SimulationEngine;
 
@@ -61,9 +69,9 @@ class MPPIController : public Controller
     std::vector<float> buildSplineMatrix();
 
   private:
-    dr_env_config envC{};
+    DrAdapterEnv envC{};
     dr_mppi_config cfgC{};
-    std::vector<float> grids; // host copies of the track grids (p, dp, t, kappa)
+    std::vector<float> grids; // host copies of the track grids (p, dp, t, kappa) or of the racelines
     int seed = 0;
     dr_mppi* h = nullptr;
 };
@@ -91,7 +99,7 @@ class PRMPPIController : public Controller
     float max_nu = 0.001f;
 
   private:
-    dr_env_config envC{};
+    DrAdapterEnv envC{};
     dr_prmppi_config cfgC{};
     std::vector<float> grids;
     int seed = 0;

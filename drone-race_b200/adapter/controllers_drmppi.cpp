@@ -29,6 +29,107 @@ void check(int status, const char* what)
         throw std::runtime_error(std::format("{}: {} ({})", what, dr_status_string(status), dr_last_error()));
 }
 
+// a host copy of n floats at p, which may be device memory (the engine passes the device
+// copy of the environment, engine.cpp:26,37,42)
+void hostCopy(const float* p, size_t n, float* out)
+{
+    cudaPointerAttributes attr{};
+    bool dev = cudaPointerGetAttributes(&attr, p) == cudaSuccess && attr.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+    if (dev)
+    {
+        if (cudaMemcpy(out, p, n * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+            throw std::runtime_error("copying the track from the device failed");
+    }
+    else
+        std::memcpy(out, p, n * sizeof(float));
+}
+
+#ifdef USE_ENV_DRONERACE
+// dr_gate_env_config from the gate race's EnvironmentConfig (env_dronerace_defs.h:60-93)
+void envFromRef(const EnvironmentConfig& c, dr_gate_env_config& e, std::vector<float>& track)
+{
+    constexpr int NTS = DR_N_TRACK_SAMPLES;
+    static_assert(Env::N_RACELINES == DR_GATE_RACELINES && Env::N_AGENTS == DR_GATE_AGENTS, "gate race sizes");
+    static_assert(Env::N_GATES <= DR_GATE_MAX_GATES && Env::N_OBSTACLES <= DR_GATE_MAX_OBSTACLES && Env::N_ROUND_OBSTACLES <= DR_GATE_MAX_OBSTACLES,
+                  "gate race sizes");
+    std::memset(&e, 0, sizeof(e));
+    e.n_theta = N_TRUE_MODELS;
+    for (int d = 0; d < DR_DIM; d++)
+    {
+        e.arena_min[d] = c.arenaMin[d];
+        e.arena_max[d] = c.arenaMax[d];
+    }
+    e.dt = c.dt;
+    e.send_states = c.sendStates ? 1 : 0;
+    e.drone_radius = c.droneRadius;
+    e.pos_noise_level = c.posNoiseLevel;
+    e.speed_noise_level = c.speedNoiseLevel;
+    e.action_noise_level = c.actionNoiseLevel;
+    for (int a = 0; a < Env::N_AGENTS; a++)
+    {
+        e.max_speed[a] = c.maxSpeed[a];
+        e.max_accel[a] = c.maxAccel[a];
+    }
+    e.n_win_laps = c.nWinLaps;
+    e.target_distance = c.targetDistance;
+    e.n_gates = Env::N_GATES;
+    for (int i = 0; i < Env::N_GATES * DR_DIM; i++)
+    {
+        e.gate_centers[i] = c.gateCenters[i];
+        e.gate_vectors[i] = c.gateVectors[i];
+    }
+    for (int i = 0; i < Env::N_GATES; i++)
+        e.gate_radius[i] = c.gateRadius[i];
+    e.n_obstacles = Env::N_OBSTACLES;
+    for (int i = 0; i < Env::N_OBSTACLES * DR_DIM * 2; i++)
+        e.obstacles[i] = c.obstacles[i];
+    e.n_round_obstacles = Env::N_ROUND_OBSTACLES;
+    for (int i = 0; i < Env::N_ROUND_OBSTACLES * DR_DIM; i++)
+        e.round_obs_centers[i] = c.roundObsCenters[i];
+    for (int i = 0; i < Env::N_ROUND_OBSTACLES; i++)
+        e.round_obs_radius[i] = c.roundObsRadius[i];
+    for (int th = 0; th < N_TRUE_MODELS; th++)
+    {
+        e.init_belief[th] = c.initBelief[th];
+        const auto& p = c.oppPid[th];
+        e.opp_pid[th] = dr_pid_config{p.kp, p.kd, p.repulsionFactor, p.repulsionPower, p.repulsionDistFact, p.racelineIndex, p.actionNoise};
+    }
+    e.i_mppi = c.iMppi;
+    track.assign((size_t)Env::N_RACELINES * NTS * DR_DIM, 0.0f);
+    hostCopy(c.trackPoints, track.size(), track.data());
+    e.track_points = track.data();
+}
+
+dr_gate_state stateFromRef(const SimState& s)
+{
+    dr_gate_state r;
+    std::memset(&r, 0, sizeof(r));
+    for (int i = 0; i < Env::N_AGENTS * DR_DIM; i++)
+    {
+        r.pos[i] = s.pos[i];
+        r.vel[i] = s.vel[i];
+    }
+    for (int i = 0; i < Env::N_AGENTS * Env::N_RACELINES; i++)
+        r.S[i] = s.S[i];
+    for (int a = 0; a < Env::N_AGENTS; a++)
+    {
+        r.laps[a] = s.laps[a];
+        r.gates[a] = s.gates[a];
+    }
+    return r;
+}
+
+int createMppi(const dr_gate_env_config* e, const dr_mppi_config* c, uint64_t seed, const float* nominal, int dev, dr_mppi** h)
+{
+    return dr_gate_mppi_create(e, c, seed, nominal, dev, nullptr, h);
+}
+
+int stepMppi(dr_mppi* h, const dr_gate_state* s, const float* belief, float* out, dr_mppi_info* info)
+{
+    return dr_gate_mppi_step(h, s, belief, out, info);
+}
+#else
 // dr_env_config from the reference's EnvironmentConfig, whose grid pointers are device
 // pointers here (the engine passes the device copy, engine.cpp:26,37,42).
 void envFromRef(const EnvironmentConfig& c, dr_env_config& e, std::vector<float>& grids)
@@ -77,16 +178,7 @@ void envFromRef(const EnvironmentConfig& c, dr_env_config& e, std::vector<float>
     size_t off = 0;
     for (int i = 0; i < 4; i++)
     {
-        cudaPointerAttributes attr{};
-        bool dev = cudaPointerGetAttributes(&attr, src[i]) == cudaSuccess && attr.type == cudaMemoryTypeDevice;
-        cudaGetLastError();
-        if (dev)
-        {
-            if (cudaMemcpy(grids.data() + off, src[i], n[i] * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
-                throw std::runtime_error("copying the track grids from the device failed");
-        }
-        else
-            std::memcpy(grids.data() + off, src[i], n[i] * sizeof(float));
+        hostCopy(src[i], n[i], grids.data() + off);
         off += n[i];
     }
     e.p_grid = grids.data();
@@ -112,6 +204,17 @@ dr_sim_state stateFromRef(const SimState& s)
     }
     return r;
 }
+
+int createMppi(const dr_env_config* e, const dr_mppi_config* c, uint64_t seed, const float* nominal, int dev, dr_mppi** h)
+{
+    return dr_mppi_create(e, c, seed, nominal, dev, nullptr, h);
+}
+
+int stepMppi(dr_mppi* h, const dr_sim_state* s, const float* belief, float* out, dr_mppi_info* info)
+{
+    return dr_mppi_step(h, s, belief, out, info);
+}
+#endif
 
 } // namespace
 
@@ -183,11 +286,11 @@ void MPPIController::getControl(const SimState& state, float* outAction)
     {
         int dev = 0;
         cudaGetDevice(&dev);
-        check(dr_mppi_create(&envC, &cfgC, (uint64_t)seed, h_nominal.data(), dev, nullptr, &h), "dr_mppi_create");
+        check(createMppi(&envC, &cfgC, (uint64_t)seed, h_nominal.data(), dev, &h), "dr_mppi_create");
     }
-    dr_sim_state s = stateFromRef(state);
+    auto s = stateFromRef(state);
     dr_mppi_info info{};
-    check(dr_mppi_step(h, &s, h_belief.data(), outAction, &info), "dr_mppi_step");
+    check(stepMppi(h, &s, h_belief.data(), outAction, &info), "dr_mppi_step");
     check(dr_mppi_get_fail_counts(h, failCountNew.data(), failCountOld.data(), failCount.data(), failCount.size()), "dr_mppi_get_fail_counts");
     check(dr_mppi_get_nominal(h, h_nominal.data(), h_nominal.size()), "dr_mppi_get_nominal");
     epsilon = info.epsilon;
@@ -249,6 +352,11 @@ void PRMPPIController::getControl(const SimState& state, float* outAction)
 {
     if (!engine)
         throw std::runtime_error("PRMPPI: engine not set");
+#ifdef USE_ENV_DRONERACE
+    (void)state;
+    (void)outAction;
+    throw std::runtime_error("PRMPPI: libdrmppi provides PR-MPPI on the strategic race only");
+#else
     if (!h)
     {
         int dev = 0;
@@ -261,4 +369,5 @@ void PRMPPIController::getControl(const SimState& state, float* outAction)
     check(dr_prmppi_get_nominals(h, h_nom_nominal.data(), h_rob_nominal.data(), h_nom_nominal.size()), "dr_prmppi_get_nominals");
     resetNom = info.reset_nom != 0;
     useNomPlan = info.use_nom_plan != 0;
+#endif
 }

@@ -42,7 +42,7 @@ def build(ref: bool = True) -> None:
 
     targets = ["port"]
     if ref and Path(os.environ.get("DR_REFERENCE", "/root/reference")).exists():
-        targets += ["ref", "engine"]
+        targets += ["ref", "engine", "adapter_gate"]
     subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "-j4", *targets], check=True)
 
 

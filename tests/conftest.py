@@ -45,6 +45,8 @@ def _ensure_oracle():
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "-j4", "ref"], check=True)
     if ref_src.exists() and not (O.REF_DIR / "libengine_dropin.so").exists() and drb.abi.LIB_PATH.exists():
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "engine"], check=True)
+    if ref_src.exists() and not (O.REF_DIR / "libadapter_gate.so").exists() and drb.abi.LIB_PATH.exists():
+        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "adapter_gate"], check=True)
 
 
 _ensure_oracle()

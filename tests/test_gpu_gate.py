@@ -202,3 +202,27 @@ def test_gate_state_type_is_checked(gpu):
     out = np.zeros(2, np.float32)
     rc = abi.lib().dr_mppi_step(ctl.handle, C.byref(abi.dr_sim_state()), abi.fptr(sc.belief()), abi.fptr(out), None)
     assert rc == abi.DR_ERR_INVALID_ARG
+
+
+@pytest.mark.skipif(not (O.REF_DIR / "libadapter_gate.so").exists(), reason="gate adapter build not present")
+def test_cpp_adapter_on_the_gate_race(gpu):
+    """The C++ drop-in (adapter/controllers.h + controllers_drmppi.cpp) compiled against the
+    reference's headers for the gate race: its MPPIController::getControl sequence equals
+    the Python controller's on the same configuration (both run this library)."""
+    import ctypes as CT
+
+    sc = small_gate(True, K=512, T=32, n_verif=512, noise=True, agent=1)
+    L = CT.CDLL(str(O.REF_DIR / "libadapter_gate.so"))
+    L.adapter_gate_run.restype = CT.c_int
+    L.adapter_gate_run.argtypes = [CT.POINTER(abi.dr_gate_env_config), CT.POINTER(abi.dr_mppi_config), CT.c_int, CT.POINTER(abi.dr_gate_state), CT.c_int,
+                                   CT.POINTER(CT.c_float), CT.POINTER(CT.c_float)]
+    n, nn = 3, (sc.n_theta + 1) * sc.mppi.n_timesteps * 2
+    acts = np.zeros((n, 2), np.float32)
+    noms = np.zeros((n, nn), np.float32)
+    assert L.adapter_gate_run(CT.byref(sc.env), CT.byref(sc.mppi), sc.seed, CT.byref(sc.state), n, abi.fptr(acts), abi.fptr(noms)) == 0
+    ctl = _ctl(sc)
+    ctl.engine = object()
+    for k in range(n):
+        a = ctl.getControl(sc.state)
+        assert np.array_equal(a, acts[k])
+        assert np.array_equal(ctl.h_nominal, noms[k])
