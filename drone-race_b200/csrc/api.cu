@@ -37,6 +37,7 @@ std::string& lastError()
 struct dr_mppi
 {
     int envKind = 0; // 0 strategic race, 1 gate race
+    int iMppi = 0;   // gate race: the ego's agent index
     int device = 0;
     cudaStream_t stream = nullptr;
     bool ownStream = false;
@@ -166,6 +167,7 @@ struct dr_mppi_batch
 {
     std::vector<dr_mppi*> hs;
     int envKind = 0;
+    int iMppi = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool ownStream = false;
@@ -202,12 +204,12 @@ struct dr_mppi_batch
 
     cudaError_t launchRollout(const LaunchArgs& a) const
     {
-        return envKind ? launchGateRollout(a, nth, spl, rollSmem) : launchMppiRollout(a, nopp, nth, spl, rollSmem);
+        return envKind ? launchGateRollout(a, nth, iMppi, spl, rollSmem) : launchMppiRollout(a, nopp, nth, spl, rollSmem);
     }
 
     cudaError_t launchVerify(const LaunchArgs& a) const
     {
-        return envKind ? launchGateVerify(a, nth, verSmem, nullptr, nullptr) : launchMppiVerify(a, nopp, nth, verSmem, nullptr, nullptr);
+        return envKind ? launchGateVerify(a, nth, iMppi, verSmem, nullptr, nullptr) : launchMppiVerify(a, nopp, nth, verSmem, nullptr, nullptr);
     }
 
     // kernels of one control step, reading inputs from `in` (device)
@@ -372,10 +374,12 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     b->spl = hs[0]->spl;
     b->verify = hs[0]->cfg.verify != 0;
     b->envKind = hs[0]->envKind;
+    b->iMppi = hs[0]->iMppi;
     for (int i = 0; i < n; i++)
         if (!hs[i] || hs[i]->device != b->device || hs[i]->nopp != b->nopp || hs[i]->nth != b->nth || hs[i]->spl != b->spl ||
-            (hs[i]->cfg.verify != 0) != b->verify || hs[i]->envKind != b->envKind)
-            return fail(DR_ERR_INVALID_ARG, "a batch needs controllers on one device with equal environment kind, n_opp, n_theta, use_splines and verify");
+            (hs[i]->cfg.verify != 0) != b->verify || hs[i]->envKind != b->envKind || hs[i]->iMppi != b->iMppi)
+            return fail(DR_ERR_INVALID_ARG,
+                        "a batch needs controllers on one device with equal environment kind, ego index, n_opp, n_theta, use_splines and verify");
     CK(cudaSetDevice(b->device));
     b->stream = stream;
     b->ownStream = ownStream;
@@ -534,6 +538,7 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
         return rc;
     auto h = std::make_unique<dr_mppi>();
     h->envKind = env ? 0 : 1;
+    h->iMppi = env ? 0 : genv->i_mppi;
     h->device = device;
     if (env)
     {
@@ -1066,7 +1071,7 @@ static int debugVerify(dr_mppi* h, const St* state, const float* belief, const f
         a.mppiIn = dIn;
         a.tiles = dT;
         a.nTiles = (int)tiles.size();
-        e = h->envKind ? launchGateVerify(a, h->nth, gateVerifySmem(h->nth, T), dFt, dTh)
+        e = h->envKind ? launchGateVerify(a, h->nth, h->iMppi, gateVerifySmem(h->nth, T), dFt, dTh)
                        : launchMppiVerify(a, h->nopp, h->nth, mppiVerifySmem(h->nth, T), dFt, dTh);
         std::vector<unsigned> fc(2 * T);
         if (e == cudaSuccess)

@@ -762,7 +762,7 @@ extern "C" int dr_gate_env_step(const dr_gate_env_config* env, int true_theta, c
     if (e == cudaSuccess)
         e = cudaMemcpy(db, belief, env->n_theta * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-        e = launchGateEnvStep(nullptr, env->n_theta, dgp, dtr, true_theta, action[0], action[1], ds, db, update_belief, (uint32_t)seed,
+        e = launchGateEnvStep(nullptr, env->n_theta, env->i_mppi, dgp, dtr, true_theta, action[0], action[1], ds, db, update_belief, (uint32_t)seed,
                               (uint32_t)(seed >> 32), (uint32_t)step, dt);
     if (e == cudaSuccess)
         e = cudaMemcpy(state, ds, sizeof(dr_gate_state), cudaMemcpyDeviceToHost);

@@ -68,7 +68,7 @@ __host__ __device__ inline GateSmem gateRolloutLayout(int nbp, int T, int M, boo
 
 // fullRolloutKernel (kernels.cu:34-171) + aggregateBranchCostsKernel (175-217) on the
 // gate race: environmentStep<true, true, false> (kernels.cu:141-143).
-template <int NTH, bool SPL>
+template <int NTH, bool SPL, int ME>
 __global__ void __launch_bounds__(GRB) gate_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles)
 {
     constexpr int NBP = NTH + 1;
@@ -179,14 +179,14 @@ __global__ void __launch_bounds__(GRB) gate_rollout(const MppiDev* __restrict__ 
                 ego1 = sKn[(b * T + local) * 2 + 1] + e1;
             }
             bool branched = false;
-            StepOut o = gateStep<NTH, true, true, false, true>(t, th, sTrack, G, ego0, ego1, st, bs, branched, minConf, rng, gateMargin);
+            StepOut o = gateStep<NTH, true, true, false, true, ME>(t, th, sTrack, G, ego0, ego1, st, bs, branched, minConf, rng, gateMargin);
             if (branched)
                 tOrigin = t + 1;
             stop = (o.term != TERM_NONE);
             cost += gateStateCost(o, G, D.cfg.w) * decay;
             decay *= DECAY;
         }
-        cost += gateFinalCost(st, G, D.cfg.w.finalAdvWeight, D.cfg.w.finalOppAdvWeight);
+        cost += gateFinalCost<ME>(st, G, D.cfg.w.finalAdvWeight, D.cfg.w.finalOppAdvWeight);
         pt = bs.predTheta;
         bt = bs.branchingTime;
     }
@@ -235,8 +235,11 @@ __global__ void __launch_bounds__(GRB) gate_rollout(const MppiDev* __restrict__ 
 // verifyNominalFailureKernel (kernels.cu:488-551) on the gate race:
 // environmentStep<true, true, false, false>; one thread per sample, both plans in one
 // grid, the CTA's warps in step (a barrier per step) as in mppi_verify.
-template <int NTH>
-__global__ void __launch_bounds__(VERIFY_TILE, 1) gate_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
+#ifndef GATE_VERIFY_MIN_BLOCKS
+#define GATE_VERIFY_MIN_BLOCKS 1
+#endif
+template <int NTH, int ME>
+__global__ void __launch_bounds__(VERIFY_TILE, GATE_VERIFY_MIN_BLOCKS) gate_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
                                                              int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
 {
     constexpr int NBP = NTH + 1;
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(VERIFY_TILE, 1) gate_verify(const MppiDev* __r
             int b = bs.predTheta;
             float e0 = sPlan[(b * T + local) * 2], e1 = sPlan[(b * T + local) * 2 + 1];
             bool branched = false;
-            StepOut o = gateStep<NTH, true, true, false, false>(t, theta, sTrack, G, e0, e1, st, bs, branched, minConf, rng, gateMargin);
+            StepOut o = gateStep<NTH, true, true, false, false, ME>(t, theta, sTrack, G, e0, e1, st, bs, branched, minConf, rng, gateMargin);
             if (branched)
                 tOrigin = t + 1;
             if (o.term == TERM_LOSE)
@@ -350,7 +353,7 @@ __global__ void __launch_bounds__(VERIFY_TILE, 1) gate_verify(const MppiDev* __r
 }
 
 // One true-dynamics step (environmentStep with noise, as the engine's dynStep).
-template <int NTH>
+template <int NTH, int ME>
 __global__ void gate_env_step_kernel(const GateParams* __restrict__ gp, const float* __restrict__ track, int trueTheta, float a0, float a1,
                                      dr_gate_state* st, float* belief, int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term)
 {
@@ -375,9 +378,9 @@ __global__ void gate_env_step_kernel(const GateParams* __restrict__ gp, const fl
     bool branched = false;
     StepOut o;
     if (updateBelief)
-        o = gateStep<NTH, true, false, false, true>(0, trueTheta, track, sG, a0, a1, s, bs, branched, 2.0f, rng, 0.0f);
+        o = gateStep<NTH, true, false, false, true, ME>(0, trueTheta, track, sG, a0, a1, s, bs, branched, 2.0f, rng, 0.0f);
     else
-        o = gateStep<NTH, false, false, false, true>(0, trueTheta, track, sG, a0, a1, s, bs, branched, 2.0f, rng, 0.0f);
+        o = gateStep<NTH, false, false, false, true, ME>(0, trueTheta, track, sG, a0, a1, s, bs, branched, 2.0f, rng, 0.0f);
     storeGState(*st, s);
     for (int i = 0; i < NTH; i++)
         belief[i] = bs.belief[i];
@@ -407,67 +410,74 @@ int gateRolloutSamplesPerBlock(int nth)
     return GRB / nth;
 }
 
-template <int NTH> static cudaError_t launchGateRolloutT(const LaunchArgs& a, bool spl, size_t smem)
+template <int NTH, int ME> static cudaError_t launchGateRolloutT(const LaunchArgs& a, bool spl, size_t smem)
 {
     if (spl)
     {
-        auto k = gate_rollout<NTH, true>;
+        auto k = gate_rollout<NTH, true, ME>;
         ensureSmem(k, smem);
         k<<<a.nTiles, GRB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles);
     }
     else
     {
-        auto k = gate_rollout<NTH, false>;
+        auto k = gate_rollout<NTH, false, ME>;
         ensureSmem(k, smem);
         k<<<a.nTiles, GRB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles);
     }
     return cudaGetLastError();
 }
 
-template <int NTH> static cudaError_t launchGateVerifyT(const LaunchArgs& a, size_t smem, int* ft, int* th)
+template <int NTH, int ME> static cudaError_t launchGateVerifyT(const LaunchArgs& a, size_t smem, int* ft, int* th)
 {
-    auto k = gate_verify<NTH>;
+    auto k = gate_verify<NTH, ME>;
     ensureSmem(k, smem);
     k<<<a.nTiles, VERIFY_TILE, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, ft, th);
     return cudaGetLastError();
 }
 
-cudaError_t launchGateRollout(const LaunchArgs& a, int nth, bool spl, size_t smem)
-{
-    switch (nth)
-    {
-    case 1: return launchGateRolloutT<1>(a, spl, smem);
-    case 2: return launchGateRolloutT<2>(a, spl, smem);
-    case 4: return launchGateRolloutT<4>(a, spl, smem);
-    case 8: return launchGateRolloutT<8>(a, spl, smem);
-    default: return cudaErrorInvalidValue;
+// (n_theta, ego index) -> instantiation
+#define GATE_DISPATCH(NTH_, ME_, CALL)                                                                                                                \
+    switch ((NTH_) * 2 + (ME_))                                                                                                                      \
+    {                                                                                                                                                \
+    case 1 * 2 + 0: return CALL(1, 0);                                                                                                              \
+    case 1 * 2 + 1: return CALL(1, 1);                                                                                                              \
+    case 2 * 2 + 0: return CALL(2, 0);                                                                                                              \
+    case 2 * 2 + 1: return CALL(2, 1);                                                                                                              \
+    case 4 * 2 + 0: return CALL(4, 0);                                                                                                              \
+    case 4 * 2 + 1: return CALL(4, 1);                                                                                                              \
+    case 8 * 2 + 0: return CALL(8, 0);                                                                                                              \
+    case 8 * 2 + 1: return CALL(8, 1);                                                                                                              \
+    default: return cudaErrorInvalidValue;                                                                                                           \
     }
+
+cudaError_t launchGateRollout(const LaunchArgs& a, int nth, int me, bool spl, size_t smem)
+{
+#define CALL(P, Q) launchGateRolloutT<P, Q>(a, spl, smem)
+    GATE_DISPATCH(nth, me, CALL)
+#undef CALL
 }
 
-cudaError_t launchGateVerify(const LaunchArgs& a, int nth, size_t smem, int* dbgFailTime, int* dbgTheta)
+cudaError_t launchGateVerify(const LaunchArgs& a, int nth, int me, size_t smem, int* dbgFailTime, int* dbgTheta)
 {
-    switch (nth)
-    {
-    case 1: return launchGateVerifyT<1>(a, smem, dbgFailTime, dbgTheta);
-    case 2: return launchGateVerifyT<2>(a, smem, dbgFailTime, dbgTheta);
-    case 4: return launchGateVerifyT<4>(a, smem, dbgFailTime, dbgTheta);
-    case 8: return launchGateVerifyT<8>(a, smem, dbgFailTime, dbgTheta);
-    default: return cudaErrorInvalidValue;
-    }
+#define CALL(P, Q) launchGateVerifyT<P, Q>(a, smem, dbgFailTime, dbgTheta)
+    GATE_DISPATCH(nth, me, CALL)
+#undef CALL
 }
 
-cudaError_t launchGateEnvStep(cudaStream_t stream, int nth, const GateParams* gp, const float* track, int trueTheta, float a0, float a1,
+template <int NTH, int ME>
+static cudaError_t launchGateEnvStepT(cudaStream_t stream, const GateParams* gp, const float* track, int trueTheta, float a0, float a1, dr_gate_state* st,
+                                      float* belief, int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term)
+{
+    gate_env_step_kernel<NTH, ME><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term);
+    return cudaGetLastError();
+}
+
+cudaError_t launchGateEnvStep(cudaStream_t stream, int nth, int me, const GateParams* gp, const float* track, int trueTheta, float a0, float a1,
                               dr_gate_state* st, float* belief, int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term)
 {
-    switch (nth)
-    {
-    case 1: gate_env_step_kernel<1><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term); break;
-    case 2: gate_env_step_kernel<2><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term); break;
-    case 4: gate_env_step_kernel<4><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term); break;
-    case 8: gate_env_step_kernel<8><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term); break;
-    default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+#define CALL(P, Q) launchGateEnvStepT<P, Q>(stream, gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term)
+    GATE_DISPATCH(nth, me, CALL)
+#undef CALL
 }
 
 } // namespace dr

@@ -188,13 +188,17 @@ __device__ __forceinline__ float projectGreedy(const float* __restrict__ tp, flo
     return ((float)bI) / NTS;
 }
 
-// computePIDAction, :473-541, for hypothesis th
-__device__ __forceinline__ void pidAction(int agent, const GState& s, const GateParams& G, const float* __restrict__ track, int th, float& out0,
-                                          float& out1)
+// computePIDAction, :473-541, for hypothesis th. The agent is a template parameter and
+// the raceline's arc length is selected, so that the state stays in registers.
+template <int AGENT>
+__device__ __forceinline__ void pidAction(const GState& s, const GateParams& G, const float* __restrict__ track, int th, float& out0, float& out1)
 {
+    constexpr int agent = AGENT;
+    static_assert(G_NR == 2, "two racelines");
     const int rl = G.pidRaceline[th];
+    const float sRl = rl == 0 ? s.S[agent * G_NR] : s.S[agent * G_NR + 1];
     float tx, ty;
-    sampleCenterline(track + rl * NTS * 2, s.S[agent * G_NR + rl] + G.targetDistance, tx, ty);
+    sampleCenterline(track + rl * NTS * 2, sRl + G.targetDistance, tx, ty);
     const float cx = s.pos[agent * 2], cy = s.pos[agent * 2 + 1];
     const float vx = s.vel[agent * 2], vy = s.vel[agent * 2 + 1];
     float sqError = 0.0f;
@@ -224,7 +228,7 @@ __device__ __forceinline__ void pidAction(int agent, const GState& s, const Gate
     const float repF = G.pidRepF[th];
     if (repF != 0.0f)
     {
-        const int other = 1 - agent;
+        constexpr int other = 1 - agent;
         float d0 = s.pos[other * 2] - cx, d1 = s.pos[other * 2 + 1] - cy;
         float dist2 = 0.0f;
         dist2 += d0 * d0;
@@ -295,10 +299,11 @@ __device__ __forceinline__ void updateGates(const GateParams& G, const float* __
     }
 }
 
-// trackBoundaryDist<false>, :262-307 (the opponent-win shortcut is applied by callers)
-__device__ __forceinline__ float gateBoundaryDist(const GState& s, const GateParams& G)
+// trackBoundaryDist<false>, :262-307 (the opponent-win shortcut is applied by callers);
+// ME is the ego's index (envConfig.iMppi)
+template <int ME> __device__ __forceinline__ float gateBoundaryDist(const GState& s, const GateParams& G)
 {
-    const int me = G.iMppi;
+    constexpr int me = ME;
     const float c0 = s.pos[me * 2], c1 = s.pos[me * 2 + 1];
     float minDist = INFINITY;
     minDist = fminf(minDist, fminf(c0 - G.arenaMin[0], G.arenaMax[0] - c0));
@@ -331,11 +336,11 @@ __device__ __forceinline__ float gateBoundaryDist(const GState& s, const GatePar
 }
 
 // isWinner, :316-360 (the upper arena test adds the radius, as the reference does)
-__device__ __forceinline__ bool gateIsWinner(const GState& s, const GateParams& G)
+template <int ME> __device__ __forceinline__ bool gateIsWinner(const GState& s, const GateParams& G)
 {
-    if (s.laps[G.iMppi] >= G.nWinLaps)
+    if (s.laps[ME] >= G.nWinLaps)
         return true;
-    const int o = 1 - G.iMppi;
+    constexpr int o = 1 - ME;
     const float c0 = s.pos[o * 2], c1 = s.pos[o * 2 + 1];
     const float radius = G.droneRadius;
     if (c0 < G.arenaMin[0] + radius || c0 > G.arenaMax[0] + radius)
@@ -366,8 +371,9 @@ __device__ __forceinline__ bool gateIsWinner(const GState& s, const GateParams& 
 }
 
 // getAnyAdvance, :374-394
-__device__ __forceinline__ float gateAdvance(const GState& s, const GateParams& G, int agent)
+template <int AGENT> __device__ __forceinline__ float gateAdvance(const GState& s, const GateParams& G)
 {
+    constexpr int agent = AGENT;
     float sqGateDist = 0.0f, sqConsGateDist = 0.0f;
     int nextGate = (s.gates[agent] + 1) % G.nGates;
     float scale = 0.8f;
@@ -383,11 +389,11 @@ __device__ __forceinline__ float gateAdvance(const GState& s, const GateParams& 
 
 // environmentStep<UPD, BR, ADDMARGIN, LOSE>, :546-680. The ego's action is (ego0, ego1);
 // the returned StepOut carries what the running cost needs.
-template <int NTH, bool UPD, bool BR, bool ADDMARGIN, bool LOSE>
+template <int NTH, bool UPD, bool BR, bool ADDMARGIN, bool LOSE, int ME>
 __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* __restrict__ track, const GateParams& G, float ego0, float ego1,
                                             GState& s, BState<NTH>& bs, bool& branched, float minConf, EnvNoise& rng, float gateMargin)
 {
-    const int me = G.iMppi, opp = 1 - me;
+    constexpr int me = ME, opp = 1 - ME;
     float prevPos[G_NA * 2];
 #pragma unroll
     for (int i = 0; i < G_NA * 2; i++)
@@ -400,7 +406,7 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
     {
 #pragma unroll
         for (int th = 0; th < NTH; th++)
-            pidAction(opp, s, G, track, th, nom0[th], nom1[th]);
+            pidAction<opp>(s, G, track, th, nom0[th], nom1[th]);
         u0 = nom0[0];
         u1 = nom1[0];
 #pragma unroll
@@ -412,7 +418,7 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
             }
     }
     else
-        pidAction(opp, s, G, track, trueTheta, u0, u1);
+        pidAction<opp>(s, G, track, trueTheta, u0, u1);
     {
         float an = G.pidNoise[trueTheta];
         if (an != 0.0f)
@@ -531,8 +537,8 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
     // terminal checks (:672-679)
     StepOut r;
     bool oppWon = s.laps[opp] >= G.nWinLaps;
-    float bdRaw = gateBoundaryDist(s, G);
-    bool winner = gateIsWinner(s, G);
+    float bdRaw = gateBoundaryDist<ME>(s, G);
+    bool winner = gateIsWinner<ME>(s, G);
     float bdTerm = (LOSE && oppWon) ? -1.0f : bdRaw;
     int term = TERM_NONE;
     if (bdTerm < G.droneRadius)
@@ -566,11 +572,12 @@ __device__ __forceinline__ float gateStateCost(const StepOut& o, const GateParam
 }
 
 // finalCost (costs.cuh:31-39)
+template <int ME>
 __device__ __forceinline__ float gateFinalCost(const GState& s, const GateParams& G, float finalAdvWeight, float finalOppAdvWeight)
 {
-    float cost = -finalAdvWeight * gateAdvance(s, G, G.iMppi);
+    float cost = -finalAdvWeight * gateAdvance<ME>(s, G);
     if (finalOppAdvWeight != 0.0f)
-        cost += finalOppAdvWeight * gateAdvance(s, G, 1 - G.iMppi);
+        cost += finalOppAdvWeight * gateAdvance<1 - ME>(s, G);
     return cost;
 }
 

@@ -41,9 +41,10 @@ bool gateSupported(int nth);
 int gateRolloutSamplesPerBlock(int nth);
 size_t gateRolloutSmem(int nth, int T, int M, bool spl);
 size_t gateVerifySmem(int nth, int T);
-cudaError_t launchGateRollout(const LaunchArgs& a, int nth, bool spl, size_t smem);
-cudaError_t launchGateVerify(const LaunchArgs& a, int nth, size_t smem, int* dbgFailTime, int* dbgTheta);
-cudaError_t launchGateEnvStep(cudaStream_t stream, int nth, const GateParams* gp, const float* track, int trueTheta, float a0, float a1,
+// `me`: the ego's agent index (the environment's i_mppi)
+cudaError_t launchGateRollout(const LaunchArgs& a, int nth, int me, bool spl, size_t smem);
+cudaError_t launchGateVerify(const LaunchArgs& a, int nth, int me, size_t smem, int* dbgFailTime, int* dbgTheta);
+cudaError_t launchGateEnvStep(cudaStream_t stream, int nth, int me, const GateParams* gp, const float* track, int trueTheta, float a0, float a1,
                               dr_gate_state* st, float* belief, int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term);
 
 bool prSupported(int nopp, int nth);
