@@ -13,12 +13,15 @@ from pathlib import Path
 
 import numpy as np
 
+DR_ABI_VERSION = 2
 DR_DIM = 2
 DR_MAX_OPP = 3
 DR_MAX_AGENTS = 4
 DR_MAX_THETA = 8
 DR_MAX_KNOTS = 64
 DR_MAX_T = 256
+DR_GRAD_MAX_STEPS = 8
+DR_GRAD_WEIGHTS = 6
 DR_N_TRACK_SAMPLES = 512
 
 DR_OK = 0
@@ -147,6 +150,9 @@ class dr_mppi_info(C.Structure):
         ("inv_temperature", C.c_float),
         ("nonfinite_costs", C.c_int32),
         ("verif_timeouts", C.c_int32),
+        ("grad_cost_plain", C.c_float),
+        ("grad_cost_refined", C.c_float),
+        ("grad_best_step", C.c_int32),
     ]
 
 
@@ -296,6 +302,9 @@ _PROTOS = {
     "dr_mppi_rollout_costs_noalloc": (C.c_int, [C.POINTER(dr_env_config), C.POINTER(dr_mppi_config), C.c_uint64, C.c_uint64, C.POINTER(dr_sim_state),
                                                 C.POINTER(C.c_float), C.c_void_p, C.c_void_p, C.c_void_p]),
     "dr_spline_matrix": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    "dr_mppi_nominal_grad": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_int, C.c_void_p]),
+    "dr_mppi_set_grad_refine": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_int]),
     "dr_env_step": (C.c_int, [C.POINTER(dr_env_config), C.c_int, C.POINTER(C.c_float), C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_int)]),
     "dr_gate_mppi_create": (C.c_int, [C.POINTER(dr_gate_env_config), C.POINTER(dr_mppi_config), C.c_uint64, C.POINTER(C.c_float), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dr_gate_mppi_step": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_mppi_info)]),
@@ -346,6 +355,8 @@ def lib(path: str | os.PathLike | None = None) -> C.CDLL:
         f = getattr(L, name)
         f.restype = res
         f.argtypes = args
+    if L.dr_abi_version() != DR_ABI_VERSION:
+        raise RuntimeError(f"{p}: ABI version {L.dr_abi_version()}, these bindings expect {DR_ABI_VERSION}: rebuild it")
     if path is None:
         _lib = L
     return L

@@ -96,6 +96,13 @@ class MPPIController(Controller):
         check(lib().dr_mppi_get_nominal(self._h, abi.fptr(out), out.size), "dr_mppi_get_nominal")
         return out
 
+    def set_grad_refine(self, steps: int, step_size: float = 0.05, ckpt_stride: int = 0) -> None:
+        """Gradient-refined MPPI: `steps` projected gradient steps on the noise-free
+        rollout objective after each update, the best of the plain update and the
+        iterates kept (dr_mppi_set_grad_refine). Strategic race only; call it before
+        batching this controller."""
+        check(lib().dr_mppi_set_grad_refine(self._h, int(steps), float(step_size), int(ckpt_stride)), "dr_mppi_set_grad_refine")
+
     def knots(self) -> np.ndarray:
         M = int(self.mppiConfig.n_knots) if self.mppiConfig.use_splines else self.T
         out = np.zeros(self.nbp * M * 2, np.float32)

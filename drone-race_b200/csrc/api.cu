@@ -59,6 +59,13 @@ struct dr_mppi
     int pendBranch = -1, pendUseNew = 0;
     ClopperPearson cp;
     dr_mppi_batch* self = nullptr; // batch of one used by dr_mppi_step
+    // gradient refinement after the update (dr_mppi_set_grad_refine)
+    int gradSteps = 0, gradCkpt = 1;
+    float gradAlpha = 0.05f;
+    // dr_mppi_nominal_grad: device input record and job table
+    MppiIn* dGradIn = nullptr;
+    GradJob* dGradJobs = nullptr;
+    int gradJobsCap = 0;
 
     MppiIn input(const dr_sim_state& s, const float* belief) const
     {
@@ -159,6 +166,20 @@ struct dr_mppi
             info->inv_temperature = lambda;
             info->nonfinite_costs = stats[0];
             info->verif_timeouts = stats[1];
+            const float* gstat = (const float*)(r + ((const unsigned char*)desc.gstat - (const unsigned char*)desc.fail));
+            if (gradSteps > 0)
+            {
+                const int bestIt = std::min(std::max((int)gstat[DR_GRAD_MAX_STEPS + 1], 0), DR_GRAD_MAX_STEPS);
+                info->grad_cost_plain = gstat[0];
+                info->grad_cost_refined = gstat[bestIt];
+                info->grad_best_step = bestIt;
+            }
+            else
+            {
+                info->grad_cost_plain = 0.0f;
+                info->grad_cost_refined = 0.0f;
+                info->grad_best_step = -1;
+            }
         }
     }
 };
@@ -178,6 +199,9 @@ struct dr_mppi_batch
     MppiIn* hIn = nullptr;
     Tile *dRoll = nullptr, *dUpd = nullptr, *dVer = nullptr, *dVerNew = nullptr, *dVerOld = nullptr;
     int nRoll = 0, nUpd = 0, nVer = 0, nVerNew = 0, nVerOld = 0;
+    GradJob* dGrad = nullptr; // gradient refinement jobs (controllers with it on)
+    int nGrad = 0;
+    size_t gradSmemB = 0;
     size_t rollSmem = 0, verSmem = 0, proSmem = 0;
     bool overlap = true;                 // previous-plan verification on sideStream
     cudaStream_t sideStream = nullptr;
@@ -251,6 +275,12 @@ struct dr_mppi_batch
         if (profile)
             timer->mark("update", stream);
         CK(launchMppiUpdate(args(dUpd, nUpd, in), nth));
+        if (nGrad > 0)
+        {
+            if (profile)
+                timer->mark("grad_refine", stream);
+            CK(launchGradNominal(stream, dGrad, nGrad, nopp, nth, spl, gradSmemB));
+        }
         if (verify && nVerNew > 0)
         {
             if (profile)
@@ -330,7 +360,7 @@ struct dr_mppi_batch
         return DR_OK;
     }
 
-    void release()
+    void dropGraph()
     {
         if (graphExec)
             cudaGraphExecDestroy(graphExec);
@@ -338,6 +368,50 @@ struct dr_mppi_batch
             cudaGraphDestroy(graph);
         graphExec = nullptr;
         graph = nullptr;
+    }
+
+    // (Re)builds the gradient refinement job table from the controllers' settings.
+    int setupGrad()
+    {
+        CK(cudaSetDevice(device));
+        CK(cudaStreamSynchronize(stream));
+        dropGraph();
+        std::vector<GradJob> jobs;
+        gradSmemB = 0;
+        for (size_t i = 0; i < hs.size(); i++)
+        {
+            dr_mppi* h = hs[i];
+            if (h->gradSteps <= 0)
+                continue;
+            GradJob j{};
+            j.D = dDesc + i;
+            j.in = dIn + i;
+            j.J = h->desc.gstat;
+            j.stats = h->desc.gstat + DR_GRAD_MAX_STEPS + 1;
+            j.iters = h->gradSteps;
+            j.ckpt = h->gradCkpt;
+            j.alpha = h->gradAlpha;
+            j.write = 1;
+            jobs.push_back(j);
+            gradSmemB = std::max(gradSmemB, gradSmem(nopp, nth, h->T, h->M, h->gradCkpt, spl));
+        }
+        if (dGrad)
+            CK(cudaFree(dGrad));
+        dGrad = nullptr;
+        nGrad = (int)jobs.size();
+        if (nGrad > 0)
+        {
+            CK(cudaMalloc(&dGrad, sizeof(GradJob) * jobs.size()));
+            CK(cudaMemcpy(dGrad, jobs.data(), sizeof(GradJob) * jobs.size(), cudaMemcpyHostToDevice));
+        }
+        return DR_OK;
+    }
+
+    void release()
+    {
+        dropGraph();
+        cudaFree(dGrad);
+        dGrad = nullptr;
         cudaFree(dDesc);
         cudaFree(dIn);
         cudaFree(dRoll);
@@ -434,6 +508,9 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     CK(cudaStreamCreateWithFlags(&b->sideStream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&b->evFork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&b->evJoin, cudaEventDisableTiming));
+    int rc = b->setupGrad();
+    if (rc)
+        return rc;
     *out = b.release();
     return DR_OK;
 }
@@ -615,7 +692,8 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     A.add(counter, 16);
     // result block, one contiguous range
     size_t oFail = 0, oDense = a16(oFail + (size_t)2 * T * 4), oPrev = oDense + a16((size_t)nbp * T * 2 * 4), oNu = oPrev + a16((size_t)nbp * T * 2 * 4),
-           oMin = oNu + a16((size_t)nbp * 4), oStats = oMin + a16((size_t)nbp * M * 4), resBytes = oStats + 16;
+           oMin = oNu + a16((size_t)nbp * 4), oStats = oMin + a16((size_t)nbp * M * 4), oGrad = oStats + 16,
+           resBytes = oGrad + a16((DR_GRAD_MAX_STEPS + 3) * 4);
     unsigned char* res;
     A.add(res, resBytes);
     CK(A.alloc());
@@ -625,6 +703,7 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     nu = (float*)(res + oNu);
     minCosts = (float*)(res + oMin);
     stats = (int*)(res + oStats);
+    D.gstat = (float*)(res + oGrad);
     D.grids = env ? grids : nullptr;
     D.gate = gp;
     D.gtrack = gtrack;
@@ -715,6 +794,8 @@ int dr_mppi_destroy(dr_mppi* h)
         h->self->release();
         delete h->self;
     }
+    cudaFree(h->dGradIn);
+    cudaFree(h->dGradJobs);
     h->arena.release();
     if (h->hRes)
         cudaFreeHost(h->hRes);
@@ -796,6 +877,79 @@ int dr_mppi_io_bytes(const dr_mppi* h, size_t* h2d, size_t* d2h)
         *h2d = sizeof(MppiIn);
     if (d2h)
         *d2h = h->desc.resBytes;
+    return DR_OK;
+}
+
+int dr_mppi_set_grad_refine(dr_mppi* h, int steps, float step_size, int ckpt_stride)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    if (h->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "the gradient path is built for the strategic race");
+    if (steps < 0 || steps > DR_GRAD_MAX_STEPS)
+        return fail(DR_ERR_INVALID_ARG, "steps must be in [0, DR_GRAD_MAX_STEPS]");
+    if (steps > 0 && !(step_size > 0.0f && std::isfinite(step_size)))
+        return fail(DR_ERR_INVALID_ARG, "step_size must be positive");
+    if (ckpt_stride < 0 || ckpt_stride > h->T)
+        return fail(DR_ERR_INVALID_ARG, "ckpt_stride must be in [0, n_timesteps]");
+    const int ck = ckpt_stride ? ckpt_stride : gradDefaultStride(h->T);
+    if (steps > 0 && gradSmem(h->nopp, h->nth, h->T, h->M, ck, h->spl) > 227 * 1024)
+        return fail(DR_ERR_INVALID_ARG, "checkpoint stride x horizon too large for shared memory");
+    h->gradSteps = steps;
+    h->gradAlpha = step_size;
+    h->gradCkpt = ck;
+    return h->self->setupGrad();
+}
+
+int dr_mppi_nominal_grad(dr_mppi* h, const dr_sim_state* state, const float* belief, int n, const float* knots_dev, const float* weights_dev,
+                         float* cost_dev, float* d_knots_dev, float* d_weights_dev, int ckpt_stride, void* stream)
+{
+    if (!h || !state || !belief || !knots_dev || !cost_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "the gradient path is built for the strategic race");
+    if (n < 1 || n > 65535)
+        return fail(DR_ERR_INVALID_ARG, "n must be in [1, 65535]");
+    if (ckpt_stride < 0 || ckpt_stride > h->T)
+        return fail(DR_ERR_INVALID_ARG, "ckpt_stride must be in [0, n_timesteps]");
+    const int ck = ckpt_stride ? ckpt_stride : gradDefaultStride(h->T);
+    const size_t smem = gradSmem(h->nopp, h->nth, h->T, h->M, ck, h->spl);
+    if (smem > 227 * 1024)
+        return fail(DR_ERR_INVALID_ARG, "checkpoint stride x horizon too large for shared memory");
+    CK(cudaSetDevice(h->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!h->dGradIn)
+        CK(cudaMalloc(&h->dGradIn, sizeof(MppiIn)));
+    if (h->gradJobsCap < n)
+    {
+        CK(cudaStreamSynchronize(s));
+        cudaFree(h->dGradJobs);
+        h->dGradJobs = nullptr;
+        h->gradJobsCap = 0;
+        CK(cudaMalloc(&h->dGradJobs, sizeof(GradJob) * (size_t)n));
+        h->gradJobsCap = n;
+    }
+    const MppiIn in = h->input(*state, belief);
+    const size_t nU = (size_t)h->nbp * h->M * 2;
+    std::vector<GradJob> jobs((size_t)n);
+    for (int i = 0; i < n; i++)
+    {
+        GradJob& j = jobs[(size_t)i];
+        j = GradJob{};
+        j.D = h->self->dDesc;
+        j.in = h->dGradIn;
+        j.U = knots_dev + nU * (size_t)i;
+        j.w6 = weights_dev ? weights_dev + (size_t)DR_GRAD_WEIGHTS * i : nullptr;
+        j.J = cost_dev + i;
+        j.gU = d_knots_dev ? d_knots_dev + nU * (size_t)i : nullptr;
+        j.gW = d_weights_dev ? d_weights_dev + (size_t)DR_GRAD_WEIGHTS * i : nullptr;
+        j.iters = 0;
+        j.ckpt = ck;
+    }
+    // pageable sources: both copies are staged before the calls return
+    CK(cudaMemcpyAsync(h->dGradIn, &in, sizeof(MppiIn), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->dGradJobs, jobs.data(), sizeof(GradJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+    CK(launchGradNominal(s, h->dGradJobs, n, h->nopp, h->nth, h->spl, smem));
     return DR_OK;
 }
 

@@ -39,7 +39,8 @@ struct MppiIn
 
 // Device buffers of an MPPI instance. `res` is the start of the contiguous result
 // block copied to the host after each step:
-//   fail[2][T] u32 | dense[nbp][T][2] | prevDense[nbp][T][2] | nu[nbp] | minCosts[nbp][M] | stats[4] i32
+//   fail[2][T] u32 | dense[nbp][T][2] | prevDense[nbp][T][2] | nu[nbp] | minCosts[nbp][M] | stats[4] i32 |
+//   gstat[DR_GRAD_MAX_STEPS + 3] f32
 struct MppiDev
 {
     EnvParams env;       // strategic race (for the gate race only maxAccel[0], the ego's, is set)
@@ -60,6 +61,7 @@ struct MppiDev
     float* nu;           // [nbp]
     float* minCosts;     // [nbp][M]
     int* stats;          // [0] non-finite costs, [1] timeouts
+    float* gstat;        // gradient refinement: objective of iterates 0..DR_GRAD_MAX_STEPS, best iterate, last iterate
     size_t resBytes;
 };
 

@@ -47,6 +47,28 @@ cudaError_t launchGateVerify(const LaunchArgs& a, int nth, int me, size_t smem, 
 cudaError_t launchGateEnvStep(cudaStream_t stream, int nth, int me, const GateParams* gp, const float* track, int trueTheta, float a0, float a1,
                               dr_gate_state* st, float* belief, int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term);
 
+// One gradient-path job (grad_kernels.cu): the objective of an instance's noise-free
+// rollout at a start point U, its gradients, and optionally projected gradient steps.
+struct GradJob
+{
+    const MppiDev* D;
+    const MppiIn* in;
+    const float* U;  // start point [nbp][M][2] (null: the instance's knots)
+    const float* w6; // cost weights, grad::WeightIndex order (null: the instance's)
+    float* J;        // objective of each iterate, [iters + 1] (or null)
+    float* gU;       // gradient at the start point with respect to U (or null)
+    float* gW;       // gradient at the start point with respect to the weights (or null)
+    float* stats;    // [0] iterate with the lowest objective, [1] last iterate evaluated (or null)
+    int iters;       // projected gradient steps (0: evaluate once)
+    int ckpt;        // checkpoint stride of the adjoint sweep, 1..T
+    float alpha;     // step, as a fraction of the ego's acceleration limit
+    int write;       // write the best iterate to the instance's knots and dense plan
+};
+
+size_t gradSmem(int nopp, int nth, int T, int M, int ckpt, bool spl);
+int gradDefaultStride(int T);
+cudaError_t launchGradNominal(cudaStream_t stream, const GradJob* jobs, int nJobs, int nopp, int nth, bool spl, size_t smem);
+
 bool prSupported(int nopp, int nth);
 int prRolloutSamplesPerBlock();
 size_t prRolloutSmem(int T);

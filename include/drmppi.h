@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define DR_ABI_VERSION 1
+#define DR_ABI_VERSION 2
 
 #define DR_DIM 2             /* reference EnvStratRace::DIM == ACTION_DIM (env_stratrace_defs.h:9,15) */
 #define DR_MAX_OPP 3         /* reference N_OPP (compile-time 1, env_stratrace_defs.h:10) */
@@ -35,6 +35,8 @@ extern "C" {
 #define DR_MAX_THETA 8       /* reference N_TRUE_MODELS (compile-time 2) */
 #define DR_MAX_KNOTS 64      /* reference MAX_N_KNOTS = 60 (include/config.h:27) */
 #define DR_MAX_T 256         /* longest horizon accepted (dense mode: nKnots = nTimesteps) */
+#define DR_GRAD_MAX_STEPS 8  /* gradient steps of the refinement (dr_mppi_set_grad_refine) */
+#define DR_GRAD_WEIGHTS 6    /* cost weights the gradient path differentiates (dr_mppi_nominal_grad) */
 #define DR_N_TRACK_SAMPLES 512 /* reference N_TRACK_SAMPLES (env_stratrace_defs.h:11) */
 
 /* Status codes. */
@@ -177,6 +179,10 @@ typedef struct dr_mppi_info
     float inv_temperature;       /* temperature after this step's adaptation */
     int32_t nonfinite_costs;     /* number of samples whose cost was not finite */
     int32_t verif_timeouts;      /* always 0 unless a bounded wait gave up */
+    /* gradient refinement (dr_mppi_set_grad_refine; no counterpart in the reference) */
+    float grad_cost_plain;       /* objective of the plain MPPI update */
+    float grad_cost_refined;     /* objective of the plan kept (<= grad_cost_plain) */
+    int32_t grad_best_step;      /* gradient steps in the plan kept (0: the plain update), -1 when off */
 } dr_mppi_info;
 
 /* Per-step outputs of a PR-MPPI controller (src/engine.cpp:171-212). */
@@ -250,6 +256,34 @@ int dr_mppi_batch_set_profiling(dr_mppi_batch* b, int on);
  * with the rollout and the update; 0: everything in order on the batch's stream. */
 int dr_mppi_batch_set_overlap(dr_mppi_batch* b, int on);
 int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** names, float* ms, int n, int* count);
+
+/* ---- gradient path (no counterpart in the reference) -----------------------------
+ * The objective of an MPPI controller's noise-free rollout of the control sequence U
+ * (the spline knots, or the dense controls; (n_theta+1) x M x DR_DIM floats), rolled out
+ * as fullRolloutKernel does (kernels.cu:34-171: branch plans switched on the belief
+ * threshold, DECAY-discounted stateCost plus finalCost, costs.cuh:7-39) with every noise
+ * source off, under each hypothesis compatible with the current commitment, averaged
+ * with the belief weights as aggregateBranchCostsKernel averages (kernels.cu:175-217).
+ * Strategic race only.
+ *
+ * dr_mppi_nominal_grad: for n start points knots_dev [n][(n_theta+1)][M][DR_DIM] and
+ * cost weights weights_dev [n][DR_GRAD_WEIGHTS] (NULL: the controller's), in the order
+ * boundary_cost, outside_cost, win_cost, opp_win_cost, final_adv_weight,
+ * final_opp_adv_weight, writes cost_dev [n], and, where not NULL, the gradients
+ * d_knots_dev [n][(n_theta+1)][M][DR_DIM] and d_weights_dev [n][DR_GRAD_WEIGHTS]. All
+ * arrays are device memory; the work is enqueued on `stream` (NULL: legacy default)
+ * and the call returns without waiting. The adjoint sweep keeps the rollout state every
+ * ckpt_stride steps and recomputes between them (0: ceil(sqrt(n_timesteps))).
+ * Calls on one controller must not run concurrently on different streams. */
+int dr_mppi_nominal_grad(dr_mppi* h, const dr_sim_state* state, const float* belief, int n, const float* knots_dev, const float* weights_dev,
+                         float* cost_dev, float* d_knots_dev, float* d_weights_dev, int ckpt_stride, void* stream);
+/* Gradient-refined MPPI: after each MPPI update, `steps` projected gradient steps on the
+ * objective above (each control moves by at most step_size x the ego's max_accel, then
+ * the per-knot acceleration clamp); the plan with the lowest objective among the plain
+ * update and the gradient iterates is kept. steps = 0 (the default) turns it off;
+ * 0 <= steps <= DR_GRAD_MAX_STEPS. ckpt_stride as above. Set it before creating a
+ * batch of this controller. */
+int dr_mppi_set_grad_refine(dr_mppi* h, int steps, float step_size, int ckpt_stride);
 
 /* ---- MPPI test hooks (component parity against the reference kernels) ----------- */
 /* Control perturbation the next step will draw, in the reference layout

@@ -86,6 +86,7 @@ def port() -> C.CDLL:
             "orc_gate_costs": (None, [GE, M, GS, f]),
             "orc_count_ops": (C.c_int, [E, M, S, f, f, f, u64, u64, C.c_int, C.c_int, C.c_int, d]),
             "orc_gate_count_ops": (C.c_int, [GE, M, GS, f, f, f, u64, u64, C.c_int, C.c_int, C.c_int, d]),
+            "orc_nominal_cost": (C.c_int, [E, M, S, f, f, d, d, d, d, d, i]),
         }
         for n, (r, args) in protos.items():
             fn = getattr(L, n)
@@ -363,3 +364,26 @@ def pr_candidates(sc, cand1, cand2, thetas, step, stream, prec=32, impl="port"):
 
 S_PR_CAND_ENV = 8
 S_PR_SAFE_ENV = 9
+
+
+# ---- gradient path (FP64 forward-mode reference) ------------------------------------------
+
+def nominal_cost(sc, state, belief, U, w6=None, dU=None, dW=None, B=None):
+    """FP64 objective of the noise-free rollout of the control sequence U
+    ((n_theta+1, M, 2)) and its directional derivative along (dU, dW).
+
+    Returns (J, dJ, sig) with sig (n_theta, 3): steps rolled out, predTheta and
+    branchingTime per hypothesis (-1 where incompatible)."""
+    c = sc.mppi
+    if B is None:
+        B = spline_matrix(c) if c.use_splines else np.zeros((1, 1), np.float32)
+    U = np.ascontiguousarray(U, np.float64)
+    out = np.zeros(2, np.float64)
+    sig = np.zeros((sc.n_theta, 3), np.int32)
+    w = None if w6 is None else np.ascontiguousarray(w6, np.float64)
+    du = None if dU is None else np.ascontiguousarray(dU, np.float64)
+    dw = None if dW is None else np.ascontiguousarray(dW, np.float64)
+    port().orc_nominal_cost(C.byref(sc.env), C.byref(c), C.byref(state), _f(np.ascontiguousarray(belief, np.float32)),
+                            _f(np.ascontiguousarray(B, np.float32)), _d(U), None if w is None else _d(w), None if du is None else _d(du),
+                            None if dw is None else _d(dw), _d(out), _i(sig))
+    return float(out[0]), float(out[1]), sig

@@ -122,5 +122,5 @@ def test_wrong_nominal_size_raises_like_the_reference():
 def test_status_strings():
     for s in range(8):
         assert abi.lib().dr_status_string(s)
-    assert abi.lib().dr_abi_version() == 1
+    assert abi.lib().dr_abi_version() == abi.DR_ABI_VERSION == 2
     assert abi.lib().dr_supported(1, 2) == 1 and abi.lib().dr_supported(1, 3) == 0
