@@ -60,7 +60,18 @@ FLOPS_PER_VERIFY_STEP = 571.0     # verification step (noise-free ego plan)
 N_GATES = 8
 GATE_FLOPS_PER_ROLLOUT_STEP = 486.3
 GATE_FLOPS_PER_VERIFY_STEP = 473.4
+
+# --workload grad: gradient-refined MPPI on the strategic race, a quarter of the samples
+# (K = 1024) and 3 projected gradient steps of the noise-free rollout objective after each
+# update (dr_mppi_set_grad_refine), beside plain MPPI at K = 4096 in closed loop.
+K_GRAD = 1024
+GRAD_STEPS = 3
+GRAD_STEP_SIZE = 0.05
 WL = {"kind": "strat"}  # the workload of this run (set from --workload)
+
+
+def _K() -> int:
+    return K_GRAD if WL["kind"] == "grad" else K
 
 
 def _flops():
@@ -70,10 +81,17 @@ def _flops():
 
 
 def _workload_name() -> str:
-    return "gate_mppi_4x4096x64_8gates" if WL["kind"] == "gates" else "mppi_4x4096x64"
+    if WL["kind"] == "gates":
+        return "gate_mppi_4x4096x64_8gates"
+    if WL["kind"] == "grad":
+        return f"grad_mppi_4x{K_GRAD}x64_{GRAD_STEPS}steps"
+    return "mppi_4x4096x64"
 
 
 def _unit() -> str:
+    if WL["kind"] == "grad":
+        return (f"control steps/s (4 agents x K={K_GRAD} x H=64 MPPI + {GRAD_STEPS} projected gradient steps, verification V=2^17 x 40, "
+                "all agents advanced once; strategic race)")
     race = f"gate race, {N_GATES} gates" if WL["kind"] == "gates" else "strategic race"
     return f"control steps/s (4 agents x K=4096 x H=64 MPPI, verification V=2^17 x 40, all agents advanced once; {race})"
 
@@ -103,7 +121,7 @@ def workload(rank: int):
     S = drb.scenarios
     if WL["kind"] == "gates":
         return [S.gate_race(agent=a, seed=rank, K=K, T=H, use_splines=False, n_verif=V, n_gates=N_GATES) for a in range(AGENTS)]
-    return [S.circle_race(agent=a, seed=rank, K=K, T=H, use_splines=False, n_theta=N_THETA, n_verif=V) for a in range(AGENTS)]
+    return [S.circle_race(agent=a, seed=rank, K=_K(), T=H, use_splines=False, n_theta=N_THETA, n_verif=V) for a in range(AGENTS)]
 
 
 class Clocks:
@@ -238,11 +256,79 @@ def cpu_baseline_reference(scs, target_s: float = 10.0, max_reps: int = 100000, 
     t_roll /= reps
     t_ver /= reps
     # scale: rollout work ~ samples, verification ~ samples (x2 plans); 4 agents
-    step_s = AGENTS * (t_roll * (K / k_s) + 2 * t_ver * (V / v_s))
+    step_s = AGENTS * (t_roll * (_K() / k_s) + 2 * t_ver * (V / v_s))
     return {"value": 1.0 / step_s, "unit": "control_steps/s", "cores": threads, "kind": kind,
             "sample": f"1 agent: rollout of {k_s} samples x {N_THETA} hypotheses x {H} steps and one verification pass of {v_s} samples x {VERIF_H} steps, "
-                      f"{reps} repetitions ({time.perf_counter() - t0:.1f} s), scaled to 4 agents x K={K} and 2 x V={V}",
+                      f"{reps} repetitions ({time.perf_counter() - t0:.1f} s), scaled to 4 agents x K={_K()} and 2 x V={V}",
             "ms_per_control_step": step_s * 1e3}
+
+
+def _race_cost_step(sc, st) -> float:
+    """stateCost (costs.cuh:7-28) of a true state of the strategic race, undiscounted."""
+    e, c = sc.env, sc.mppi
+    r = e.drone_radius
+    n = e.n_opp + 1
+    p = np.array(st.pos[: 2 * n], np.float64).reshape(n, 2)
+    opp_won = any(st.laps[o] >= e.n_win_laps for o in range(1, n))
+    bd = min(min(np.linalg.norm(p[o] - p[0]) for o in range(1, n)) - r, e.track_width - abs(st.lat_dist[0]))
+    winner = st.laps[0] >= e.n_win_laps or any(abs(st.lat_dist[o]) > e.track_width - r for o in range(1, n))
+    cost = 0.0
+    if bd < c.boundary_threshold_factor * r:
+        cost += c.boundary_cost * (bd / r) ** 2
+    if bd < r * c.coll_dist_factor:
+        cost += c.outside_cost
+    if opp_won:
+        cost += c.opp_win_cost
+    if winner:
+        cost -= c.win_cost
+    return cost
+
+
+def closed_loop_compare(n_steps: int = 300) -> dict:
+    """Gradient-refined MPPI (K = K_GRAD, GRAD_STEPS steps) against plain MPPI (K = 4096)
+    in closed loop: each of the 4 benchmark agents races its opponent for n_steps control
+    steps (true dynamics on the device, true hypothesis 0, belief updated), the race cost
+    of the executed trajectory (sum of stateCost plus finalCost) and the wall time per
+    control step (host loop: getControl + environment step) recorded for either arm."""
+    drb = _package()
+    import drone_race_b200.controllers as ctl_mod
+
+    abi = drb.abi
+    arms = {}
+    for name, k, g in (("plain", K, 0), ("grad", K_GRAD, GRAD_STEPS)):
+        costs, progress, ms, outcome, improved = [], [], [], [], 0
+        for a in range(AGENTS):
+            sc = drb.scenarios.circle_race(agent=a, seed=0, K=k, T=H, use_splines=False, n_theta=N_THETA, n_verif=V)
+            ctl = ctl_mod.MPPIController(sc.env, sc.mppi, sc.seed)
+            ctl.engine = object()
+            if g:
+                ctl.set_grad_refine(g, GRAD_STEP_SIZE, 0)
+            st = abi.dr_sim_state.from_buffer_copy(sc.state)
+            bel = np.zeros(abi.DR_MAX_THETA, np.float32)
+            bel[: N_THETA] = sc.belief()
+            run_cost, term, t = 0.0, 0, 0
+            t0 = time.perf_counter()
+            for t in range(n_steps):
+                ctl.h_belief[:] = bel[: N_THETA]
+                act = ctl.getControl(st)
+                improved += int(g > 0 and ctl.info.grad_best_step > 0)
+                term = ctl_mod.env_step(sc.env, 0, act, st, bel, True, sc.seed, t)
+                run_cost += _race_cost_step(sc, st)
+                if term:
+                    break
+            ms.append((time.perf_counter() - t0) / (t + 1) * 1e3)
+            prog = st.S[0] / sc.env.track_length + st.laps[0]
+            costs.append(run_cost - sc.mppi.final_adv_weight * prog)
+            progress.append(prog)
+            outcome.append({0: "running", 1: "lost", 2: "won", 3: "opponent won"}.get(term, str(term)) + f" after {t + 1} steps")
+            ctl.close()
+        arms[name] = {"K": k, "grad_steps": g, "race_cost_mean": float(np.mean(costs)), "race_costs": costs, "progress_mean": float(np.mean(progress)),
+                      "ms_per_control_step_wall": float(np.mean(ms)), "outcomes": outcome}
+        if g:
+            arms[name]["steps_refined"] = improved
+    arms["what"] = (f"{AGENTS} agents x up to {n_steps} closed-loop control steps each; race cost = sum of stateCost over the executed states + "
+                    "finalCost of the last (lower is better); the episode ends at a terminal state")
+    return arms
 
 
 def run_ours(args) -> None:
@@ -257,6 +343,9 @@ def run_ours(args) -> None:
     scs = workload(rank)
     stream = torch.cuda.Stream()  # non-default stream: the batch captures a CUDA graph on it
     ctls = [ctl_mod.MPPIController(s.env, s.mppi, s.seed, device=local, stream=stream.cuda_stream) for s in scs]
+    if WL["kind"] == "grad":
+        for c in ctls:
+            c.set_grad_refine(GRAD_STEPS, GRAD_STEP_SIZE, 0)
     batch = ctl_mod.MPPIBatch(ctls, stream=stream.cuda_stream)
     if args.no_overlap:
         batch.set_overlap(False)
@@ -335,7 +424,7 @@ def run_ours(args) -> None:
         kt_serial = batch.kernel_times()
         batch.set_profiling(False)
         batch.set_overlap(True)
-    units = {"rollout": AGENTS * K * N_THETA * H, "verify": AGENTS * 2 * V * VERIF_H}
+    units = {"rollout": AGENTS * _K() * N_THETA * H, "verify": AGENTS * 2 * V * VERIF_H}
     flops_unit = dict(zip(("rollout", "verify"), _flops()))
     dom = max(kt_serial, key=kt_serial.get) if kt_serial else None
     roof = roof_step = None
@@ -357,7 +446,7 @@ def run_ours(args) -> None:
         cpu = cpu_baseline_reference(scs)
         cpu.pop("ms_per_control_step", None)
 
-    rollout_steps = AGENTS * K * N_THETA * H
+    rollout_steps = AGENTS * _K() * N_THETA * H
     line = {
         "metric": "control_steps_per_s",
         "value": value,
@@ -371,7 +460,7 @@ def run_ours(args) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded tracks and states; no dataset)",
-        "config": {"workload": _workload_name(), "agents": AGENTS, "K": K, "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
+        "config": {"workload": _workload_name(), "agents": AGENTS, "K": _K(), "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
                    "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": f"replicas x{world}",
                    "l2": "working set per step < L2; steps are dependent control steps of the same controllers"},
         "rollout_steps_per_s": world * rollout_steps * args.steps / (ms / 1e3),
@@ -385,6 +474,8 @@ def run_ours(args) -> None:
         "cpu_baseline": cpu,
         "clocks": clk,
     }
+    if WL["kind"] == "grad" and rank == 0 and world == 1 and not args.quick:
+        line["grad_vs_plain"] = closed_loop_compare()
     if rank == 0:
         print(json.dumps(line), flush=True)
     batch.close()
@@ -434,6 +525,10 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if WL["kind"] == "grad":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no gradient-refined MPPI; its plain MPPI arm is --workload strat"}),
+              flush=True)
+        return
     scs = workload(0)
     steps_ms = []
     base = None
@@ -458,7 +553,7 @@ def run_reference(args) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded tracks and states; no dataset)",
-        "config": {"workload": _workload_name(), "agents": AGENTS, "K": K, "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
+        "config": {"workload": _workload_name(), "agents": AGENTS, "K": _K(), "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
                    "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "control_steps/s", "cores": base["cores"], "kind": base["kind"], "sample": base["sample"]},
         "e2e": {"value": value, "unit": "control steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -475,8 +570,9 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e, no CPU baseline): for profiler runs")
     ap.add_argument("--no-overlap", action="store_true", help="run the previous plan's verification after the rollout instead of beside it")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="strat", choices=["strat", "gates"],
-                    help="strat: the strategic race (the headline workload); gates: the gate race (EnvDroneRace)")
+    ap.add_argument("--workload", default="strat", choices=["strat", "gates", "grad"],
+                    help="strat: the strategic race (the headline workload); gates: the gate race (EnvDroneRace); "
+                         "grad: gradient-refined MPPI at K=1024 with a closed-loop comparison against plain MPPI at K=4096")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")
     args = ap.parse_args()

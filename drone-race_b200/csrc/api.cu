@@ -892,7 +892,7 @@ int dr_mppi_set_grad_refine(dr_mppi* h, int steps, float step_size, int ckpt_str
         return fail(DR_ERR_INVALID_ARG, "step_size must be positive");
     if (ckpt_stride < 0 || ckpt_stride > h->T)
         return fail(DR_ERR_INVALID_ARG, "ckpt_stride must be in [0, n_timesteps]");
-    const int ck = ckpt_stride ? ckpt_stride : gradDefaultStride(h->T);
+    const int ck = ckpt_stride ? ckpt_stride : gradDefaultStride(h->nopp, h->nth, h->T, h->M, h->spl);
     if (steps > 0 && gradSmem(h->nopp, h->nth, h->T, h->M, ck, h->spl) > 227 * 1024)
         return fail(DR_ERR_INVALID_ARG, "checkpoint stride x horizon too large for shared memory");
     h->gradSteps = steps;
@@ -912,7 +912,7 @@ int dr_mppi_nominal_grad(dr_mppi* h, const dr_sim_state* state, const float* bel
         return fail(DR_ERR_INVALID_ARG, "n must be in [1, 65535]");
     if (ckpt_stride < 0 || ckpt_stride > h->T)
         return fail(DR_ERR_INVALID_ARG, "ckpt_stride must be in [0, n_timesteps]");
-    const int ck = ckpt_stride ? ckpt_stride : gradDefaultStride(h->T);
+    const int ck = ckpt_stride ? ckpt_stride : gradDefaultStride(h->nopp, h->nth, h->T, h->M, h->spl);
     const size_t smem = gradSmem(h->nopp, h->nth, h->T, h->M, ck, h->spl);
     if (smem > 227 * 1024)
         return fail(DR_ERR_INVALID_ARG, "checkpoint stride x horizon too large for shared memory");

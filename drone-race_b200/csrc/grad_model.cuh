@@ -7,7 +7,10 @@
 // value-only evaluation of a step and a value-and-tangent evaluation of the same step
 // produce the same values and take the same discrete decisions: the projection window's
 // nearest sample, the action and speed clamps, the branches of the opponent policy, the
-// belief threshold and the terminal tests. The tangent is the directional derivative of
+// belief threshold and the terminal tests. Division, square root and exponential use the
+// hardware approximations (reciprocal, reciprocal square root, exp2; about 2 ulp): the
+// gradient path is not held to bit parity with the reference, and these shorten the
+// dependent chain of a step, which bounds its latency. The tangent is the directional derivative of
 // the piecewise-smooth step along the seeded input direction with every discrete
 // decision held. Where only values are used the tangent arithmetic is dead code and the
 // compiler removes it.
@@ -46,10 +49,15 @@ __device__ __forceinline__ Dv operator*(Dv a, Dv b)
 {
     return Dv{__fmul_rn(a.v, b.v), a.d * b.v + a.v * b.d};
 }
+__device__ __forceinline__ float rcp(float x)
+{
+    return __fdividef(1.0f, x);
+}
 __device__ __forceinline__ Dv operator/(Dv a, Dv b)
 {
-    const float q = __fdiv_rn(a.v, b.v);
-    return Dv{q, (a.d - q * b.d) / b.v};
+    const float r = rcp(b.v);
+    const float q = __fmul_rn(a.v, r);
+    return Dv{q, (a.d - q * b.d) * r};
 }
 __device__ __forceinline__ Dv operator+(Dv a, float b)
 {
@@ -77,12 +85,14 @@ __device__ __forceinline__ Dv operator*(float a, Dv b)
 }
 __device__ __forceinline__ Dv operator/(Dv a, float b)
 {
-    return Dv{__fdiv_rn(a.v, b), a.d / b};
+    const float r = rcp(b);
+    return Dv{__fmul_rn(a.v, r), a.d * r};
 }
 __device__ __forceinline__ Dv operator/(float a, Dv b)
 {
-    const float q = __fdiv_rn(a, b.v);
-    return Dv{q, -q * b.d / b.v};
+    const float r = rcp(b.v);
+    const float q = __fmul_rn(a, r);
+    return Dv{q, -q * b.d * r};
 }
 __device__ __forceinline__ Dv& operator+=(Dv& a, Dv b)
 {
@@ -107,12 +117,14 @@ __device__ __forceinline__ Dv& operator/=(Dv& a, Dv b)
 
 __device__ __forceinline__ Dv dsqrt(Dv a)
 {
-    const float r = __fsqrt_rn(a.v);
-    return Dv{r, r > 0.0f ? a.d / (2.0f * r) : 0.0f};
+    if (!(a.v > 0.0f))
+        return Dv{0.0f, 0.0f};
+    const float rs = rsqrtf(a.v);
+    return Dv{__fmul_rn(a.v, rs), a.d * 0.5f * rs};
 }
 __device__ __forceinline__ Dv dexp(Dv a)
 {
-    const float e = expf(a.v);
+    const float e = __expf(a.v);
     return Dv{e, a.d * e};
 }
 __device__ __forceinline__ Dv dabs(Dv a)
@@ -299,7 +311,7 @@ __device__ __forceinline__ Dv gsample1(const float* __restrict__ arr, GPos q)
 // distance.
 __device__ __forceinline__ Dv gproject(const Track& tr, float L, Dv px, Dv py, float prevS, Dv& lat)
 {
-    prevS = __fdiv_rn(prevS, L);
+    prevS = __fmul_rn(prevS, rcp(L));
     prevS = __fsub_rn(prevS, floorf(prevS));
     const int idxPrev = (int)__fmul_rn(prevS, (float)NTS);
     float best = INFINITY;

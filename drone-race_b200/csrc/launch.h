@@ -66,7 +66,8 @@ struct GradJob
 };
 
 size_t gradSmem(int nopp, int nth, int T, int M, int ckpt, bool spl);
-int gradDefaultStride(int T);
+// checkpoint stride for ckpt == 0: 1 (every state kept) when it fits, else ceil(sqrt(T))
+int gradDefaultStride(int nopp, int nth, int T, int M, bool spl);
 cudaError_t launchGradNominal(cudaStream_t stream, const GradJob* jobs, int nJobs, int nopp, int nth, bool spl, size_t smem);
 
 bool prSupported(int nopp, int nth);

@@ -273,8 +273,10 @@ int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** names, float* 
  * d_knots_dev [n][(n_theta+1)][M][DR_DIM] and d_weights_dev [n][DR_GRAD_WEIGHTS]. All
  * arrays are device memory; the work is enqueued on `stream` (NULL: legacy default)
  * and the call returns without waiting. The adjoint sweep keeps the rollout state every
- * ckpt_stride steps and recomputes between them (0: ceil(sqrt(n_timesteps))).
- * Calls on one controller must not run concurrently on different streams. */
+ * ckpt_stride steps and recomputes between them (1: every state kept, no recomputation;
+ * 0: 1 when the states fit in shared memory, else ceil(sqrt(n_timesteps))); the result
+ * does not depend on it. Calls on one controller must not run concurrently on different
+ * streams. */
 int dr_mppi_nominal_grad(dr_mppi* h, const dr_sim_state* state, const float* belief, int n, const float* knots_dev, const float* weights_dev,
                          float* cost_dev, float* d_knots_dev, float* d_weights_dev, int ckpt_stride, void* stream);
 /* Gradient-refined MPPI: after each MPPI update, `steps` projected gradient steps on the
