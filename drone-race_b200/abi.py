@@ -305,6 +305,12 @@ _PROTOS = {
     "dr_mppi_nominal_grad": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_int, C.c_void_p]),
     "dr_mppi_set_grad_refine": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_int]),
+    "dr_mppi_batch_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dr_mppi_batch_env_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint64, C.c_void_p]),
+    "dr_track_grids": (C.c_int, [C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                 C.POINTER(C.c_float)]),
+    "dr_debug_cp": (C.c_int, [C.POINTER(C.c_uint32), C.c_int, C.c_uint32, C.c_double, C.c_int, C.POINTER(C.c_double)]),
+    "dr_debug_cp_host": (C.c_int, [C.POINTER(C.c_uint32), C.c_int, C.c_uint32, C.c_double, C.c_int, C.POINTER(C.c_double)]),
     "dr_env_step": (C.c_int, [C.POINTER(dr_env_config), C.c_int, C.POINTER(C.c_float), C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_int)]),
     "dr_gate_mppi_create": (C.c_int, [C.POINTER(dr_gate_env_config), C.POINTER(dr_mppi_config), C.c_uint64, C.POINTER(C.c_float), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dr_gate_mppi_step": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_mppi_info)]),

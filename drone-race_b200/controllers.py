@@ -248,7 +248,24 @@ class MPPIBatch:
         check(lib().dr_mppi_batch_set_overlap(self._b, int(on)), "dr_mppi_batch_set_overlap")
 
     def step_dev(self, states_dev_ptr: int, beliefs_dev_ptr: int) -> None:
+        """The control step's kernels on device-resident inputs, without its tail
+        (dr_mppi_batch_step_dev)."""
         check(lib().dr_mppi_batch_step_dev(self._b, C.c_void_p(states_dev_ptr), C.c_void_p(beliefs_dev_ptr)), "dr_mppi_batch_step_dev")
+
+    def step_device(self, states_dev_ptr: int, beliefs_dev_ptr: int, actions_dev_ptr: int, infos_dev_ptr: int) -> None:
+        """The whole control step on the device, tail included (dr_mppi_batch_step_device):
+        n states / n x DR_MAX_THETA beliefs in, n x 2 actions and n dr_mppi_info out, all
+        device pointers; returns without waiting."""
+        check(lib().dr_mppi_batch_step_device(self._b, C.c_void_p(states_dev_ptr), C.c_void_p(beliefs_dev_ptr), C.c_void_p(actions_dev_ptr),
+                                              C.c_void_p(infos_dev_ptr)), "dr_mppi_batch_step_device")
+
+    def env_step_device(self, true_theta_dev_ptr: int, actions_dev_ptr: int, states_dev_ptr: int, beliefs_dev_ptr: int, update_belief: bool, seed: int,
+                        terms_dev_ptr: int) -> None:
+        """Every controller's race advanced by one true-dynamics step on the device
+        (dr_mppi_batch_env_step_device)."""
+        check(lib().dr_mppi_batch_env_step_device(self._b, C.c_void_p(true_theta_dev_ptr), C.c_void_p(actions_dev_ptr), C.c_void_p(states_dev_ptr),
+                                                  C.c_void_p(beliefs_dev_ptr), int(update_belief), int(seed), C.c_void_p(terms_dev_ptr)),
+              "dr_mppi_batch_env_step_device")
 
     def set_profiling(self, on: bool) -> None:
         check(lib().dr_mppi_batch_set_profiling(self._b, int(on)), "dr_mppi_batch_set_profiling")

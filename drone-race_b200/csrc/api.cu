@@ -202,6 +202,11 @@ struct dr_mppi_batch
     GradJob* dGrad = nullptr; // gradient refinement jobs (controllers with it on)
     int nGrad = 0;
     size_t gradSmemB = 0;
+    // device-resident stepping: the controller state lives in dIn while devCtl is set
+    bool devCtl = false;
+    cudaGraph_t devGraph = nullptr;
+    cudaGraphExec_t devGraphExec = nullptr;
+    const void* devKey[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t rollSmem = 0, verSmem = 0, proSmem = 0;
     bool overlap = true;                 // previous-plan verification on sideStream
     cudaStream_t sideStream = nullptr;
@@ -348,6 +353,9 @@ struct dr_mppi_batch
             return fail(DR_ERR_INVALID_ARG, envKind ? "gate-race controllers: step them with the dr_gate_* functions"
                                                     : "strategic-race controllers: step them with dr_mppi_step / dr_mppi_batch_step");
         CK(cudaSetDevice(device));
+        int prc = pullDeviceControl();
+        if (prc)
+            return prc;
         for (int i = 0; i < n; i++)
             hIn[i] = hs[i]->input(states[i], beliefs + (size_t)i * beliefStride);
         bool profile = profiling;
@@ -357,6 +365,93 @@ struct dr_mppi_batch
         CK(cudaStreamSynchronize(stream));
         for (int i = 0; i < n; i++)
             hs[i]->finish(beliefs + (size_t)i * beliefStride, actions + 2 * i, infos ? infos + i : nullptr);
+        return DR_OK;
+    }
+
+    void dropDevGraph()
+    {
+        if (devGraphExec)
+            cudaGraphExecDestroy(devGraphExec);
+        if (devGraph)
+            cudaGraphDestroy(devGraph);
+        devGraphExec = nullptr;
+        devGraph = nullptr;
+    }
+
+    // Fully device-resident step: state and belief from device memory, the device tail
+    // writes actions and infos to device memory and carries the controller state (the
+    // input records' temperature, step counter and warm-start shift) to the next step.
+    int stepDevice(const void* states, const float* beliefs, float* actions, dr_mppi_info* infos)
+    {
+        const int n = (int)hs.size();
+        CK(cudaSetDevice(device));
+        if (!devCtl)
+        {
+            // the controllers' host state, once; from here on it lives in the device records
+            dropDevGraph();
+            std::vector<float> zero(DR_MAX_THETA, 0.0f);
+            for (int i = 0; i < n; i++)
+                hIn[i] = envKind ? hs[i]->input(dr_gate_state{}, zero.data()) : hs[i]->input(dr_sim_state{}, zero.data());
+            CK(cudaMemcpyAsync(dIn, hIn, sizeof(MppiIn) * n, cudaMemcpyHostToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+            devCtl = true;
+        }
+        const size_t stBytes = envKind ? sizeof(dr_gate_state) : sizeof(dr_sim_state);
+        auto body = [&](bool profile) -> int {
+            for (int i = 0; i < n; i++)
+            {
+                CK(cudaMemcpyAsync(&dIn[i].state, (const unsigned char*)states + i * stBytes, stBytes, cudaMemcpyDeviceToDevice, stream));
+                CK(cudaMemcpyAsync(&dIn[i].belief, beliefs + (size_t)i * DR_MAX_THETA, DR_MAX_THETA * 4, cudaMemcpyDeviceToDevice, stream));
+            }
+            int rc = launchAll(dIn, profile, &timer);
+            if (rc)
+                return rc;
+            CK(launchMppiFinish(stream, dDesc, dIn, actions, infos, n));
+            return DR_OK;
+        };
+        if (profiling || !useGraph)
+            return body(profiling);
+        const void* key[4] = {states, beliefs, actions, infos};
+        if (devGraphExec && std::memcmp(key, devKey, sizeof(key)) != 0)
+            dropDevGraph();
+        if (!devGraphExec)
+        {
+            CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            int rc = body(false);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(stream, &g);
+            if (rc)
+                return rc;
+            CK(e);
+            devGraph = g;
+            CK(cudaGraphInstantiate(&devGraphExec, devGraph, 0));
+            std::memcpy(devKey, key, sizeof(key));
+        }
+        CK(cudaGraphLaunch(devGraphExec, stream));
+        return DR_OK;
+    }
+
+    // Copies the controller state carried by the device records back to the controllers
+    // (after device-resident steps, before a host step).
+    int pullDeviceControl()
+    {
+        if (!devCtl)
+            return DR_OK;
+        const int n = (int)hs.size();
+        std::vector<MppiIn> tmp((size_t)n);
+        CK(cudaStreamSynchronize(stream));
+        CK(cudaMemcpy(tmp.data(), dIn, sizeof(MppiIn) * n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; i++)
+        {
+            dr_mppi* h = hs[i];
+            h->lambda = tmp[i].lambda;
+            h->step = (h->step & ~(uint64_t)0xffffffffu) | tmp[i].step;
+            if (tmp[i].step < (uint32_t)h->step)
+                h->step += (uint64_t)1 << 32;
+            h->pendBranch = tmp[i].pendBranch;
+            h->pendUseNew = tmp[i].pendUseNew;
+        }
+        devCtl = false;
         return DR_OK;
     }
 
@@ -376,6 +471,13 @@ struct dr_mppi_batch
         CK(cudaSetDevice(device));
         CK(cudaStreamSynchronize(stream));
         dropGraph();
+        dropDevGraph();
+        {
+            std::vector<MppiDev> descs;
+            for (auto* h : hs)
+                descs.push_back(h->desc);
+            CK(cudaMemcpy(dDesc, descs.data(), sizeof(MppiDev) * descs.size(), cudaMemcpyHostToDevice));
+        }
         std::vector<GradJob> jobs;
         gradSmemB = 0;
         for (size_t i = 0; i < hs.size(); i++)
@@ -410,6 +512,7 @@ struct dr_mppi_batch
     void release()
     {
         dropGraph();
+        dropDevGraph();
         cudaFree(dGrad);
         dGrad = nullptr;
         cudaFree(dDesc);
@@ -669,6 +772,12 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
         h->cfg.min_nu = 0.0005f; // controllers.h:47-48
         h->cfg.max_nu = 0.001f;
     }
+    D.cfg.beta = cfg->beta;
+    D.cfg.maxVerifEps = cfg->max_verif_eps;
+    D.cfg.minNu = h->cfg.min_nu;
+    D.cfg.maxNu = h->cfg.max_nu;
+    D.cfg.verify = cfg->verify ? 1 : 0;
+    D.cfg.gradSteps = 0;
 
     // device memory
     float *grids, *B, *knots, *costsTrue, *costs, *dense, *prevDense, *nu, *minCosts;
@@ -898,6 +1007,7 @@ int dr_mppi_set_grad_refine(dr_mppi* h, int steps, float step_size, int ckpt_str
     h->gradSteps = steps;
     h->gradAlpha = step_size;
     h->gradCkpt = ck;
+    h->desc.cfg.gradSteps = steps;
     return h->self->setupGrad();
 }
 
@@ -1037,6 +1147,9 @@ int dr_mppi_batch_step_dev(dr_mppi_batch* b, const dr_sim_state* states_dev, con
     if (!b || !states_dev || !beliefs_dev)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
     CK(cudaSetDevice(b->device));
+    int prc = b->pullDeviceControl();
+    if (prc)
+        return prc;
     const int n = (int)b->hs.size();
     for (int i = 0; i < n; i++)
     {
@@ -1053,6 +1166,59 @@ int dr_mppi_batch_step_dev(dr_mppi_batch* b, const dr_sim_state* states_dev, con
         CK(cudaMemcpyAsync(&b->dIn[i].belief, beliefs_dev + (size_t)i * DR_MAX_THETA, DR_MAX_THETA * 4, cudaMemcpyDeviceToDevice, b->stream));
     }
     return b->launchAll(b->dIn, b->profiling, &b->timer);
+}
+
+int dr_mppi_batch_step_device(dr_mppi_batch* b, const void* states_dev, const float* beliefs_dev, float* actions_dev, dr_mppi_info* infos_dev)
+{
+    if (!b || !states_dev || !beliefs_dev || !actions_dev || !infos_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return b->stepDevice(states_dev, beliefs_dev, actions_dev, infos_dev);
+}
+
+int dr_mppi_batch_env_step_device(dr_mppi_batch* b, const int32_t* true_theta_dev, const float* actions_dev, dr_sim_state* states_dev,
+                                  float* beliefs_dev, int update_belief, uint64_t seed, int32_t* terms_dev)
+{
+    if (!b || !true_theta_dev || !actions_dev || !states_dev || !beliefs_dev || !terms_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (b->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "the batch environment step is built for the strategic race");
+    if (!b->devCtl)
+        return fail(DR_ERR_STATE, "step the batch with dr_mppi_batch_step_device first");
+    CK(cudaSetDevice(b->device));
+    CK(launchBatchEnvStep(b->stream, b->nopp, b->nth, b->dDesc, b->dIn, (int)b->hs.size(), true_theta_dev, actions_dev, states_dev, beliefs_dev,
+                          update_belief, (uint32_t)seed, (uint32_t)(seed >> 32), terms_dev));
+    return DR_OK;
+}
+
+int dr_debug_cp(const uint32_t* k, int n, uint32_t N, double alpha, int upper, double* out)
+{
+    if (!k || !out || n < 1)
+        return fail(DR_ERR_INVALID_ARG, "bad argument");
+    uint32_t* dk = nullptr;
+    double* dout = nullptr;
+    cudaError_t e = cudaMalloc(&dk, sizeof(uint32_t) * n);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dout, sizeof(double) * n);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dk, k, sizeof(uint32_t) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = launchCp(nullptr, dk, n, N, alpha, upper, dout);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(dk);
+    cudaFree(dout);
+    CK(e);
+    return DR_OK;
+}
+
+int dr_debug_cp_host(const uint32_t* k, int n, uint32_t N, double alpha, int upper, double* out)
+{
+    if (!k || !out || n < 1)
+        return fail(DR_ERR_INVALID_ARG, "bad argument");
+    ClopperPearson cp;
+    for (int i = 0; i < n; i++)
+        out[i] = upper ? cp.upper(k[i], N, alpha) : cp.lower(k[i], N, alpha);
+    return DR_OK;
 }
 
 // ---- test hooks -------------------------------------------------------------------------------

@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <memory>
 #include <vector>
+#include <cmath>
+#include <cstring>
 
 #include <cuda_runtime.h>
 
@@ -722,6 +724,50 @@ extern "C" int dr_env_step(const dr_env_config* env, int true_theta, const float
     cudaFree(db);
     cudaFree(dt);
     CK(e);
+    return DR_OK;
+}
+
+extern "C" int dr_track_grids(const double* q, int n_tracks, float* p_grid, float* dp_grid, float* t_grid, float* kappa_grid, float* track_length)
+{
+    if (!q || n_tracks < 1 || !p_grid || !dp_grid || !t_grid || !kappa_grid || !track_length)
+        return fail(DR_ERR_INVALID_ARG, "bad argument");
+    for (size_t i = 0; i < (size_t)n_tracks * DR_N_TRACK_SAMPLES * 2; i++)
+        if (!std::isfinite(q[i]))
+            return fail(DR_ERR_INVALID_ARG, "track samples must be finite");
+    const int NS = DR_N_TRACK_SAMPLES;
+    const size_t perTrack = (size_t)NS * 7;
+    double* dq = nullptr;
+    float* dout = nullptr;
+    float* dlen = nullptr;
+    cudaError_t e = cudaMalloc(&dq, sizeof(double) * n_tracks * NS * 2);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dout, sizeof(float) * perTrack * n_tracks);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dlen, sizeof(float) * n_tracks);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dq, q, sizeof(double) * n_tracks * NS * 2, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = launchTrackGrids(nullptr, dq, n_tracks, dout, dlen);
+    std::vector<float> out;
+    if (e == cudaSuccess)
+    {
+        out.resize(perTrack * n_tracks);
+        e = cudaMemcpy(out.data(), dout, sizeof(float) * out.size(), cudaMemcpyDeviceToHost);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(track_length, dlen, sizeof(float) * n_tracks, cudaMemcpyDeviceToHost);
+    cudaFree(dq);
+    cudaFree(dout);
+    cudaFree(dlen);
+    CK(e);
+    for (int r = 0; r < n_tracks; r++)
+    {
+        const float* o = out.data() + perTrack * r;
+        std::memcpy(p_grid + (size_t)r * NS * 2, o, sizeof(float) * NS * 2);
+        std::memcpy(dp_grid + (size_t)r * NS * 2, o + NS * 2, sizeof(float) * NS * 2);
+        std::memcpy(t_grid + (size_t)r * NS * 2, o + NS * 4, sizeof(float) * NS * 2);
+        std::memcpy(kappa_grid + (size_t)r * NS, o + NS * 6, sizeof(float) * NS);
+    }
     return DR_OK;
 }
 

@@ -14,17 +14,26 @@
 #include <cstring>
 #include <unordered_map>
 
+#if defined(__CUDACC__)
+#define DR_HD __host__ __device__
+#else
+#define DR_HD
+#endif
+
 namespace dr
 {
 
+// The quantile functions below compile for the host (the host tail of the control step)
+// and for the device (the device tail, finish_kernels.cu); both use the C math library's
+// double-precision functions by their global names.
 namespace cpdetail
 {
-inline double betacf(double a, double b, double x)
+DR_HD inline double betacf(double a, double b, double x)
 {
     const double tiny = 1e-300;
     double qab = a + b, qap = a + 1.0, qam = a - 1.0;
     double c = 1.0, d = 1.0 - qab * x / qap;
-    if (std::fabs(d) < tiny)
+    if (::fabs(d) < tiny)
         d = tiny;
     d = 1.0 / d;
     double h = d;
@@ -33,49 +42,49 @@ inline double betacf(double a, double b, double x)
         int m2 = 2 * m;
         double aa = m * (b - m) * x / ((qam + m2) * (a + m2));
         d = 1.0 + aa * d;
-        if (std::fabs(d) < tiny)
+        if (::fabs(d) < tiny)
             d = tiny;
         c = 1.0 + aa / c;
-        if (std::fabs(c) < tiny)
+        if (::fabs(c) < tiny)
             c = tiny;
         d = 1.0 / d;
         h *= d * c;
         aa = -(a + m) * (qab + m) * x / ((a + m2) * (qap + m2));
         d = 1.0 + aa * d;
-        if (std::fabs(d) < tiny)
+        if (::fabs(d) < tiny)
             d = tiny;
         c = 1.0 + aa / c;
-        if (std::fabs(c) < tiny)
+        if (::fabs(c) < tiny)
             c = tiny;
         d = 1.0 / d;
         double del = d * c;
         h *= del;
-        if (std::fabs(del - 1.0) < 1e-16)
+        if (::fabs(del - 1.0) < 1e-16)
             break;
     }
     return h;
 }
 
-inline double lbeta(double a, double b)
+DR_HD inline double lbeta(double a, double b)
 {
-    return std::lgamma(a) + std::lgamma(b) - std::lgamma(a + b);
+    return ::lgamma(a) + ::lgamma(b) - ::lgamma(a + b);
 }
 
 // I_x(a, b)
-inline double ibeta(double a, double b, double x)
+DR_HD inline double ibeta(double a, double b, double x)
 {
     if (x <= 0.0)
         return 0.0;
     if (x >= 1.0)
         return 1.0;
-    double bt = std::exp(a * std::log(x) + b * std::log1p(-x) - lbeta(a, b));
+    double bt = ::exp(a * ::log(x) + b * ::log1p(-x) - lbeta(a, b));
     if (x < (a + 1.0) / (a + b + 2.0))
         return bt * betacf(a, b, x) / a;
     return 1.0 - bt * betacf(b, a, 1.0 - x) / b;
 }
 
 // x with I_x(a, b) = p
-inline double ibeta_inv(double a, double b, double p)
+DR_HD inline double ibeta_inv(double a, double b, double p)
 {
     if (p <= 0.0)
         return 0.0;
@@ -93,16 +102,35 @@ inline double ibeta_inv(double a, double b, double p)
             lo = x;
         else
             hi = x;
-        double logpdf = (a - 1.0) * std::log(x) + (b - 1.0) * std::log1p(-x) - lb;
-        double pdf = std::exp(logpdf);
-        double xn = (pdf > 0.0 && std::isfinite(pdf)) ? x - f / pdf : -1.0;
+        double logpdf = (a - 1.0) * ::log(x) + (b - 1.0) * ::log1p(-x) - lb;
+        double pdf = ::exp(logpdf);
+        double xn = (pdf > 0.0 && isfinite(pdf)) ? x - f / pdf : -1.0;
         if (!(xn > lo && xn < hi))
             xn = 0.5 * (lo + hi);
-        if (std::fabs(xn - x) <= 1e-16 * std::fmax(x, 1e-300) || hi - lo <= 1e-17)
+        if (::fabs(xn - x) <= 1e-16 * ::fmax(x, 1e-300) || hi - lo <= 1e-17)
             return xn;
         x = xn;
     }
     return x;
+}
+// quantile(beta(k, n-k+1), alpha), 0 for k == 0 (state.h:134-141)
+DR_HD inline double cpLower(uint32_t k, uint32_t n, double alpha)
+{
+    if (k == 0)
+        return 0.0;
+    if (k == n)
+        return ::pow(alpha, 1.0 / (double)n);
+    return ibeta_inv((double)k, (double)(n - k + 1), alpha);
+}
+
+// quantile(beta(k+1, n-k), 1-alpha), 1 for k == n (state.h:144-151)
+DR_HD inline double cpUpper(uint32_t k, uint32_t n, double alpha)
+{
+    if (k == n)
+        return 1.0;
+    if (k == 0)
+        return -::expm1(::log(alpha) / (double)n);
+    return ibeta_inv((double)(k + 1), (double)(n - k), 1.0 - alpha);
 }
 } // namespace cpdetail
 
@@ -114,22 +142,14 @@ class ClopperPearson
     {
         if (k == 0)
             return 0.0;
-        return memo(0, k, n, alpha, [&] {
-            if (k == n)
-                return std::pow(alpha, 1.0 / (double)n);
-            return cpdetail::ibeta_inv((double)k, (double)(n - k + 1), alpha);
-        });
+        return memo(0, k, n, alpha, [&] { return cpdetail::cpLower(k, n, alpha); });
     }
     // quantile(beta(k+1, n-k), 1-alpha), 1 for k == n (state.h:144-151)
     double upper(uint32_t k, uint32_t n, double alpha)
     {
         if (k == n)
             return 1.0;
-        return memo(1, k, n, alpha, [&] {
-            if (k == 0)
-                return -std::expm1(std::log(alpha) / (double)n);
-            return cpdetail::ibeta_inv((double)(k + 1), (double)(n - k), 1.0 - alpha);
-        });
+        return memo(1, k, n, alpha, [&] { return cpdetail::cpUpper(k, n, alpha); });
     }
 
   private:

@@ -20,6 +20,10 @@ struct MppiCfgDev
     float gateMargin; // gateTraversalMargin (gate race)
     MppiCostW w;
     uint32_t k0, k1; // Philox key (seed)
+    // host-tail parameters, for the device tail (finish_kernels.cu)
+    float beta, maxVerifEps, minNu, maxNu;
+    int verify;
+    int gradSteps; // gradient refinement steps (0: off)
 };
 
 // Per-step input of an MPPI instance (one H2D copy per step for the whole batch).

@@ -70,6 +70,16 @@ size_t gradSmem(int nopp, int nth, int T, int M, int ckpt, bool spl);
 int gradDefaultStride(int nopp, int nth, int T, int M, bool spl);
 cudaError_t launchGradNominal(cudaStream_t stream, const GradJob* jobs, int nJobs, int nopp, int nth, bool spl, size_t smem);
 
+// Device tail of the control step and the batch's true-dynamics step (finish_kernels.cu).
+cudaError_t launchMppiFinish(cudaStream_t stream, const MppiDev* insts, MppiIn* in, float* actions, dr_mppi_info* infos, int nInst);
+cudaError_t launchBatchEnvStep(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, const int* trueTheta,
+                               const float* actions, dr_sim_state* states, float* beliefs, int updateBelief, uint32_t k0, uint32_t k1, int* terms);
+cudaError_t launchCp(cudaStream_t stream, const uint32_t* k, int n, uint32_t N, double alpha, int upper, double* out);
+
+// Track grids of nTracks tracks from their 512 samples q [nTracks][512][2] (track_kernels.cu);
+// out [nTracks][7 x 512]: p[512][2] | dp[512][2] | t[512][2] | kappa[512].
+cudaError_t launchTrackGrids(cudaStream_t stream, const double* q, int nTracks, float* out, float* lengths);
+
 bool prSupported(int nopp, int nth);
 int prRolloutSamplesPerBlock();
 size_t prRolloutSmem(int T);

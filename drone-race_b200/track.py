@@ -53,6 +53,28 @@ def track_grids(track_function: Callable[[float], np.ndarray], n: int = N_TRACK_
     return TrackGrids(float(np.float32(L)), f32(p), f32(dp), f32(t), f32(kappa))
 
 
+def track_grids_gpu(track_functions: list[Callable[[float], np.ndarray]], n: int = N_TRACK_SAMPLES) -> list[TrackGrids]:
+    """`track_grids` for many tracks at once on the GPU (dr_track_grids): the track
+    functions are sampled here, the arc-length spline and the grids are computed on the
+    device, one CTA per track."""
+    import ctypes as C
+
+    from . import abi
+
+    if n != N_TRACK_SAMPLES:
+        raise ValueError("the device path samples 512 points per track")
+    R = len(track_functions)
+    q = np.ascontiguousarray(np.stack([np.array([f(k / n) for k in range(n)], dtype=np.float64) for f in track_functions]))
+    p = np.zeros((R, n, 2), np.float32)
+    dp = np.zeros((R, n, 2), np.float32)
+    t = np.zeros((R, n, 2), np.float32)
+    kap = np.zeros((R, n), np.float32)
+    L = np.zeros(R, np.float32)
+    abi.check(abi.lib().dr_track_grids(q.ctypes.data_as(C.POINTER(C.c_double)), R, abi.fptr(p), abi.fptr(dp), abi.fptr(t), abi.fptr(kap), abi.fptr(L)),
+              "dr_track_grids")
+    return [TrackGrids(float(L[r]), p[r], dp[r], t[r], kap[r]) for r in range(R)]
+
+
 def circle_track(radius: float = 6.0) -> Callable[[float], np.ndarray]:
     """The reference's round track (python-src/main.py:867-868)."""
     return lambda f: radius * np.array([np.cos(2 * np.pi * f), np.sin(2 * np.pi * f)])

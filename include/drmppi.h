@@ -249,6 +249,24 @@ int dr_mppi_batch_step(dr_mppi_batch* b, const dr_sim_state* states, const float
  * device (n records), results stay on the device; no host synchronisation. */
 int dr_mppi_batch_step_dev(dr_mppi_batch* b, const dr_sim_state* states_dev, const float* beliefs_dev);
 int dr_mppi_batch_set_graph(dr_mppi_batch* b, int use_graph);
+/* Fully device-resident control step: the host tail of getControl (mppi_controller.cu:
+ * 363-456: Clopper-Pearson certification, plan choice, epsilon, branch, temperature,
+ * warm-start shift) runs on the device too. states_dev (n dr_sim_state, or n
+ * dr_gate_state for a gate-race batch) and beliefs_dev (n x DR_MAX_THETA) are read from
+ * device memory; actions_dev (n x DR_DIM) and infos_dev (n) are written to device memory.
+ * Enqueued on the batch's stream without waiting; replayed from a CUDA graph while the
+ * four pointers stay the same. The controller state carried from step to step stays on
+ * the device; the host mirrors (dr_mppi_get_nominal, fail counts) are not refreshed by
+ * it. A later host step (dr_mppi_batch_step, dr_mppi_step) first copies that state back. */
+int dr_mppi_batch_step_device(dr_mppi_batch* b, const void* states_dev, const float* beliefs_dev, float* actions_dev, dr_mppi_info* infos_dev);
+/* True-dynamics step of every controller's race on the device (engine dynStep,
+ * engine.cpp:286-312; strategic race): states_dev and beliefs_dev (as above) advanced in
+ * place with actions_dev under true_theta_dev (n); terms_dev (n) receives the terminal
+ * type. The noise is the Philox stream that dr_env_step(seed, step) draws, at each
+ * controller's step counter (its number of control steps so far). After a
+ * dr_mppi_batch_step_device; no host synchronisation. */
+int dr_mppi_batch_env_step_device(dr_mppi_batch* b, const int32_t* true_theta_dev, const float* actions_dev, dr_sim_state* states_dev,
+                                  float* beliefs_dev, int update_belief, uint64_t seed, int32_t* terms_dev);
 /* Per-kernel device time of the batch's steps (CUDA events on its stream), averaged
  * over the steps recorded since profiling was switched on (also for *_step_dev). */
 int dr_mppi_batch_set_profiling(dr_mppi_batch* b, int on);
@@ -288,6 +306,11 @@ int dr_mppi_nominal_grad(dr_mppi* h, const dr_sim_state* state, const float* bel
 int dr_mppi_set_grad_refine(dr_mppi* h, int steps, float step_size, int ckpt_stride);
 
 /* ---- MPPI test hooks (component parity against the reference kernels) ----------- */
+/* Clopper-Pearson bounds (state.h:134-151) of n counts k out of N at level alpha, as the
+ * device tail evaluates them (dr_debug_cp) and as the host tail does (dr_debug_cp_host);
+ * upper != 0: the upper bound. */
+int dr_debug_cp(const uint32_t* k, int n, uint32_t N, double alpha, int upper, double* out);
+int dr_debug_cp_host(const uint32_t* k, int n, uint32_t N, double alpha, int upper, double* out);
 /* Control perturbation the next step will draw, in the reference layout
  * noise[(n_theta+1)][M][K][DR_DIM] (kernels.cu:28). */
 int dr_mppi_debug_noise(dr_mppi* h, float* noise, size_t n);
@@ -356,6 +379,15 @@ int dr_mppi_rollout_costs_noalloc(const dr_env_config* env, const dr_mppi_config
 /* Natural-cubic-spline basis B (T x M, row-major) of the knots tau_0..tau_{M-1}: the
  * reference's MPPIController::buildSplineMatrix (src/mppi_controller.cu:56-141). */
 int dr_spline_matrix(int T, int M, const int32_t* knots, float* out);
+
+/* ---- track preprocessing on the device (python-src/utils.py:390-427) -------------
+ * The StratRace track grids of n_tracks tracks from their track functions sampled at
+ * DR_N_TRACK_SAMPLES points (q: n_tracks x 512 x 2, host): the cumulative chord length as
+ * the spline parameter, periodic cubic splines x(s), y(s) (the reference's scipy
+ * CubicSpline, bc_type="periodic"), evaluated at 512 uniform arc lengths. Outputs (host)
+ * per track: p_grid and dp_grid (512 x 2), t_grid (512 x 2, unit tangent), kappa_grid (512),
+ * track_length (1); computed in double precision, stored as float32. */
+int dr_track_grids(const double* q, int n_tracks, float* p_grid, float* dp_grid, float* t_grid, float* kappa_grid, float* track_length);
 
 /* ---- environment step on the device (reference engine dynStep, engine.cpp:286-312) */
 /* Advances `state` in place by one true-dynamics step for the ego action, with the
