@@ -278,6 +278,7 @@ _PROTOS = {
     "dr_mppi_batch_set_graph": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_batch_set_overlap": (C.c_int, [C.c_void_p, C.c_int]),
+    "dr_mppi_batch_set_priority": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "dr_prmppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_prmppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),

@@ -247,6 +247,9 @@ class MPPIBatch:
     def set_overlap(self, on: bool) -> None:
         check(lib().dr_mppi_batch_set_overlap(self._b, int(on)), "dr_mppi_batch_set_overlap")
 
+    def set_priority(self, on: bool) -> None:
+        check(lib().dr_mppi_batch_set_priority(self._b, int(on)), "dr_mppi_batch_set_priority")
+
     def step_dev(self, states_dev_ptr: int, beliefs_dev_ptr: int) -> None:
         """The control step's kernels on device-resident inputs, without its tail
         (dr_mppi_batch_step_dev)."""

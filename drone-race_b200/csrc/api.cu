@@ -209,6 +209,15 @@ struct dr_mppi_batch
     const void* devKey[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t rollSmem = 0, verSmem = 0, proSmem = 0;
     bool overlap = true;                 // previous-plan verification on sideStream
+    // The critical path of a step (prologue, rollout, update, refinement, new-plan
+    // verification, tail) runs on hiStream, created with the device's highest stream
+    // priority, and the previous plan's verification on sideStream, with the lowest: when
+    // the update is launched, its CTAs are dispatched ahead of the side verification's
+    // waiting CTAs instead of behind them.
+    bool prio = true;
+    cudaStream_t hiStream = nullptr;
+    cudaStream_t execStream = nullptr; // stream the kernels of launchAll go to (hiStream or stream)
+    cudaEvent_t evIn = nullptr, evOut = nullptr;
     cudaStream_t sideStream = nullptr;
     cudaEvent_t evFork = nullptr, evJoin = nullptr;
     Timer timerSide;
@@ -223,7 +232,7 @@ struct dr_mppi_batch
     LaunchArgs args(const Tile* tiles, int n, const MppiIn* in) const
     {
         LaunchArgs a;
-        a.stream = stream;
+        a.stream = execStream ? execStream : stream;
         a.mppi = dDesc;
         a.mppiIn = in;
         a.tiles = tiles;
@@ -242,22 +251,35 @@ struct dr_mppi_batch
     }
 
     // kernels of one control step, reading inputs from `in` (device)
-    int launchAll(const MppiIn* in, bool profile, Timer* timer)
+    // finish != null: the device tail after the kernels (fully device-resident steps)
+    int launchAll(const MppiIn* in, bool profile, Timer* timer, MppiIn* finishIn = nullptr, float* actions = nullptr, dr_mppi_info* infos = nullptr)
     {
         const int n = (int)hs.size();
+        cudaStream_t ex = prio && hiStream ? hiStream : stream;
+        if (ex != stream)
+        {
+            CK(cudaEventRecord(evIn, stream));
+            CK(cudaStreamWaitEvent(ex, evIn, 0));
+        }
+        execStream = ex;
+        struct Restore
+        {
+            cudaStream_t& s;
+            ~Restore() { s = nullptr; }
+        } restore{execStream};
         if (profile)
         {
             timer->begin();
-            timer->mark("prologue", stream);
+            timer->mark("prologue", ex);
         }
         CK(launchMppiPrologue(args(nullptr, 0, in), n, proSmem));
         // The previous plan's verification needs only the prologue's shifted plan, so it
         // runs on a second stream while the rollout (a few warps per SM) and the update
         // run on the first; the new plan's verification follows the update.
-        const bool side = verify && overlap && nVerOld > 0;
+        bool side = verify && overlap && nVerOld > 0;
         if (side)
         {
-            CK(cudaEventRecord(evFork, stream));
+            CK(cudaEventRecord(evFork, ex));
             CK(cudaStreamWaitEvent(sideStream, evFork, 0));
             if (profile)
             {
@@ -275,33 +297,47 @@ struct dr_mppi_batch
             CK(cudaEventRecord(evJoin, sideStream));
         }
         if (profile)
-            timer->mark("rollout", stream);
+            timer->mark("rollout", ex);
         CK(launchRollout(args(dRoll, nRoll, in)));
         if (profile)
-            timer->mark("update", stream);
+            timer->mark("update", ex);
         CK(launchMppiUpdate(args(dUpd, nUpd, in), nth));
         if (nGrad > 0)
         {
             if (profile)
-                timer->mark("grad_refine", stream);
-            CK(launchGradNominal(stream, dGrad, nGrad, nopp, nth, spl, gradSmemB));
+                timer->mark("grad_refine", ex);
+            CK(launchGradNominal(ex, dGrad, nGrad, nopp, nth, spl, gradSmemB));
         }
         if (verify && nVerNew > 0)
         {
             if (profile)
-                timer->mark(side ? "verify_new" : "verify", stream);
+                timer->mark(side ? "verify_new" : "verify", ex);
             if (side)
                 CK(launchVerify(args(dVerNew, nVerNew, in)));
             else
                 CK(launchVerify(args(dVer, nVer, in)));
         }
+        if (finishIn)
+        {
+            if (side)
+                CK(cudaStreamWaitEvent(ex, evJoin, 0));
+            if (profile)
+                timer->mark("finish", ex);
+            CK(launchMppiFinish(ex, dDesc, finishIn, actions, infos, n));
+            side = false;
+        }
         if (profile)
         {
-            timer->mark("end", stream);
+            timer->mark("end", ex);
             timer->end();
         }
         if (side)
             CK(cudaStreamWaitEvent(stream, evJoin, 0));
+        if (ex != stream)
+        {
+            CK(cudaEventRecord(evOut, ex));
+            CK(cudaStreamWaitEvent(stream, evOut, 0));
+        }
         return DR_OK;
     }
 
@@ -339,7 +375,7 @@ struct dr_mppi_batch
                 return rc;
             CK(e);
             graph = g;
-            CK(cudaGraphInstantiate(&graphExec, graph, 0));
+            CK(cudaGraphInstantiate(&graphExec, graph, cudaGraphInstantiateFlagUseNodePriority));
         }
         CK(cudaGraphLaunch(graphExec, stream));
         runs++;
@@ -403,11 +439,7 @@ struct dr_mppi_batch
                 CK(cudaMemcpyAsync(&dIn[i].state, (const unsigned char*)states + i * stBytes, stBytes, cudaMemcpyDeviceToDevice, stream));
                 CK(cudaMemcpyAsync(&dIn[i].belief, beliefs + (size_t)i * DR_MAX_THETA, DR_MAX_THETA * 4, cudaMemcpyDeviceToDevice, stream));
             }
-            int rc = launchAll(dIn, profile, &timer);
-            if (rc)
-                return rc;
-            CK(launchMppiFinish(stream, dDesc, dIn, actions, infos, n));
-            return DR_OK;
+            return launchAll(dIn, profile, &timer, dIn, actions, infos);
         };
         if (profiling || !useGraph)
             return body(profiling);
@@ -424,7 +456,7 @@ struct dr_mppi_batch
                 return rc;
             CK(e);
             devGraph = g;
-            CK(cudaGraphInstantiate(&devGraphExec, devGraph, 0));
+            CK(cudaGraphInstantiate(&devGraphExec, devGraph, cudaGraphInstantiateFlagUseNodePriority));
             std::memcpy(devKey, key, sizeof(key));
         }
         CK(cudaGraphLaunch(devGraphExec, stream));
@@ -531,6 +563,15 @@ struct dr_mppi_batch
             cudaEventDestroy(evFork);
         if (evJoin)
             cudaEventDestroy(evJoin);
+        if (evIn)
+            cudaEventDestroy(evIn);
+        if (evOut)
+            cudaEventDestroy(evOut);
+        if (hiStream)
+        {
+            cudaStreamSynchronize(hiStream);
+            cudaStreamDestroy(hiStream);
+        }
         if (ownStream && stream)
             cudaStreamDestroy(stream);
     }
@@ -608,9 +649,16 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
         CK(cudaMemcpy(b->dVer, ver.data(), sizeof(Tile) * ver.size(), cudaMemcpyHostToDevice));
     b->dVerNew = b->dVer;
     b->dVerOld = b->dVer + b->nVerNew;
-    CK(cudaStreamCreateWithFlags(&b->sideStream, cudaStreamNonBlocking));
+    {
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&b->sideStream, cudaStreamNonBlocking, least));
+        CK(cudaStreamCreateWithPriority(&b->hiStream, cudaStreamNonBlocking, greatest));
+    }
     CK(cudaEventCreateWithFlags(&b->evFork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&b->evJoin, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&b->evIn, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&b->evOut, cudaEventDisableTiming));
     int rc = b->setupGrad();
     if (rc)
         return rc;
@@ -799,6 +847,8 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     A.add(binfo, (size_t)nth * K * 4);
     A.add(costs, (size_t)nbp * K * 4);
     A.add(counter, 16);
+    double* cpTab;
+    A.add(cpTab, sizeof(double) * 3 * CP_TAB);
     // result block, one contiguous range
     size_t oFail = 0, oDense = a16(oFail + (size_t)2 * T * 4), oPrev = oDense + a16((size_t)nbp * T * 2 * 4), oNu = oPrev + a16((size_t)nbp * T * 2 * 4),
            oMin = oNu + a16((size_t)nbp * 4), oStats = oMin + a16((size_t)nbp * M * 4), oGrad = oStats + 16,
@@ -813,6 +863,7 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     minCosts = (float*)(res + oMin);
     stats = (int*)(res + oStats);
     D.gstat = (float*)(res + oGrad);
+    D.cpTab = cpTab;
     D.grids = env ? grids : nullptr;
     D.gate = gp;
     D.gtrack = gtrack;
@@ -845,6 +896,19 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     {
         std::vector<float> Bm = splineMatrix(T, M, h->cfg.knots);
         CK(cudaMemcpy(B, Bm.data(), Bm.size() * 4, cudaMemcpyHostToDevice));
+    }
+    {
+        // the device tail's Clopper-Pearson table (counts below CP_TAB)
+        std::vector<double> tab(3 * (size_t)CP_TAB);
+        const uint32_t Vv = (uint32_t)h->V, V1 = (uint32_t)std::max(h->V, 1);
+        const double beta = (double)cfg->beta;
+        for (int k = 0; k < CP_TAB; k++)
+        {
+            tab[k] = (uint32_t)k <= Vv && Vv > 0 ? h->cp.upper((uint32_t)k, Vv, beta / 2.0) : 1.0;
+            tab[CP_TAB + k] = (uint32_t)k <= Vv && Vv > 0 ? h->cp.lower((uint32_t)k, Vv, beta / 2.0) : 0.0;
+            tab[2 * CP_TAB + k] = (uint32_t)k <= V1 ? h->cp.upper((uint32_t)k, V1, beta) : 1.0;
+        }
+        CK(cudaMemcpy(cpTab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
     h->hNominal.assign((size_t)nbp * T * 2, 0.0f);
     if (nominal)
@@ -1454,14 +1518,23 @@ extern "C" int dr_mppi_batch_set_overlap(dr_mppi_batch* b, int on)
 {
     if (!b)
         return fail(DR_ERR_INVALID_ARG, "NULL batch");
-    if (b->graphExec)
-    {
-        cudaGraphExecDestroy(b->graphExec);
-        cudaGraphDestroy(b->graph);
-        b->graphExec = nullptr;
-        b->graph = nullptr;
-    }
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->stream));
+    b->dropGraph();
+    b->dropDevGraph();
     b->overlap = on != 0;
+    return DR_OK;
+}
+
+extern "C" int dr_mppi_batch_set_priority(dr_mppi_batch* b, int on)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->stream));
+    b->dropGraph();
+    b->dropDevGraph();
+    b->prio = on != 0;
     return DR_OK;
 }
 

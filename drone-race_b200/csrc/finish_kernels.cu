@@ -5,8 +5,10 @@
 //                     363-456) for every controller of a batch: Clopper-Pearson
 //                     certification of the new plan against the previous one from the two
 //                     failure histograms (computeCertifiedLoss, mppi_controller.cu:468-501;
-//                     the beta quantiles of state.h:134-151 evaluated in double precision,
-//                     one thread per horizon step), the plan choice, the partial and total
+//                     the beta quantiles of state.h:134-151, one thread per horizon step,
+//                     read from a table the host fills once per controller for counts below
+//                     CP_TAB and evaluated in double precision above), the plan choice, the
+//                     partial and total
 //                     epsilon (computeEpsilon, :503-514), the branch whose first action is
 //                     sent, the temperature adaptation, and the warm-start shift of the next
 //                     step (written into the batch's device input records, which carry the
@@ -68,15 +70,22 @@ __global__ void __launch_bounds__(FB) mppi_finish(const MppiDev* __restrict__ in
         }
         __syncthreads();
     }
-    // certified loss: max_t upper(new_t) - lower(old_t), starting from -1
+    // certified loss: max_t upper(new_t) - lower(old_t), starting from -1; counts below
+    // CP_TAB read the host's table (the same function, evaluated once per controller)
+    const double* tab = D.cpTab;
     double d = -1.0;
     if (verify && tid < T)
-        d = fmax(d, cpdetail::cpUpper(cN[tid], V, beta / 2.0) - cpdetail::cpLower(cO[tid], V, beta / 2.0));
+    {
+        const uint32_t kn = cN[tid], ko = cO[tid];
+        const double up = kn < (uint32_t)CP_TAB ? tab[kn] : cpdetail::cpUpper(kn, V, beta / 2.0);
+        const double lo = ko < (uint32_t)CP_TAB ? tab[CP_TAB + ko] : cpdetail::cpLower(ko, V, beta / 2.0);
+        d = fmax(d, up - lo);
+    }
     // the two epsilon candidates (new plan kept or previous plan kept)
     if (tid == DR_MAX_T + 32 || tid == DR_MAX_T + 33)
     {
         const uint32_t tot = tid == DR_MAX_T + 32 ? cN[T - 1] : cO[T - 1];
-        sEps[tid - DR_MAX_T - 32] = cpdetail::cpUpper(tot, V > 0 ? V : 1u, beta);
+        sEps[tid - DR_MAX_T - 32] = tot < (uint32_t)CP_TAB ? tab[2 * CP_TAB + tot] : cpdetail::cpUpper(tot, V > 0 ? V : 1u, beta);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)

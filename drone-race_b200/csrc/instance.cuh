@@ -66,8 +66,13 @@ struct MppiDev
     float* minCosts;     // [nbp][M]
     int* stats;          // [0] non-finite costs, [1] timeouts
     float* gstat;        // gradient refinement: objective of iterates 0..DR_GRAD_MAX_STEPS, best iterate, last iterate
+    // Clopper-Pearson bounds for counts k < CP_TAB, filled on the host at creation:
+    // [0] upper(k, V, beta/2), [1] lower(k, V, beta/2), [2] upper(k, max(V, 1), beta)
+    const double* cpTab;
     size_t resBytes;
 };
+
+constexpr int CP_TAB = 1024;
 
 struct PrCfgDev
 {

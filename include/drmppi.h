@@ -273,6 +273,10 @@ int dr_mppi_batch_set_profiling(dr_mppi_batch* b, int on);
 /* 1 (default): the previous plan's verification runs on a second stream concurrently
  * with the rollout and the update; 0: everything in order on the batch's stream. */
 int dr_mppi_batch_set_overlap(dr_mppi_batch* b, int on);
+/* 1 (default): the step's critical path runs on an internal stream of the device's highest
+ * priority and the side verification on one of the lowest; 0: both at the batch stream's
+ * and the side stream's default priorities (for measurement). */
+int dr_mppi_batch_set_priority(dr_mppi_batch* b, int on);
 int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** names, float* ms, int n, int* count);
 
 /* ---- gradient path (no counterpart in the reference) -----------------------------
