@@ -145,3 +145,33 @@ def test_device_closed_loop_matches_host_loop(gpu):
     for i in range(n):
         assert bytes(final[i]) == bytes(states[i]), i
         assert np.array_equal(bel_dev.cpu().numpy()[i], bels[i])
+
+
+def test_gate_race_device_steps_match_host_steps(gpu):
+    """The device tail on gate-race controllers (dr_gate_state records)."""
+    torch = _torch()
+    n = 2
+    scs = [H.small_gate(False, K=512, T=40, n_verif=1024, seed=5 + a, noise=True) for a in range(n)]
+    A = [drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed) for sc in scs]
+    B = [drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed) for sc in scs]
+    ba, bb = drb.controllers.MPPIBatch(A), drb.controllers.MPPIBatch(B)
+    states = [sc.state for sc in scs]
+    beliefs = np.stack([np.array(sc.env.init_belief[: sc.env.n_theta], np.float32) for sc in scs])
+    st_dev = torch.frombuffer(bytearray(bytes((abi.dr_gate_state * n)(*states))), dtype=torch.uint8).cuda()
+    bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+    bel[:, : beliefs.shape[1]] = beliefs
+    bel_dev = torch.from_numpy(bel).cuda()
+    act_dev = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    info_dev = torch.zeros(C.sizeof(abi.dr_mppi_info) * n, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    for k in range(4):
+        a_host = ba.step(states, beliefs)
+        bb.step_device(st_dev.data_ptr(), bel_dev.data_ptr(), act_dev.data_ptr(), info_dev.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(a_host, act_dev.cpu().numpy()), k
+        di = _infos(info_dev, n)
+        for i in range(n):
+            h, d = ba.infos[i], di[i]
+            assert (h.use_new_plan, h.branch_idx, h.fail_count_total) == (d.use_new_plan, d.branch_idx, d.fail_count_total)
+            assert h.inv_temperature == d.inv_temperature and h.nu == d.nu
+            assert abs(h.epsilon - d.epsilon) <= 1e-9 * abs(h.epsilon)

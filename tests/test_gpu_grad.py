@@ -190,3 +190,51 @@ def test_uneven_batch_with_refinement_equals_single_controllers(gpu):
         assert np.array_equal(a1, a2)
         for c1, c2 in zip(singles, batched):
             assert np.array_equal(c1.h_nominal, c2.h_nominal)
+
+
+def _multi_scenario(nopp: int, nth: int, spl: bool):
+    """Small strategic race with nopp opponents and nth distinguishable hypotheses."""
+    S = drb.scenarios
+    r = 0.4
+    grids = drb.track.track_grids(drb.track.circle_track(6.0))
+    kinds = [("insensitive", "default"), ("insensitive", "no-block"), ("default", "default"), ("conservative", "no-block")]
+    configs = []
+    for th in range(nth):
+        s1, s3 = kinds[th % 4]
+        p = S.opp_preset(r, s1=s1, s3=s3, speed_scale=0.8 + 0.4 * th / max(nth - 1, 1))
+        configs.append([p] * nopp)
+    env = S.make_env(grids, n_opp=nopp, opp_configs=configs, dt=0.1, drone_radius=r, max_speed=[3, 2, 2, 2], max_accel=[2, 3, 3, 3],
+                     track_width=2.0, kV=5.0, max_opp_lat_dist_fact=1.9)
+    idx = [int(v) for v in np.round(np.linspace(0.05, 0.2, nopp + 1) * 512)]
+    st = S.initial_state(grids, idx, nopp)
+    sc = S.Scenario(env=env, grids=grids, state=st, name=f"multi_{nopp}_{nth}")
+    sc.mppi = S.make_mppi(K=256, T=40, use_splines=spl, M=10, n_verif_samples=512, verif_horizon=30, final_opp_adv_weight=20.0)
+    return sc
+
+
+@pytest.mark.parametrize("nopp,nth", [(2, 2), (1, 4), (1, 8), (1, 1)])
+def test_gradient_matches_fp64_reference_other_sizes(gpu, nopp, nth):
+    """The other compiled (n_opp, n_theta) combinations: two opponents, and 1, 4 and 8
+    hypotheses (clusters of up to 8 CTAs)."""
+    sc = _multi_scenario(nopp, nth, True)
+    c = sc.mppi
+    ctl = drb.controllers.MPPIController(sc.env, c, 17)
+    rng = np.random.default_rng(nopp * 10 + nth)
+    U = rng.normal(0, 0.7, (sc.n_theta + 1, O.mk(c), 2)).astype(np.float32)
+    belief = np.array(sc.env.init_belief[: sc.n_theta], np.float32)
+    w6 = _weights(c, final_opp=20.0)
+    J, dU, dW = _kernel(ctl, sc, belief, U, w6)
+    J64, _, _ = O.nominal_cost(sc, sc.state, belief, U.astype(np.float64), w6=w6.astype(np.float64))
+    assert abs(J[0] - J64) <= 1e-4 * max(1.0, abs(J64)), (J[0], J64)
+    gnorm = np.sqrt((dU[0].astype(np.float64) ** 2).sum() + (dW[0].astype(np.float64) ** 2).sum())
+    errs = []
+    for _ in range(16):
+        d = rng.normal(0, 1, U.shape)
+        d /= np.linalg.norm(d)
+        dw = rng.normal(0, 1, 6)
+        dw /= np.linalg.norm(dw)
+        _, jvp, _ = O.nominal_cost(sc, sc.state, belief, U.astype(np.float64), w6=w6.astype(np.float64), dU=d, dW=dw)
+        errs.append(abs(float((dU[0].astype(np.float64) * d).sum() + (dW[0].astype(np.float64) * dw).sum()) - jvp) / gnorm)
+    errs = np.array(errs)
+    print(f"nopp={nopp} nth={nth} J={J[0]:.6g} |g|={gnorm:.4g} err median {np.median(errs):.2e} max {errs.max():.2e}")
+    assert np.median(errs) < 1e-4 and errs.max() < 1e-3, errs
