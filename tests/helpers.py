@@ -95,21 +95,24 @@ class OracleMPPI:
             knots, dense, mins, nu, costs = O.mppi_update(sc, belief, ct, bu, bt, noise, self.B, self.knots, prec=self.prec)
             self.knots = knots.reshape(self.nbp, self.M, 2)
             self.dense = dense.reshape(self.nbp, self.T, 2)
-            fc_new, _, _ = O.mppi_verify(sc, belief, self.dense, self.step, 0, prec=self.prec)
-            fc_old, _, _ = O.mppi_verify(sc, belief, self.prev, self.step, 1, prec=self.prec)
+            if c.verify:
+                fc_new, _, _ = O.mppi_verify(sc, belief, self.dense, self.step, 0, prec=self.prec)
+                fc_old, _, _ = O.mppi_verify(sc, belief, self.prev, self.step, 1, prec=self.prec)
+            else:
+                fc_new = fc_old = np.zeros(self.T, np.uint32)
         finally:
             sc.state = old_state
             c.inv_temperature = cfg_lam
         V = c.n_verif_samples
         cert = -1.0
         tn = to = 0
-        for t in range(self.T):
+        for t in range(self.T if c.verify else 0):
             tn += int(fc_new[t])
             to += int(fc_old[t])
             e1 = O.port().orc_cp_upper(tn, V, float(np.float32(c.beta)) / 2.0)
             e2 = O.port().orc_cp_lower(to, V, float(np.float32(c.beta)) / 2.0)
             cert = max(cert, e1 - e2)
-        use_new = cert < float(np.float32(c.max_verif_eps))
+        use_new = cert < float(np.float32(c.max_verif_eps)) if c.verify else True
         chosen = self.dense if use_new else self.prev
         self.h_nominal = chosen.copy()
         bidx = 0

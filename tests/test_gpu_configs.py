@@ -1,0 +1,76 @@
+"""The benchmark's other configurations as parity cases.
+
+C1 (single drone, K 1024, H 50, 8-point ellipse track, start at rest 3 m before the line):
+one control step against the FP64 oracle, then the closed-loop episode of up to 200 steps
+run by the CUDA controller (true dynamics on the device) against the same episode run by
+the FP64 oracle controller and the oracle's FP64 environment step. The two trajectories
+are not expected to agree bit for bit (FP32 against FP64, chaotic over an episode); the
+outcome, its step and the final progress are.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import O, drb
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+S = drb.scenarios
+abi = drb.abi
+
+
+def _c1():
+    sc = S.ellipse_race(seed=0, K=1024, T=50, n_verif=4096)
+    # with 4096 verification samples no new plan certifies at max_verif_eps 1e-3 (the upper
+    # bound of zero failures is 3e-3): the episode runs plain MPPI, verification off
+    sc.mppi.verify = 0
+    return sc
+
+
+def test_c1_single_drone_against_fp64_oracle(gpu):
+    sc = _c1()
+    ctl = drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed)
+    ctl.engine = object()
+    ref = H.OracleMPPI(sc, prec=64)
+    a_gpu = ctl.getControl(sc.state)
+    a_ref, _ = ref.get_control(sc.state, sc.belief())
+    print("first action", a_gpu, np.asarray(a_ref, np.float32))
+    # FP32 costs against FP64 costs of the same 1024 x 2 rollouts, through exp weights
+    assert np.max(np.abs(a_gpu - np.asarray(a_ref, np.float32))) < 2e-2
+    # closed loop, CUDA controller and device environment step
+    ctl2 = drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed)
+    ctl2.engine = object()
+    st = abi.dr_sim_state.from_buffer_copy(sc.state)
+    bel = np.zeros(abi.DR_MAX_THETA, np.float32)
+    bel[: sc.n_theta] = sc.belief()
+    term_g, t_g = 0, 0
+    for t in range(200):
+        ctl2.h_belief[:] = bel[: sc.n_theta]
+        a = ctl2.getControl(st)
+        term_g = drb.controllers.env_step(sc.env, 0, a, st, bel, True, sc.seed, t + 1)
+        t_g = t + 1
+        if term_g:
+            break
+    prog_g = st.S[0] / sc.env.track_length + st.laps[0]
+    # closed loop, FP64 oracle controller and FP64 environment step
+    ref2 = H.OracleMPPI(sc, prec=64)
+    st2 = abi.dr_sim_state.from_buffer_copy(sc.state)
+    bel2 = np.zeros(abi.DR_MAX_THETA, np.float32)
+    bel2[: sc.n_theta] = sc.belief()
+    term_o, t_o = 0, 0
+    for t in range(200):
+        a, _ = ref2.get_control(st2, bel2[: sc.n_theta].copy())
+        act = np.ascontiguousarray(a, np.float32)
+        term_o = O.port().orc_env_step(64, C.byref(sc.env), 0, O._f(act), C.byref(st2), O._f(bel2), 1, 0, 2.0, 0, 1, sc.seed, t + 1, 0)
+        t_o = t + 1
+        if term_o:
+            break
+    prog_o = st2.S[0] / sc.env.track_length + st2.laps[0]
+    print(f"CUDA: term {term_g} after {t_g} steps, progress {prog_g:.5f}; FP64 oracle: term {term_o} after {t_o} steps, progress {prog_o:.5f}")
+    assert term_g == term_o
+    assert abs(t_g - t_o) <= 3
+    assert abs(prog_g - prog_o) <= 0.01

@@ -43,12 +43,13 @@ def test_pr_noise_and_thetas_bit_exact(gpu, nth):
     assert np.array_equal(th, O.pr_thetas(sc, 0, belief))
 
 
-@pytest.mark.parametrize("nth", [2, 8])
-def test_pr_rollout_matches_reference_kernel(gpu, nth):
+@pytest.mark.parametrize("nth,K,T", [(2, 512, 40), (8, 512, 40), (8, 2048, 64)])
+def test_pr_rollout_matches_reference_kernel(gpu, nth, K, T):
     """PRMPPIfullRolloutKernel (prmppi_kernels.cu:55-130) on the same perturbation and
-    hypotheses: running and safety cost of every (nominal/robust, p, sample)."""
+    hypotheses: running and safety cost of every (nominal/robust, p, sample). The last case
+    is the benchmark's PR-MPPI configuration per agent (8 hypotheses, P 8, K 2048, H 64)."""
     variant = O.ref_variant_name(nth, True)
-    sc = small_pr(nth, K=512, T=40, noise=False)
+    sc = small_pr(nth, K=K, T=T, noise=False)
     rng = np.random.default_rng(11)
     nominal = rng.normal(0, 0.8, (sc.prmppi.n_timesteps, 2)).astype(np.float32)
     ctl = drb.controllers.PRMPPIController(sc.env, sc.prmppi, sc.seed, nominal=nominal)
