@@ -306,6 +306,11 @@ _PROTOS = {
     "dr_mppi_nominal_grad": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_int, C.c_void_p]),
     "dr_mppi_set_grad_refine": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_int]),
+    "dr_mppi_set_shard": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dr_mppi_shard_begin": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_void_p]),
+    "dr_mppi_shard_sums": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dr_mppi_shard_update": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dr_mppi_shard_finish": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_mppi_info)]),
     "dr_mppi_batch_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dr_mppi_batch_env_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint64, C.c_void_p]),
     "dr_track_grids": (C.c_int, [C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),

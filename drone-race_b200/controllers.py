@@ -219,6 +219,58 @@ def _kernel_times(fn, h) -> dict[str, float]:
     return {names[i].decode(): float(ms[i]) for i in range(cnt.value)}
 
 
+class ShardedMPPIController(MPPIController):
+    """One MPPI controller whose samples are split across the processes of a
+    torch.distributed group (one process per GPU): this process rolls out and verifies its
+    share, and the partial minima, weighted sums and failure histograms are combined with
+    three all-reduces per step (dr_mppi_set_shard / dr_mppi_shard_*). With the gloo
+    backend the partials travel through host memory; with NCCL they stay on the device."""
+
+    def __init__(self, env, cfg: abi.dr_mppi_config, seed: int, rank: int, world: int, group=None, nominal: np.ndarray | None = None,
+                 device: int = 0):
+        import torch
+
+        super().__init__(env, cfg, seed, nominal=nominal, device=device)
+        check(lib().dr_mppi_set_shard(self._h, int(rank), int(world)), "dr_mppi_set_shard")
+        self.group = group
+        M = int(cfg.n_knots) if cfg.use_splines else self.T
+        dev = torch.device("cuda", device)
+        self._mins = torch.empty(self.nbp * M, dtype=torch.float32, device=dev)
+        self._sums = torch.empty(self.nbp * M * 3, dtype=torch.float32, device=dev)
+        self._hist = torch.empty(2 * self.T, dtype=torch.int32, device=dev)
+
+    def _all_reduce(self, t, op) -> None:
+        import torch
+        import torch.distributed as dist
+
+        if dist.get_backend(self.group) == "gloo":
+            x = t.cpu()
+            dist.all_reduce(x, op=op, group=self.group)
+            t.copy_(x)
+        else:
+            dist.all_reduce(t, op=op, group=self.group)
+        torch.cuda.current_stream(t.device).synchronize()
+
+    def getControl(self, state) -> np.ndarray:  # noqa: N802
+        import torch.distributed as dist
+
+        if self.engine is None:
+            raise RuntimeError("MPPI: engine not set")
+        P = lambda t: C.c_void_p(t.data_ptr())
+        bel = abi.fptr(self.h_belief)
+        st = C.byref(_state(state, False))
+        check(lib().dr_mppi_shard_begin(self._h, st, bel, P(self._mins)), "dr_mppi_shard_begin")
+        self._all_reduce(self._mins, dist.ReduceOp.MIN)
+        check(lib().dr_mppi_shard_sums(self._h, P(self._mins), P(self._sums)), "dr_mppi_shard_sums")
+        self._all_reduce(self._sums, dist.ReduceOp.SUM)
+        check(lib().dr_mppi_shard_update(self._h, P(self._mins), P(self._sums), P(self._hist)), "dr_mppi_shard_update")
+        self._all_reduce(self._hist, dist.ReduceOp.SUM)
+        out = np.zeros(2, np.float32)
+        check(lib().dr_mppi_shard_finish(self._h, P(self._hist), bel, abi.fptr(out), C.byref(self.info)), "dr_mppi_shard_finish")
+        self._pull()
+        return out
+
+
 class MPPIBatch:
     """Several MPPI controllers (one per agent) advanced by one launch sequence."""
 

@@ -62,6 +62,10 @@ struct dr_mppi
     // gradient refinement after the update (dr_mppi_set_grad_refine)
     int gradSteps = 0, gradCkpt = 1;
     float gradAlpha = 0.05f;
+    // sample sharding across processes (dr_mppi_set_shard): this process's samples and
+    // verification samples
+    int shardRank = 0, shardWorld = 1;
+    int sLo = 0, sHi = 0, vLo = 0, vHi = 0;
     // dr_mppi_nominal_grad: device input record and job table
     MppiIn* dGradIn = nullptr;
     GradJob* dGradJobs = nullptr;
@@ -404,6 +408,54 @@ struct dr_mppi_batch
         return DR_OK;
     }
 
+    // ---- sample-sharded step of a batch of one (dr_mppi_shard_*) ----
+    int shardBegin(const MppiIn& hin, float* mins)
+    {
+        CK(cudaSetDevice(device));
+        hIn[0] = hin;
+        CK(cudaMemcpyAsync(dIn, hIn, sizeof(MppiIn), cudaMemcpyHostToDevice, stream));
+        CK(launchMppiPrologue(args(nullptr, 0, dIn), 1, proSmem));
+        if (verify && nVerOld > 0)
+            CK(launchVerify(args(dVerOld, nVerOld, dIn)));
+        CK(launchRollout(args(dRoll, nRoll, dIn)));
+        CK(launchShardMin(args(dUpd, nUpd, dIn), nth, mins));
+        CK(cudaStreamSynchronize(stream));
+        return DR_OK;
+    }
+
+    int shardSums(const float* mins, float* sums)
+    {
+        CK(cudaSetDevice(device));
+        CK(launchShardSums(args(dUpd, nUpd, dIn), nth, mins, sums));
+        CK(cudaStreamSynchronize(stream));
+        return DR_OK;
+    }
+
+    int shardUpdate(const float* mins, const float* sums, uint32_t* hist)
+    {
+        CK(cudaSetDevice(device));
+        CK(launchShardApply(stream, dDesc, 1, nth, mins, sums));
+        if (nGrad > 0)
+            CK(launchGradNominal(stream, dGrad, nGrad, nopp, nth, spl, gradSmemB));
+        if (verify && nVerNew > 0)
+            CK(launchVerify(args(dVerNew, nVerNew, dIn)));
+        CK(cudaMemcpyAsync(hist, hs[0]->desc.fail, sizeof(uint32_t) * 2 * hs[0]->T, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaStreamSynchronize(stream));
+        return DR_OK;
+    }
+
+    int shardFinish(const uint32_t* hist, const float* belief, float* action, dr_mppi_info* info)
+    {
+        CK(cudaSetDevice(device));
+        CK(cudaMemcpyAsync(hs[0]->desc.fail, hist, sizeof(uint32_t) * 2 * hs[0]->T, cudaMemcpyDeviceToDevice, stream));
+        int rc = copyResults();
+        if (rc)
+            return rc;
+        CK(cudaStreamSynchronize(stream));
+        hs[0]->finish(belief, action, info);
+        return DR_OK;
+    }
+
     void dropDevGraph()
     {
         if (devGraphExec)
@@ -609,14 +661,14 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     {
         dr_mppi* h = hs[i];
         descs.push_back(h->desc);
-        for (int s0 = 0; s0 < h->K; s0 += spb)
-            roll.push_back(Tile{i, s0, std::min(spb, h->K - s0), 0});
+        for (int s0 = h->sLo; s0 < h->sHi; s0 += spb)
+            roll.push_back(Tile{i, s0, std::min(spb, h->sHi - s0), 0});
         for (int bk = 0; bk < h->nbp * h->M; bk++)
             upd.push_back(Tile{i, bk, 0, 0});
         if (b->verify)
             for (int plan = 0; plan < 2; plan++)
-                for (int v0 = 0; v0 < h->V; v0 += VERIFY_TILE)
-                    (plan == 0 ? ver : verOld).push_back(Tile{i, v0, std::min(VERIFY_TILE, h->V - v0), plan});
+                for (int v0 = h->vLo; v0 < h->vHi; v0 += VERIFY_TILE)
+                    (plan == 0 ? ver : verOld).push_back(Tile{i, v0, std::min(VERIFY_TILE, h->vHi - v0), plan});
         maxT = std::max(maxT, h->T);
         maxM = std::max(maxM, h->M);
         maxNbpT = std::max(maxNbpT, h->nbp * h->T);
@@ -826,6 +878,10 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     D.cfg.maxNu = h->cfg.max_nu;
     D.cfg.verify = cfg->verify ? 1 : 0;
     D.cfg.gradSteps = 0;
+    D.cfg.sLo = 0;
+    D.cfg.sHi = K;
+    h->sHi = K;
+    h->vHi = h->V;
 
     // device memory
     float *grids, *B, *knots, *costsTrue, *costs, *dense, *prevDense, *nu, *minCosts;
@@ -982,6 +1038,8 @@ int dr_mppi_step(dr_mppi* h, const dr_sim_state* state, const float* belief, flo
 {
     if (!h || !state || !belief || !out_action)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->shardWorld > 1)
+        return fail(DR_ERR_STATE, "a sample-sharded controller steps through dr_mppi_shard_*");
     return h->self->step(state, belief, h->nth, out_action, info);
 }
 
@@ -1051,6 +1109,64 @@ int dr_mppi_io_bytes(const dr_mppi* h, size_t* h2d, size_t* d2h)
     if (d2h)
         *d2h = h->desc.resBytes;
     return DR_OK;
+}
+
+int dr_mppi_set_shard(dr_mppi* h, int rank, int world)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    if (h->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "sample sharding is built for the strategic race");
+    if (world < 1 || rank < 0 || rank >= world || world > h->K)
+        return fail(DR_ERR_INVALID_ARG, "need 0 <= rank < world <= n_samples");
+    h->shardRank = rank;
+    h->shardWorld = world;
+    h->sLo = (int)((int64_t)h->K * rank / world);
+    h->sHi = (int)((int64_t)h->K * (rank + 1) / world);
+    h->vLo = (int)((int64_t)h->V * rank / world);
+    h->vHi = (int)((int64_t)h->V * (rank + 1) / world);
+    h->desc.cfg.sLo = h->sLo;
+    h->desc.cfg.sHi = h->sHi;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->self)
+    {
+        h->self->release();
+        delete h->self;
+        h->self = nullptr;
+    }
+    dr_mppi* raw = h;
+    return buildMppiBatch(&raw, 1, h->stream, false, &h->self);
+}
+
+int dr_mppi_shard_begin(dr_mppi* h, const dr_sim_state* state, const float* belief, float* mins_dev)
+{
+    if (!h || !state || !belief || !mins_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "sample sharding is built for the strategic race");
+    return h->self->shardBegin(h->input(*state, belief), mins_dev);
+}
+
+int dr_mppi_shard_sums(dr_mppi* h, const float* mins_dev, float* sums_dev)
+{
+    if (!h || !mins_dev || !sums_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->shardSums(mins_dev, sums_dev);
+}
+
+int dr_mppi_shard_update(dr_mppi* h, const float* mins_dev, const float* sums_dev, uint32_t* hist_dev)
+{
+    if (!h || !mins_dev || !sums_dev || !hist_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->shardUpdate(mins_dev, sums_dev, hist_dev);
+}
+
+int dr_mppi_shard_finish(dr_mppi* h, const uint32_t* hist_dev, const float* belief, float* out_action, dr_mppi_info* info)
+{
+    if (!h || !hist_dev || !belief || !out_action)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->shardFinish(hist_dev, belief, out_action, info);
 }
 
 int dr_mppi_set_grad_refine(dr_mppi* h, int steps, float step_size, int ckpt_stride)

@@ -24,6 +24,7 @@ struct MppiCfgDev
     float beta, maxVerifEps, minNu, maxNu;
     int verify;
     int gradSteps; // gradient refinement steps (0: off)
+    int sLo, sHi;  // this process's samples when the controller is sample-sharded (else 0, K)
 };
 
 // Per-step input of an MPPI instance (one H2D copy per step for the whole batch).

@@ -34,6 +34,10 @@ cudaError_t launchMppiPrologue(const LaunchArgs& a, int nInst, size_t smem);
 cudaError_t launchMppiRollout(const LaunchArgs& a, int nopp, int nth, bool spl, size_t smem);
 cudaError_t launchMppiUpdate(const LaunchArgs& a, int nth);
 cudaError_t launchMppiAggregate(const LaunchArgs& a, int nth, int K);
+// sample-sharded update phases (one controller's samples split across processes)
+cudaError_t launchShardMin(const LaunchArgs& a, int nth, float* mins);
+cudaError_t launchShardSums(const LaunchArgs& a, int nth, const float* mins, float* sums);
+cudaError_t launchShardApply(cudaStream_t stream, const MppiDev* insts, int nInst, int nth, const float* mins, const float* sums);
 cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem, int* dbgFailTime, int* dbgTheta);
 cudaError_t launchMppiNoise(const LaunchArgs& a, size_t n, float* out);
 

@@ -563,6 +563,190 @@ template <int NTH> __global__ void __launch_bounds__(UB) mppi_update(const MppiD
 }
 
 // ---------------------------------------------------------------------------------------
+// sample-sharded update: one controller's samples split across processes (one per GPU),
+// the partial results combined by the caller's collectives between the three phases
+// ---------------------------------------------------------------------------------------
+// phase 1: masked minimum over this process's samples [sLo, sHi) per (branch plan, knot)
+// (computeMaskedMinCostsKernel, kernels.cu:221-301); the caller takes the minimum over
+// the processes
+template <int NTH> __global__ void __launch_bounds__(UB) mppi_shard_min(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in,
+                                                                        const Tile* __restrict__ tiles, float* __restrict__ mins)
+{
+    __shared__ float sMin[UB / 32];
+    const Tile tile = tiles[blockIdx.x];
+    const MppiDev& D = insts[tile.inst];
+    const MppiIn& I = in[tile.inst];
+    const int K = D.cfg.K, T = D.cfg.T, M = D.cfg.M, sLo = D.cfg.sLo, sHi = D.cfg.sHi;
+    const bool spl = D.cfg.useSplines != 0;
+    const int b = tile.s0 / M, k = tile.s0 % M;
+    const int tid = threadIdx.x;
+    float belief[NTH];
+#pragma unroll
+    for (int i = 0; i < NTH; i++)
+        belief[i] = I.belief[i];
+    const int initPred = findConfident<NTH>(belief, D.cfg.minConf);
+    const float* costs = D.costs + (size_t)b * K;
+    float mn = INFINITY;
+    if (initPred == 0 || initPred == b)
+        for (int s = sLo + tid; s < sHi; s += UB)
+        {
+            float coeff = sampleCoeff<NTH>(D, belief, b, k, s, spl, T, M, K);
+            if (coeff > MIN_COEFF)
+            {
+                float c = costs[s];
+                if (c < mn)
+                    mn = c;
+            }
+        }
+    mn = warp_min(mn);
+    if ((tid & 31) == 0)
+        sMin[tid >> 5] = mn;
+    __syncthreads();
+    if (tid == 0)
+    {
+        float minC = sMin[0];
+#pragma unroll
+        for (int w = 1; w < UB / 32; w++)
+            minC = fminf(minC, sMin[w]);
+        mins[b * M + k] = minC;
+    }
+}
+
+// phase 2: this process's weighted sums of the regenerated perturbations with the
+// minimum over all processes (weightedAverageKernelUnified, kernels.cu:307-408):
+// sums[(b, k)] = (sum w coeff eps0, sum w coeff eps1, sum w coeff); the caller adds them up
+template <int NTH> __global__ void __launch_bounds__(UB) mppi_shard_sums(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in,
+                                                                         const Tile* __restrict__ tiles, const float* __restrict__ mins,
+                                                                         float* __restrict__ sums)
+{
+    __shared__ float sNum0[UB], sNum1[UB], sDen[UB];
+    const Tile tile = tiles[blockIdx.x];
+    const MppiDev& D = insts[tile.inst];
+    const MppiIn& I = in[tile.inst];
+    const int K = D.cfg.K, T = D.cfg.T, M = D.cfg.M, sLo = D.cfg.sLo, sHi = D.cfg.sHi;
+    const bool spl = D.cfg.useSplines != 0;
+    const int b = tile.s0 / M, k = tile.s0 % M;
+    const int tid = threadIdx.x;
+    float belief[NTH];
+#pragma unroll
+    for (int i = 0; i < NTH; i++)
+        belief[i] = I.belief[i];
+    const float* costs = D.costs + (size_t)b * K;
+    const float minC = mins[b * M + k];
+    const float lambda = I.lambda;
+    const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+    float num0 = 0.0f, num1 = 0.0f, den = 0.0f;
+    if (!isinf(minC))
+        for (int s = sLo + tid; s < sHi; s += UB)
+        {
+            float coeff = sampleCoeff<NTH>(D, belief, b, k, s, spl, T, M, K);
+            if (coeff > MIN_COEFF)
+            {
+                float cost = costs[s];
+                float w = expf(-(cost - minC) / lambda);
+                U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)(b * M + k), step, S_MPPI_EPS, 0);
+                float eps0 = scaled_normal(D.cfg.sigma0, r.x);
+                float eps1 = scaled_normal(D.cfg.sigma1, r.y);
+                num0 += w * coeff * eps0;
+                num1 += w * coeff * eps1;
+                den += w * coeff;
+            }
+        }
+    sNum0[tid] = num0;
+    sNum1[tid] = num1;
+    sDen[tid] = den;
+    __syncthreads();
+#pragma unroll
+    for (int stride = UB / 2; stride >= 32; stride >>= 1)
+    {
+        if (tid < stride)
+        {
+            sNum0[tid] += sNum0[tid + stride];
+            sNum1[tid] += sNum1[tid + stride];
+            sDen[tid] += sDen[tid + stride];
+        }
+        __syncthreads();
+    }
+    if (tid < 32)
+    {
+        float a0 = sNum0[tid], a1 = sNum1[tid], dd = sDen[tid];
+#pragma unroll
+        for (int stride = 16; stride > 0; stride >>= 1)
+        {
+            a0 += __shfl_down_sync(0xffffffffu, a0, stride);
+            a1 += __shfl_down_sync(0xffffffffu, a1, stride);
+            dd += __shfl_down_sync(0xffffffffu, dd, stride);
+        }
+        if (tid == 0)
+        {
+            float* o = sums + (size_t)(b * M + k) * 3;
+            o[0] = a0;
+            o[1] = a1;
+            o[2] = dd;
+        }
+    }
+}
+
+// phase 3: the update from the sums over all processes, then interpolateSplineKernel and
+// clampNominalKernel (kernels.cu:411-456); one block per instance
+__global__ void __launch_bounds__(UB) mppi_shard_apply(const MppiDev* __restrict__ insts, int nbp, const float* __restrict__ mins,
+                                                       const float* __restrict__ sums)
+{
+    const MppiDev& D = insts[blockIdx.x];
+    const int T = D.cfg.T, M = D.cfg.M;
+    const bool spl = D.cfg.useSplines != 0;
+    const int tid = threadIdx.x;
+    for (int v = tid; v < nbp * M; v += UB)
+    {
+        const int b = v / M, k = v % M;
+        const float a0 = sums[v * 3], a1 = sums[v * 3 + 1], dd = sums[v * 3 + 2];
+        if (dd > 1e-30f)
+        {
+            D.knots[v * 2 + 0] += a0 / dd;
+            D.knots[v * 2 + 1] += a1 / dd;
+        }
+        if (k == 0)
+            D.nu[b] = dd;
+        D.minCosts[v] = mins[v];
+    }
+    __syncthreads();
+    if (spl)
+    {
+        for (int idx = tid; idx < nbp * T * 2; idx += UB)
+        {
+            int dim = idx & 1, t = (idx >> 1) % T, br = (idx >> 1) / T;
+            float sum = 0.0f;
+            for (int m = 0; m < M; m++)
+                sum += D.B[t * M + m] * D.knots[(br * M + m) * 2 + dim];
+            D.dense[idx] = sum;
+        }
+        __syncthreads();
+    }
+    const float maxAccel = D.env.maxAccel[0];
+    for (int v = tid; v < nbp * M; v += UB)
+    {
+        float x0 = D.knots[v * 2], x1 = D.knots[v * 2 + 1];
+        float sq = 0.0f;
+        sq += x0 * x0;
+        sq += x1 * x1;
+        float maxSq = maxAccel * maxAccel;
+        if (sq > maxSq)
+        {
+            float scale = maxAccel / sqrtf(sq);
+            x0 *= scale;
+            x1 *= scale;
+        }
+        D.knots[v * 2] = x0;
+        D.knots[v * 2 + 1] = x1;
+        if (!spl)
+        {
+            D.dense[v * 2] = x0;
+            D.dense[v * 2 + 1] = x1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // verification
 // ---------------------------------------------------------------------------------------
 template <int NOPP, int NTH>
@@ -786,6 +970,38 @@ cudaError_t launchMppiUpdate(const LaunchArgs& a, int nth)
     case 8: mppi_update<8><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles); break;
     default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launchShardMin(const LaunchArgs& a, int nth, float* mins)
+{
+    switch (nth)
+    {
+    case 1: mppi_shard_min<1><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins); break;
+    case 2: mppi_shard_min<2><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins); break;
+    case 4: mppi_shard_min<4><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins); break;
+    case 8: mppi_shard_min<8><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchShardSums(const LaunchArgs& a, int nth, const float* mins, float* sums)
+{
+    switch (nth)
+    {
+    case 1: mppi_shard_sums<1><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins, sums); break;
+    case 2: mppi_shard_sums<2><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins, sums); break;
+    case 4: mppi_shard_sums<4><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins, sums); break;
+    case 8: mppi_shard_sums<8><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins, sums); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchShardApply(cudaStream_t stream, const MppiDev* insts, int nInst, int nth, const float* mins, const float* sums)
+{
+    mppi_shard_apply<<<nInst, UB, 0, stream>>>(insts, nth + 1, mins, sums);
     return cudaGetLastError();
 }
 

@@ -309,6 +309,32 @@ int dr_mppi_nominal_grad(dr_mppi* h, const dr_sim_state* state, const float* bel
  * batch of this controller. */
 int dr_mppi_set_grad_refine(dr_mppi* h, int steps, float step_size, int ckpt_stride);
 
+/* ---- sample sharding of one controller across processes (one per GPU) -----------
+ * No counterpart in the reference. Process `rank` of `world` rolls out the samples
+ * [rank K / world, (rank+1) K / world) and verifies [rank V / world, (rank+1) V / world),
+ * with every random stream keyed by the global sample index, so the union over the
+ * processes is the single-process workload. A step is four calls, with the caller's
+ * collectives (e.g. torch.distributed over NCCL) in between, on device buffers it owns:
+ *   dr_mppi_shard_begin   prologue, previous-plan verification, rollout, and this
+ *                         process's masked minimum per (branch plan, knot) -> mins_dev
+ *                         ((n_theta+1) x M floats)         caller: all-reduce MIN
+ *   dr_mppi_shard_sums    this process's weighted sums with the global minima
+ *                         -> sums_dev ((n_theta+1) x M x 3) caller: all-reduce SUM
+ *   dr_mppi_shard_update  the update from the summed sums (then interpolation, clamp,
+ *                         gradient refinement if set), new-plan verification
+ *                         -> hist_dev (2 x n_timesteps u32: new, previous plan)
+ *                                                            caller: all-reduce SUM
+ *   dr_mppi_shard_finish  the host tail on the summed histograms -> action, info
+ * Each call returns after its work on the controller's stream has completed. The
+ * results equal the single-process step's up to the order of the floating-point sums
+ * (the per-process partial sums are added in rank order). dr_mppi_step is refused on a
+ * sharded controller. */
+int dr_mppi_set_shard(dr_mppi* h, int rank, int world);
+int dr_mppi_shard_begin(dr_mppi* h, const dr_sim_state* state, const float* belief, float* mins_dev);
+int dr_mppi_shard_sums(dr_mppi* h, const float* mins_dev, float* sums_dev);
+int dr_mppi_shard_update(dr_mppi* h, const float* mins_dev, const float* sums_dev, uint32_t* hist_dev);
+int dr_mppi_shard_finish(dr_mppi* h, const uint32_t* hist_dev, const float* belief, float* out_action, dr_mppi_info* info);
+
 /* ---- MPPI test hooks (component parity against the reference kernels) ----------- */
 /* Clopper-Pearson bounds (state.h:134-151) of n counts k out of N at level alpha, as the
  * device tail evaluates them (dr_debug_cp) and as the host tail does (dr_debug_cp_host);
