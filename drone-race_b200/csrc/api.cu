@@ -1355,18 +1355,22 @@ int dr_mppi_batch_step_device(dr_mppi_batch* b, const void* states_dev, const fl
     return b->stepDevice(states_dev, beliefs_dev, actions_dev, infos_dev);
 }
 
-int dr_mppi_batch_env_step_device(dr_mppi_batch* b, const int32_t* true_theta_dev, const float* actions_dev, dr_sim_state* states_dev,
-                                  float* beliefs_dev, int update_belief, uint64_t seed, int32_t* terms_dev)
+int dr_mppi_batch_env_step_device(dr_mppi_batch* b, const int32_t* true_theta_dev, const float* actions_dev, void* states_dev, float* beliefs_dev,
+                                  int update_belief, uint64_t seed, int32_t* terms_dev)
 {
     if (!b || !true_theta_dev || !actions_dev || !states_dev || !beliefs_dev || !terms_dev)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
-    if (b->envKind != 0)
-        return fail(DR_ERR_UNSUPPORTED, "the batch environment step is built for the strategic race");
     if (!b->devCtl)
         return fail(DR_ERR_STATE, "step the batch with dr_mppi_batch_step_device first");
     CK(cudaSetDevice(b->device));
-    CK(launchBatchEnvStep(b->stream, b->nopp, b->nth, b->dDesc, b->dIn, (int)b->hs.size(), true_theta_dev, actions_dev, states_dev, beliefs_dev,
-                          update_belief, (uint32_t)seed, (uint32_t)(seed >> 32), terms_dev));
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    const int n = (int)b->hs.size();
+    if (b->envKind)
+        CK(launchGateBatchEnvStep(b->stream, b->nth, b->iMppi, b->dDesc, b->dIn, n, true_theta_dev, actions_dev, (dr_gate_state*)states_dev, beliefs_dev,
+                                  update_belief, k0, k1, terms_dev));
+    else
+        CK(launchBatchEnvStep(b->stream, b->nopp, b->nth, b->dDesc, b->dIn, n, true_theta_dev, actions_dev, (dr_sim_state*)states_dev, beliefs_dev,
+                              update_belief, k0, k1, terms_dev));
     return DR_OK;
 }
 

@@ -394,6 +394,48 @@ __global__ void gate_env_step_kernel(const GateParams* __restrict__ gp, const fl
     *term = o.term;
 }
 
+// The same for every controller of a batch (dr_mppi_batch_env_step_device): one CTA per
+// controller, its gate parameters and racelines, the action it sent, the noise stream of
+// its step counter.
+template <int NTH, int ME>
+__global__ void gate_batch_env_step(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const int* __restrict__ trueTheta,
+                                    const float* __restrict__ actions, dr_gate_state* __restrict__ states, float* __restrict__ beliefs, int updateBelief,
+                                    uint32_t k0, uint32_t k1, int* __restrict__ terms)
+{
+    __shared__ GateParams sG;
+    const int inst = blockIdx.x;
+    const MppiDev& D = insts[inst];
+    if (threadIdx.x == 0)
+    {
+        sG = *D.gate;
+        gateDeviceTerms(sG, *D.gate, 0, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x != 0)
+        return;
+    GState s;
+    loadGState(s, states[inst]);
+    float* belief = beliefs + (size_t)inst * DR_MAX_THETA;
+    BState<NTH> bs;
+    for (int i = 0; i < NTH; i++)
+        bs.belief[i] = belief[i];
+    bs.predTheta = 0;
+    bs.branchingTime = -1;
+    EnvNoise rng(k0, k1, 0u, 0u, in[inst].step, S_ENV_STEP);
+    rng.begin_step(0);
+    bool branched = false;
+    const float a0 = actions[inst * 2], a1 = actions[inst * 2 + 1];
+    StepOut o;
+    if (updateBelief)
+        o = gateStep<NTH, true, false, false, true, ME>(0, trueTheta[inst], D.gtrack, sG, a0, a1, s, bs, branched, 2.0f, rng, 0.0f);
+    else
+        o = gateStep<NTH, false, false, false, true, ME>(0, trueTheta[inst], D.gtrack, sG, a0, a1, s, bs, branched, 2.0f, rng, 0.0f);
+    storeGState(states[inst], s);
+    for (int i = 0; i < NTH; i++)
+        belief[i] = bs.belief[i];
+    terms[inst] = o.term;
+}
+
 // ---------------------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------------------
@@ -477,6 +519,22 @@ static cudaError_t launchGateEnvStepT(cudaStream_t stream, const GateParams* gp,
 {
     gate_env_step_kernel<NTH, ME><<<1, 32, 0, stream>>>(gp, track, trueTheta, a0, a1, st, belief, updateBelief, k0, k1, step, term);
     return cudaGetLastError();
+}
+
+template <int NTH, int ME>
+static cudaError_t launchGateBatchEnvStepT(cudaStream_t stream, const MppiDev* insts, const MppiIn* in, int nInst, const int* trueTheta, const float* actions,
+                                           dr_gate_state* states, float* beliefs, int updateBelief, uint32_t k0, uint32_t k1, int* terms)
+{
+    gate_batch_env_step<NTH, ME><<<nInst, 32, 0, stream>>>(insts, in, trueTheta, actions, states, beliefs, updateBelief, k0, k1, terms);
+    return cudaGetLastError();
+}
+
+cudaError_t launchGateBatchEnvStep(cudaStream_t stream, int nth, int me, const MppiDev* insts, const MppiIn* in, int nInst, const int* trueTheta,
+                                   const float* actions, dr_gate_state* states, float* beliefs, int updateBelief, uint32_t k0, uint32_t k1, int* terms)
+{
+#define CALL(P, Q) launchGateBatchEnvStepT<P, Q>(stream, insts, in, nInst, trueTheta, actions, states, beliefs, updateBelief, k0, k1, terms)
+    GATE_DISPATCH(nth, me, CALL)
+#undef CALL
 }
 
 cudaError_t launchGateEnvStep(cudaStream_t stream, int nth, int me, const GateParams* gp, const float* track, int trueTheta, float a0, float a1,

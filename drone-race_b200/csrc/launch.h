@@ -48,6 +48,8 @@ size_t gateVerifySmem(int nth, int T);
 // `me`: the ego's agent index (the environment's i_mppi)
 cudaError_t launchGateRollout(const LaunchArgs& a, int nth, int me, bool spl, size_t smem);
 cudaError_t launchGateVerify(const LaunchArgs& a, int nth, int me, size_t smem, int* dbgFailTime, int* dbgTheta);
+cudaError_t launchGateBatchEnvStep(cudaStream_t stream, int nth, int me, const MppiDev* insts, const MppiIn* in, int nInst, const int* trueTheta,
+                                   const float* actions, dr_gate_state* states, float* beliefs, int updateBelief, uint32_t k0, uint32_t k1, int* terms);
 cudaError_t launchGateEnvStep(cudaStream_t stream, int nth, int me, const GateParams* gp, const float* track, int trueTheta, float a0, float a1,
                               dr_gate_state* st, float* belief, int updateBelief, uint32_t k0, uint32_t k1, uint32_t step, int* term);
 

@@ -260,13 +260,14 @@ int dr_mppi_batch_set_graph(dr_mppi_batch* b, int use_graph);
  * it. A later host step (dr_mppi_batch_step, dr_mppi_step) first copies that state back. */
 int dr_mppi_batch_step_device(dr_mppi_batch* b, const void* states_dev, const float* beliefs_dev, float* actions_dev, dr_mppi_info* infos_dev);
 /* True-dynamics step of every controller's race on the device (engine dynStep,
- * engine.cpp:286-312; strategic race): states_dev and beliefs_dev (as above) advanced in
- * place with actions_dev under true_theta_dev (n); terms_dev (n) receives the terminal
- * type. The noise is the Philox stream that dr_env_step(seed, step) draws, at each
- * controller's step counter (its number of control steps so far). After a
- * dr_mppi_batch_step_device; no host synchronisation. */
-int dr_mppi_batch_env_step_device(dr_mppi_batch* b, const int32_t* true_theta_dev, const float* actions_dev, dr_sim_state* states_dev,
-                                  float* beliefs_dev, int update_belief, uint64_t seed, int32_t* terms_dev);
+ * engine.cpp:286-312): states_dev (n dr_sim_state, or n dr_gate_state for a gate-race
+ * batch) and beliefs_dev (as above) advanced in place with actions_dev under
+ * true_theta_dev (n); terms_dev (n) receives the terminal type. The noise is the Philox
+ * stream that dr_env_step / dr_gate_env_step (seed, step) draw, at each controller's step
+ * counter (its number of control steps so far). After a dr_mppi_batch_step_device; no
+ * host synchronisation. */
+int dr_mppi_batch_env_step_device(dr_mppi_batch* b, const int32_t* true_theta_dev, const float* actions_dev, void* states_dev, float* beliefs_dev,
+                                  int update_belief, uint64_t seed, int32_t* terms_dev);
 /* Per-kernel device time of the batch's steps (CUDA events on its stream), averaged
  * over the steps recorded since profiling was switched on (also for *_step_dev). */
 int dr_mppi_batch_set_profiling(dr_mppi_batch* b, int on);

@@ -175,3 +175,46 @@ def test_gate_race_device_steps_match_host_steps(gpu):
             assert (h.use_new_plan, h.branch_idx, h.fail_count_total) == (d.use_new_plan, d.branch_idx, d.fail_count_total)
             assert h.inv_temperature == d.inv_temperature and h.nu == d.nu
             assert abs(h.epsilon - d.epsilon) <= 1e-9 * abs(h.epsilon)
+
+
+def test_gate_race_device_closed_loop_matches_host_loop(gpu):
+    """The gate race's closed loop on the device (gate_batch_env_step) against the loop
+    driven by the host with dr_gate_mppi_batch_step and dr_gate_env_step."""
+    torch = _torch()
+    n, steps, seed = 2, 12, 77
+    scs = [H.small_gate(False, K=256, T=32, n_verif=512, seed=5 + a, noise=True) for a in range(n)]
+    A = [drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed) for sc in scs]
+    B = [drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed) for sc in scs]
+    ba, bb = drb.controllers.MPPIBatch(A), drb.controllers.MPPIBatch(B)
+    nth = scs[0].env.n_theta
+    states = [abi.dr_gate_state.from_buffer_copy(sc.state) for sc in scs]
+    bels = [np.array(sc.env.init_belief[:nth], np.float32) for sc in scs]
+    terms_h = []
+    for t in range(steps):
+        act = ba.step(states, np.stack(bels))
+        row = []
+        for i, sc in enumerate(scs):
+            term, states[i], bels[i] = drb.controllers.gate_env_step(sc.env, 0, act[i], states[i], bels[i], True, seed, t + 1)
+            row.append(term)
+        terms_h.append(row)
+    st_dev = torch.frombuffer(bytearray(bytes((abi.dr_gate_state * n)(*[sc.state for sc in scs]))), dtype=torch.uint8).cuda()
+    bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+    for i, sc in enumerate(scs):
+        bel[i, :nth] = sc.env.init_belief[:nth]
+    bel_dev = torch.from_numpy(bel).cuda()
+    act_dev = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    info_dev = torch.zeros(C.sizeof(abi.dr_mppi_info) * n, dtype=torch.uint8, device="cuda")
+    theta_dev = torch.zeros(n, dtype=torch.int32, device="cuda")
+    term_dev = torch.zeros(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    terms_d = []
+    for t in range(steps):
+        bb.step_device(st_dev.data_ptr(), bel_dev.data_ptr(), act_dev.data_ptr(), info_dev.data_ptr())
+        bb.env_step_device(theta_dev.data_ptr(), act_dev.data_ptr(), st_dev.data_ptr(), bel_dev.data_ptr(), True, seed, term_dev.data_ptr())
+        torch.cuda.synchronize()
+        terms_d.append(term_dev.cpu().numpy().tolist())
+    assert terms_h == terms_d
+    final = (abi.dr_gate_state * n).from_buffer_copy(st_dev.cpu().numpy().tobytes())
+    for i in range(n):
+        assert bytes(final[i]) == bytes(states[i]), i
+        assert np.array_equal(bel_dev.cpu().numpy()[i, :nth], bels[i])
