@@ -529,9 +529,12 @@ struct dr_mppi_batch
         {
             dr_mppi* h = hs[i];
             h->lambda = tmp[i].lambda;
-            h->step = (h->step & ~(uint64_t)0xffffffffu) | tmp[i].step;
-            if (tmp[i].step < (uint32_t)h->step)
-                h->step += (uint64_t)1 << 32;
+            // the device record carries the low 32 bits of the step counter
+            const uint64_t prev = h->step;
+            uint64_t next = (prev & ~(uint64_t)0xffffffffu) | tmp[i].step;
+            if (next < prev)
+                next += (uint64_t)1 << 32;
+            h->step = next;
             h->pendBranch = tmp[i].pendBranch;
             h->pendUseNew = tmp[i].pendUseNew;
         }

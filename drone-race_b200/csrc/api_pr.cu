@@ -6,6 +6,8 @@
 #include <vector>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -671,6 +673,42 @@ __global__ void env_step_kernel(EnvParams Eh, const float* __restrict__ grids, i
     *term = o.term;
 }
 
+namespace
+{
+// Device scratch of the single environment steps (dr_env_step, dr_gate_env_step): one
+// block per device, allocated on first use and kept for the process; the calls of a
+// process share it under a mutex (each call is synchronous).
+// Layout: [parameters / grids / racelines] | [state record | belief | terminal type].
+constexpr size_t ENV_SCRATCH_PARAMS = 48 * 1024, ENV_SCRATCH_IO = 1024;
+std::mutex g_envMu;
+std::map<int, unsigned char*> g_envScratch;
+
+cudaError_t envScratch(int dev, unsigned char** out)
+{
+    auto it = g_envScratch.find(dev);
+    if (it != g_envScratch.end())
+    {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    unsigned char* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, ENV_SCRATCH_PARAMS + ENV_SCRATCH_IO);
+    if (e == cudaSuccess)
+        g_envScratch[dev] = p;
+    *out = p;
+    return e;
+}
+
+// host image of the io part: state record, belief, terminal type
+template <class St> struct EnvIo
+{
+    St state;
+    float belief[DR_MAX_THETA];
+    int term;
+};
+static_assert(sizeof(EnvIo<dr_sim_state>) <= ENV_SCRATCH_IO && sizeof(EnvIo<dr_gate_state>) <= ENV_SCRATCH_IO, "env step scratch");
+} // namespace
+
 extern "C" int dr_env_step(const dr_env_config* env, int true_theta, const float* action, dr_sim_state* state, float* belief, int update_belief,
                            uint64_t seed, uint64_t step, int* term)
 {
@@ -685,45 +723,34 @@ extern "C" int dr_env_step(const dr_env_config* env, int true_theta, const float
     CK(cudaGetDevice(&dev));
     std::vector<float> g = packGrids(*env);
     EnvParams E = toEnvParams(*env);
-    float* dg = nullptr;
-    dr_sim_state* ds = nullptr;
-    float* db = nullptr;
-    int* dt = nullptr;
-    cudaError_t e = cudaMalloc(&dg, GRID_FLOATS * 4);
-    if (e == cudaSuccess)
-        e = cudaMalloc(&ds, sizeof(dr_sim_state));
-    if (e == cudaSuccess)
-        e = cudaMalloc(&db, DR_MAX_THETA * 4);
-    if (e == cudaSuccess)
-        e = cudaMalloc(&dt, 4);
-    if (e == cudaSuccess)
+    std::lock_guard<std::mutex> lock(g_envMu);
+    unsigned char* base = nullptr;
+    CK(envScratch(dev, &base));
+    float* dg = (float*)base;
+    EnvIo<dr_sim_state>* dio = (EnvIo<dr_sim_state>*)(base + ENV_SCRATCH_PARAMS);
+    EnvIo<dr_sim_state> io{};
+    io.state = *state;
+    for (int i = 0; i < env->n_theta; i++)
+        io.belief[i] = belief[i];
+    CK(cudaMemcpy(dg, g.data(), GRID_FLOATS * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dio, &io, sizeof(io), cudaMemcpyHostToDevice));
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    switch (env->n_opp * 16 + env->n_theta)
     {
-        cudaMemcpy(dg, g.data(), GRID_FLOATS * 4, cudaMemcpyHostToDevice);
-        cudaMemcpy(ds, state, sizeof(dr_sim_state), cudaMemcpyHostToDevice);
-        cudaMemcpy(db, belief, env->n_theta * 4, cudaMemcpyHostToDevice);
-        uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-        switch (env->n_opp * 16 + env->n_theta)
-        {
-        case 17: env_step_kernel<1, 1><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
-        case 18: env_step_kernel<1, 2><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
-        case 20: env_step_kernel<1, 4><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
-        case 24: env_step_kernel<1, 8><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
-        case 34: env_step_kernel<2, 2><<<1, 128>>>(E, dg, true_theta, action[0], action[1], ds, db, update_belief, k0, k1, (uint32_t)step, dt); break;
-        default: break;
-        }
-        e = cudaGetLastError();
-        if (e == cudaSuccess)
-            e = cudaMemcpy(state, ds, sizeof(dr_sim_state), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess)
-            e = cudaMemcpy(belief, db, env->n_theta * 4, cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess && term)
-            e = cudaMemcpy(term, dt, 4, cudaMemcpyDeviceToHost);
+    case 17: env_step_kernel<1, 1><<<1, 128>>>(E, dg, true_theta, action[0], action[1], &dio->state, dio->belief, update_belief, k0, k1, (uint32_t)step, &dio->term); break;
+    case 18: env_step_kernel<1, 2><<<1, 128>>>(E, dg, true_theta, action[0], action[1], &dio->state, dio->belief, update_belief, k0, k1, (uint32_t)step, &dio->term); break;
+    case 20: env_step_kernel<1, 4><<<1, 128>>>(E, dg, true_theta, action[0], action[1], &dio->state, dio->belief, update_belief, k0, k1, (uint32_t)step, &dio->term); break;
+    case 24: env_step_kernel<1, 8><<<1, 128>>>(E, dg, true_theta, action[0], action[1], &dio->state, dio->belief, update_belief, k0, k1, (uint32_t)step, &dio->term); break;
+    case 34: env_step_kernel<2, 2><<<1, 128>>>(E, dg, true_theta, action[0], action[1], &dio->state, dio->belief, update_belief, k0, k1, (uint32_t)step, &dio->term); break;
+    default: break;
     }
-    cudaFree(dg);
-    cudaFree(ds);
-    cudaFree(db);
-    cudaFree(dt);
-    CK(e);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(&io, dio, sizeof(io), cudaMemcpyDeviceToHost));
+    *state = io.state;
+    for (int i = 0; i < env->n_theta; i++)
+        belief[i] = io.belief[i];
+    if (term)
+        *term = io.term;
     return DR_OK;
 }
 
@@ -734,6 +761,16 @@ extern "C" int dr_track_grids(const double* q, int n_tracks, float* p_grid, floa
     for (size_t i = 0; i < (size_t)n_tracks * DR_N_TRACK_SAMPLES * 2; i++)
         if (!std::isfinite(q[i]))
             return fail(DR_ERR_INVALID_ARG, "track samples must be finite");
+    // the spline parameter (cumulative chord length) must increase strictly, as scipy's
+    // CubicSpline requires of the reference's knots
+    for (int r = 0; r < n_tracks; r++)
+        for (int k = 0; k < DR_N_TRACK_SAMPLES; k++)
+        {
+            const double* a = q + ((size_t)r * DR_N_TRACK_SAMPLES + k) * 2;
+            const double* b = q + ((size_t)r * DR_N_TRACK_SAMPLES + (k + 1) % DR_N_TRACK_SAMPLES) * 2;
+            if (a[0] == b[0] && a[1] == b[1])
+                return fail(DR_ERR_INVALID_ARG, "consecutive track samples must differ");
+        }
     const int NS = DR_N_TRACK_SAMPLES;
     const size_t perTrack = (size_t)NS * 7;
     double* dq = nullptr;
@@ -785,43 +822,30 @@ extern "C" int dr_gate_env_step(const dr_gate_env_config* env, int true_theta, c
     CK(cudaGetDevice(&dev));
     GateParams hp = toGateParams(*env);
     std::vector<float> tr = packGateTrack(*env);
-    GateParams* dgp = nullptr;
-    float* dtr = nullptr;
-    dr_gate_state* ds = nullptr;
-    float* db = nullptr;
-    int* dt = nullptr;
-    cudaError_t e = cudaMalloc(&dgp, sizeof(GateParams));
-    if (e == cudaSuccess)
-        e = cudaMalloc(&dtr, tr.size() * 4);
-    if (e == cudaSuccess)
-        e = cudaMalloc(&ds, sizeof(dr_gate_state));
-    if (e == cudaSuccess)
-        e = cudaMalloc(&db, DR_MAX_THETA * 4);
-    if (e == cudaSuccess)
-        e = cudaMalloc(&dt, 4);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(dgp, &hp, sizeof(GateParams), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(dtr, tr.data(), tr.size() * 4, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(ds, state, sizeof(dr_gate_state), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(db, belief, env->n_theta * 4, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-        e = launchGateEnvStep(nullptr, env->n_theta, env->i_mppi, dgp, dtr, true_theta, action[0], action[1], ds, db, update_belief, (uint32_t)seed,
-                              (uint32_t)(seed >> 32), (uint32_t)step, dt);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(state, ds, sizeof(dr_gate_state), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(belief, db, env->n_theta * 4, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && term)
-        e = cudaMemcpy(term, dt, 4, cudaMemcpyDeviceToHost);
-    cudaFree(dgp);
-    cudaFree(dtr);
-    cudaFree(ds);
-    cudaFree(db);
-    cudaFree(dt);
-    CK(e);
+    const size_t trOff = (sizeof(GateParams) + 255) & ~(size_t)255;
+    if (trOff + tr.size() * 4 > ENV_SCRATCH_PARAMS)
+        return fail(DR_ERR_INVALID_ARG, "gate parameters too large");
+    std::lock_guard<std::mutex> lock(g_envMu);
+    unsigned char* base = nullptr;
+    CK(envScratch(dev, &base));
+    GateParams* dgp = (GateParams*)base;
+    float* dtr = (float*)(base + trOff);
+    EnvIo<dr_gate_state>* dio = (EnvIo<dr_gate_state>*)(base + ENV_SCRATCH_PARAMS);
+    EnvIo<dr_gate_state> io{};
+    io.state = *state;
+    for (int i = 0; i < env->n_theta; i++)
+        io.belief[i] = belief[i];
+    CK(cudaMemcpy(dgp, &hp, sizeof(GateParams), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dtr, tr.data(), tr.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dio, &io, sizeof(io), cudaMemcpyHostToDevice));
+    CK(launchGateEnvStep(nullptr, env->n_theta, env->i_mppi, dgp, dtr, true_theta, action[0], action[1], &dio->state, dio->belief, update_belief,
+                         (uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)step, &dio->term));
+    CK(cudaMemcpy(&io, dio, sizeof(io), cudaMemcpyDeviceToHost));
+    *state = io.state;
+    for (int i = 0; i < env->n_theta; i++)
+        belief[i] = io.belief[i];
+    if (term)
+        *term = io.term;
     return DR_OK;
 }
 

@@ -124,3 +124,25 @@ def test_status_strings():
         assert abi.lib().dr_status_string(s)
     assert abi.lib().dr_abi_version() == abi.DR_ABI_VERSION == 2
     assert abi.lib().dr_supported(1, 2) == 1 and abi.lib().dr_supported(1, 3) == 0
+
+
+def test_invalid_track_samples_and_cp_arguments_are_rejected():
+    """dr_track_grids refuses non-finite samples and repeated consecutive samples (the
+    arc-length spline parameter must increase strictly, as scipy's CubicSpline requires
+    in the reference), before any device work; the test hooks refuse bad sizes."""
+    n = abi.DR_N_TRACK_SAMPLES
+    ang = np.arange(n) * 2 * np.pi / n
+    q = np.ascontiguousarray(np.stack([6 * np.cos(ang), 6 * np.sin(ang)], axis=1)[None], np.float64)
+    out = [np.zeros((1, n, 2), np.float32), np.zeros((1, n, 2), np.float32), np.zeros((1, n, 2), np.float32), np.zeros((1, n), np.float32),
+           np.zeros(1, np.float32)]
+    ptrs = [abi.fptr(a) for a in out]
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    bad = q.copy()
+    bad[0, 7, 1] = np.nan
+    assert abi.lib().dr_track_grids(dp(bad), 1, *ptrs) == abi.DR_ERR_INVALID_ARG
+    bad = q.copy()
+    bad[0, 8] = bad[0, 7]
+    assert abi.lib().dr_track_grids(dp(bad), 1, *ptrs) == abi.DR_ERR_INVALID_ARG
+    assert abi.lib().dr_track_grids(dp(q), 0, *ptrs) == abi.DR_ERR_INVALID_ARG
+    k = np.zeros(1, np.uint32)
+    assert abi.lib().dr_debug_cp_host(abi.uptr(k), 0, 10, 0.05, 1, dp(np.zeros(1))) == abi.DR_ERR_INVALID_ARG
