@@ -7,7 +7,8 @@ with V = 2^17 samples over 40 steps (the reference front-end's setting), on a se
 synthetic track (closed Catmull-Rom through 12 control points jittered +-5 m around a
 40 m circle). One control step = every agent's getControl once.
 
-value : control steps/s with inputs resident in HBM (device pipeline, CUDA events)
+value : control steps/s with inputs resident in HBM (dr_mppi_batch_step_device: the
+        whole control step on the device, its host tail included; CUDA events)
 e2e   : control steps/s through the C ABI with host buffers (dr_mppi_batch_step: inputs
         copied from pinned host memory, results copied back, host tail included)
 
@@ -67,6 +68,13 @@ GATE_FLOPS_PER_VERIFY_STEP = 473.4
 K_GRAD = 1024
 GRAD_STEPS = 3
 GRAD_STEP_SIZE = 0.05
+# --workload pr: PR-MPPI (the reference's PRMPPIController) on the strategic race with the
+# benchmark's PR configuration per agent: 8 opponent hypotheses (lateral aggressiveness
+# U(0, 2) m, speed scale U(0.8, 1.2), belief ~ Dirichlet(1)), P = 8 sampled hypotheses,
+# K = 2048, H = 64. FLOPs per PR rollout step (one hypothesis' policy, no belief update,
+# PRMPPIstateCost and PRMPPIsafetyCost) counted like the others (orc_pr_count_ops).
+K_PR, P_PR, NTH_PR = 2048, 8, 8
+PR_FLOPS_PER_ROLLOUT_STEP = 623.5
 WL = {"kind": "strat"}  # the workload of this run (set from --workload)
 
 
@@ -81,6 +89,8 @@ def _flops():
 
 
 def _workload_name() -> str:
+    if WL["kind"] == "pr":
+        return f"prmppi_4x{P_PR}x{K_PR}x64_{NTH_PR}hyp"
     if WL["kind"] == "gates":
         return "gate_mppi_4x4096x64_8gates"
     if WL["kind"] == "grad":
@@ -89,6 +99,8 @@ def _workload_name() -> str:
 
 
 def _unit() -> str:
+    if WL["kind"] == "pr":
+        return f"control steps/s (4 agents x PR-MPPI with P={P_PR} hypotheses x K={K_PR} x H=64, nominal and robust plans; all agents advanced once)"
     if WL["kind"] == "grad":
         return (f"control steps/s (4 agents x K={K_GRAD} x H=64 MPPI + {GRAD_STEPS} projected gradient steps, verification V=2^17 x 40, "
                 "all agents advanced once; strategic race)")
@@ -358,10 +370,17 @@ def run_ours(args) -> None:
     bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
     bel[:, :N_THETA] = beliefs
     bel_dev = torch.from_numpy(bel).to("cuda")
+    act_dev = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    info_dev = torch.zeros(C.sizeof(abi.dr_mppi_info) * n, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+
+    def dev_step():
+        # the whole control step on the device, its tail included (dr_mppi_batch_step_device)
+        batch.step_device(st_dev.data_ptr(), bel_dev.data_ptr(), act_dev.data_ptr(), info_dev.data_ptr())
 
     # ---- device-resident throughput -------------------------------------------------------
     for _ in range(args.warmup):
-        batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+        dev_step()
     torch.cuda.synchronize()
     batch.set_profiling(True)
     _barrier(world)
@@ -372,7 +391,7 @@ def run_ours(args) -> None:
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+        dev_step()
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -415,11 +434,11 @@ def run_ours(args) -> None:
         batch.set_overlap(False)
         serial_steps = max(10, min(50, args.steps))
         for _ in range(3):
-            batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+            dev_step()
         torch.cuda.synchronize()
         batch.set_profiling(True)
         for _ in range(serial_steps):
-            batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+            dev_step()
         torch.cuda.synchronize()
         kt_serial = batch.kernel_times()
         batch.set_profiling(False)
@@ -520,6 +539,204 @@ def reference_cuda_timing(scs, warmup: int = 3, steps: int = 20) -> dict | None:
                     "CUDA events; (ii) MPPIController::getControl per agent incl. verification, wall clock"}
 
 
+def _pr_workload(rank: int):
+    drb = _package()
+    return [drb.scenarios.robust_race(agent=a, seed=rank, K=K_PR, T=H, P=P_PR, n_theta=NTH_PR) for a in range(AGENTS)]
+
+
+def cpu_baseline_pr(scs, target_s: float = 10.0, max_reps: int = 100000, k_s: int = 512) -> dict:
+    """The reference's CPU PR-MPPI rollout (its model functions, oracle/_ref, OpenMP) on a
+    bounded sample of one agent: k_s samples x P hypotheses x nominal and robust plans x
+    H steps, scaled to the 4-agent step (the rollout is the PR step's work)."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O
+
+    drb = _package()
+    O.set_abi(drb.abi)
+    variant = O.ref_variant_name(NTH_PR, True)
+    kind = "reference" if O.ref_available(variant) else "port"
+    threads = os.cpu_count() or 1
+    sc = scs[0]
+    c = sc.prmppi
+    c_small = type(c).from_buffer_copy(c)
+    c_small.n_samples = k_s
+    sc.prmppi = c_small
+    noise = O.pr_noise(sc, 0)
+    thetas = O.pr_thetas(sc, 0, sc.belief())
+    nom = np.zeros((H, 2), np.float32)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        if kind == "reference":
+            O.pr_rollout(sc, nom, nom, noise, thetas, 0, impl=variant, nthreads=threads)
+        else:
+            O.pr_rollout(sc, nom.astype(np.float64), nom.astype(np.float64), noise, thetas, 0, prec=32)
+        reps += 1
+        if time.perf_counter() - t0 > target_s or reps >= max_reps:
+            break
+    el = (time.perf_counter() - t0) / reps
+    sc.prmppi = c
+    step_s = AGENTS * el * (K_PR / k_s)
+    return {"value": 1.0 / step_s, "unit": "control_steps/s", "cores": threads, "kind": kind,
+            "sample": f"1 agent: PR rollout of {k_s} samples x {P_PR} hypotheses x 2 plans x {H} steps, {reps} repetitions "
+                      f"({time.perf_counter() - t0:.1f} s), scaled to 4 agents x K={K_PR}",
+            "ms_per_control_step": step_s * 1e3}
+
+
+def run_ours_pr(args) -> None:
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    drb = _package()
+    import drone_race_b200.controllers as ctl_mod
+
+    abi = drb.abi
+    scs = _pr_workload(rank)
+    stream = torch.cuda.Stream()
+    ctls = [ctl_mod.PRMPPIController(s.env, s.prmppi, s.seed, device=local, stream=stream.cuda_stream) for s in scs]
+    batch = ctl_mod.PRMPPIBatch(ctls, stream=stream.cuda_stream)
+    n = len(ctls)
+    states = [s.state for s in scs]
+    beliefs = np.stack([s.belief() for s in scs])
+    st_dev = torch.frombuffer(bytearray(bytes((abi.dr_sim_state * n)(*states))), dtype=torch.uint8).to("cuda")
+    bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+    bel[:, :NTH_PR] = beliefs
+    bel_dev = torch.from_numpy(bel).to("cuda")
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+    torch.cuda.synchronize()
+    batch.set_profiling(True)
+    _barrier(world)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    _barrier(world)
+    ms = _max_over_ranks(e0.elapsed_time(e1), world)
+    kt = batch.kernel_times()
+    batch.set_profiling(False)
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+    for c in ctls:
+        c.engine = object()
+    e2e_steps = 0 if args.quick else args.steps
+    for _ in range(0 if args.quick else args.warmup):
+        batch.step(states, beliefs)
+    torch.cuda.synchronize()
+    _barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        batch.step(states, beliefs)
+    t1 = time.perf_counter()
+    _barrier(world)
+    e2e_s = _max_over_ranks(max(t1 - t0, 1e-9), world)
+    h2d = d2h = 0
+    for c in ctls:
+        a, b = C.c_size_t(), C.c_size_t()
+        abi.lib().dr_prmppi_io_bytes(c.handle, C.byref(a), C.byref(b))
+        h2d += a.value
+        d2h += b.value
+    units = AGENTS * 2 * P_PR * K_PR * H
+    dom = max(kt, key=kt.get) if kt else None
+    roof = None
+    if dom and "rollout" in dom and clk.get("sm_mhz"):
+        peak = 2 * 128 * 148 * clk["sm_mhz"] * 1e6 / 1e12
+        achieved = units * PR_FLOPS_PER_ROLLOUT_STEP / (kt[dom] / 1e3) / 1e12
+        roof = {"bound": "fp32", "kernel": f"pr_{dom}" if not dom.startswith("pr") else dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": "FP32 FMA rate of 148 SMs x 128 lanes at the median SM clock sampled during the timed region (MEASURED_PEAKS.json has no FP32 figure)",
+                "units_per_launch": units, "flops_per_unit": PR_FLOPS_PER_ROLLOUT_STEP, "kernel_ms": kt[dom],
+                "measured": "CUDA events around each launch on its stream over the timed region"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.quick:
+        cpu = cpu_baseline_pr(scs)
+        cpu.pop("ms_per_control_step", None)
+    line = {
+        "metric": "control_steps_per_s",
+        "value": value,
+        "unit": _unit(),
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded tracks, hypotheses and beliefs; no dataset)",
+        "config": {"workload": _workload_name(), "agents": AGENTS, "K": K_PR, "H": H, "P": P_PR, "n_theta": NTH_PR, "n_opp": 1,
+                   "parallelism": f"replicas x{world}", "l2": "working set per step < L2; steps are dependent control steps of the same controllers"},
+        "rollout_steps_per_s": world * units * args.steps / (ms / 1e3),
+        "kernel_ms": kt,
+        "e2e": None if args.quick else {"value": world * args.steps / e2e_s, "unit": "control steps/s", "h2d_bytes_per_step": h2d,
+                                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s / args.steps * 1e3},
+        "gpu_launches": len(kt) * args.steps,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for c in ctls:
+        c.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_reference_pr(args) -> None:
+    """Reference arm of --workload pr: the reference's CPU PR rollout (host threads), and
+    on a GPU box its own PRMPPIController::getControl on the same 4 agents."""
+    scs = _pr_workload(0)
+    ms = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline_pr(scs, target_s=min(20.0, 120.0 / max(1, args.warmup + args.steps)), max_reps=1)
+        if i >= args.warmup:
+            ms.append(r["ms_per_control_step"])
+        base = r
+    v = 1e3 / statistics.mean(ms)
+    ref_cuda = None
+    try:
+        import torch
+
+        if torch.cuda.is_available() and not args.no_reference_cuda:
+            sys.path.insert(0, str(ROOT))
+            from oracle import oracle as O
+
+            drb = _package()
+            O.set_abi(drb.abi)
+            variant = O.ref_variant_name(NTH_PR, True)
+            if O.ref_available(variant):
+                out = (C.c_double * 2)()
+                sc = scs[0]
+                rc = O.ref(variant).refc_prmppi_time(C.byref(sc.env), C.byref(sc.prmppi), C.byref(sc.state), AGENTS, 3, 20, out)
+                ref_cuda = ({"getcontrol_ms_per_step": out[0], "control_steps_per_s": 1e3 / out[0], "steps": 20, "warmup": 3,
+                             "what": "reference PRMPPIController::getControl per agent, wall clock, compiled from its sources"}
+                            if rc == 0 else {"error": f"reference CUDA timing failed with status {rc}"})
+    except Exception as e:  # measurement only
+        ref_cuda = {"error": repr(e)}
+    print(json.dumps({"impl": "reference", "metric": "control_steps_per_s", "value": v, "unit": _unit(), "n_gpus": 1, "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                      "data": "synthetic (seeded tracks, hypotheses and beliefs; no dataset)",
+                      "config": {"workload": _workload_name(), "agents": AGENTS, "K": K_PR, "H": H, "P": P_PR, "n_theta": NTH_PR,
+                                 "parallelism": "host threads"},
+                      "cpu_baseline": {"value": v, "unit": "control_steps/s", "cores": base["cores"], "kind": base["kind"], "sample": base["sample"]},
+                      "e2e": {"value": v, "unit": "control steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                      "reference_cuda": ref_cuda}), flush=True)
+
+
 def run_reference(args) -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -528,6 +745,9 @@ def run_reference(args) -> None:
     if WL["kind"] == "grad":
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no gradient-refined MPPI; its plain MPPI arm is --workload strat"}),
               flush=True)
+        return
+    if WL["kind"] == "pr":
+        run_reference_pr(args)
         return
     scs = workload(0)
     steps_ms = []
@@ -570,9 +790,10 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e, no CPU baseline): for profiler runs")
     ap.add_argument("--no-overlap", action="store_true", help="run the previous plan's verification after the rollout instead of beside it")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="strat", choices=["strat", "gates", "grad"],
+    ap.add_argument("--workload", default="strat", choices=["strat", "gates", "grad", "pr"],
                     help="strat: the strategic race (the headline workload); gates: the gate race (EnvDroneRace); "
-                         "grad: gradient-refined MPPI at K=1024 with a closed-loop comparison against plain MPPI at K=4096")
+                         "grad: gradient-refined MPPI at K=1024 with a closed-loop comparison against plain MPPI at K=4096; "
+                         "pr: PR-MPPI, 4 agents x 8 hypotheses x K=2048")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")
     args = ap.parse_args()
@@ -581,6 +802,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif WL["kind"] == "pr":
+        run_ours_pr(args)
     else:
         run_ours(args)
 

@@ -87,6 +87,7 @@ def port() -> C.CDLL:
             "orc_count_ops": (C.c_int, [E, M, S, f, f, f, u64, u64, C.c_int, C.c_int, C.c_int, d]),
             "orc_gate_count_ops": (C.c_int, [GE, M, GS, f, f, f, u64, u64, C.c_int, C.c_int, C.c_int, d]),
             "orc_nominal_cost": (C.c_int, [E, M, S, f, f, d, d, d, d, d, i]),
+            "orc_pr_count_ops": (C.c_int, [E, PR, S, f, f, C.c_int, u64, u64, C.c_int, C.c_int, d]),
         }
         for n, (r, args) in protos.items():
             fn = getattr(L, n)

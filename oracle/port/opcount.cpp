@@ -299,3 +299,51 @@ extern "C" int orc_gate_count_ops(const dr_gate_env_config* ec, const dr_mppi_co
     return countOps<gate::Env<CF>, gate::State<CF>>(env, mc, s0, belief0, nominal, noise, seed, step, nsamples, kind, dedup, out,
                                                     [margin](int k) { return gate::Flags{true, true, false, k == 0, true, margin}; });
 }
+
+// The PR-MPPI rollout step (PRMPPIfullRolloutKernel, prmppi_kernels.cu:55-130):
+// environmentStep<false, false, true> under one sampled hypothesis, PRMPPIstateCost and
+// PRMPPIsafetyCost each step. out as orc_count_ops; nsamples samples of the nominal
+// controls plus noise [T][K][2] under hypothesis `theta`.
+extern "C" int orc_pr_count_ops(const dr_env_config* ec, const dr_prmppi_config* pc, const dr_sim_state* s0, const float* nominal, const float* noise,
+                                int theta, uint64_t seed, uint64_t step, int nsamples, int dedup, double* out)
+{
+    Env<CF> env(*ec);
+    CountCtx ctx;
+    ctx.dedup = dedup != 0;
+    const int K = pc->n_samples, T = pc->n_timesteps;
+    PrCosts<CF> cc{pc->coll_dist_factor, pc->boundary_cost, pc->boundary_threshold_factor, pc->win_cost,
+                   pc->opp_win_cost,     pc->final_adv_weight, pc->final_opp_adv_weight, pc->safety_weight};
+    const StepFlags flags{false, false, true, true, false};
+    double steps = 0;
+    for (int s = 0; s < nsamples && s < K; s++)
+    {
+        State<CF> st = State<CF>::from(*s0);
+        Branch<CF> bs{};
+        CF running = 0.0, safe = -INFINITY, decay = 1.0;
+        bool stop = false;
+        EnvNoise rng(seed, (uint32_t)s, 0u, step, S_PR_ROLL_ENV);
+        for (int t = 0; t < T && !stop; t++)
+        {
+            ctx.seen.clear();
+            g_ctx = nullptr;
+            rng.begin_step((uint32_t)t);
+            g_ctx = &ctx;
+            CF ego[DIM];
+            for (int d = 0; d < DIM; d++)
+                ego[d] = CF(nominal[t * DIM + d]) + CF(noise[((size_t)t * K + s) * DIM + d]);
+            bool branched = false;
+            int term = environmentStep(t, theta, env, ego, flags, st, bs, branched, CF(0.0), rng);
+            stop = (term != TERM_NONE);
+            running += decay * prStateCost(st, env, cc);
+            safe = fmax(safe, prSafetyCost(st, env, cc));
+            decay *= CF(DECAY);
+            g_ctx = nullptr;
+            steps += 1;
+        }
+    }
+    g_ctx = nullptr;
+    const OpStats& o = ctx.s;
+    double v[10] = {o.add, o.mul, o.div, o.sqrt_, o.exp_, o.log_, o.pow_, o.minmax, o.cmp, steps};
+    std::memcpy(out, v, sizeof(v));
+    return 0;
+}
