@@ -26,6 +26,19 @@ namespace dr
 {
 
 constexpr int PRB = 128;
+// Rollout CTA: 512 threads, two CTAs per SM (64 registers a thread), whose warps take a
+// barrier every step (`__syncthreads_or` on the still-running samples) so the warps that
+// share an SM sub-partition fetch the same instructions; the benchmark's 4 x 2 x 8 x 2048
+// rollouts then fit in one wave of 296 CTAs.
+#ifndef PR_ROLL_TILE
+#define PR_ROLL_TILE 512
+#endif
+// two CTAs a SM where one opponent keeps the state in 64 registers; one with two opponents
+template <int NOPP>
+constexpr int prRollMinBlocks()
+{
+    return NOPP <= 1 ? 2 : 1;
+}
 constexpr int PUB = 256;
 
 __host__ __device__ __forceinline__ size_t pa16(size_t x)
@@ -115,14 +128,15 @@ __host__ __device__ inline PrRollSmem prLayout(int T)
     L.nom = off;
     off = a16(off + (size_t)T * 2 * 4);
     L.red = off;
-    off = a16(off + (size_t)PRB * 2 * 4);
+    off = a16(off + (size_t)PR_ROLL_TILE * 2 * 4);
     L.total = off;
     return L;
 }
 
 // tile: inst, s0 (first sample), count (samples), aux (0 nominal / 1 robust)
 template <int NOPP, int NTH>
-__global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, const Tile* __restrict__ tiles)
+__global__ void __launch_bounds__(PR_ROLL_TILE, prRollMinBlocks<NOPP>()) pr_rollout(const PrDev* __restrict__ insts, const PrIn* __restrict__ in,
+                                                                              const Tile* __restrict__ tiles)
 {
     constexpr int NA = NOPP + 1;
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -155,12 +169,11 @@ __global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ inst
     }
     const EnvParams& E = *sE;
     const Track tr = trackIn(sGrid);
-    const int spb = PRB / P;
+    const int spb = PR_ROLL_TILE / P;
     const int sl = threadIdx.x / P, p = threadIdx.x % P;
     const int s = tile.s0 + sl;
     const bool valid = sl < spb && sl < tile.count;
     float running = 0.0f, safe = -INFINITY;
-    if (valid)
     {
         const int theta = D.thetas[p];
         DState<NA> st;
@@ -170,25 +183,35 @@ __global__ void __launch_bounds__(PRB) pr_rollout(const PrDev* __restrict__ inst
         const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
         EnvNoise rng(k0, k1, (uint32_t)s, ((((uint32_t)robust << 8) | (uint32_t)p) << 16), step, S_PR_ROLL_ENV);
         float decay = 1.0f;
-        bool stop = false;
         const SafetyMargin margin = safetyMargin(E, D.cfg.collDistFactor);
-        for (int t = 0; t < T && !stop; t++)
+        bool active = valid;
+        for (int t = 0; t < T; t++)
         {
+            // every thread of the CTA takes this barrier once per step (T is uniform); it
+            // keeps the warps on the same step and ends the loop once all samples are done
+            if (!__syncthreads_or(active))
+                break;
+            if (!active)
+                continue;
             rng.begin_step((uint32_t)t);
             U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)t, step, S_PR_EPS, 0);
             float ego0 = sNom[t * 2] + scaled_normal(D.cfg.sigma0, r.x);
             float ego1 = sNom[t * 2 + 1] + scaled_normal(D.cfg.sigma1, r.y);
             bool branched = false;
             StepOut o = envStep<NOPP, NTH, false, false, true, false>(t, theta, tr, E, ego0, ego1, st, bs, branched, 0.0f, rng);
-            stop = (o.term != TERM_NONE);
+            if (o.term != TERM_NONE)
+                active = false;
             running += decay * prStateCost(o, E, D.cfg.boundaryThresholdFactor, D.cfg.boundaryCost, D.cfg.winCost, D.cfg.oppWinCost);
             safe = fmaxf(safe, prSafetyCost(o, margin));
             decay *= DECAY;
         }
-        running += finalCost<NOPP>(st, E, D.cfg.finalAdvWeight, D.cfg.finalOppAdvWeight);
-        float* out = robust ? D.costRob : D.costNom;
-        out[((size_t)p * K + s) * 2 + 0] = running;
-        out[((size_t)p * K + s) * 2 + 1] = safe;
+        if (valid)
+        {
+            running += finalCost<NOPP>(st, E, D.cfg.finalAdvWeight, D.cfg.finalOppAdvWeight);
+            float* out = robust ? D.costRob : D.costNom;
+            out[((size_t)p * K + s) * 2 + 0] = running;
+            out[((size_t)p * K + s) * 2 + 1] = safe;
+        }
     }
     red[threadIdx.x * 2] = running;
     red[threadIdx.x * 2 + 1] = safe;
@@ -419,7 +442,7 @@ bool prSupported(int nopp, int nth)
 
 int prRolloutSamplesPerBlock()
 {
-    return PRB;
+    return PR_ROLL_TILE;
 }
 
 size_t prRolloutSmem(int T)
@@ -442,7 +465,7 @@ template <int NOPP, int NTH> static cudaError_t prRollT(const LaunchArgs& a, siz
 {
     auto k = pr_rollout<NOPP, NTH>;
     ensureSmem(k, smem);
-    k<<<a.nTiles, PRB, smem, a.stream>>>(a.pr, a.prIn, a.tiles);
+    k<<<a.nTiles, PR_ROLL_TILE, smem, a.stream>>>(a.pr, a.prIn, a.tiles);
     return cudaGetLastError();
 }
 
