@@ -75,6 +75,14 @@ GRAD_STEP_SIZE = 0.05
 # PRMPPIstateCost and PRMPPIsafetyCost) counted like the others (orc_pr_count_ops).
 K_PR, P_PR, NTH_PR = 2048, 8, 8
 PR_FLOPS_PER_ROLLOUT_STEP = 623.5
+# --workload races: many independent races of uneven sizes in one batch per control mode
+# (scenarios.uneven_races: 256 races, U{1..8} agents each, K log-uniform [256, 16384],
+# H in {32, 48, 64, 96}, tracks through U{6..16} points, dense and spline controls by
+# race), verification of 4096 samples over min(40, H) steps per agent; one control step =
+# every agent of every race advanced once. Measured with one CTA per tile, with persistent
+# launches fed by the device work queue, and with the shapes the autotuner picks.
+N_RACES = 256
+V_RACES = 4096
 WL = {"kind": "strat"}  # the workload of this run (set from --workload)
 
 
@@ -737,10 +745,162 @@ def run_reference_pr(args) -> None:
                       "reference_cuda": ref_cuda}), flush=True)
 
 
+def run_ours_races(args) -> None:
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    drb = _package()
+    import drone_race_b200.controllers as ctl_mod
+
+    abi = drb.abi
+    scs = drb.scenarios.uneven_races(N_RACES, seed=rank, n_verif=V_RACES)
+    groups = [g for g in ([s for s in scs if not s.mppi.use_splines], [s for s in scs if s.mppi.use_splines]) if g]
+    runs = []
+    for g in groups:
+        stream = torch.cuda.Stream()
+        ctls = [ctl_mod.MPPIController(s.env, s.mppi, s.seed, device=local, stream=stream.cuda_stream) for s in g]
+        batch = ctl_mod.MPPIBatch(ctls, stream=stream.cuda_stream)
+        n = len(g)
+        states = [s.state for s in g]
+        st_dev = torch.frombuffer(bytearray(bytes((type(states[0]) * n)(*states))), dtype=torch.uint8).to("cuda")
+        bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+        bel[:, :N_THETA] = np.stack([s.belief() for s in g])
+        runs.append({"stream": stream, "ctls": ctls, "batch": batch, "scs": g, "st": st_dev, "bel": torch.from_numpy(bel).to("cuda"),
+                     "act": torch.zeros((n, 2), dtype=torch.float32, device="cuda"),
+                     "info": torch.zeros(C.sizeof(abi.dr_mppi_info) * n, dtype=torch.uint8, device="cuda")})
+    torch.cuda.synchronize()
+    n_agents = len(scs)
+
+    def dev_step():
+        for r in runs:
+            r["batch"].step_device(r["st"].data_ptr(), r["bel"].data_ptr(), r["act"].data_ptr(), r["info"].data_ptr())
+
+    def timed(steps: int):
+        for _ in range(args.warmup):
+            dev_step()
+        torch.cuda.synchronize()
+        _barrier(world)
+        s0 = runs[0]["stream"]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s0)
+        for r in runs[1:]:
+            r["stream"].wait_event(e0)
+        for _ in range(steps):
+            dev_step()
+        for r in runs[1:]:
+            ev = torch.cuda.Event()
+            ev.record(r["stream"])
+            s0.wait_event(ev)
+        e1.record(s0)
+        torch.cuda.synchronize()
+        _barrier(world)
+        return _max_over_ranks(e0.elapsed_time(e1), world)
+
+    shapes = {}
+    for name, shape in (("one_cta_per_tile", (0, 0)), ("persistent_queue", (-1, -1))):
+        for r in runs:
+            r["batch"].set_persistent(*shape)
+        shapes[name] = {"ms_per_step": timed(args.steps) / args.steps}
+    tune = [r["batch"].autotune(5) for r in runs]
+    clocks = Clocks(local)
+    clocks.start()
+    ms = timed(args.steps)
+    clk = clocks.stop()
+    shapes["autotuned"] = {"ms_per_step": ms / args.steps, "choices": [{k: t[k] for k in ("rollout_ctas_per_sm", "verify_ctas_per_sm")} for t in tune],
+                           "candidates_ms": [{"rollout": t["rollout"], "verify": t["verify"]} for t in tune]}
+    for v in shapes.values():
+        v["agent_control_steps_per_s"] = world * n_agents / (v["ms_per_step"] / 1e3)
+    ms_per_step = ms / args.steps
+    # per-kernel device times with the tuned shapes
+    for r in runs:
+        r["batch"].set_profiling(True)
+    for _ in range(max(3, min(10, args.steps))):
+        dev_step()
+    torch.cuda.synchronize()
+    kts = [r["batch"].kernel_times() for r in runs]
+    for r in runs:
+        r["batch"].set_profiling(False)
+    # end to end through the C ABI with host buffers (both batches, one after the other)
+    e2e = None
+    if not args.quick:
+        for r in runs:
+            for c in r["ctls"]:
+                c.engine = object()
+        host = [([s.state for s in r["scs"]], np.stack([s.belief() for s in r["scs"]])) for r in runs]
+        for _ in range(2):
+            for r, (st, be) in zip(runs, host):
+                r["batch"].step(st, be)
+        torch.cuda.synchronize()
+        e2e_steps = max(3, min(20, args.steps))
+        _barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for r, (st, be) in zip(runs, host):
+                r["batch"].step(st, be)
+        t1 = time.perf_counter()
+        _barrier(world)
+        e2e_s = _max_over_ranks(t1 - t0, world)
+        h2d = d2h = 0
+        for r in runs:
+            for c in r["ctls"]:
+                a, b = C.c_size_t(), C.c_size_t()
+                abi.lib().dr_mppi_io_bytes(c.handle, C.byref(a), C.byref(b))
+                h2d += a.value
+                d2h += b.value
+        e2e = {"value": world * n_agents * e2e_steps / e2e_s, "unit": "agent control steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e2e_s / e2e_steps * 1e3}
+    rollout_units = sum(s.mppi.n_samples * N_THETA * s.mppi.n_timesteps for s in scs)
+    verify_units = sum(2 * V_RACES * min(40, s.mppi.n_timesteps) for s in scs)
+    kt_sum = {}
+    for kt in kts:
+        for k, v in kt.items():
+            kt_sum[k] = kt_sum.get(k, 0.0) + v
+    roof = None
+    if clk.get("sm_mhz"):
+        peak = 2 * 128 * 148 * clk["sm_mhz"] * 1e6 / 1e12
+        ach = (rollout_units * FLOPS_PER_ROLLOUT_STEP + verify_units * FLOPS_PER_VERIFY_STEP) / (ms_per_step / 1e3) / 1e12
+        roof = {"bound": "fp32", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                "scope": "all FP32 work of one control step of every agent (dense-control FLOP counts; spline evaluation not counted) / device step time",
+                "peak_source": "FP32 FMA rate of 148 SMs x 128 lanes at the median SM clock sampled during the timed region"}
+    line = {
+        "metric": "agent_control_steps_per_s",
+        "value": shapes["autotuned"]["agent_control_steps_per_s"],
+        "unit": f"agent control steps/s ({N_RACES} races, {n_agents} agents of uneven K/H, every agent advanced once per step)",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uneven races; no dataset)",
+        "config": {"workload": f"uneven_races_{N_RACES}", "agents": n_agents, "K_total": sum(s.mppi.n_samples for s in scs),
+                   "H": sorted({s.mppi.n_timesteps for s in scs}), "verif_samples": V_RACES, "batches": len(runs), "parallelism": f"replicas x{world}",
+                   "l2": "working set per step > L2 (costs and plans of all agents)"},
+        "shapes": shapes,
+        "rollout_steps_per_s": world * rollout_units / (ms_per_step / 1e3),
+        "kernel_ms": kt_sum,
+        "e2e": e2e,
+        "gpu_launches": sum(len(kt) for kt in kts) * args.steps,
+        "roofline": roof,
+        "cpu_baseline": None,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for r in runs:
+        r["batch"].close()
+        for c in r["ctls"]:
+            c.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
 def run_reference(args) -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return
+    if WL["kind"] == "races":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference steps one controller per getControl call and has no multi-race batch; "
+                                                              "its per-controller rate is the strat workload's reference arm"}), flush=True)
         return
     if WL["kind"] == "grad":
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no gradient-refined MPPI; its plain MPPI arm is --workload strat"}),
@@ -790,10 +950,11 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e, no CPU baseline): for profiler runs")
     ap.add_argument("--no-overlap", action="store_true", help="run the previous plan's verification after the rollout instead of beside it")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="strat", choices=["strat", "gates", "grad", "pr"],
+    ap.add_argument("--workload", default="strat", choices=["strat", "gates", "grad", "pr", "races"],
                     help="strat: the strategic race (the headline workload); gates: the gate race (EnvDroneRace); "
                          "grad: gradient-refined MPPI at K=1024 with a closed-loop comparison against plain MPPI at K=4096; "
-                         "pr: PR-MPPI, 4 agents x 8 hypotheses x K=2048")
+                         "pr: PR-MPPI, 4 agents x 8 hypotheses x K=2048; "
+                         "races: 256 independent races of uneven K/H in one batch per control mode")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")
     args = ap.parse_args()
@@ -804,6 +965,8 @@ def main():
         run_reference(args)
     elif WL["kind"] == "pr":
         run_ours_pr(args)
+    elif WL["kind"] == "races":
+        run_ours_races(args)
     else:
         run_ours(args)
 

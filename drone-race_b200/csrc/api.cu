@@ -254,6 +254,44 @@ struct dr_mppi_batch
         return envKind ? launchGateVerify(a, nth, iMppi, verSmem, nullptr, nullptr) : launchMppiVerify(a, nopp, nth, verSmem, nullptr, nullptr);
     }
 
+    // Persistent launches of the rollout and the verification: perSm CTAs per SM take the
+    // tiles from a device work queue (a ticket counter, zeroed by a memset node before
+    // each launch) until the table is exhausted; the tables list the longest tiles first.
+    // perSm 0 launches one CTA per tile.
+    enum QueueSlot
+    {
+        Q_ROLL = 0,
+        Q_VER_NEW = 1,
+        Q_VER_OLD = 2,
+        Q_VER_ALL = 3
+    };
+    unsigned* dQueue = nullptr;
+    int numSms = 0;
+    int rollPerSm = 0, verPerSm = 0;
+
+    LaunchArgs qargs(const Tile* tiles, int n, const MppiIn* in, QueueSlot slot, int perSm, cudaStream_t s) const
+    {
+        LaunchArgs a = args(tiles, n, in);
+        a.stream = s;
+        if (perSm > 0 && envKind == 0 && dQueue)
+        {
+            a.queue = dQueue + slot;
+            a.grid = perSm * numSms;
+        }
+        return a;
+    }
+
+    cudaError_t launchQueued(const LaunchArgs& a, bool verification) const
+    {
+        if (a.queue)
+        {
+            cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(unsigned), a.stream);
+            if (e != cudaSuccess)
+                return e;
+        }
+        return verification ? launchVerify(a) : launchRollout(a);
+    }
+
     // kernels of one control step, reading inputs from `in` (device)
     // finish != null: the device tail after the kernels (fully device-resident steps)
     int launchAll(const MppiIn* in, bool profile, Timer* timer, MppiIn* finishIn = nullptr, float* actions = nullptr, dr_mppi_info* infos = nullptr)
@@ -290,9 +328,7 @@ struct dr_mppi_batch
                 timerSide.begin();
                 timerSide.mark("verify_old", sideStream);
             }
-            LaunchArgs a = args(dVerOld, nVerOld, in);
-            a.stream = sideStream;
-            CK(launchVerify(a));
+            CK(launchQueued(qargs(dVerOld, nVerOld, in, Q_VER_OLD, verPerSm, sideStream), true));
             if (profile)
             {
                 timerSide.mark("end", sideStream);
@@ -302,7 +338,7 @@ struct dr_mppi_batch
         }
         if (profile)
             timer->mark("rollout", ex);
-        CK(launchRollout(args(dRoll, nRoll, in)));
+        CK(launchQueued(qargs(dRoll, nRoll, in, Q_ROLL, rollPerSm, ex), false));
         if (profile)
             timer->mark("update", ex);
         CK(launchMppiUpdate(args(dUpd, nUpd, in), nth));
@@ -317,9 +353,9 @@ struct dr_mppi_batch
             if (profile)
                 timer->mark(side ? "verify_new" : "verify", ex);
             if (side)
-                CK(launchVerify(args(dVerNew, nVerNew, in)));
+                CK(launchQueued(qargs(dVerNew, nVerNew, in, Q_VER_NEW, verPerSm, ex), true));
             else
-                CK(launchVerify(args(dVer, nVer, in)));
+                CK(launchQueued(qargs(dVer, nVer, in, Q_VER_ALL, verPerSm, ex), true));
         }
         if (finishIn)
         {
@@ -607,6 +643,8 @@ struct dr_mppi_batch
         cudaFree(dRoll);
         cudaFree(dUpd);
         cudaFree(dVer);
+        cudaFree(dQueue);
+        dQueue = nullptr;
         if (hIn)
             cudaFreeHost(hIn);
         if (sideStream)
@@ -676,6 +714,18 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
         maxM = std::max(maxM, h->M);
         maxNbpT = std::max(maxNbpT, h->nbp * h->T);
     }
+    // longest tiles first (stable, so equal tiles keep controller order): a persistent
+    // launch takes them in this order, and a static grid is dispatched roughly in it
+    auto byWork = [&](std::vector<Tile>& v, bool verification) {
+        std::stable_sort(v.begin(), v.end(), [&](const Tile& x, const Tile& y) {
+            const long long wx = (long long)x.count * (verification ? hs[x.inst]->H : hs[x.inst]->T);
+            const long long wy = (long long)y.count * (verification ? hs[y.inst]->H : hs[y.inst]->T);
+            return wx > wy;
+        });
+    };
+    byWork(roll, false);
+    byWork(ver, true);
+    byWork(verOld, true);
     // tile table: new-plan tiles first, then previous-plan tiles
     b->nVerNew = (int)ver.size();
     b->nVerOld = (int)verOld.size();
@@ -704,6 +754,9 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
         CK(cudaMemcpy(b->dVer, ver.data(), sizeof(Tile) * ver.size(), cudaMemcpyHostToDevice));
     b->dVerNew = b->dVer;
     b->dVerOld = b->dVer + b->nVerNew;
+    CK(cudaMalloc(&b->dQueue, sizeof(unsigned) * 4));
+    CK(cudaMemset(b->dQueue, 0, sizeof(unsigned) * 4));
+    CK(cudaDeviceGetAttribute(&b->numSms, cudaDevAttrMultiProcessorCount, b->device));
     {
         int least = 0, greatest = 0;
         CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -1658,6 +1711,218 @@ extern "C" int dr_mppi_batch_set_priority(dr_mppi_batch* b, int on)
     b->dropGraph();
     b->dropDevGraph();
     b->prio = on != 0;
+    return DR_OK;
+}
+
+namespace
+{
+// Resolves a requested CTAs-per-SM count for a persistent launch: -1 = as many as fit.
+int resolvePerSm(const dr_mppi_batch* b, int req, bool verification, int* out)
+{
+    if (req == 0)
+    {
+        *out = 0;
+        return DR_OK;
+    }
+    const int fit = mppiResident(b->nopp, b->nth, verification, b->spl, verification ? b->verSmem : b->rollSmem);
+    if (fit <= 0)
+        return fail(DR_ERR_CUDA, "persistent launch: no CTA of this kernel fits on an SM");
+    if (req < 0)
+        req = fit;
+    if (req > fit)
+        return fail(DR_ERR_INVALID_ARG, "persistent launch: " + std::to_string(req) + " CTAs per SM requested, " + std::to_string(fit) + " fit");
+    *out = req;
+    return DR_OK;
+}
+
+// Median device time of `reps` runs of `launch` on `s` (after one untimed run).
+template <typename F> int timeLaunch(cudaStream_t s, int reps, F launch, float* ms)
+{
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    std::vector<float> t;
+    int rc = DR_OK;
+    for (int r = -1; r < reps && rc == DR_OK; r++)
+    {
+        cudaError_t e = cudaEventRecord(e0, s);
+        if (e == cudaSuccess)
+            e = launch();
+        if (e == cudaSuccess)
+            e = cudaEventRecord(e1, s);
+        if (e == cudaSuccess)
+            e = cudaEventSynchronize(e1);
+        float x = 0.0f;
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(&x, e0, e1);
+        if (e != cudaSuccess)
+            rc = fail(DR_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+        else if (r >= 0)
+            t.push_back(x);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc)
+        return rc;
+    std::sort(t.begin(), t.end());
+    *ms = t[t.size() / 2];
+    return DR_OK;
+}
+} // namespace
+
+extern "C" int dr_mppi_batch_set_persistent(dr_mppi_batch* b, int rollout_ctas_per_sm, int verify_ctas_per_sm)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    if (b->envKind != 0 && (rollout_ctas_per_sm != 0 || verify_ctas_per_sm != 0))
+        return fail(DR_ERR_UNSUPPORTED, "persistent launches are built for the strategic race");
+    CK(cudaSetDevice(b->device));
+    int r = 0, v = 0;
+    int rc = resolvePerSm(b, rollout_ctas_per_sm, false, &r);
+    if (rc)
+        return rc;
+    rc = resolvePerSm(b, verify_ctas_per_sm, true, &v);
+    if (rc)
+        return rc;
+    CK(cudaStreamSynchronize(b->stream));
+    b->dropGraph();
+    b->dropDevGraph();
+    b->rollPerSm = r;
+    b->verPerSm = v;
+    return DR_OK;
+}
+
+extern "C" int dr_mppi_batch_autotune(dr_mppi_batch* b, int reps, dr_tune_report* out)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    if (reps < 1 || reps > 1000)
+        return fail(DR_ERR_INVALID_ARG, "reps must be in 1..1000");
+    if (b->runs == 0 && !b->devCtl)
+        return fail(DR_ERR_STATE, "autotune needs one completed step of the batch");
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->stream));
+    dr_tune_report rep{};
+    cudaStream_t s = b->stream;
+    const bool persistOk = b->envKind == 0;
+    // rollout grid
+    {
+        std::vector<int> cand{0};
+        const int fit = persistOk ? mppiResident(b->nopp, b->nth, false, b->spl, b->rollSmem) : 0;
+        for (int c = 1; c <= fit && (int)cand.size() < DR_TUNE_MAX_CANDIDATES; c++)
+            cand.push_back(c);
+        float best = INFINITY;
+        for (int c : cand)
+        {
+            float ms = 0.0f;
+            int rc = timeLaunch(s, reps, [&] { return b->launchQueued(b->qargs(b->dRoll, b->nRoll, b->dIn, dr_mppi_batch::Q_ROLL, c, s), false); }, &ms);
+            if (rc)
+                return rc;
+            rep.rollout_cand[rep.n_rollout] = c;
+            rep.rollout_ms[rep.n_rollout++] = ms;
+            if (ms < best)
+            {
+                best = ms;
+                rep.rollout_ctas_per_sm = c;
+            }
+        }
+    }
+    // verification grid (both plans in one launch)
+    if (b->verify && b->nVer > 0)
+    {
+        std::vector<int> cand{0};
+        const int fit = persistOk ? mppiResident(b->nopp, b->nth, true, b->spl, b->verSmem) : 0;
+        for (int c = 1; c <= fit && (int)cand.size() < DR_TUNE_MAX_CANDIDATES; c++)
+            cand.push_back(c);
+        float best = INFINITY;
+        for (int c : cand)
+        {
+            float ms = 0.0f;
+            int rc = timeLaunch(s, reps, [&] { return b->launchQueued(b->qargs(b->dVer, b->nVer, b->dIn, dr_mppi_batch::Q_VER_ALL, c, s), true); }, &ms);
+            if (rc)
+                return rc;
+            rep.verify_cand[rep.n_verify] = c;
+            rep.verify_ms[rep.n_verify++] = ms;
+            if (ms < best)
+            {
+                best = ms;
+                rep.verify_ctas_per_sm = c;
+            }
+        }
+    }
+    // checkpoint stride of the gradient refinement, timed without writing the plans
+    if (b->nGrad > 0)
+    {
+        std::vector<int> cand{0};
+        int maxT = 0;
+        for (auto* h : b->hs)
+            if (h->gradSteps > 0)
+                maxT = std::max(maxT, h->T);
+        const int sq = (int)std::ceil(std::sqrt((double)maxT));
+        for (int c : {1, sq, 2 * sq})
+            if (c >= 1 && c <= maxT && std::find(cand.begin(), cand.end(), c) == cand.end())
+                cand.push_back(c);
+        std::vector<GradJob> base(b->nGrad);
+        CK(cudaMemcpy(base.data(), b->dGrad, sizeof(GradJob) * b->nGrad, cudaMemcpyDeviceToHost));
+        GradJob* dJobs = nullptr;
+        CK(cudaMalloc(&dJobs, sizeof(GradJob) * b->nGrad));
+        float best = INFINITY;
+        int rc = DR_OK;
+        for (int c : cand)
+        {
+            std::vector<GradJob> jobs = base;
+            size_t smem = 0;
+            bool fits = true;
+            for (auto& j : jobs)
+            {
+                const dr_mppi* h = nullptr;
+                for (size_t i = 0; i < b->hs.size(); i++)
+                    if (j.D == b->dDesc + i)
+                        h = b->hs[i];
+                if (!h)
+                    continue;
+                j.write = 0;
+                j.ckpt = c > 0 ? std::min(c, h->T) : gradDefaultStride(b->nopp, b->nth, h->T, h->M, b->spl);
+                const size_t need = gradSmem(b->nopp, b->nth, h->T, h->M, j.ckpt, b->spl);
+                if (need > 227 * 1024)
+                    fits = false;
+                smem = std::max(smem, need);
+            }
+            if (!fits)
+                continue;
+            if (cudaMemcpy(dJobs, jobs.data(), sizeof(GradJob) * jobs.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            {
+                rc = fail(DR_ERR_CUDA, "autotune: job copy failed");
+                break;
+            }
+            float ms = 0.0f;
+            rc = timeLaunch(s, reps, [&] { return launchGradNominal(s, dJobs, b->nGrad, b->nopp, b->nth, b->spl, smem); }, &ms);
+            if (rc)
+                break;
+            rep.grad_cand[rep.n_grad] = c;
+            rep.grad_ms[rep.n_grad++] = ms;
+            if (ms < best)
+            {
+                best = ms;
+                rep.grad_ckpt = c;
+            }
+        }
+        cudaFree(dJobs);
+        if (rc)
+            return rc;
+        for (auto* h : b->hs)
+            if (h->gradSteps > 0)
+                h->gradCkpt = rep.grad_ckpt > 0 ? std::min(rep.grad_ckpt, h->T) : gradDefaultStride(b->nopp, b->nth, h->T, h->M, b->spl);
+        rc = b->setupGrad();
+        if (rc)
+            return rc;
+    }
+    b->dropGraph();
+    b->dropDevGraph();
+    b->rollPerSm = rep.rollout_ctas_per_sm;
+    b->verPerSm = rep.verify_ctas_per_sm;
+    if (out)
+        *out = rep;
     return DR_OK;
 }
 

@@ -73,6 +73,21 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
     return false;
 }
 
+// The tile a CTA works on in iteration `iter` of its tile loop. A static launch (no queue)
+// has one CTA per tile: its own, once. A persistent launch takes the next ticket of the
+// device work queue (tiles in table order, so the table lists the longest tiles first);
+// a ticket past the table's end ends the loop. `sTicket` is a shared word; the caller
+// takes a barrier between two calls.
+__device__ __forceinline__ int nextTile(unsigned* queue, int iter, int* sTicket)
+{
+    if (!queue)
+        return iter == 0 ? (int)blockIdx.x : 0x7fffffff;
+    if (threadIdx.x == 0)
+        *sTicket = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    return *sTicket;
+}
+
 __device__ __forceinline__ float warp_min(float v)
 {
 #pragma unroll

@@ -19,7 +19,17 @@ struct LaunchArgs
     const PrIn* prIn = nullptr;
     const Tile* tiles = nullptr;
     int nTiles = 0;
+    // Persistent launch: `grid` CTAs take tiles from the device work queue `queue` (a
+    // ticket counter, zero when the launch starts) until the table is exhausted. With no
+    // queue, one CTA per tile.
+    unsigned* queue = nullptr;
+    int grid = 0;
 };
+
+inline int launchGrid(const LaunchArgs& a)
+{
+    return a.queue ? (a.grid < a.nTiles ? a.grid : a.nTiles) : a.nTiles;
+}
 
 // Samples per verification CTA (one thread each). The CTA's warps step through the
 // horizon together (a barrier per step), so the warps sharing an SM sub-partition fetch
@@ -39,6 +49,8 @@ cudaError_t launchShardMin(const LaunchArgs& a, int nth, float* mins);
 cudaError_t launchShardSums(const LaunchArgs& a, int nth, const float* mins, float* sums);
 cudaError_t launchShardApply(cudaStream_t stream, const MppiDev* insts, int nInst, int nth, const float* mins, const float* sums);
 cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem, int* dbgFailTime, int* dbgTheta);
+// CTAs per SM of the persistent rollout (verify = false) or verification kernel
+int mppiResident(int nopp, int nth, bool verify, bool spl, size_t smem);
 cudaError_t launchMppiNoise(const LaunchArgs& a, size_t n, float* out);
 
 bool gateSupported(int nth);

@@ -159,46 +159,13 @@ __host__ __device__ inline RolloutSmem rolloutLayout(int nbp, int T, int M, bool
     return L;
 }
 
+// One rollout tile: SPB samples x NTH hypotheses, a thread each, with the tile's
+// instance already staged in shared memory; then the tile's aggregation.
 template <int NOPP, int NTH, bool SPL>
-__global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles)
+__device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, const Tile& tile, int K, int T, int M, const EnvParams& E, const float* sGrid,
+                                            const float* sKn, const float* sB, float* vbuf, float* red)
 {
     constexpr int NA = NOPP + 1;
-    constexpr int NBP = NTH + 1;
-    constexpr int SPB = RB / NTH; // samples per block
-    extern __shared__ __align__(128) unsigned char smraw[];
-    const Tile tile = tiles[blockIdx.x];
-    const MppiDev& D = insts[tile.inst];
-    const MppiIn& I = in[tile.inst];
-    const int K = D.cfg.K, T = D.cfg.T, M = D.cfg.M;
-    const RolloutSmem L = rolloutLayout(NBP, T, M, SPL);
-    uint64_t* bar = (uint64_t*)smraw;
-    EnvParams* sE = (EnvParams*)(smraw + L.env);
-    float* sGrid = (float*)(smraw + L.grids);
-    float* sKn = (float*)(smraw + L.knots);
-    float* sB = (float*)(smraw + L.B);
-    float* vbuf = (float*)(smraw + L.vbuf);
-    float* red = (float*)(smraw + L.red);
-
-    const uint32_t knBytes = (uint32_t)align16((size_t)NBP * M * 2 * 4);
-    const uint32_t bBytes = SPL ? (uint32_t)align16((size_t)T * M * 4) : 0u;
-    if (threadIdx.x == 0)
-    {
-        mbar_init(bar, 1);
-        mbar_expect_tx(bar, GRID_FLOATS * 4 + knBytes + bBytes);
-        bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
-        bulk_g2s(sKn, D.knots, knBytes, bar);
-        if (SPL)
-            bulk_g2s(sB, D.B, bBytes, bar);
-    }
-    copyEnv(sE, &D.env);
-    __syncthreads();
-    if (!__syncthreads_and(mbar_wait(bar, 0)))
-    {
-        if (threadIdx.x == 0)
-            atomicAdd(&D.stats[1], 1);
-        return;
-    }
-    const EnvParams& E = *sE;
     const Track tr = trackIn(sGrid);
 
     const int th = threadIdx.x % NTH;
@@ -337,6 +304,62 @@ __global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ i
             }
             D.costs[(size_t)(th + 1) * K + s] = (den > 1e-30f) ? (num / den) : INFINITY;
         }
+    }
+}
+
+template <int NOPP, int NTH, bool SPL, bool PQ>
+__global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles, int nTiles,
+                                                   unsigned* __restrict__ queue)
+{
+    constexpr int NBP = NTH + 1;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ int sTicket;
+    uint64_t* bar = (uint64_t*)smraw;
+    if (threadIdx.x == 0)
+        mbar_init(bar, 1);
+    int staged = -1;     // instance whose track, knots and basis are in shared memory
+    uint32_t phase = 0u; // parity of the staging barrier's next phase
+    for (int iter = 0;; iter++)
+    {
+        const int ti = nextTile(PQ ? queue : nullptr, iter, &sTicket);
+        if (ti >= nTiles)
+            break;
+        const Tile tile = tiles[ti];
+        const MppiDev& D = insts[tile.inst];
+        const MppiIn& I = in[tile.inst];
+        const int K = D.cfg.K, T = D.cfg.T, M = D.cfg.M;
+        const RolloutSmem L = rolloutLayout(NBP, T, M, SPL);
+        EnvParams* sE = (EnvParams*)(smraw + L.env);
+        float* sGrid = (float*)(smraw + L.grids);
+        float* sKn = (float*)(smraw + L.knots);
+        float* sB = (float*)(smraw + L.B);
+        float* vbuf = (float*)(smraw + L.vbuf);
+        float* red = (float*)(smraw + L.red);
+        if (tile.inst != staged)
+        {
+            const uint32_t knBytes = (uint32_t)align16((size_t)NBP * M * 2 * 4);
+            const uint32_t bBytes = SPL ? (uint32_t)align16((size_t)T * M * 4) : 0u;
+            if (threadIdx.x == 0)
+            {
+                mbar_expect_tx(bar, GRID_FLOATS * 4 + knBytes + bBytes);
+                bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
+                bulk_g2s(sKn, D.knots, knBytes, bar);
+                if (SPL)
+                    bulk_g2s(sB, D.B, bBytes, bar);
+            }
+            copyEnv(sE, &D.env);
+            __syncthreads();
+            if (!__syncthreads_and(mbar_wait(bar, phase)))
+            {
+                if (threadIdx.x == 0)
+                    atomicAdd(&D.stats[1], 1);
+                return;
+            }
+            phase ^= 1u;
+            staged = tile.inst;
+        }
+        rolloutTile<NOPP, NTH, SPL>(D, I, tile, K, T, M, *sE, sGrid, sKn, sB, vbuf, red);
+        __syncthreads(); // the next tile's staging and reduction buffer reuse shared memory
     }
 }
 
@@ -749,130 +772,150 @@ __global__ void __launch_bounds__(UB) mppi_shard_apply(const MppiDev* __restrict
 // ---------------------------------------------------------------------------------------
 // verification
 // ---------------------------------------------------------------------------------------
-template <int NOPP, int NTH>
+template <int NOPP, int NTH, bool PQ>
 __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) mppi_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
-                                                  int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
+                                                  int nTiles, unsigned* __restrict__ queue, int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
 {
     constexpr int NA = NOPP + 1;
     constexpr int NBP = NTH + 1;
     extern __shared__ __align__(128) unsigned char smraw[];
-    const Tile tile = tiles[blockIdx.x];
-    const MppiDev& D = insts[tile.inst];
-    const MppiIn& I = in[tile.inst];
-    const int T = D.cfg.T, H = D.cfg.H;
-    const int plan = tile.aux;
+    __shared__ int sTicket;
     uint64_t* bar = (uint64_t*)smraw;
     EnvParams* sE = (EnvParams*)(smraw + 16);
     const size_t offG = align16(16 + sizeof(EnvParams));
     float* sGrid = (float*)(smraw + offG);
     float* sPlan = (float*)(smraw + offG + GRID_FLOATS * 4);
-    const uint32_t planBytes = (uint32_t)align16((size_t)NBP * T * 2 * 4);
-    unsigned* hist = (unsigned*)(smraw + offG + GRID_FLOATS * 4 + planBytes);
     if (threadIdx.x == 0)
-    {
         mbar_init(bar, 1);
-        mbar_expect_tx(bar, GRID_FLOATS * 4 + planBytes);
-        bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
-        bulk_g2s(sPlan, plan == 0 ? D.dense : D.prevDense, planBytes, bar);
-    }
-    copyEnv(sE, &D.env);
-    for (int i = threadIdx.x; i < T; i += blockDim.x)
-        hist[i] = 0u;
-    __syncthreads();
-    if (!__syncthreads_and(mbar_wait(bar, 0)))
+    int staged = -1;     // (instance, plan) whose track and plan are in shared memory
+    uint32_t phase = 0u; // parity of the staging barrier's next phase
+    for (int iter = 0;; iter++)
     {
-        if (threadIdx.x == 0)
-            atomicAdd(&D.stats[1], 1);
-        return;
-    }
-    const EnvParams& E = *sE;
-    const Track tr = trackIn(sGrid);
-    const int v = tile.s0 + threadIdx.x;
-    bool active = threadIdx.x < tile.count; // idle lanes of a partial tile still take the barriers
-    {
-        const float minConf = D.cfg.minConf;
-        DState<NA> st;
-#pragma unroll
-        for (int a = 0; a < NA; a++)
+        const int ti = nextTile(PQ ? queue : nullptr, iter, &sTicket);
+        if (ti >= nTiles)
+            break;
+        const Tile tile = tiles[ti];
+        const MppiDev& D = insts[tile.inst];
+        const MppiIn& I = in[tile.inst];
+        const int T = D.cfg.T, H = D.cfg.H;
+        const int plan = tile.aux;
+        const uint32_t planBytes = (uint32_t)align16((size_t)NBP * T * 2 * 4);
+        unsigned* hist = (unsigned*)(smraw + offG + GRID_FLOATS * 4 + planBytes);
+        const int key = tile.inst * 2 + plan;
+        if (key != staged)
         {
-            st.pos[2 * a] = I.state.pos[2 * a];
-            st.pos[2 * a + 1] = I.state.pos[2 * a + 1];
-            st.vel[2 * a] = I.state.vel[2 * a];
-            st.vel[2 * a + 1] = I.state.vel[2 * a + 1];
-            st.S[a] = I.state.S[a];
-            st.lat[a] = I.state.lat_dist[a];
-            st.laps[a] = I.state.laps[a];
-        }
-        st.locate(E.trackLength);
-        BState<NTH> bs;
-#pragma unroll
-        for (int i = 0; i < NTH; i++)
-            bs.belief[i] = I.belief[i];
-        bs.predTheta = findConfident<NTH>(bs.belief, minConf);
-        bs.branchingTime = bs.predTheta == 0 ? -1 : 0;
-        // sampleModelFromBelief (state.h:118-131) on a Philox uniform
-        const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
-        float u = uniform_from_word(draw(k0, k1, (uint32_t)v, (uint32_t)plan, step, S_VERIF_THETA, 0).x);
-        int theta = NTH - 1;
-        {
-            float cdf = 0.0f;
-            bool found = false;
-#pragma unroll
-            for (int kk = 0; kk < NTH; kk++)
+            if (threadIdx.x == 0)
             {
-                cdf += bs.belief[kk];
-                if (!found && u <= cdf)
+                mbar_expect_tx(bar, GRID_FLOATS * 4 + planBytes);
+                bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
+                bulk_g2s(sPlan, plan == 0 ? D.dense : D.prevDense, planBytes, bar);
+            }
+            copyEnv(sE, &D.env);
+        }
+        for (int i = threadIdx.x; i < T; i += blockDim.x)
+            hist[i] = 0u;
+        __syncthreads();
+        if (key != staged)
+        {
+            if (!__syncthreads_and(mbar_wait(bar, phase)))
+            {
+                if (threadIdx.x == 0)
+                    atomicAdd(&D.stats[1], 1);
+                return;
+            }
+            phase ^= 1u;
+            staged = key;
+        }
+        const EnvParams& E = *sE;
+        const Track tr = trackIn(sGrid);
+        const int v = tile.s0 + threadIdx.x;
+        bool active = threadIdx.x < tile.count; // idle lanes of a partial tile still take the barriers
+        {
+            const float minConf = D.cfg.minConf;
+            DState<NA> st;
+#pragma unroll
+            for (int a = 0; a < NA; a++)
+            {
+                st.pos[2 * a] = I.state.pos[2 * a];
+                st.pos[2 * a + 1] = I.state.pos[2 * a + 1];
+                st.vel[2 * a] = I.state.vel[2 * a];
+                st.vel[2 * a + 1] = I.state.vel[2 * a + 1];
+                st.S[a] = I.state.S[a];
+                st.lat[a] = I.state.lat_dist[a];
+                st.laps[a] = I.state.laps[a];
+            }
+            st.locate(E.trackLength);
+            BState<NTH> bs;
+#pragma unroll
+            for (int i = 0; i < NTH; i++)
+                bs.belief[i] = I.belief[i];
+            bs.predTheta = findConfident<NTH>(bs.belief, minConf);
+            bs.branchingTime = bs.predTheta == 0 ? -1 : 0;
+            // sampleModelFromBelief (state.h:118-131) on a Philox uniform
+            const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+            float u = uniform_from_word(draw(k0, k1, (uint32_t)v, (uint32_t)plan, step, S_VERIF_THETA, 0).x);
+            int theta = NTH - 1;
+            {
+                float cdf = 0.0f;
+                bool found = false;
+#pragma unroll
+                for (int kk = 0; kk < NTH; kk++)
                 {
-                    theta = kk;
-                    found = true;
+                    cdf += bs.belief[kk];
+                    if (!found && u <= cdf)
+                    {
+                        theta = kk;
+                        found = true;
+                    }
                 }
             }
-        }
-        EnvNoise rng(k0, k1, (uint32_t)v, (uint32_t)plan << 16, step, S_VERIF_ENV);
-        int tOrigin = 0, t = 0, tEnd = H;
-        bool failed = false;
-        for (; t < H; t++)
-        {
-            // every thread of the CTA takes this barrier once per step (H is uniform); it
-            // keeps the warps on the same step and ends the loop once all samples are done
-            if (!__syncthreads_or(active))
-                break;
-            if (!active)
-                continue;
-            rng.begin_step((uint32_t)t);
-            int local = t - tOrigin;
-            int b = bs.predTheta;
-            float e0 = sPlan[(b * T + local) * 2], e1 = sPlan[(b * T + local) * 2 + 1];
-            bool branched = false;
-            StepOut o = envStep<NOPP, NTH, true, true, false, true>(t, theta, tr, E, e0, e1, st, bs, branched, minConf, rng);
-            if (branched)
-                tOrigin = t + 1;
-            if (o.term == TERM_LOSE)
+            EnvNoise rng(k0, k1, (uint32_t)v, (uint32_t)plan << 16, step, S_VERIF_ENV);
+            int tOrigin = 0, t = 0, tEnd = H;
+            bool failed = false;
+            for (; t < H; t++)
             {
-                failed = true;
-                active = false;
-                tEnd = t;
+                // every thread of the CTA takes this barrier once per step (H is uniform); it
+                // keeps the warps on the same step and ends the loop once all samples are done
+                if (!__syncthreads_or(active))
+                    break;
+                if (!active)
+                    continue;
+                rng.begin_step((uint32_t)t);
+                int local = t - tOrigin;
+                int b = bs.predTheta;
+                float e0 = sPlan[(b * T + local) * 2], e1 = sPlan[(b * T + local) * 2 + 1];
+                bool branched = false;
+                StepOut o = envStep<NOPP, NTH, true, true, false, true>(t, theta, tr, E, e0, e1, st, bs, branched, minConf, rng);
+                if (branched)
+                    tOrigin = t + 1;
+                if (o.term == TERM_LOSE)
+                {
+                    failed = true;
+                    active = false;
+                    tEnd = t;
+                }
+                else if (o.term == TERM_WIN || o.term == TERM_OPP_WIN)
+                {
+                    active = false;
+                    tEnd = t;
+                }
             }
-            else if (o.term == TERM_WIN || o.term == TERM_OPP_WIN)
+            if (failed)
+                atomicAdd(&hist[tEnd], 1u);
+            if (threadIdx.x < tile.count)
             {
-                active = false;
-                tEnd = t;
+                if (dbgFailTime)
+                    dbgFailTime[v] = failed ? tEnd : -1;
+                if (dbgTheta)
+                    dbgTheta[v] = theta;
             }
         }
-        if (failed)
-            atomicAdd(&hist[tEnd], 1u);
-        if (threadIdx.x < tile.count)
-        {
-            if (dbgFailTime)
-                dbgFailTime[v] = failed ? tEnd : -1;
-            if (dbgTheta)
-                dbgTheta[v] = theta;
-        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < T; i += blockDim.x)
+            if (hist[i])
+                atomicAdd(&D.fail[plan * T + i], hist[i]);
+        __syncthreads(); // the next tile's staging and histogram reuse shared memory
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < T; i += blockDim.x)
-        if (hist[i])
-            atomicAdd(&D.fail[plan * T + i], hist[i]);
 }
 
 // perturbation of the next step in the reference layout noise[nbp][M][K][2] (test hook)
@@ -904,29 +947,48 @@ size_t mppiVerifySmem(int nth, int T)
     return align16(16 + sizeof(EnvParams)) + GRID_FLOATS * 4 + ((((size_t)(nth + 1) * T * 2 * 4) + 15) & ~(size_t)15) + (size_t)T * 4;
 }
 
+template <int NOPP, int NTH, bool SPL> static cudaError_t launchRolloutS(const LaunchArgs& a, size_t smem)
+{
+    auto k = a.queue ? mppi_rollout<NOPP, NTH, SPL, true> : mppi_rollout<NOPP, NTH, SPL, false>;
+    ensureSmem(k, smem);
+    k<<<launchGrid(a), RB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue);
+    return cudaGetLastError();
+}
+
 template <int NOPP, int NTH> static cudaError_t launchRolloutT(const LaunchArgs& a, bool spl, size_t smem)
 {
-    if (spl)
-    {
-        auto k = mppi_rollout<NOPP, NTH, true>;
-        ensureSmem(k, smem);
-        k<<<a.nTiles, RB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles);
-    }
-    else
-    {
-        auto k = mppi_rollout<NOPP, NTH, false>;
-        ensureSmem(k, smem);
-        k<<<a.nTiles, RB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles);
-    }
-    return cudaGetLastError();
+    return spl ? launchRolloutS<NOPP, NTH, true>(a, smem) : launchRolloutS<NOPP, NTH, false>(a, smem);
 }
 
 template <int NOPP, int NTH> static cudaError_t launchVerifyT(const LaunchArgs& a, size_t smem, int* ft, int* th)
 {
-    auto k = mppi_verify<NOPP, NTH>;
+    auto k = a.queue ? mppi_verify<NOPP, NTH, true> : mppi_verify<NOPP, NTH, false>;
     ensureSmem(k, smem);
-    k<<<a.nTiles, VERIFY_TILE, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, ft, th);
+    k<<<launchGrid(a), VERIFY_TILE, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue, ft, th);
     return cudaGetLastError();
+}
+
+// CTAs of the persistent rollout / verification kernel that fit on one SM at once, for
+// the given dynamic shared memory: the persistent grid is at most this times the SMs.
+template <int NOPP, int NTH> static int residentT(bool verify, bool spl, size_t smem)
+{
+    int n = 0;
+    if (verify)
+    {
+        ensureSmem(mppi_verify<NOPP, NTH, true>, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_verify<NOPP, NTH, true>, VERIFY_TILE, smem);
+    }
+    else if (spl)
+    {
+        ensureSmem(mppi_rollout<NOPP, NTH, true, true>, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_rollout<NOPP, NTH, true, true>, RB, smem);
+    }
+    else
+    {
+        ensureSmem(mppi_rollout<NOPP, NTH, false, true>, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_rollout<NOPP, NTH, false, true>, RB, smem);
+    }
+    return n;
 }
 
 #define DR_DISPATCH(NOPP_, NTH_, CALL)                                                                                                               \
@@ -938,6 +1000,17 @@ template <int NOPP, int NTH> static cudaError_t launchVerifyT(const LaunchArgs& 
     case 1 * 16 + 8: return CALL(1, 8);                                                                                                             \
     case 2 * 16 + 2: return CALL(2, 2);                                                                                                             \
     default: return cudaErrorInvalidValue;                                                                                                           \
+    }
+
+#define DR_DISPATCH_INT(NOPP_, NTH_, CALL)                                                                                                           \
+    switch (NOPP_ * 16 + NTH_)                                                                                                                       \
+    {                                                                                                                                                \
+    case 1 * 16 + 1: return CALL(1, 1);                                                                                                             \
+    case 1 * 16 + 2: return CALL(1, 2);                                                                                                             \
+    case 1 * 16 + 4: return CALL(1, 4);                                                                                                             \
+    case 1 * 16 + 8: return CALL(1, 8);                                                                                                             \
+    case 2 * 16 + 2: return CALL(2, 2);                                                                                                             \
+    default: return 0;                                                                                                                               \
     }
 
 bool mppiSupported(int nopp, int nth)
@@ -1017,6 +1090,13 @@ cudaError_t launchMppiAggregate(const LaunchArgs& a, int nth, int K)
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+int mppiResident(int nopp, int nth, bool verify, bool spl, size_t smem)
+{
+#define CALL(P, Q) residentT<P, Q>(verify, spl, smem)
+    DR_DISPATCH_INT(nopp, nth, CALL)
+#undef CALL
 }
 
 cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem, int* dbgFailTime, int* dbgTheta)

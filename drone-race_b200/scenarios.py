@@ -239,14 +239,24 @@ def ellipse_race(seed: int = 0, K: int = 1024, T: int = 50, use_splines: bool = 
     return sc
 
 
+_CIRCLE_GRIDS: dict[tuple[int, int], TrackGrids] = {}
+
+
+def _circle_grids(seed: int, n_points: int) -> TrackGrids:
+    key = (seed, n_points)
+    if key not in _CIRCLE_GRIDS:
+        _CIRCLE_GRIDS[key] = track_grids(catmull_rom_closed(jittered_circle_points(seed, n_points)))
+    return _CIRCLE_GRIDS[key]
+
+
 def circle_race(agent: int = 0, seed: int = 0, K: int = 4096, T: int = 64, use_splines: bool = False, n_theta: int = 2, n_verif: int = 2**17,
-                sampling_noise: float = 1.0) -> Scenario:
+                sampling_noise: float = 1.0, n_points: int = 12) -> Scenario:
     """Per-agent MPPI workload of the 4-agent benchmark: a closed Catmull-Rom track
-    through 12 control points jittered +-5 m around a 40 m circle (seeded), drone
-    radius 0.5, collision (outside) weight 1e3, lambda = 1. Agents start at different
-    places along the same track."""
+    through n_points (12) control points jittered +-5 m around a 40 m circle (seeded),
+    drone radius 0.5, collision (outside) weight 1e3, lambda = 1. Agents start at
+    different places along the same track."""
     r = 0.5
-    grids = track_grids(catmull_rom_closed(jittered_circle_points(seed, 12)))
+    grids = _circle_grids(seed, n_points)
     base = [opp_preset(r, s1="insensitive", s3="default"), opp_preset(r, s1="insensitive", s3="no-block"),
             opp_preset(r, s1="default", s3="default"), opp_preset(r, s1="conservative", s3="no-block")]
     presets = [base[i % 4] for i in range(n_theta)]
@@ -257,6 +267,27 @@ def circle_race(agent: int = 0, seed: int = 0, K: int = 4096, T: int = 64, use_s
     sc.mppi = make_mppi(K=K, T=T, use_splines=use_splines, M=20, inv_temperature=1.0, sampling_noise=sampling_noise, n_verif_samples=n_verif,
                         verif_horizon=min(40, T), outside_cost=1e3)
     return sc
+
+
+def uneven_races(n_races: int = 256, seed: int = 0, n_verif: int = 4096) -> list[Scenario]:
+    """Many independent races of uneven sizes, one scenario per agent: per race U{1..8}
+    agents on a track through U{6..16} control points jittered around a 40 m circle, and
+    one control mode (dense or spline controls, alternating by race); per agent K
+    log-uniform in [256, 16384] and H in {32, 48, 64, 96}, verification of n_verif
+    samples over min(40, H) steps. `Scenario.name` is "race<r>/agent<a>"."""
+    rng = np.random.default_rng(50_000 + seed)
+    out = []
+    for race in range(n_races):
+        n_agents = int(rng.integers(1, 9))
+        n_points = int(rng.integers(6, 17))
+        spl = bool(race % 2)
+        for a in range(n_agents):
+            K = int(round(float(np.exp(rng.uniform(np.log(256), np.log(16384))))))
+            T = int(rng.choice([32, 48, 64, 96]))
+            sc = circle_race(agent=a, seed=seed * 100_000 + race, K=K, T=T, use_splines=spl, n_verif=n_verif, n_points=n_points)
+            sc.name = f"race{race}/agent{a}"
+            out.append(sc)
+    return out
 
 
 def robust_race(agent: int = 0, seed: int = 0, K: int = 2048, T: int = 64, P: int = 8, n_theta: int = 8) -> Scenario:
