@@ -390,6 +390,12 @@ def run_ours(args) -> None:
     for _ in range(args.warmup):
         dev_step()
     torch.cuda.synchronize()
+    # launch shapes (grid, lockstep, checkpoint stride) chosen by the library's autotuner on
+    # this batch, before the timed region
+    tune = batch.autotune(10)
+    for _ in range(args.warmup):
+        dev_step()
+    torch.cuda.synchronize()
     batch.set_profiling(True)
     _barrier(world)
     torch.cuda.synchronize()
@@ -496,6 +502,9 @@ def run_ours(args) -> None:
         "e2e": None if args.quick else {"value": world * args.steps / e2e_s, "unit": "control steps/s", "h2d_bytes_per_step": h2d,
                                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s / args.steps * 1e3},
         "gpu_launches": len(kt) * args.steps,
+        "autotune": {"rollout_ctas_per_sm": tune["rollout_ctas_per_sm"], "rollout_lockstep": tune["rollout_lockstep"],
+                     "verify_ctas_per_sm": tune["verify_ctas_per_sm"], "grad_ckpt": tune["grad_ckpt"],
+                     "rollout_ms": {f"{c}x{l}": v for (c, l), v in tune["rollout"].items()}, "verify_ms": tune["verify"], "grad_ms": tune["grad"]},
         "roofline": roof,
         "roofline_step": roof_step,
         "cpu_baseline": cpu,
@@ -798,7 +807,7 @@ def run_ours_races(args) -> None:
         return _max_over_ranks(e0.elapsed_time(e1), world)
 
     shapes = {}
-    for name, shape in (("one_cta_per_tile", (0, 0)), ("persistent_queue", (-1, -1))):
+    for name, shape in (("one_cta_per_tile", (0, 0, 0)), ("persistent_queue", (-1, -1, 0)), ("one_cta_per_tile_lockstep", (0, 0, 1))):
         for r in runs:
             r["batch"].set_persistent(*shape)
         shapes[name] = {"ms_per_step": timed(args.steps) / args.steps}
@@ -807,8 +816,9 @@ def run_ours_races(args) -> None:
     clocks.start()
     ms = timed(args.steps)
     clk = clocks.stop()
-    shapes["autotuned"] = {"ms_per_step": ms / args.steps, "choices": [{k: t[k] for k in ("rollout_ctas_per_sm", "verify_ctas_per_sm")} for t in tune],
-                           "candidates_ms": [{"rollout": t["rollout"], "verify": t["verify"]} for t in tune]}
+    shapes["autotuned"] = {"ms_per_step": ms / args.steps,
+                           "choices": [{k: t[k] for k in ("rollout_ctas_per_sm", "rollout_lockstep", "verify_ctas_per_sm")} for t in tune],
+                           "candidates_ms": [{"rollout": {f"{c}x{l}": v for (c, l), v in t["rollout"].items()}, "verify": t["verify"]} for t in tune]}
     for v in shapes.values():
         v["agent_control_steps_per_s"] = world * n_agents / (v["ms_per_step"] / 1e3)
     ms_per_step = ms / args.steps

@@ -228,18 +228,20 @@ class dr_gate_state(C.Structure):
     ]
 
 
-DR_TUNE_MAX_CANDIDATES = 8
+DR_TUNE_MAX_CANDIDATES = 12
 
 
 class dr_tune_report(C.Structure):
     _fields_ = [
         ("rollout_ctas_per_sm", C.c_int),
+        ("rollout_lockstep", C.c_int),
         ("verify_ctas_per_sm", C.c_int),
         ("grad_ckpt", C.c_int),
         ("n_rollout", C.c_int),
         ("n_verify", C.c_int),
         ("n_grad", C.c_int),
         ("rollout_cand", C.c_int * DR_TUNE_MAX_CANDIDATES),
+        ("rollout_lock", C.c_int * DR_TUNE_MAX_CANDIDATES),
         ("rollout_ms", C.c_float * DR_TUNE_MAX_CANDIDATES),
         ("verify_cand", C.c_int * DR_TUNE_MAX_CANDIDATES),
         ("verify_ms", C.c_float * DR_TUNE_MAX_CANDIDATES),
@@ -299,7 +301,7 @@ _PROTOS = {
     "dr_mppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_batch_set_overlap": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_batch_set_priority": (C.c_int, [C.c_void_p, C.c_int]),
-    "dr_mppi_batch_set_persistent": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dr_mppi_batch_set_persistent": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "dr_mppi_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dr_mppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "dr_prmppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),

@@ -302,11 +302,12 @@ class MPPIBatch:
     def set_priority(self, on: bool) -> None:
         check(lib().dr_mppi_batch_set_priority(self._b, int(on)), "dr_mppi_batch_set_priority")
 
-    def set_persistent(self, rollout_ctas_per_sm: int, verify_ctas_per_sm: int) -> None:
+    def set_persistent(self, rollout_ctas_per_sm: int, verify_ctas_per_sm: int, rollout_lockstep: bool = False) -> None:
         """Launch shape of the rollout and the verification: 0 = one CTA per tile, n > 0 =
         a persistent launch of n CTAs per SM fed by a device work queue, -1 = as many as
-        fit (dr_mppi_batch_set_persistent)."""
-        check(lib().dr_mppi_batch_set_persistent(self._b, int(rollout_ctas_per_sm), int(verify_ctas_per_sm)), "dr_mppi_batch_set_persistent")
+        fit; rollout_lockstep = a barrier per step in the rollout (dr_mppi_batch_set_persistent)."""
+        check(lib().dr_mppi_batch_set_persistent(self._b, int(rollout_ctas_per_sm), int(verify_ctas_per_sm), int(rollout_lockstep)),
+              "dr_mppi_batch_set_persistent")
 
     def autotune(self, reps: int = 5) -> dict:
         """Times the batch's launch-shape candidates on its current inputs and keeps the
@@ -315,9 +316,10 @@ class MPPIBatch:
         check(lib().dr_mppi_batch_autotune(self._b, int(reps), C.byref(r)), "dr_mppi_batch_autotune")
         return {
             "rollout_ctas_per_sm": r.rollout_ctas_per_sm,
+            "rollout_lockstep": r.rollout_lockstep,
             "verify_ctas_per_sm": r.verify_ctas_per_sm,
             "grad_ckpt": r.grad_ckpt,
-            "rollout": {int(r.rollout_cand[i]): float(r.rollout_ms[i]) for i in range(r.n_rollout)},
+            "rollout": {(int(r.rollout_cand[i]), int(r.rollout_lock[i])): float(r.rollout_ms[i]) for i in range(r.n_rollout)},
             "verify": {int(r.verify_cand[i]): float(r.verify_ms[i]) for i in range(r.n_verify)},
             "grad": {int(r.grad_cand[i]): float(r.grad_ms[i]) for i in range(r.n_grad)},
         }

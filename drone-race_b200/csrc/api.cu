@@ -268,11 +268,13 @@ struct dr_mppi_batch
     unsigned* dQueue = nullptr;
     int numSms = 0;
     int rollPerSm = 0, verPerSm = 0;
+    int rollLock = 0; // rollout threads of a CTA step through the horizon together
 
-    LaunchArgs qargs(const Tile* tiles, int n, const MppiIn* in, QueueSlot slot, int perSm, cudaStream_t s) const
+    LaunchArgs qargs(const Tile* tiles, int n, const MppiIn* in, QueueSlot slot, int perSm, cudaStream_t s, int lock = -1) const
     {
         LaunchArgs a = args(tiles, n, in);
         a.stream = s;
+        a.lockstep = lock < 0 ? rollLock : lock;
         if (perSm > 0 && envKind == 0 && dQueue)
         {
             a.queue = dQueue + slot;
@@ -328,7 +330,10 @@ struct dr_mppi_batch
                 timerSide.begin();
                 timerSide.mark("verify_old", sideStream);
             }
-            CK(launchQueued(qargs(dVerOld, nVerOld, in, Q_VER_OLD, verPerSm, sideStream), true));
+            // one CTA per tile here whatever the verification shape: the critical path's
+            // CTAs (higher stream priority) are dispatched as these CTAs finish, which a
+            // persistent grid holding every SM until its queue drains would prevent
+            CK(launchQueued(qargs(dVerOld, nVerOld, in, Q_VER_OLD, 0, sideStream), true));
             if (profile)
             {
                 timerSide.mark("end", sideStream);
@@ -1770,11 +1775,11 @@ template <typename F> int timeLaunch(cudaStream_t s, int reps, F launch, float* 
 }
 } // namespace
 
-extern "C" int dr_mppi_batch_set_persistent(dr_mppi_batch* b, int rollout_ctas_per_sm, int verify_ctas_per_sm)
+extern "C" int dr_mppi_batch_set_persistent(dr_mppi_batch* b, int rollout_ctas_per_sm, int verify_ctas_per_sm, int rollout_lockstep)
 {
     if (!b)
         return fail(DR_ERR_INVALID_ARG, "NULL batch");
-    if (b->envKind != 0 && (rollout_ctas_per_sm != 0 || verify_ctas_per_sm != 0))
+    if (b->envKind != 0 && (rollout_ctas_per_sm != 0 || verify_ctas_per_sm != 0 || rollout_lockstep != 0))
         return fail(DR_ERR_UNSUPPORTED, "persistent launches are built for the strategic race");
     CK(cudaSetDevice(b->device));
     int r = 0, v = 0;
@@ -1789,6 +1794,7 @@ extern "C" int dr_mppi_batch_set_persistent(dr_mppi_batch* b, int rollout_ctas_p
     b->dropDevGraph();
     b->rollPerSm = r;
     b->verPerSm = v;
+    b->rollLock = rollout_lockstep != 0;
     return DR_OK;
 }
 
@@ -1805,27 +1811,34 @@ extern "C" int dr_mppi_batch_autotune(dr_mppi_batch* b, int reps, dr_tune_report
     dr_tune_report rep{};
     cudaStream_t s = b->stream;
     const bool persistOk = b->envKind == 0;
-    // rollout grid
+    // rollout grid (one CTA per tile, or the two fullest persistent grids) x lockstep
     {
         std::vector<int> cand{0};
         const int fit = persistOk ? mppiResident(b->nopp, b->nth, false, b->spl, b->rollSmem) : 0;
-        for (int c = 1; c <= fit && (int)cand.size() < DR_TUNE_MAX_CANDIDATES; c++)
-            cand.push_back(c);
+        for (int c : {fit - 1, fit})
+            if (c >= 1 && std::find(cand.begin(), cand.end(), c) == cand.end())
+                cand.push_back(c);
         float best = INFINITY;
-        for (int c : cand)
-        {
-            float ms = 0.0f;
-            int rc = timeLaunch(s, reps, [&] { return b->launchQueued(b->qargs(b->dRoll, b->nRoll, b->dIn, dr_mppi_batch::Q_ROLL, c, s), false); }, &ms);
-            if (rc)
-                return rc;
-            rep.rollout_cand[rep.n_rollout] = c;
-            rep.rollout_ms[rep.n_rollout++] = ms;
-            if (ms < best)
+        for (int lock = 0; lock < 2; lock++)
+            for (int c : cand)
             {
-                best = ms;
-                rep.rollout_ctas_per_sm = c;
+                if (rep.n_rollout >= DR_TUNE_MAX_CANDIDATES)
+                    break;
+                float ms = 0.0f;
+                int rc = timeLaunch(
+                    s, reps, [&] { return b->launchQueued(b->qargs(b->dRoll, b->nRoll, b->dIn, dr_mppi_batch::Q_ROLL, c, s, lock), false); }, &ms);
+                if (rc)
+                    return rc;
+                rep.rollout_cand[rep.n_rollout] = c;
+                rep.rollout_lock[rep.n_rollout] = lock;
+                rep.rollout_ms[rep.n_rollout++] = ms;
+                if (ms < best)
+                {
+                    best = ms;
+                    rep.rollout_ctas_per_sm = c;
+                    rep.rollout_lockstep = lock;
+                }
             }
-        }
     }
     // verification grid (both plans in one launch)
     if (b->verify && b->nVer > 0)
@@ -1920,6 +1933,7 @@ extern "C" int dr_mppi_batch_autotune(dr_mppi_batch* b, int reps, dr_tune_report
     b->dropGraph();
     b->dropDevGraph();
     b->rollPerSm = rep.rollout_ctas_per_sm;
+    b->rollLock = rep.rollout_lockstep;
     b->verPerSm = rep.verify_ctas_per_sm;
     if (out)
         *out = rep;

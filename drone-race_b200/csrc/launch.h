@@ -24,6 +24,8 @@ struct LaunchArgs
     // queue, one CTA per tile.
     unsigned* queue = nullptr;
     int grid = 0;
+    // rollout: 1 = the CTA's threads step through the horizon together (a barrier per step)
+    int lockstep = 0;
 };
 
 inline int launchGrid(const LaunchArgs& a)

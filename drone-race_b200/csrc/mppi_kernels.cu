@@ -163,7 +163,7 @@ __host__ __device__ inline RolloutSmem rolloutLayout(int nbp, int T, int M, bool
 // instance already staged in shared memory; then the tile's aggregation.
 template <int NOPP, int NTH, bool SPL>
 __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, const Tile& tile, int K, int T, int M, const EnvParams& E, const float* sGrid,
-                                            const float* sKn, const float* sB, float* vbuf, float* red)
+                                            const float* sKn, const float* sB, float* vbuf, float* red, bool lock)
 {
     constexpr int NA = NOPP + 1;
     const Track tr = trackIn(sGrid);
@@ -187,7 +187,7 @@ __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, c
 
     float cost = INFINITY;
     int pt = pt0, bt = bt0;
-    if (valid && compatible)
+    bool active = valid && compatible; // idle and incompatible lanes still take the barriers
     {
         DState<NA> st;
 #pragma unroll
@@ -208,14 +208,26 @@ __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, c
             bs.belief[i] = belief0[i];
         bs.predTheta = pt0;
         bs.branchingTime = bt0;
-        cost = 0.0f;
-        bool stop = false;
+        if (active)
+            cost = 0.0f;
         float decay = 1.0f;
         int tOrigin = 0;
         EnvNoise rng(k0, k1, (uint32_t)s, (uint32_t)th << 16, step, S_MPPI_ROLL_ENV);
         int curB = -1;
-        for (int t = 0; t < T && !stop; t++)
+        for (int t = 0; t < T; t++)
         {
+            // lockstep: every thread of the CTA takes this barrier once per step (T is
+            // uniform), keeping the warps on the same step; otherwise a thread leaves
+            // the loop when its rollout ends
+            if (lock)
+            {
+                if (!__syncthreads_or(active))
+                    break;
+            }
+            else if (!active)
+                break;
+            if (!active)
+                continue;
             rng.begin_step((uint32_t)t);
             const int local = t - tOrigin;
             const int b = bs.predTheta;
@@ -257,13 +269,17 @@ __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, c
             StepOut o = envStep<NOPP, NTH, true, true, true, true>(t, th, tr, E, ego0, ego1, st, bs, branched, minConf, rng);
             if (branched)
                 tOrigin = t + 1;
-            stop = (o.term != TERM_NONE);
+            if (o.term != TERM_NONE)
+                active = false;
             cost += stateCost(o, E, D.cfg.w) * decay;
             decay *= DECAY;
         }
-        cost += finalCost<NOPP>(st, E, D.cfg.w.finalAdvWeight, D.cfg.w.finalOppAdvWeight);
-        pt = bs.predTheta;
-        bt = bs.branchingTime;
+        if (valid && compatible)
+        {
+            cost += finalCost<NOPP>(st, E, D.cfg.w.finalAdvWeight, D.cfg.w.finalOppAdvWeight);
+            pt = bs.predTheta;
+            bt = bs.branchingTime;
+        }
     }
     if (valid)
     {
@@ -308,8 +324,8 @@ __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, c
 }
 
 template <int NOPP, int NTH, bool SPL, bool PQ>
-__global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles, int nTiles,
-                                                   unsigned* __restrict__ queue)
+__global__ void __launch_bounds__(RB, 4) mppi_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles, int nTiles,
+                                                   unsigned* __restrict__ queue, int lockstep)
 {
     constexpr int NBP = NTH + 1;
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -358,7 +374,7 @@ __global__ void __launch_bounds__(RB) mppi_rollout(const MppiDev* __restrict__ i
             phase ^= 1u;
             staged = tile.inst;
         }
-        rolloutTile<NOPP, NTH, SPL>(D, I, tile, K, T, M, *sE, sGrid, sKn, sB, vbuf, red);
+        rolloutTile<NOPP, NTH, SPL>(D, I, tile, K, T, M, *sE, sGrid, sKn, sB, vbuf, red, lockstep != 0);
         __syncthreads(); // the next tile's staging and reduction buffer reuse shared memory
     }
 }
@@ -951,7 +967,7 @@ template <int NOPP, int NTH, bool SPL> static cudaError_t launchRolloutS(const L
 {
     auto k = a.queue ? mppi_rollout<NOPP, NTH, SPL, true> : mppi_rollout<NOPP, NTH, SPL, false>;
     ensureSmem(k, smem);
-    k<<<launchGrid(a), RB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue);
+    k<<<launchGrid(a), RB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue, a.lockstep);
     return cudaGetLastError();
 }
 

@@ -281,21 +281,27 @@ int dr_mppi_batch_set_priority(dr_mppi_batch* b, int on);
 /* Launch shape of the rollout and the verification (strategic race batches). 0 (default):
  * one CTA per tile. n > 0: a persistent launch of n CTAs per SM that take tiles from a
  * device work queue until every controller's tiles are done; -1: as many CTAs per SM as
- * fit. The tile tables list the longest tiles first in both shapes; results are the same.
- * A gate-race batch accepts only 0 (DR_ERR_UNSUPPORTED otherwise). No counterpart in the
- * reference, which launches one controller's kernels at a time. */
-int dr_mppi_batch_set_persistent(dr_mppi_batch* b, int rollout_ctas_per_sm, int verify_ctas_per_sm);
-#define DR_TUNE_MAX_CANDIDATES 8
+ * fit. rollout_lockstep 1: the rollout threads of a CTA take a barrier every step (the
+ * verification always does). The tile tables list the longest tiles first in both shapes;
+ * results are the same in every shape. The previous plan's verification, when it runs
+ * beside the rollout (dr_mppi_batch_set_overlap), keeps one CTA per tile so that the
+ * step's critical path gets SMs as its CTAs finish. A gate-race batch accepts only 0, 0, 0
+ * (DR_ERR_UNSUPPORTED otherwise). No counterpart in the reference, which launches one
+ * controller's kernels at a time. */
+int dr_mppi_batch_set_persistent(dr_mppi_batch* b, int rollout_ctas_per_sm, int verify_ctas_per_sm, int rollout_lockstep);
+#define DR_TUNE_MAX_CANDIDATES 12
 /* What dr_mppi_batch_autotune measured and chose. Candidate values: CTAs per SM of a
  * persistent launch (0 = one CTA per tile) for the rollout and the verification; the
  * adjoint's checkpoint stride for the gradient refinement (0 = the default policy). */
 typedef struct dr_tune_report
 {
     int rollout_ctas_per_sm; /* chosen */
+    int rollout_lockstep;    /* chosen */
     int verify_ctas_per_sm;  /* chosen */
     int grad_ckpt;           /* chosen (0 when no controller of the batch refines) */
     int n_rollout, n_verify, n_grad;
     int rollout_cand[DR_TUNE_MAX_CANDIDATES];
+    int rollout_lock[DR_TUNE_MAX_CANDIDATES];
     float rollout_ms[DR_TUNE_MAX_CANDIDATES]; /* median device time of one launch */
     int verify_cand[DR_TUNE_MAX_CANDIDATES];
     float verify_ms[DR_TUNE_MAX_CANDIDATES];
@@ -304,7 +310,8 @@ typedef struct dr_tune_report
 } dr_tune_report;
 /* Times the launch-shape candidates of this batch on its current inputs (`reps` timed
  * launches each after one untimed one, CUDA events on the batch stream) and keeps the
- * fastest: rollout and verification grid (one CTA per tile, or 1..max persistent CTAs per
+ * fastest: rollout grid (one CTA per tile, or the fullest persistent grids) with and
+ * without lockstep, verification grid (one CTA per tile, or 1..max persistent CTAs per
  * SM) and, for controllers with gradient refinement, the checkpoint stride (every state
  * kept when it fits, ceil(sqrt T), 2 ceil(sqrt T)). None of the choices changes a result.
  * The timed launches write only per-step scratch (costs, failure histograms, gradient

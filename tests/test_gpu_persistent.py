@@ -72,7 +72,7 @@ def _same(x, y):
 
 
 @pytest.mark.parametrize("spl", [True, False])
-@pytest.mark.parametrize("shape", [(-1, -1), (1, 1), (2, 0), (0, 1)])
+@pytest.mark.parametrize("shape", [(-1, -1, 0), (1, 1, 1), (2, 0, 0), (0, 1, 1), (0, 0, 1)])
 def test_persistent_equals_static_grid(gpu, spl, shape):
     ref, _ = _run(spl, False, None)
     got, _ = _run(spl, False, shape)
@@ -86,10 +86,10 @@ def test_autotune_keeps_results_and_reports(gpu):
     got, rep = _run(True, True, None, tune=True)
     _same(ref, got)
     print("autotune:", rep)
-    assert 0 in rep["rollout"] and len(rep["rollout"]) >= 2
+    assert (0, 0) in rep["rollout"] and (0, 1) in rep["rollout"] and len(rep["rollout"]) >= 4
     assert 0 in rep["verify"] and len(rep["verify"]) >= 2
     assert len(rep["grad"]) >= 2
-    assert rep["rollout_ctas_per_sm"] in rep["rollout"]
+    assert (rep["rollout_ctas_per_sm"], rep["rollout_lockstep"]) in rep["rollout"]
     assert rep["verify_ctas_per_sm"] in rep["verify"]
     assert rep["grad_ckpt"] in rep["grad"]
     assert all(v > 0 for d in ("rollout", "verify", "grad") for v in rep[d].values())
@@ -122,7 +122,7 @@ def test_persistent_device_resident_loop(gpu):
             acts.append(actions.cpu().numpy().copy())
         return np.stack(acts)
 
-    assert np.array_equal(loop(None), loop((-1, -1)))
+    assert np.array_equal(loop(None), loop((-1, -1, 1)))
 
 
 def test_persistent_errors(gpu):
@@ -132,10 +132,10 @@ def test_persistent_errors(gpu):
         batch.autotune(3)  # no step yet
     assert e.value.status == abi.DR_ERR_STATE
     with pytest.raises(abi.DrError):
-        batch.set_persistent(64, 0)  # more CTAs per SM than fit
+        batch.set_persistent(64, 0, 0)  # more CTAs per SM than fit
     g = H.small_gate(False, K=256, T=40)
     gb = drb.controllers.MPPIBatch([drb.controllers.MPPIController(g.env, g.mppi, g.seed)])
-    gb.set_persistent(0, 0)
+    gb.set_persistent(0, 0, 0)
     with pytest.raises(abi.DrError) as e:
-        gb.set_persistent(1, 1)
+        gb.set_persistent(1, 1, 0)
     assert e.value.status == abi.DR_ERR_UNSUPPORTED
