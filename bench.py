@@ -806,16 +806,29 @@ def run_ours_races(args) -> None:
         _barrier(world)
         return _max_over_ranks(e0.elapsed_time(e1), world)
 
-    shapes = {}
-    for name, shape in (("one_cta_per_tile", (0, 0, 0)), ("persistent_queue", (-1, -1, 0)), ("one_cta_per_tile_lockstep", (0, 0, 1))):
-        for r in runs:
-            r["batch"].set_persistent(*shape)
-        shapes[name] = {"ms_per_step": timed(args.steps) / args.steps}
+    # The controllers' plans keep changing from step to step (and with them how long the
+    # rollouts run before they end), so the launch shapes are timed in interleaved rounds
+    # after a longer warm-up, each shape for a third of the steps per round.
+    for _ in range(10):
+        dev_step()
+    torch.cuda.synchronize()
+    fixed = (("one_cta_per_tile", (0, 0, 0)), ("persistent_queue", (-1, -1, 0)), ("one_cta_per_tile_lockstep", (0, 0, 1)))
     tune = [r["batch"].autotune(5) for r in runs]
+    tuned = [(t["rollout_ctas_per_sm"], t["verify_ctas_per_sm"], t["rollout_lockstep"]) for t in tune]
+    per_round = max(1, args.steps // 3)
+    totals = {name: 0.0 for name, _ in fixed}
+    totals["autotuned"] = 0.0
     clocks = Clocks(local)
     clocks.start()
-    ms = timed(args.steps)
+    for _ in range(3):
+        for name, shape in fixed + (("autotuned", None),):
+            for r, tshape in zip(runs, tuned):
+                r["batch"].set_persistent(*(shape if shape is not None else tshape))
+            totals[name] += timed(per_round)
     clk = clocks.stop()
+    n_timed = 3 * per_round
+    shapes = {name: {"ms_per_step": totals[name] / n_timed} for name, _ in fixed}
+    ms = totals["autotuned"] * args.steps / n_timed
     shapes["autotuned"] = {"ms_per_step": ms / args.steps,
                            "choices": [{k: t[k] for k in ("rollout_ctas_per_sm", "rollout_lockstep", "verify_ctas_per_sm")} for t in tune],
                            "candidates_ms": [{"rollout": {f"{c}x{l}": v for (c, l), v in t["rollout"].items()}, "verify": t["verify"]} for t in tune]}
