@@ -70,6 +70,32 @@ def test_gradient_matches_fp64_reference(gpu, spl, seed):
     assert np.median(errs) < 1e-4 and errs.max() < 1e-3, errs
 
 
+@pytest.mark.parametrize("spl", [True, False])
+@pytest.mark.parametrize("seed", [11, 12])
+def test_gradient_matches_torch_fp64_autograd(gpu, spl, seed):
+    """The whole gradient (controls and weights) against the PyTorch FP64 autograd
+    transcription of the objective (oracle/torch_model.py, reverse mode)."""
+    from oracle import torch_model as TM
+
+    sc = H.small_mppi(spl, K=256, T=40)
+    c = sc.mppi
+    ctl = H.mppi_ctl(sc)
+    rng = np.random.default_rng(seed)
+    U = rng.normal(0, 0.7, (sc.n_theta + 1, O.mk(c), 2)).astype(np.float32)
+    belief = np.array(sc.env.init_belief[: sc.n_theta], np.float32)
+    w6 = _weights(c)
+    J, dU, dW = _kernel(ctl, sc, belief, U, w6)
+    B = O.spline_matrix(c) if spl else None
+    J64, gU, gW = TM.nominal_grad(sc.env, c, sc.state, belief, U.astype(np.float64), w6.astype(np.float64), B)
+    assert abs(J[0] - J64) <= 1e-4 * max(1.0, abs(J64)), (J[0], J64)
+    g64 = np.concatenate([gU.ravel(), gW])
+    g32 = np.concatenate([dU[0].ravel(), dW[0]]).astype(np.float64)
+    rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
+    print(f"spl={spl} seed={seed}: |g|={np.linalg.norm(g64):.4g}, |g32 - g64| / |g64| = {rel:.2e}")
+    # FP32 forward and adjoint against the FP64 reverse-mode gradient: 2e-3 of |g|
+    assert rel < 2e-3, rel
+
+
 def test_checkpoint_stride_does_not_change_the_result(gpu):
     sc = H.small_mppi(True, K=256, T=40)
     ctl = H.mppi_ctl(sc)
