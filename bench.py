@@ -63,10 +63,10 @@ GATE_FLOPS_PER_ROLLOUT_STEP = 486.3
 GATE_FLOPS_PER_VERIFY_STEP = 473.4
 
 # --workload grad: gradient-refined MPPI on the strategic race, a quarter of the samples
-# (K = 1024) and 3 projected gradient steps of the noise-free rollout objective after each
+# (K = 1024) and one projected gradient step (--grad-steps) of the noise-free rollout objective after each
 # update (dr_mppi_set_grad_refine), beside plain MPPI at K = 4096 in closed loop.
 K_GRAD = 1024
-GRAD_STEPS = 3
+GRAD_STEPS = 1
 GRAD_STEP_SIZE = 0.05
 # --workload pr: PR-MPPI (the reference's PRMPPIController) on the strategic race with the
 # benchmark's PR configuration per agent: 8 opponent hypotheses (lateral aggressiveness
@@ -978,9 +978,11 @@ def main():
                          "grad: gradient-refined MPPI at K=1024 with a closed-loop comparison against plain MPPI at K=4096; "
                          "pr: PR-MPPI, 4 agents x 8 hypotheses x K=2048; "
                          "races: 256 independent races of uneven K/H in one batch per control mode")
+    ap.add_argument("--grad-steps", type=int, default=GRAD_STEPS, help="grad workload: projected gradient steps after each update")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")
     args = ap.parse_args()
+    globals()["GRAD_STEPS"] = args.grad_steps
     WL["kind"] = args.workload
     if args.warmup < 3:
         args.warmup = 3
