@@ -1740,6 +1740,10 @@ int resolvePerSm(const dr_mppi_batch* b, int req, bool verification, int* out)
     return DR_OK;
 }
 
+// A candidate launch shape replaces the current choice only when it is faster by more
+// than 2 %; the default shape is timed first.
+constexpr float TUNE_MARGIN = 0.98f;
+
 // Median device time of `reps` runs of `launch` on `s` (after one untimed run).
 template <typename F> int timeLaunch(cudaStream_t s, int reps, F launch, float* ms)
 {
@@ -1832,7 +1836,9 @@ extern "C" int dr_mppi_batch_autotune(dr_mppi_batch* b, int reps, dr_tune_report
                 rep.rollout_cand[rep.n_rollout] = c;
                 rep.rollout_lock[rep.n_rollout] = lock;
                 rep.rollout_ms[rep.n_rollout++] = ms;
-                if (ms < best)
+                // the first candidate is the default shape; another replaces it only when
+                // faster by more than the tuner's margin (launch-to-launch spread)
+                if (rep.n_rollout == 1 ? true : ms < best * TUNE_MARGIN)
                 {
                     best = ms;
                     rep.rollout_ctas_per_sm = c;
@@ -1856,7 +1862,7 @@ extern "C" int dr_mppi_batch_autotune(dr_mppi_batch* b, int reps, dr_tune_report
                 return rc;
             rep.verify_cand[rep.n_verify] = c;
             rep.verify_ms[rep.n_verify++] = ms;
-            if (ms < best)
+            if (rep.n_verify == 1 ? true : ms < best * TUNE_MARGIN)
             {
                 best = ms;
                 rep.verify_ctas_per_sm = c;
@@ -1914,7 +1920,7 @@ extern "C" int dr_mppi_batch_autotune(dr_mppi_batch* b, int reps, dr_tune_report
                 break;
             rep.grad_cand[rep.n_grad] = c;
             rep.grad_ms[rep.n_grad++] = ms;
-            if (ms < best)
+            if (rep.n_grad == 1 ? true : ms < best * TUNE_MARGIN)
             {
                 best = ms;
                 rep.grad_ckpt = c;

@@ -313,7 +313,8 @@ typedef struct dr_tune_report
  * fastest: rollout grid (one CTA per tile, or the fullest persistent grids) with and
  * without lockstep, verification grid (one CTA per tile, or 1..max persistent CTAs per
  * SM) and, for controllers with gradient refinement, the checkpoint stride (every state
- * kept when it fits, ceil(sqrt T), 2 ceil(sqrt T)). None of the choices changes a result.
+ * kept when it fits, ceil(sqrt T), 2 ceil(sqrt T)). A candidate replaces the default (timed
+ * first) only when it is more than 2 % faster. None of the choices changes a result.
  * The timed launches write only per-step scratch (costs, failure histograms, gradient
  * statistics), which the next step overwrites; the controllers' plans and state are not
  * touched. Needs one completed step of the batch (DR_ERR_STATE before). `out` may be NULL.
