@@ -226,7 +226,7 @@ def _barrier(world: int):
         dist.barrier()
 
 
-def cpu_baseline_reference(scs, target_s: float = 10.0, max_reps: int = 100000, k_s: int = 4096, v_s: int = 32768) -> dict:
+def cpu_baseline_reference(scs, target_s: float = 10.0, max_reps: int = 100000, k_s: int = 4096, v_s: int = 32768, fp64: bool = True) -> dict:
     """The reference's CPU path (its model functions from oracle/_ref, OpenMP) on a bounded
     sample of one agent's control step, scaled to the 4-agent control step. The sample
     controls agent 0 from its start state with an all-zero plan (the plan only steers the
@@ -272,15 +272,42 @@ def cpu_baseline_reference(scs, target_s: float = 10.0, max_reps: int = 100000, 
         reps += 1
         if e - t0 > target_s or reps >= max_reps:
             break
-    sc.mppi = c
     t_roll /= reps
     t_ver /= reps
     # scale: rollout work ~ samples, verification ~ samples (x2 plans); 4 agents
     step_s = AGENTS * (t_roll * (_K() / k_s) + 2 * t_ver * (V / v_s))
-    return {"value": 1.0 / step_s, "unit": "control_steps/s", "cores": threads, "kind": kind,
-            "sample": f"1 agent: rollout of {k_s} samples x {N_THETA} hypotheses x {H} steps and one verification pass of {v_s} samples x {VERIF_H} steps, "
-                      f"{reps} repetitions ({time.perf_counter() - t0:.1f} s), scaled to 4 agents x K={_K()} and 2 x V={V}",
-            "ms_per_control_step": step_s * 1e3}
+    sample = (f"1 agent: rollout of {k_s} samples x {N_THETA} hypotheses x {H} steps and one verification pass of {v_s} samples x {VERIF_H} steps, "
+              f"{reps} repetitions ({time.perf_counter() - t0:.1f} s), scaled to 4 agents x K={_K()} and 2 x V={V}")
+    if not fp64:
+        sc.mppi = c
+        return {"value": 1.0 / step_s, "unit": "control_steps/s", "cores": threads, "kind": kind, "sample": sample, "ms_per_control_step": step_s * 1e3}
+    # the FP64 transcription of the same model (the oracle port at double precision,
+    # OpenMP over all host threads) on a quarter of the sample, a few seconds
+    f0 = time.perf_counter()
+    f_reps = 0
+    f_roll = f_ver = 0.0
+    c_q = type(c).from_buffer_copy(c_small)
+    c_q.n_samples = k_s // 4
+    c_q.n_verif_samples = v_s // 4
+    sc.mppi = c_q
+    noise_q = O.mppi_noise(sc, 0)
+    while True:
+        a = time.perf_counter()
+        O.mppi_rollout(sc, belief, nominal, noise_q, None, 0, prec=64)
+        b = time.perf_counter()
+        O.mppi_verify(sc, belief, nominal.astype(np.float64), 0, 0, prec=64)
+        e = time.perf_counter()
+        f_roll += b - a
+        f_ver += e - b
+        f_reps += 1
+        if e - f0 > target_s / 3 or f_reps >= max_reps:
+            break
+    sc.mppi = c
+    f_step = AGENTS * (f_roll / f_reps * (_K() / (k_s // 4)) + 2 * f_ver / f_reps * (V / (v_s // 4)))
+    fp64 = {"value": 1.0 / f_step, "unit": "control_steps/s", "cores": threads, "kind": "port (FP64 transcription)",
+            "sample": f"1 agent: rollout of {k_s // 4} samples and one verification pass of {v_s // 4} samples, {f_reps} repetitions, scaled likewise"}
+    return {"value": 1.0 / step_s, "unit": "control_steps/s", "cores": threads, "kind": kind, "sample": sample,
+            "ms_per_control_step": step_s * 1e3, "fp64_transcription": fp64}
 
 
 def _race_cost_step(sc, st) -> float:
@@ -936,7 +963,7 @@ def run_reference(args) -> None:
     steps_ms = []
     base = None
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline_reference(scs, target_s=min(20.0, 120.0 / max(1, args.warmup + args.steps)), max_reps=1)
+        r = cpu_baseline_reference(scs, target_s=min(20.0, 120.0 / max(1, args.warmup + args.steps)), max_reps=1, fp64=False)
         if i >= args.warmup:
             steps_ms.append(r["ms_per_control_step"])
         base = r
