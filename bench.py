@@ -396,6 +396,8 @@ def run_ours(args) -> None:
     batch = ctl_mod.MPPIBatch(ctls, stream=stream.cuda_stream)
     if args.no_overlap:
         batch.set_overlap(False)
+    if args.side_verify is not None:
+        batch.set_side_verify(args.side_verify)
     n = len(ctls)
     states = [s.state for s in scs]
     beliefs = np.stack([s.belief() for s in scs])
@@ -1005,6 +1007,8 @@ def main():
                          "grad: gradient-refined MPPI at K=1024 with a closed-loop comparison against plain MPPI at K=4096; "
                          "pr: PR-MPPI, 4 agents x 8 hypotheses x K=2048; "
                          "races: 256 independent races of uneven K/H in one batch per control mode")
+    ap.add_argument("--side-verify", type=int, default=None,
+                    help="CTAs per SM of the previous plan's verification beside the rollout (0: one per tile; default: the library's)")
     ap.add_argument("--grad-steps", type=int, default=GRAD_STEPS, help="grad workload: projected gradient steps after each update")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")

@@ -309,6 +309,12 @@ class MPPIBatch:
         check(lib().dr_mppi_batch_set_persistent(self._b, int(rollout_ctas_per_sm), int(verify_ctas_per_sm), int(rollout_lockstep)),
               "dr_mppi_batch_set_persistent")
 
+    def set_side_verify(self, ctas_per_sm: int) -> None:
+        """Shape of the previous plan's verification beside the critical path: n > 0 a
+        persistent grid of n CTAs per SM (default 1), 0 one CTA per tile
+        (dr_mppi_batch_set_side_verify)."""
+        check(lib().dr_mppi_batch_set_side_verify(self._b, int(ctas_per_sm)), "dr_mppi_batch_set_side_verify")
+
     def autotune(self, reps: int = 5) -> dict:
         """Times the batch's launch-shape candidates on its current inputs and keeps the
         fastest (dr_mppi_batch_autotune); returns what was measured and chosen."""

@@ -283,12 +283,20 @@ int dr_mppi_batch_set_priority(dr_mppi_batch* b, int on);
  * device work queue until every controller's tiles are done; -1: as many CTAs per SM as
  * fit. rollout_lockstep 1: the rollout threads of a CTA take a barrier every step (the
  * verification always does). The tile tables list the longest tiles first in both shapes;
- * results are the same in every shape. The previous plan's verification, when it runs
- * beside the rollout (dr_mppi_batch_set_overlap), keeps one CTA per tile so that the
- * step's critical path gets SMs as its CTAs finish. A gate-race batch accepts only 0, 0, 0
+ * results are the same in every shape. verify_ctas_per_sm applies to the new plan's
+ * verification (and to both plans when they run in one launch); the previous plan's beside
+ * the rollout has its own shape (dr_mppi_batch_set_side_verify). A gate-race batch accepts
+ * only 0, 0, 0
  * (DR_ERR_UNSUPPORTED otherwise). No counterpart in the reference, which launches one
  * controller's kernels at a time. */
 int dr_mppi_batch_set_persistent(dr_mppi_batch* b, int rollout_ctas_per_sm, int verify_ctas_per_sm, int rollout_lockstep);
+/* Shape of the previous plan's verification when it runs beside the rollout and the update
+ * (dr_mppi_batch_set_overlap 1): 0 (default) one CTA per tile; n > 0 a persistent grid of n
+ * CTAs per SM fed by the device work queue, which leaves room on every SM for the step's
+ * critical path but verifies more slowly; -1 as many as fit. Results are the same.
+ * Strategic race batches (a gate-race batch accepts only 0). No counterpart in the
+ * reference. */
+int dr_mppi_batch_set_side_verify(dr_mppi_batch* b, int ctas_per_sm);
 #define DR_TUNE_MAX_CANDIDATES 12
 /* What dr_mppi_batch_autotune measured and chose. Candidate values: CTAs per SM of a
  * persistent launch (0 = one CTA per tile) for the rollout and the verification; the

@@ -81,6 +81,25 @@ def test_persistent_equals_static_grid(gpu, spl, shape):
     assert any(int(f.sum()) > 0 for step in ref for f in step[2])
 
 
+@pytest.mark.parametrize("side", [0, 1, -1])
+def test_side_verification_shape(gpu, side):
+    """The previous plan's verification beside the rollout as one CTA per tile or as a
+    persistent grid: the same results as the default."""
+    ref, _ = _run(True, False, None)
+    scs, ctls = _controllers(True, False)
+    batch = drb.controllers.MPPIBatch(ctls)
+    batch.set_side_verify(side)
+    beliefs = np.stack([s.belief() for s in scs])
+    got = []
+    for _ in range(3):
+        a = batch.step([s.state for s in scs], beliefs)
+        for c in ctls:
+            c._pull()
+        got.append((a.copy(), [c.h_nominal.copy() for c in ctls], [np.concatenate([c.failCountNew, c.failCountOld]) for c in ctls],
+                    [(c.info.use_new_plan, c.info.nu, c.info.min_cost) for c in ctls]))
+    _same(ref, got)
+
+
 def test_autotune_keeps_results_and_reports(gpu):
     ref, _ = _run(True, True, None)
     got, rep = _run(True, True, None, tune=True)
