@@ -398,6 +398,8 @@ def run_ours(args) -> None:
         batch.set_overlap(False)
     if args.side_verify is not None:
         batch.set_side_verify(args.side_verify)
+    if args.pdl:
+        batch.set_pdl(True)
     n = len(ctls)
     states = [s.state for s in scs]
     beliefs = np.stack([s.belief() for s in scs])
@@ -1009,6 +1011,7 @@ def main():
                          "races: 256 independent races of uneven K/H in one batch per control mode")
     ap.add_argument("--side-verify", type=int, default=None,
                     help="CTAs per SM of the previous plan's verification beside the rollout (0: one per tile; default: the library's)")
+    ap.add_argument("--pdl", action="store_true", help="programmatic dependent launches of the update and the new plan's verification")
     ap.add_argument("--grad-steps", type=int, default=GRAD_STEPS, help="grad workload: projected gradient steps after each update")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")

@@ -304,6 +304,7 @@ _PROTOS = {
     "dr_mppi_batch_set_persistent": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "dr_mppi_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dr_mppi_batch_set_side_verify": (C.c_int, [C.c_void_p, C.c_int]),
+    "dr_mppi_batch_set_pdl": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "dr_prmppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_prmppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),

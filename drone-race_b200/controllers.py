@@ -315,6 +315,11 @@ class MPPIBatch:
         (dr_mppi_batch_set_side_verify)."""
         check(lib().dr_mppi_batch_set_side_verify(self._b, int(ctas_per_sm)), "dr_mppi_batch_set_side_verify")
 
+    def set_pdl(self, on: bool) -> None:
+        """Programmatic dependent launch of the update and the new plan's verification
+        (dr_mppi_batch_set_pdl)."""
+        check(lib().dr_mppi_batch_set_pdl(self._b, int(on)), "dr_mppi_batch_set_pdl")
+
     def autotune(self, reps: int = 5) -> dict:
         """Times the batch's launch-shape candidates on its current inputs and keeps the
         fastest (dr_mppi_batch_autotune); returns what was measured and chosen."""

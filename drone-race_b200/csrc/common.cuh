@@ -73,6 +73,40 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
     return false;
 }
 
+// Programmatic dependent launch (sm_90 and later). A kernel launched with the
+// programmatic-stream-serialization attribute may start while the previous kernel of its
+// stream is still running: pdl_wait() blocks until that kernel has completed and its
+// writes are visible (it returns at once in a kernel launched without the attribute).
+// pdl_trigger() allows the next such kernel to launch once every CTA of this one has
+// executed it (or exited).
+__device__ __forceinline__ void pdl_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+__device__ __forceinline__ void pdl_trigger()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launches `k` with the programmatic-stream-serialization attribute when `pdl` is set,
+// else as a plain launch.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launchMaybePdl(bool pdl, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // The tile a CTA works on in iteration `iter` of its tile loop. A static launch (no queue)
 // has one CTA per tile: its own, once. A persistent launch takes the next ticket of the
 // device work queue (tiles in table order, so the table lists the longest tiles first);

@@ -26,6 +26,9 @@ struct LaunchArgs
     int grid = 0;
     // rollout: 1 = the CTA's threads step through the horizon together (a barrier per step)
     int lockstep = 0;
+    // update / verification: launch as a programmatic dependent of the previous kernel of
+    // the stream (its CTAs take SM slots as they free up and wait in the kernel)
+    int pdl = 0;
 };
 
 inline int launchGrid(const LaunchArgs& a)

@@ -330,6 +330,7 @@ __global__ void __launch_bounds__(RB, 4) mppi_rollout(const MppiDev* __restrict_
     constexpr int NBP = NTH + 1;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ int sTicket;
+    pdl_trigger(); // the update may launch once every rollout CTA has started
     uint64_t* bar = (uint64_t*)smraw;
     if (threadIdx.x == 0)
         mbar_init(bar, 1);
@@ -459,6 +460,8 @@ template <int NTH> __global__ void __launch_bounds__(UB) mppi_update(const MppiD
     __shared__ float sNum0[UB], sNum1[UB], sDen[UB];
     __shared__ float sMin[UB / 32];
     __shared__ int sLast;
+    pdl_wait(); // the rollout's costs and branch records are complete and visible
+    pdl_trigger();
     const Tile tile = tiles[blockIdx.x];
     const MppiDev& D = insts[tile.inst];
     const MppiIn& I = in[tile.inst];
@@ -796,6 +799,7 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
     constexpr int NBP = NTH + 1;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ int sTicket;
+    pdl_wait(); // the plan to verify is complete and visible
     uint64_t* bar = (uint64_t*)smraw;
     EnvParams* sE = (EnvParams*)(smraw + 16);
     const size_t offG = align16(16 + sizeof(EnvParams));
@@ -980,8 +984,7 @@ template <int NOPP, int NTH> static cudaError_t launchVerifyT(const LaunchArgs& 
 {
     auto k = a.queue ? mppi_verify<NOPP, NTH, true> : mppi_verify<NOPP, NTH, false>;
     ensureSmem(k, smem);
-    k<<<launchGrid(a), VERIFY_TILE, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue, ft, th);
-    return cudaGetLastError();
+    return launchMaybePdl(a.pdl != 0, k, dim3(launchGrid(a)), dim3(VERIFY_TILE), smem, a.stream, a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue, ft, th);
 }
 
 // CTAs of the persistent rollout / verification kernel that fit on one SM at once, for
@@ -1051,15 +1054,15 @@ cudaError_t launchMppiRollout(const LaunchArgs& a, int nopp, int nth, bool spl, 
 
 cudaError_t launchMppiUpdate(const LaunchArgs& a, int nth)
 {
+    const bool pdl = a.pdl != 0;
     switch (nth)
     {
-    case 1: mppi_update<1><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles); break;
-    case 2: mppi_update<2><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles); break;
-    case 4: mppi_update<4><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles); break;
-    case 8: mppi_update<8><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles); break;
+    case 1: return launchMaybePdl(pdl, mppi_update<1>, dim3(a.nTiles), dim3(UB), 0, a.stream, a.mppi, a.mppiIn, a.tiles);
+    case 2: return launchMaybePdl(pdl, mppi_update<2>, dim3(a.nTiles), dim3(UB), 0, a.stream, a.mppi, a.mppiIn, a.tiles);
+    case 4: return launchMaybePdl(pdl, mppi_update<4>, dim3(a.nTiles), dim3(UB), 0, a.stream, a.mppi, a.mppiIn, a.tiles);
+    case 8: return launchMaybePdl(pdl, mppi_update<8>, dim3(a.nTiles), dim3(UB), 0, a.stream, a.mppi, a.mppiIn, a.tiles);
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 cudaError_t launchShardMin(const LaunchArgs& a, int nth, float* mins)

@@ -297,6 +297,11 @@ int dr_mppi_batch_set_persistent(dr_mppi_batch* b, int rollout_ctas_per_sm, int 
  * Strategic race batches (a gate-race batch accepts only 0). No counterpart in the
  * reference. */
 int dr_mppi_batch_set_side_verify(dr_mppi_batch* b, int ctas_per_sm);
+/* 1: the update and the new plan's verification are launched as programmatic dependents
+ * of the kernel before them (their CTAs are dispatched as SM slots free up and wait in the
+ * kernel for its results); 0 (default): plain launches. Results are the same. No
+ * counterpart in the reference. */
+int dr_mppi_batch_set_pdl(dr_mppi_batch* b, int on);
 #define DR_TUNE_MAX_CANDIDATES 12
 /* What dr_mppi_batch_autotune measured and chose. Candidate values: CTAs per SM of a
  * persistent launch (0 = one CTA per tile) for the rollout and the verification; the

@@ -81,14 +81,15 @@ def test_persistent_equals_static_grid(gpu, spl, shape):
     assert any(int(f.sum()) > 0 for step in ref for f in step[2])
 
 
-@pytest.mark.parametrize("side", [0, 1, -1])
-def test_side_verification_shape(gpu, side):
+@pytest.mark.parametrize("side,pdl", [(0, True), (1, False), (-1, True)])
+def test_side_verification_shape(gpu, side, pdl):
     """The previous plan's verification beside the rollout as one CTA per tile or as a
     persistent grid: the same results as the default."""
     ref, _ = _run(True, False, None)
     scs, ctls = _controllers(True, False)
     batch = drb.controllers.MPPIBatch(ctls)
     batch.set_side_verify(side)
+    batch.set_pdl(pdl)
     beliefs = np.stack([s.belief() for s in scs])
     got = []
     for _ in range(3):
