@@ -305,6 +305,10 @@ _PROTOS = {
     "dr_mppi_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "dr_mppi_batch_set_side_verify": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_batch_set_pdl": (C.c_int, [C.c_void_p, C.c_int]),
+    "dr_prmppi_set_shard": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dr_prmppi_shard_begin": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dr_prmppi_shard_sums": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dr_prmppi_shard_finish": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dr_mppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "dr_prmppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_prmppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),

@@ -271,6 +271,41 @@ class ShardedMPPIController(MPPIController):
         return out
 
 
+class ShardedPRMPPIController(PRMPPIController):
+    """One PR-MPPI controller whose samples are split across the processes of a
+    torch.distributed group: this process rolls out its share of the samples under every
+    hypothesis, and the three minima and the weighted sums are combined with two
+    all-reduces per step (dr_prmppi_set_shard / dr_prmppi_shard_*); the candidates'
+    re-check runs on every process."""
+
+    def __init__(self, env, cfg: abi.dr_prmppi_config, seed: int, rank: int, world: int, group=None, nominal: np.ndarray | None = None,
+                 device: int = 0):
+        import torch
+
+        super().__init__(env, cfg, seed, nominal=nominal, device=device)
+        check(lib().dr_prmppi_set_shard(self._h, int(rank), int(world)), "dr_prmppi_set_shard")
+        self.group = group
+        dev = torch.device("cuda", device)
+        self._mins = torch.empty(3, dtype=torch.float32, device=dev)
+        self._sums = torch.empty(3 * self.T * 3, dtype=torch.float32, device=dev)
+
+    _all_reduce = ShardedMPPIController._all_reduce
+
+    def getControl(self, state) -> np.ndarray:  # noqa: N802
+        import torch.distributed as dist
+
+        if self.engine is None:
+            raise RuntimeError("PRMPPI: engine not set")
+        P = lambda t: C.c_void_p(t.data_ptr())
+        check(lib().dr_prmppi_shard_begin(self._h, C.byref(_state(state)), abi.fptr(self.h_belief), P(self._mins)), "dr_prmppi_shard_begin")
+        self._all_reduce(self._mins, dist.ReduceOp.MIN)
+        check(lib().dr_prmppi_shard_sums(self._h, P(self._mins), P(self._sums)), "dr_prmppi_shard_sums")
+        self._all_reduce(self._sums, dist.ReduceOp.SUM)
+        out = np.zeros(2, np.float32)
+        check(lib().dr_prmppi_shard_finish(self._h, P(self._mins), P(self._sums), abi.fptr(out), C.byref(self.info)), "dr_prmppi_shard_finish")
+        return out
+
+
 class MPPIBatch:
     """Several MPPI controllers (one per agent) advanced by one launch sequence."""
 

@@ -36,6 +36,9 @@ struct dr_prmppi
     float lambda[3] = {1, 1, 1}; // invTempNomFull, invTempRobFull, invTempRobSafe
     uint64_t step = 0;
     dr_prmppi_batch* self = nullptr;
+    // sample sharding across processes (dr_prmppi_set_shard): this process's samples
+    int shardWorld = 1;
+    int sLo = 0, sHi = 0;
 
     PrIn input(const dr_sim_state& s, const float* belief) const
     {
@@ -218,6 +221,40 @@ struct dr_prmppi_batch
         return DR_OK;
     }
 
+    // ---- sample-sharded step of a batch of one (dr_prmppi_shard_*) ----
+    int shardBegin(const PrIn& hin, float* mins)
+    {
+        CK(cudaSetDevice(device));
+        hIn[0] = hin;
+        CK(cudaMemcpyAsync(dIn, hIn, sizeof(PrIn), cudaMemcpyHostToDevice, stream));
+        CK(launchPrPrologue(args(nullptr, 0, dIn), 1));
+        CK(launchPrRollout(args(dRoll, nRoll, dIn), nopp, nth, rollSmem));
+        CK(launchPrShardMin(stream, dDesc, mins));
+        CK(cudaStreamSynchronize(stream));
+        return DR_OK;
+    }
+
+    int shardSums(const float* mins, float* sums)
+    {
+        CK(cudaSetDevice(device));
+        CK(launchPrShardSums(stream, dDesc, dIn, hs[0]->T, mins, sums));
+        CK(cudaStreamSynchronize(stream));
+        return DR_OK;
+    }
+
+    int shardFinish(const float* mins, const float* sums, float* action, dr_prmppi_info* info)
+    {
+        CK(cudaSetDevice(device));
+        CK(launchPrShardApply(stream, dDesc, mins, sums));
+        CK(launchPrCandidates(args(nullptr, 0, dIn), nopp, nth, 1, maxT, 0));
+        int rc = copyResults();
+        if (rc)
+            return rc;
+        CK(cudaStreamSynchronize(stream));
+        hs[0]->finish(action, info);
+        return DR_OK;
+    }
+
     void release()
     {
         if (graphExec)
@@ -263,8 +300,8 @@ int buildPrBatch(dr_prmppi* const* hs, int n, cudaStream_t stream, bool ownStrea
         descs.push_back(h->desc);
         const int spb = prRolloutSamplesPerBlock() / h->P;
         for (int nr = 0; nr < 2; nr++)
-            for (int s0 = 0; s0 < h->K; s0 += spb)
-                roll.push_back(Tile{i, s0, std::min(spb, h->K - s0), nr});
+            for (int s0 = h->sLo; s0 < h->sHi; s0 += spb)
+                roll.push_back(Tile{i, s0, std::min(spb, h->sHi - s0), nr});
         for (int w = 0; w < 3 * h->T; w++)
             wa.push_back(Tile{i, w, 0, 0});
         b->maxT = std::max(b->maxT, h->T);
@@ -355,6 +392,10 @@ int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint
     D.cfg.safetyWeight = cfg->safety_weight;
     D.cfg.k0 = (uint32_t)seed;
     D.cfg.k1 = (uint32_t)(seed >> 32);
+    h->sLo = 0;
+    h->sHi = K;
+    D.cfg.sLo = 0;
+    D.cfg.sHi = K;
 
     float *grids, *costNom, *costRob, *avg, *robWork;
     unsigned* counter;
@@ -441,7 +482,53 @@ int dr_prmppi_step(dr_prmppi* h, const dr_sim_state* state, const float* belief,
 {
     if (!h || !state || !belief || !out_action)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->shardWorld > 1)
+        return fail(DR_ERR_STATE, "a sharded controller steps through dr_prmppi_shard_*");
     return h->self->step(state, belief, h->nth, out_action, info);
+}
+
+int dr_prmppi_set_shard(dr_prmppi* h, int rank, int world)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    if (world < 1 || rank < 0 || rank >= world || world > h->K)
+        return fail(DR_ERR_INVALID_ARG, "need 0 <= rank < world <= n_samples");
+    h->shardWorld = world;
+    h->sLo = (int)((int64_t)h->K * rank / world);
+    h->sHi = (int)((int64_t)h->K * (rank + 1) / world);
+    h->desc.cfg.sLo = h->sLo;
+    h->desc.cfg.sHi = h->sHi;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->self)
+    {
+        h->self->release();
+        delete h->self;
+        h->self = nullptr;
+    }
+    dr_prmppi* raw = h;
+    return buildPrBatch(&raw, 1, h->stream, false, &h->self);
+}
+
+int dr_prmppi_shard_begin(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* mins_dev)
+{
+    if (!h || !state || !belief || !mins_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->shardBegin(h->input(*state, belief), mins_dev);
+}
+
+int dr_prmppi_shard_sums(dr_prmppi* h, const float* mins_dev, float* sums_dev)
+{
+    if (!h || !mins_dev || !sums_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->shardSums(mins_dev, sums_dev);
+}
+
+int dr_prmppi_shard_finish(dr_prmppi* h, const float* mins_dev, const float* sums_dev, float* out_action, dr_prmppi_info* info)
+{
+    if (!h || !mins_dev || !sums_dev || !out_action)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    return h->self->shardFinish(mins_dev, sums_dev, out_action, info);
 }
 
 int dr_prmppi_get_nominals(const dr_prmppi* h, float* nom, float* rob, size_t n)

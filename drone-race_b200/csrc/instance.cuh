@@ -81,6 +81,7 @@ struct PrCfgDev
     float sigma0, sigma1;
     float collDistFactor, boundaryCost, boundaryThresholdFactor, winCost, oppWinCost, finalAdvWeight, finalOppAdvWeight, safetyWeight;
     uint32_t k0, k1;
+    int sLo, sHi; // this process's samples [sLo, sHi) (all of them unless sharded)
 };
 
 struct PrIn

@@ -93,6 +93,11 @@ size_t gradSmem(int nopp, int nth, int T, int M, int ckpt, bool spl);
 int gradDefaultStride(int nopp, int nth, int T, int M, bool spl);
 cudaError_t launchGradNominal(cudaStream_t stream, const GradJob* jobs, int nJobs, int nopp, int nth, bool spl, size_t smem);
 
+// sample-sharded PR-MPPI update phases (one controller's samples split across processes)
+cudaError_t launchPrShardMin(cudaStream_t stream, const PrDev* insts, float* mins);
+cudaError_t launchPrShardSums(cudaStream_t stream, const PrDev* insts, const PrIn* in, int T, const float* mins, float* sums);
+cudaError_t launchPrShardApply(cudaStream_t stream, const PrDev* insts, const float* mins, const float* sums);
+
 // Device tail of the control step and the batch's true-dynamics step (finish_kernels.cu).
 cudaError_t launchMppiFinish(cudaStream_t stream, const MppiDev* insts, MppiIn* in, float* actions, dr_mppi_info* infos, int nInst);
 cudaError_t launchBatchEnvStep(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, const int* trueTheta,

@@ -313,6 +313,143 @@ __global__ void __launch_bounds__(PUB) pr_weighted(const PrDev* __restrict__ ins
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// sample-sharded update of one controller (dr_prmppi_shard_*): this process holds samples
+// [sLo, sHi) of every hypothesis. pr_shard_min: the three minima (nominal + full cost,
+// robust + full cost, robust + safety cost) over its samples, which the caller all-reduces
+// with MIN; pr_shard_sums: its weighted sums of the absolute controls with the global
+// minima (per (which, t): sum w u0, sum w u1, sum w), all-reduced with SUM; pr_shard_apply:
+// the weighted averages from the summed sums, as pr_weighted writes them.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ const float* prArr(const PrDev& D, int which)
+{
+    return D.avg + (size_t)(which == 0 ? 0 : D.cfg.K) * 2 + (which == 2 ? 1 : 0);
+}
+
+__global__ void __launch_bounds__(PUB) pr_shard_min(const PrDev* __restrict__ insts, float* __restrict__ mins)
+{
+    __shared__ float sMin[PUB / 32];
+    const PrDev& D = insts[0];
+    const int which = blockIdx.x, tid = threadIdx.x;
+    const float* arr = prArr(D, which);
+    float mn = INFINITY;
+    for (int s = D.cfg.sLo + tid; s < D.cfg.sHi; s += PUB)
+        mn = fminf(mn, arr[(size_t)s * 2]);
+    mn = warp_min(mn);
+    if ((tid & 31) == 0)
+        sMin[tid >> 5] = mn;
+    __syncthreads();
+    if (tid == 0)
+    {
+        float m = sMin[0];
+#pragma unroll
+        for (int w = 1; w < PUB / 32; w++)
+            m = fminf(m, sMin[w]);
+        mins[which] = m;
+    }
+}
+
+// block per (which, t)
+__global__ void __launch_bounds__(PUB) pr_shard_sums(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, const float* __restrict__ mins,
+                                                     float* __restrict__ sums)
+{
+    __shared__ float sA[PUB], sB[PUB], sC[PUB];
+    const PrDev& D = insts[0];
+    const PrIn& I = in[0];
+    const int T = D.cfg.T;
+    const int which = blockIdx.x / T, t = blockIdx.x % T, tid = threadIdx.x;
+    const float* arr = prArr(D, which);
+    const float* nominal = which == 0 ? D.nom : D.rob;
+    const float minCost = mins[which];
+    const float invTemp = I.lambda[which];
+    const float nom0 = nominal[t * 2], nom1 = nominal[t * 2 + 1];
+    const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+    float num0 = 0.0f, num1 = 0.0f, den = 0.0f;
+    for (int s = D.cfg.sLo + tid; s < D.cfg.sHi; s += PUB)
+    {
+        float cost = arr[(size_t)s * 2];
+        float w = expf(-(cost - minCost) / invTemp);
+        U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)t, step, S_PR_EPS, 0);
+        float u0 = nom0 + scaled_normal(D.cfg.sigma0, r.x);
+        float u1 = nom1 + scaled_normal(D.cfg.sigma1, r.y);
+        num0 += w * u0;
+        num1 += w * u1;
+        den += w;
+    }
+    sA[tid] = num0;
+    sB[tid] = num1;
+    sC[tid] = den;
+    __syncthreads();
+#pragma unroll
+    for (int stride = PUB / 2; stride >= 32; stride >>= 1)
+    {
+        if (tid < stride)
+        {
+            sA[tid] += sA[tid + stride];
+            sB[tid] += sB[tid + stride];
+            sC[tid] += sC[tid + stride];
+        }
+        __syncthreads();
+    }
+    if (tid < 32)
+    {
+        float a0 = sA[tid], a1 = sB[tid], dd = sC[tid];
+#pragma unroll
+        for (int stride = 16; stride > 0; stride >>= 1)
+        {
+            a0 += __shfl_down_sync(0xffffffffu, a0, stride);
+            a1 += __shfl_down_sync(0xffffffffu, a1, stride);
+            dd += __shfl_down_sync(0xffffffffu, dd, stride);
+        }
+        if (tid == 0)
+        {
+            float* o = sums + ((size_t)which * T + t) * 3;
+            o[0] = a0;
+            o[1] = a1;
+            o[2] = dd;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(PUB) pr_shard_apply(const PrDev* __restrict__ insts, const float* __restrict__ mins, const float* __restrict__ sums)
+{
+    const PrDev& D = insts[0];
+    const int T = D.cfg.T;
+    for (int i = threadIdx.x; i < 3 * T; i += blockDim.x)
+    {
+        const int which = i / T, t = i % T;
+        const float* nominal = which == 0 ? D.nom : D.rob;
+        const float* sm = sums + (size_t)i * 3;
+        const float dd = sm[2];
+        float* out = which == 0 ? D.cand1 : (which == 1 ? D.cand2 : D.robWork);
+        out[t * 2] = (dd > 1e-30f) ? sm[0] / dd : nominal[t * 2];
+        out[t * 2 + 1] = (dd > 1e-30f) ? sm[1] / dd : nominal[t * 2 + 1];
+        if (t == 0)
+        {
+            D.nu[which] = dd;
+            D.minCosts[which] = mins[which];
+        }
+    }
+}
+
+cudaError_t launchPrShardMin(cudaStream_t stream, const PrDev* insts, float* mins)
+{
+    pr_shard_min<<<3, PUB, 0, stream>>>(insts, mins);
+    return cudaGetLastError();
+}
+
+cudaError_t launchPrShardSums(cudaStream_t stream, const PrDev* insts, const PrIn* in, int T, const float* mins, float* sums)
+{
+    pr_shard_sums<<<3 * T, PUB, 0, stream>>>(insts, in, mins, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launchPrShardApply(cudaStream_t stream, const PrDev* insts, const float* mins, const float* sums)
+{
+    pr_shard_apply<<<1, PUB, 0, stream>>>(insts, mins, sums);
+    return cudaGetLastError();
+}
+
 // one block per instance: threads (kind, cand, p), kind 0 = full cost, 1 = safety re-check
 template <int NOPP, int NTH>
 __global__ void __launch_bounds__(PRB) pr_candidates(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, int nInst)

@@ -391,6 +391,27 @@ int dr_mppi_shard_sums(dr_mppi* h, const float* mins_dev, float* sums_dev);
 int dr_mppi_shard_update(dr_mppi* h, const float* mins_dev, const float* sums_dev, uint32_t* hist_dev);
 int dr_mppi_shard_finish(dr_mppi* h, const uint32_t* hist_dev, const float* belief, float* out_action, dr_mppi_info* info);
 
+/* Sample sharding of one PR-MPPI controller across processes (the reference's
+ * PRMPPIController::getControl, prmppi_controller.cu:180-346, split at its reductions).
+ * dr_prmppi_set_shard gives process `rank` the samples [rank K / world, (rank+1) K / world)
+ * of every hypothesis (all P hypotheses of a sample stay together, so the per-sample
+ * averaging over hypotheses is local). Per step:
+ *   dr_prmppi_shard_begin   prologue (hypotheses drawn alike on every process), rollout of
+ *                           this process's samples -> mins_dev (3 floats: nominal + full
+ *                           cost, robust + full cost, robust + safety)   caller: MIN
+ *   dr_prmppi_shard_sums    weighted sums with the global minima -> sums_dev (3 x T x 3
+ *                           floats: sum w u0, sum w u1, sum w)           caller: SUM
+ *   dr_prmppi_shard_finish  the weighted averages from the summed sums, the candidates'
+ *                           re-check and choice (replicated on every process) and the
+ *                           host tail -> action, info
+ * Each call returns after its work has completed. Results equal the single-process
+ * step's up to the order of the floating-point sums; info->nonfinite_costs counts this
+ * process's samples. dr_prmppi_step is refused on a sharded controller. */
+int dr_prmppi_set_shard(dr_prmppi* h, int rank, int world);
+int dr_prmppi_shard_begin(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* mins_dev);
+int dr_prmppi_shard_sums(dr_prmppi* h, const float* mins_dev, float* sums_dev);
+int dr_prmppi_shard_finish(dr_prmppi* h, const float* mins_dev, const float* sums_dev, float* out_action, dr_prmppi_info* info);
+
 /* ---- MPPI test hooks (component parity against the reference kernels) ----------- */
 /* Clopper-Pearson bounds (state.h:134-151) of n counts k out of N at level alpha, as the
  * device tail evaluates them (dr_debug_cp) and as the host tail does (dr_debug_cp_host);
