@@ -161,9 +161,9 @@ __host__ __device__ inline RolloutSmem rolloutLayout(int nbp, int T, int M, bool
 
 // One rollout tile: SPB samples x NTH hypotheses, a thread each, with the tile's
 // instance already staged in shared memory; then the tile's aggregation.
-template <int NOPP, int NTH, bool SPL>
+template <int NOPP, int NTH, bool SPL, bool LOCK>
 __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, const Tile& tile, int K, int T, int M, const EnvParams& E, const float* sGrid,
-                                            const float* sKn, const float* sB, float* vbuf, float* red, bool lock)
+                                            const float* sKn, const float* sB, float* vbuf, float* red)
 {
     constexpr int NA = NOPP + 1;
     const Track tr = trackIn(sGrid);
@@ -187,7 +187,8 @@ __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, c
 
     float cost = INFINITY;
     int pt = pt0, bt = bt0;
-    bool active = valid && compatible; // idle and incompatible lanes still take the barriers
+    bool active = valid && compatible; // with LOCK, idle and incompatible lanes still take the barriers
+    if (LOCK || active)
     {
         DState<NA> st;
 #pragma unroll
@@ -216,18 +217,17 @@ __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, c
         int curB = -1;
         for (int t = 0; t < T; t++)
         {
-            // lockstep: every thread of the CTA takes this barrier once per step (T is
-            // uniform), keeping the warps on the same step; otherwise a thread leaves
-            // the loop when its rollout ends
-            if (lock)
+            if constexpr (LOCK)
             {
+                // every thread of the CTA takes this barrier once per step (T is uniform),
+                // keeping the warps on the same step
                 if (!__syncthreads_or(active))
                     break;
+                if (!active)
+                    continue;
             }
             else if (!active)
-                break;
-            if (!active)
-                continue;
+                break; // the thread's rollout ended
             rng.begin_step((uint32_t)t);
             const int local = t - tOrigin;
             const int b = bs.predTheta;
@@ -323,9 +323,9 @@ __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, c
     }
 }
 
-template <int NOPP, int NTH, bool SPL, bool PQ>
-__global__ void __launch_bounds__(RB, 4) mppi_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles, int nTiles,
-                                                   unsigned* __restrict__ queue, int lockstep)
+template <int NOPP, int NTH, bool SPL, bool PQ, bool LOCK>
+__global__ void __launch_bounds__(RB, 4) mppi_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in,
+                                                                       const Tile* __restrict__ tiles, int nTiles, unsigned* __restrict__ queue)
 {
     constexpr int NBP = NTH + 1;
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(RB, 4) mppi_rollout(const MppiDev* __restrict_
             phase ^= 1u;
             staged = tile.inst;
         }
-        rolloutTile<NOPP, NTH, SPL>(D, I, tile, K, T, M, *sE, sGrid, sKn, sB, vbuf, red, lockstep != 0);
+        rolloutTile<NOPP, NTH, SPL, LOCK>(D, I, tile, K, T, M, *sE, sGrid, sKn, sB, vbuf, red);
         __syncthreads(); // the next tile's staging and reduction buffer reuse shared memory
     }
 }
@@ -969,9 +969,10 @@ size_t mppiVerifySmem(int nth, int T)
 
 template <int NOPP, int NTH, bool SPL> static cudaError_t launchRolloutS(const LaunchArgs& a, size_t smem)
 {
-    auto k = a.queue ? mppi_rollout<NOPP, NTH, SPL, true> : mppi_rollout<NOPP, NTH, SPL, false>;
+    auto k = a.queue ? (a.lockstep ? mppi_rollout<NOPP, NTH, SPL, true, true> : mppi_rollout<NOPP, NTH, SPL, true, false>)
+                     : (a.lockstep ? mppi_rollout<NOPP, NTH, SPL, false, true> : mppi_rollout<NOPP, NTH, SPL, false, false>);
     ensureSmem(k, smem);
-    k<<<launchGrid(a), RB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue, a.lockstep);
+    k<<<launchGrid(a), RB, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue);
     return cudaGetLastError();
 }
 
@@ -999,13 +1000,13 @@ template <int NOPP, int NTH> static int residentT(bool verify, bool spl, size_t 
     }
     else if (spl)
     {
-        ensureSmem(mppi_rollout<NOPP, NTH, true, true>, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_rollout<NOPP, NTH, true, true>, RB, smem);
+        ensureSmem(mppi_rollout<NOPP, NTH, true, true, false>, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_rollout<NOPP, NTH, true, true, false>, RB, smem);
     }
     else
     {
-        ensureSmem(mppi_rollout<NOPP, NTH, false, true>, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_rollout<NOPP, NTH, false, true>, RB, smem);
+        ensureSmem(mppi_rollout<NOPP, NTH, false, true, false>, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_rollout<NOPP, NTH, false, true, false>, RB, smem);
     }
     return n;
 }
