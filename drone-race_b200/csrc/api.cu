@@ -61,6 +61,7 @@ struct dr_mppi
     dr_mppi_batch* self = nullptr; // batch of one used by dr_mppi_step
     // gradient refinement after the update (dr_mppi_set_grad_refine)
     int gradSteps = 0, gradCkpt = 1;
+    double cpBeta = 0.0; // beta of the shared Clopper-Pearson table this controller holds
     float gradAlpha = 0.05f;
     // sample sharding across processes (dr_mppi_set_shard): this process's samples and
     // verification samples
@@ -982,6 +983,7 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     A.add(counter, 16);
     double* cpTab;
     A.add(cpTab, sizeof(double) * 3 * CP_TAB);
+
     // result block, one contiguous range
     size_t oFail = 0, oDense = a16(oFail + (size_t)2 * T * 4), oPrev = oDense + a16((size_t)nbp * T * 2 * 4), oNu = oPrev + a16((size_t)nbp * T * 2 * 4),
            oMin = oNu + a16((size_t)nbp * 4), oStats = oMin + a16((size_t)nbp * M * 4), oGrad = oStats + 16,
@@ -997,6 +999,14 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     stats = (int*)(res + oStats);
     D.gstat = (float*)(res + oGrad);
     D.cpTab = cpTab;
+    D.cpFull = nullptr;
+    if (cfg->verify)
+    {
+        // failure counts of CP_TAB and more (plans that fail often) read the shared table
+        h->cpBeta = (double)cfg->beta;
+        if (!acquireCpTable(h->device, (uint32_t)h->V, h->cpBeta, &D.cpFull))
+            return fail(DR_ERR_CUDA, "Clopper-Pearson table: " + std::string(cudaGetErrorString(cudaGetLastError())));
+    }
     D.grids = env ? grids : nullptr;
     D.gate = gp;
     D.gtrack = gtrack;
@@ -1102,6 +1112,8 @@ int dr_mppi_destroy(dr_mppi* h)
     }
     cudaFree(h->dGradIn);
     cudaFree(h->dGradJobs);
+    if (h->desc.cpFull)
+        releaseCpTable(h->device, (uint32_t)h->V, h->cpBeta);
     h->arena.release();
     if (h->hRes)
         cudaFreeHost(h->hRes);

@@ -17,6 +17,10 @@
 //                     environment step of each controller's state under its true hypothesis
 //                     with the action the controller sent, belief update included.
 #include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "common.cuh"
 #include "cp.hpp"
@@ -71,21 +75,30 @@ __global__ void __launch_bounds__(FB) mppi_finish(const MppiDev* __restrict__ in
         __syncthreads();
     }
     // certified loss: max_t upper(new_t) - lower(old_t), starting from -1; counts below
-    // CP_TAB read the host's table (the same function, evaluated once per controller)
+    // CP_TAB read the host's table (the same function, evaluated once per controller),
+    // larger ones the device table shared by the controllers of the same (V, beta)
     const double* tab = D.cpTab;
+    const uint32_t V1 = V > 0 ? V : 1u;
+    auto bound = [&](int which, uint32_t k, uint32_t n, double alpha, bool upper) -> double {
+        if (k < (uint32_t)CP_TAB)
+            return tab[which * CP_TAB + k];
+        if (D.cpFull && k <= V1)
+            return D.cpFull[(size_t)which * (V1 + 1) + k];
+        return upper ? cpdetail::cpUpper(k, n, alpha) : cpdetail::cpLower(k, n, alpha);
+    };
     double d = -1.0;
     if (verify && tid < T)
     {
         const uint32_t kn = cN[tid], ko = cO[tid];
-        const double up = kn < (uint32_t)CP_TAB ? tab[kn] : cpdetail::cpUpper(kn, V, beta / 2.0);
-        const double lo = ko < (uint32_t)CP_TAB ? tab[CP_TAB + ko] : cpdetail::cpLower(ko, V, beta / 2.0);
+        const double up = bound(0, kn, V, beta / 2.0, true);
+        const double lo = bound(1, ko, V, beta / 2.0, false);
         d = fmax(d, up - lo);
     }
     // the two epsilon candidates (new plan kept or previous plan kept)
     if (tid == DR_MAX_T + 32 || tid == DR_MAX_T + 33)
     {
         const uint32_t tot = tid == DR_MAX_T + 32 ? cN[T - 1] : cO[T - 1];
-        sEps[tid - DR_MAX_T - 32] = tot < (uint32_t)CP_TAB ? tab[2 * CP_TAB + tot] : cpdetail::cpUpper(tot, V > 0 ? V : 1u, beta);
+        sEps[tid - DR_MAX_T - 32] = bound(2, tot, V1, beta, true);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
@@ -235,6 +248,101 @@ cudaError_t launchMppiFinish(cudaStream_t stream, const MppiDev* insts, MppiIn* 
 {
     mppi_finish<<<nInst, FB, 0, stream>>>(insts, in, actions, infos, nInst);
     return cudaGetLastError();
+}
+
+// The table of a (V, beta): [0] upper(k, V, beta/2), [1] lower(k, V, beta/2),
+// [2] upper(k, max(V, 1), beta) for k = 0 .. max(V, 1), one thread per entry; counts
+// below CP_TAB are left out (the controllers' own tables hold them).
+__global__ void cp_table_fill(double* __restrict__ out, uint32_t V, double beta)
+{
+    const uint32_t V1 = V > 0 ? V : 1u;
+    const size_t n = (size_t)3 * (V1 + 1);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    {
+        const int which = (int)(i / (V1 + 1));
+        const uint32_t k = (uint32_t)(i % (V1 + 1));
+        double v;
+        if (k < (uint32_t)CP_TAB)
+            v = 0.0;
+        else if (which == 0)
+            v = k <= V && V > 0 ? cpdetail::cpUpper(k, V, beta / 2.0) : 1.0;
+        else if (which == 1)
+            v = k <= V && V > 0 ? cpdetail::cpLower(k, V, beta / 2.0) : 0.0;
+        else
+            v = cpdetail::cpUpper(k, V1, beta);
+        out[i] = v;
+    }
+}
+
+namespace
+{
+struct CpTable
+{
+    double* ptr = nullptr;
+    int refs = 0;
+};
+std::mutex cpMu;
+std::map<std::tuple<int, uint32_t, uint64_t>, CpTable> cpTables;
+
+std::tuple<int, uint32_t, uint64_t> cpKey(int device, uint32_t V, double beta)
+{
+    uint64_t b;
+    std::memcpy(&b, &beta, 8);
+    return {device, V, b};
+}
+} // namespace
+
+bool acquireCpTable(int device, uint32_t V, double beta, const double** out)
+{
+    *out = nullptr;
+    const uint32_t V1 = V > 0 ? V : 1u;
+    if (V1 < (uint32_t)CP_TAB)
+        return true; // every count is in the controllers' own tables
+    std::lock_guard<std::mutex> lock(cpMu);
+    CpTable& t = cpTables[cpKey(device, V, beta)];
+    if (!t.ptr)
+    {
+        const size_t n = (size_t)3 * (V1 + 1);
+        if (cudaMalloc(&t.ptr, n * sizeof(double)) != cudaSuccess)
+        {
+            t.ptr = nullptr;
+            cpTables.erase(cpKey(device, V, beta));
+            return false;
+        }
+        // filled on a stream of its own (non-blocking: no implicit ordering with the
+        // controllers' streams, which may be capturing a graph in another thread)
+        cudaStream_t fs = nullptr;
+        bool ok = cudaStreamCreateWithFlags(&fs, cudaStreamNonBlocking) == cudaSuccess;
+        if (ok)
+        {
+            cp_table_fill<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, fs>>>(t.ptr, V, beta);
+            ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(fs) == cudaSuccess;
+            cudaStreamDestroy(fs);
+        }
+        if (!ok)
+        {
+            cudaFree(t.ptr);
+            cpTables.erase(cpKey(device, V, beta));
+            return false;
+        }
+    }
+    t.refs++;
+    *out = t.ptr;
+    return true;
+}
+
+void releaseCpTable(int device, uint32_t V, double beta)
+{
+    std::lock_guard<std::mutex> lock(cpMu);
+    auto it = cpTables.find(cpKey(device, V, beta));
+    if (it == cpTables.end())
+        return;
+    if (--it->second.refs <= 0)
+    {
+        if (it->second.ptr)
+            cudaFree(it->second.ptr);
+        cpTables.erase(it);
+    }
 }
 
 cudaError_t launchCp(cudaStream_t stream, const uint32_t* k, int n, uint32_t N, double alpha, int upper, double* out)

@@ -70,6 +70,9 @@ struct MppiDev
     // Clopper-Pearson bounds for counts k < CP_TAB, filled on the host at creation:
     // [0] upper(k, V, beta/2), [1] lower(k, V, beta/2), [2] upper(k, max(V, 1), beta)
     const double* cpTab;
+    // the same three bounds for every count, [which][k] for k <= max(V, 1), computed on the
+    // device once per (device, V, beta) and shared by the controllers that have them (or null)
+    const double* cpFull;
     size_t resBytes;
 };
 

@@ -102,6 +102,12 @@ cudaError_t launchPrShardApply(cudaStream_t stream, const PrDev* insts, const fl
 cudaError_t launchMppiFinish(cudaStream_t stream, const MppiDev* insts, MppiIn* in, float* actions, dr_mppi_info* infos, int nInst);
 cudaError_t launchBatchEnvStep(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, const int* trueTheta,
                                const float* actions, dr_sim_state* states, float* beliefs, int updateBelief, uint32_t k0, uint32_t k1, int* terms);
+// Clopper-Pearson bounds of every failure count for verification size V and level beta,
+// on `device` (current), shared by the controllers that acquire the same (V, beta) and
+// freed when the last one releases it. *out is null when V < CP_TAB (the controllers' own
+// tables hold every count); false when the allocation or the fill failed.
+bool acquireCpTable(int device, uint32_t V, double beta, const double** out);
+void releaseCpTable(int device, uint32_t V, double beta);
 cudaError_t launchCp(cudaStream_t stream, const uint32_t* k, int n, uint32_t N, double alpha, int upper, double* out);
 
 // Track grids of nTracks tracks from their 512 samples q [nTracks][512][2] (track_kernels.cu);
