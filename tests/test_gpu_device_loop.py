@@ -77,6 +77,7 @@ def test_device_steps_match_host_steps(gpu, use_splines):
     info_dev = torch.zeros(C.sizeof(abi.dr_mppi_info) * n, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
     used = set()
+    most = 0  # the largest failure count seen (1024 and above read the shared device table)
     for k in range(6):
         a_host = ba.step(states, beliefs)
         bb.step_device(st_dev.data_ptr(), bel_dev.data_ptr(), act_dev.data_ptr(), info_dev.data_ptr())
@@ -86,13 +87,14 @@ def test_device_steps_match_host_steps(gpu, use_splines):
         for i in range(n):
             h, d = ba.infos[i], di[i]
             used.add(h.use_new_plan)
+            most = max(most, int(h.fail_count_total))
             assert (h.use_new_plan, h.branch_idx, h.fail_count_total, h.nonfinite_costs) == (d.use_new_plan, d.branch_idx, d.fail_count_total,
                                                                                             d.nonfinite_costs)
             assert h.inv_temperature == d.inv_temperature and h.min_cost == d.min_cost and h.nu == d.nu
             assert abs(h.epsilon - d.epsilon) <= 1e-9 * abs(h.epsilon)
             assert abs(h.epsilon_partial - d.epsilon_partial) <= 1e-9 * max(abs(h.epsilon_partial), 1e-300)
             assert abs(h.certified_loss - d.certified_loss) <= 1e-9
-    print("plans kept:", sorted(used))
+    print("plans kept:", sorted(used), "largest failure count:", most)
     assert used == {0, 1}  # both outcomes of the certification were exercised
     # a host step after device steps continues from the state the device carried
     a1 = ba.step(states, beliefs)
@@ -101,6 +103,50 @@ def test_device_steps_match_host_steps(gpu, use_splines):
     for c1, c2 in zip(A, B):
         assert np.array_equal(c1.h_nominal, c2.h_nominal)
         assert c1.invTemperature == c2.invTemperature
+
+
+@pytest.mark.parametrize("use_splines", [True, False])
+def test_device_tail_large_failure_counts(gpu, use_splines):
+    """The ego drone starts 8 m off the track, so every verification sample of both plans
+    fails at its first step and the failure counts reach V = 2048: the device tail reads the
+    Clopper-Pearson bounds of those counts from the shared table of large counts and must
+    act exactly as the host tail."""
+    torch = _torch()
+    n = 2
+    scs = [H.small_mppi(use_splines, K=256, T=40, n_verif=2048, seed=21 + a, noise=True) for a in range(n)]
+    states = []
+    for sc in scs:
+        st = abi.dr_sim_state.from_buffer_copy(sc.state)
+        st.pos[0] += 8.0
+        st.pos[1] += 8.0
+        states.append(st)
+    A = [drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed) for sc in scs]
+    B = [drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed) for sc in scs]
+    ba, bb = drb.controllers.MPPIBatch(A), drb.controllers.MPPIBatch(B)
+    beliefs = np.stack([sc.belief() for sc in scs])
+    st_dev = torch.frombuffer(bytearray(bytes((abi.dr_sim_state * n)(*states))), dtype=torch.uint8).cuda()
+    bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+    bel[:, : beliefs.shape[1]] = beliefs
+    bel_dev = torch.from_numpy(bel).cuda()
+    act_dev = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+    info_dev = torch.zeros(C.sizeof(abi.dr_mppi_info) * n, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    most = 0
+    for k in range(3):
+        a_host = ba.step(states, beliefs)
+        bb.step_device(st_dev.data_ptr(), bel_dev.data_ptr(), act_dev.data_ptr(), info_dev.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(a_host, act_dev.cpu().numpy()), k
+        di = _infos(info_dev, n)
+        for i in range(n):
+            h, d = ba.infos[i], di[i]
+            most = max(most, int(h.fail_count_total))
+            assert (h.use_new_plan, h.branch_idx, h.fail_count_total) == (d.use_new_plan, d.branch_idx, d.fail_count_total)
+            assert abs(h.epsilon - d.epsilon) <= 1e-9 * abs(h.epsilon)
+            assert abs(h.epsilon_partial - d.epsilon_partial) <= 1e-9 * max(abs(h.epsilon_partial), 1e-300)
+            assert abs(h.certified_loss - d.certified_loss) <= 1e-9
+    print("largest failure count:", most)
+    assert most >= 1024
 
 
 def test_device_closed_loop_matches_host_loop(gpu):
