@@ -319,6 +319,10 @@ _PROTOS = {
     "dr_prmppi_create": (C.c_int, [C.POINTER(dr_env_config), C.POINTER(dr_prmppi_config), C.c_uint64, C.POINTER(C.c_float), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dr_prmppi_destroy": (C.c_int, [C.c_void_p]),
     "dr_prmppi_step": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_prmppi_info)]),
+    "dr_gate_prmppi_create": (C.c_int, [C.POINTER(dr_gate_env_config), C.POINTER(dr_prmppi_config), C.c_uint64, C.POINTER(C.c_float), C.c_int, C.c_void_p,
+                                        C.POINTER(C.c_void_p)]),
+    "dr_gate_prmppi_step": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_prmppi_info)]),
+    "dr_gate_prmppi_debug_rollout": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "dr_prmppi_get_nominals": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_size_t]),
     "dr_prmppi_get_step": (C.c_uint64, [C.c_void_p]),
     "dr_prmppi_set_step": (C.c_int, [C.c_void_p, C.c_uint64]),

@@ -154,7 +154,9 @@ class PRMPPIController(Controller):
             if nominal.size != self.T * 2:
                 raise ValueError(f"Invalid PRMPPI construction: expected nominal size {self.T * 2}, got {nominal.size}")
             nom = abi.fptr(nominal)
-        check(lib().dr_prmppi_create(C.byref(env), C.byref(cfg), seed, nom, device, C.c_void_p(stream) if stream else None, C.byref(h)), "dr_prmppi_create")
+        self.gate = isinstance(env, abi.dr_gate_env_config)
+        create = lib().dr_gate_prmppi_create if self.gate else lib().dr_prmppi_create
+        check(create(C.byref(env), C.byref(cfg), seed, nom, device, C.c_void_p(stream) if stream else None, C.byref(h)), "dr_prmppi_create")
         self._h = h
         self.info = abi.dr_prmppi_info()
         self.min_nu = float(cfg.min_nu) or 0.0005
@@ -179,7 +181,8 @@ class PRMPPIController(Controller):
         if self.engine is None:
             raise RuntimeError("PRMPPI: engine not set")
         out = np.zeros(2, np.float32)
-        check(lib().dr_prmppi_step(self._h, C.byref(_state(state)), abi.fptr(self.h_belief), abi.fptr(out), C.byref(self.info)), "dr_prmppi_step")
+        step = lib().dr_gate_prmppi_step if self.gate else lib().dr_prmppi_step
+        check(step(self._h, C.byref(_state(state, self.gate)), abi.fptr(self.h_belief), abi.fptr(out), C.byref(self.info)), "dr_prmppi_step")
         return out
 
     def nominals(self) -> tuple[np.ndarray, np.ndarray]:

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <type_traits>
 
 #include <cuda_runtime.h>
 
@@ -39,6 +40,14 @@ struct dr_prmppi
     // sample sharding across processes (dr_prmppi_set_shard): this process's samples
     int shardWorld = 1;
     int sLo = 0, sHi = 0;
+    int envKind = 0, iMppi = 0; // 1: the gate race, with the ego at index iMppi
+
+    PrIn input(const dr_gate_state& s, const float* belief) const
+    {
+        PrIn in = input(dr_sim_state{}, belief);
+        in.gstate = s;
+        return in;
+    }
 
     PrIn input(const dr_sim_state& s, const float* belief) const
     {
@@ -115,6 +124,7 @@ struct dr_prmppi_batch
     cudaStream_t stream = nullptr;
     bool ownStream = false;
     int nopp = 0, nth = 0, maxT = 0, maxP = 0;
+    int envKind = 0, iMppi = 0;
     PrDev* dDesc = nullptr;
     PrIn* dIn = nullptr;
     PrIn* hIn = nullptr;
@@ -150,13 +160,13 @@ struct dr_prmppi_batch
         CK(launchPrPrologue(args(nullptr, 0, in), n));
         if (profile)
             timer->mark("rollout", stream);
-        CK(launchPrRollout(args(dRoll, nRoll, in), nopp, nth, rollSmem));
+        CK(envKind ? launchGatePrRollout(args(dRoll, nRoll, in), nth, iMppi, rollSmem) : launchPrRollout(args(dRoll, nRoll, in), nopp, nth, rollSmem));
         if (profile)
             timer->mark("weighted", stream);
         CK(launchPrReduce(args(dWa, nWa, in)));
         if (profile)
             timer->mark("candidates", stream);
-        CK(launchPrCandidates(args(nullptr, 0, in), nopp, nth, n, maxT, 0));
+        CK(envKind ? launchGatePrCandidates(args(nullptr, 0, in), nth, iMppi, n, maxT) : launchPrCandidates(args(nullptr, 0, in), nopp, nth, n, maxT, 0));
         if (profile)
         {
             timer->mark("end", stream);
@@ -205,7 +215,7 @@ struct dr_prmppi_batch
         return DR_OK;
     }
 
-    int step(const dr_sim_state* states, const float* beliefs, int stride, float* actions, dr_prmppi_info* infos)
+    template <typename St> int step(const St* states, const float* beliefs, int stride, float* actions, dr_prmppi_info* infos)
     {
         const int n = (int)hs.size();
         CK(cudaSetDevice(device));
@@ -286,9 +296,12 @@ int buildPrBatch(dr_prmppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     b->device = hs[0]->device;
     b->nopp = hs[0]->nopp;
     b->nth = hs[0]->nth;
+    b->envKind = hs[0]->envKind;
+    b->iMppi = hs[0]->iMppi;
     for (int i = 0; i < n; i++)
-        if (!hs[i] || hs[i]->device != b->device || hs[i]->nopp != b->nopp || hs[i]->nth != b->nth)
-            return fail(DR_ERR_INVALID_ARG, "a batch needs controllers on one device with equal n_opp and n_theta");
+        if (!hs[i] || hs[i]->device != b->device || hs[i]->nopp != b->nopp || hs[i]->nth != b->nth || hs[i]->envKind != b->envKind ||
+            hs[i]->iMppi != b->iMppi)
+            return fail(DR_ERR_INVALID_ARG, "a batch needs controllers on one device with equal environment kind, ego index, n_opp and n_theta");
     CK(cudaSetDevice(b->device));
     b->stream = stream;
     b->ownStream = ownStream;
@@ -306,7 +319,7 @@ int buildPrBatch(dr_prmppi* const* hs, int n, cudaStream_t stream, bool ownStrea
             wa.push_back(Tile{i, w, 0, 0});
         b->maxT = std::max(b->maxT, h->T);
         b->maxP = std::max(b->maxP, h->P);
-        b->rollSmem = std::max(b->rollSmem, prRolloutSmem(h->T));
+        b->rollSmem = std::max(b->rollSmem, h->envKind ? gatePrRolloutSmem(h->T) : prRolloutSmem(h->T));
     }
     b->nRoll = (int)roll.size();
     b->nWa = (int)wa.size();
@@ -326,13 +339,14 @@ int buildPrBatch(dr_prmppi* const* hs, int n, cudaStream_t stream, bool ownStrea
 
 extern "C" {
 
-int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
-                     dr_prmppi** out)
+// one of env (strategic race) / genv (gate race) is given
+static int prCreate(const dr_env_config* env, const dr_gate_env_config* genv, const dr_prmppi_config* cfg, uint64_t seed, const float* nominal, int device,
+                    void* stream, dr_prmppi** out)
 {
     if (!out)
         return fail(DR_ERR_INVALID_ARG, "out is NULL");
     *out = nullptr;
-    int rc = checkEnv(env);
+    int rc = env ? checkEnv(env) : checkGateEnv(genv);
     if (rc)
         return rc;
     if (!cfg)
@@ -346,15 +360,23 @@ int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint
     for (int i = 0; i < 3; i++)
         if (!(cfg->inv_temperature > 0.0f))
             return fail(DR_ERR_INVALID_ARG, "inv_temperature must be positive");
-    if (!prSupported(env->n_opp, env->n_theta))
+    if (env ? !prSupported(env->n_opp, env->n_theta) : !gateSupported(genv->n_theta))
         return fail(DR_ERR_UNSUPPORTED, "(n_opp, n_theta) combination not compiled in");
     rc = selectDevice(device);
     if (rc)
         return rc;
     auto h = std::make_unique<dr_prmppi>();
     h->device = device;
-    h->env = *env;
-    h->env.p_grid = h->env.dp_grid = h->env.t_grid = h->env.kappa_grid = nullptr;
+    if (env)
+    {
+        h->env = *env;
+        h->env.p_grid = h->env.dp_grid = h->env.t_grid = h->env.kappa_grid = nullptr;
+    }
+    else
+    {
+        h->envKind = 1;
+        h->iMppi = genv->i_mppi;
+    }
     h->cfg = *cfg;
     if (h->cfg.min_nu == 0.0f && h->cfg.max_nu == 0.0f)
     {
@@ -362,8 +384,8 @@ int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint
         h->cfg.max_nu = 0.001f;
     }
     h->seed = seed;
-    h->nth = env->n_theta;
-    h->nopp = env->n_opp;
+    h->nth = env ? env->n_theta : genv->n_theta;
+    h->nopp = env ? env->n_opp : 1;
     h->K = cfg->n_samples;
     h->T = cfg->n_timesteps;
     h->P = cfg->P;
@@ -371,7 +393,9 @@ int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint
         h->lambda[i] = cfg->inv_temperature; // prmppi_controller.cu:39
     const int K = h->K, T = h->T, P = h->P;
     PrDev& D = h->desc;
-    D.env = toEnvParams(*env);
+    if (env)
+        D.env = toEnvParams(*env);
+    D.cfg.gateMargin = cfg->gate_traversal_margin;
     D.cfg.K = K;
     D.cfg.T = T;
     D.cfg.P = P;
@@ -397,10 +421,17 @@ int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint
     D.cfg.sLo = 0;
     D.cfg.sHi = K;
 
-    float *grids, *costNom, *costRob, *avg, *robWork;
+    float *grids = nullptr, *costNom, *costRob, *avg, *robWork, *gtrack = nullptr;
+    GateParams* gp = nullptr;
     unsigned* counter;
     Arena& A = h->arena;
-    A.add(grids, GRID_FLOATS * 4);
+    if (env)
+        A.add(grids, GRID_FLOATS * 4);
+    else
+    {
+        A.add(gp, sizeof(GateParams));
+        A.add(gtrack, GATE_TRACK_FLOATS * 4);
+    }
     A.add(costNom, (size_t)P * K * 2 * 4);
     A.add(costRob, (size_t)P * K * 2 * 4);
     A.add(avg, (size_t)2 * K * 2 * 4);
@@ -413,6 +444,8 @@ int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint
     A.add(res, resBytes);
     CK(A.alloc());
     D.grids = grids;
+    D.gate = gp;
+    D.gtrack = gtrack;
     D.costNom = costNom;
     D.costRob = costRob;
     D.avg = avg;
@@ -431,8 +464,18 @@ int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint
     D.decision = (int*)(res + oDec);
     D.stats = (int*)(res + oStats);
     D.resBytes = resBytes;
-    std::vector<float> g = packGrids(*env);
-    CK(cudaMemcpy(grids, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    if (env)
+    {
+        std::vector<float> g = packGrids(*env);
+        CK(cudaMemcpy(grids, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    }
+    else
+    {
+        GateParams hp = toGateParams(*genv);
+        CK(cudaMemcpy(gp, &hp, sizeof(GateParams), cudaMemcpyHostToDevice));
+        std::vector<float> t = packGateTrack(*genv);
+        CK(cudaMemcpy(gtrack, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+    }
     h->hNom.assign((size_t)T * 2, 0.0f);
     if (nominal)
         std::memcpy(h->hNom.data(), nominal, h->hNom.size() * 4);
@@ -455,6 +498,22 @@ int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint
         return rc;
     *out = h.release();
     return DR_OK;
+}
+
+int dr_prmppi_create(const dr_env_config* env, const dr_prmppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
+                     dr_prmppi** out)
+{
+    if (!env)
+        return fail(DR_ERR_INVALID_ARG, "env is NULL");
+    return prCreate(env, nullptr, cfg, seed, nominal, device, stream, out);
+}
+
+int dr_gate_prmppi_create(const dr_gate_env_config* env, const dr_prmppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
+                          dr_prmppi** out)
+{
+    if (!env)
+        return fail(DR_ERR_INVALID_ARG, "env is NULL");
+    return prCreate(nullptr, env, cfg, seed, nominal, device, stream, out);
 }
 
 int dr_prmppi_destroy(dr_prmppi* h)
@@ -484,6 +543,17 @@ int dr_prmppi_step(dr_prmppi* h, const dr_sim_state* state, const float* belief,
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
     if (h->shardWorld > 1)
         return fail(DR_ERR_STATE, "a sharded controller steps through dr_prmppi_shard_*");
+    if (h->envKind != 0)
+        return fail(DR_ERR_INVALID_ARG, "a gate-race controller steps through dr_gate_prmppi_step");
+    return h->self->step(state, belief, h->nth, out_action, info);
+}
+
+int dr_gate_prmppi_step(dr_prmppi* h, const dr_gate_state* state, const float* belief, float* out_action, dr_prmppi_info* info)
+{
+    if (!h || !state || !belief || !out_action)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->envKind != 1)
+        return fail(DR_ERR_INVALID_ARG, "a strategic-race controller steps through dr_prmppi_step");
     return h->self->step(state, belief, h->nth, out_action, info);
 }
 
@@ -491,6 +561,8 @@ int dr_prmppi_set_shard(dr_prmppi* h, int rank, int world)
 {
     if (!h)
         return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    if (h->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "sample sharding is built for the strategic race");
     if (world < 1 || rank < 0 || rank >= world || world > h->K)
         return fail(DR_ERR_INVALID_ARG, "need 0 <= rank < world <= n_samples");
     h->shardWorld = world;
@@ -672,10 +744,14 @@ int dr_prmppi_debug_noise(dr_prmppi* h, const float* belief, float* noise, size_
     return DR_OK;
 }
 
-int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* cost_nom, float* cost_rob)
+} // extern "C"
+
+template <typename St> static int prDebugRollout(dr_prmppi* h, const St* state, const float* belief, float* cost_nom, float* cost_rob)
 {
     if (!h || !state || !belief)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->envKind != (std::is_same<St, dr_gate_state>::value ? 1 : 0))
+        return fail(DR_ERR_INVALID_ARG, "state type does not match the controller's environment");
     CK(cudaSetDevice(h->device));
     dr_prmppi_batch* b = h->self;
     std::vector<float> nom(h->hNom.size()), rob(h->hRob.size());
@@ -684,7 +760,8 @@ int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float
     b->hIn[0] = h->input(*state, belief);
     CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(PrIn), cudaMemcpyHostToDevice, h->stream));
     CK(launchPrPrologue(b->args(nullptr, 0, b->dIn), 1));
-    CK(launchPrRollout(b->args(b->dRoll, b->nRoll, b->dIn), h->nopp, h->nth, b->rollSmem));
+    CK(h->envKind ? launchGatePrRollout(b->args(b->dRoll, b->nRoll, b->dIn), h->nth, h->iMppi, b->rollSmem)
+                  : launchPrRollout(b->args(b->dRoll, b->nRoll, b->dIn), h->nopp, h->nth, b->rollSmem));
     size_t nb = (size_t)h->P * h->K * 2 * 4;
     if (cost_nom)
         CK(cudaMemcpyAsync(cost_nom, h->desc.costNom, nb, cudaMemcpyDeviceToHost, h->stream));
@@ -695,6 +772,18 @@ int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float
     CK(cudaMemcpy(h->desc.nom, nom.data(), nom.size() * 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->desc.rob, rob.data(), rob.size() * 4, cudaMemcpyHostToDevice));
     return DR_OK;
+}
+
+extern "C" {
+
+int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* cost_nom, float* cost_rob)
+{
+    return prDebugRollout(h, state, belief, cost_nom, cost_rob);
+}
+
+int dr_gate_prmppi_debug_rollout(dr_prmppi* h, const dr_gate_state* state, const float* belief, float* cost_nom, float* cost_rob)
+{
+    return prDebugRollout(h, state, belief, cost_nom, cost_rob);
 }
 
 } // extern "C"

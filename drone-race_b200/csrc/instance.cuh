@@ -85,11 +85,16 @@ struct PrCfgDev
     float collDistFactor, boundaryCost, boundaryThresholdFactor, winCost, oppWinCost, finalAdvWeight, finalOppAdvWeight, safetyWeight;
     uint32_t k0, k1;
     int sLo, sHi; // this process's samples [sLo, sHi) (all of them unless sharded)
+    float gateMargin; // gateTraversalMargin (gate race)
 };
 
 struct PrIn
 {
-    dr_sim_state state;
+    union
+    {
+        dr_sim_state state;   // strategic race
+        dr_gate_state gstate; // gate race
+    };
     float belief[DR_MAX_THETA];
     float lambda[3];
     uint32_t step;
@@ -103,6 +108,8 @@ struct PrDev
     EnvParams env;
     PrCfgDev cfg;
     const float* grids;
+    const GateParams* gate; // gate race: parameters and racelines (GATE_TRACK_FLOATS), else null
+    const float* gtrack;
     float* costNom;   // [P][K][2]
     float* costRob;   // [P][K][2]
     float* avg;       // [2][K][2] per-sample averaged (full, safe) for nom / rob

@@ -93,6 +93,12 @@ size_t gradSmem(int nopp, int nth, int T, int M, int ckpt, bool spl);
 int gradDefaultStride(int nopp, int nth, int T, int M, bool spl);
 cudaError_t launchGradNominal(cudaStream_t stream, const GradJob* jobs, int nJobs, int nopp, int nth, bool spl, size_t smem);
 
+// PR-MPPI on the gate race (gate_pr_kernels.cu); prologue and weighted averages are shared
+size_t gatePrRolloutSmem(int T);
+int gatePrRolloutSamplesPerBlock();
+cudaError_t launchGatePrRollout(const LaunchArgs& a, int nth, int me, size_t smem);
+cudaError_t launchGatePrCandidates(const LaunchArgs& a, int nth, int me, int nInst, int maxT);
+
 // sample-sharded PR-MPPI update phases (one controller's samples split across processes)
 cudaError_t launchPrShardMin(cudaStream_t stream, const PrDev* insts, float* mins);
 cudaError_t launchPrShardSums(cudaStream_t stream, const PrDev* insts, const PrIn* in, int T, const float* mins, float* sums);

@@ -583,6 +583,16 @@ int dr_gate_mppi_create(const dr_gate_env_config* env, const dr_mppi_config* cfg
                         dr_mppi** out);
 /* MPPIController::getControl (src/mppi_controller.cu:250-466) on the gate race. */
 int dr_gate_mppi_step(dr_mppi* h, const dr_gate_state* state, const float* belief, float* out_action, dr_mppi_info* info);
+/* PR-MPPI on the gate race: the reference's PRMPPIController built with USE_ENV_DRONERACE
+ * (its PR-MPPI kernels and cost functions over the gate race's environment,
+ * include/environments/env_dronerace.h). Same configuration, results and info as the
+ * strategic race's; the state is a dr_gate_state and the ego is env->i_mppi.
+ * dr_prmppi_step refuses a gate-race controller and dr_gate_prmppi_step a strategic one. */
+int dr_gate_prmppi_create(const dr_gate_env_config* env, const dr_prmppi_config* cfg, uint64_t seed, const float* nominal, int device, void* stream,
+                          dr_prmppi** out);
+int dr_gate_prmppi_step(dr_prmppi* h, const dr_gate_state* state, const float* belief, float* out_action, dr_prmppi_info* info);
+/* Test hook: as dr_prmppi_debug_rollout, on the gate race. */
+int dr_gate_prmppi_debug_rollout(dr_prmppi* h, const dr_gate_state* state, const float* belief, float* cost_nom, float* cost_rob);
 int dr_gate_mppi_batch_step(dr_mppi_batch* b, const dr_gate_state* states, const float* beliefs, float* out_actions, dr_mppi_info* infos);
 /* Test hooks, as dr_mppi_debug_rollout / dr_mppi_debug_verify (same outputs). */
 int dr_gate_mppi_debug_rollout(dr_mppi* h, const dr_gate_state* state, const float* belief, float* costs_true, int32_t* branch_used,
