@@ -947,6 +947,25 @@ def run_ours_races(args) -> None:
         dist.destroy_process_group()
 
 
+def reference_cpu_step(scs, variant: str, threads: int, noises) -> float:
+    """One control step of the 4-agent workload on the reference's own CPU path (its
+    model functions in host loops, oracle/_ref, OpenMP over `threads`): per agent the
+    full K-sample rollout, the update (aggregation, masked minima, weighted averages,
+    clamp), and the verification of the new and the previous plan over V samples x the
+    verification horizon. Returns the seconds it took."""
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    for sc, noise in zip(scs, noises):
+        belief = sc.belief()
+        prev = np.zeros((N_THETA + 1, H, 2), np.float32)
+        ct, bu, bt = O.mppi_rollout(sc, belief, prev, noise, None, 0, impl=variant, nthreads=threads)
+        _, dense, _, _, _ = O.mppi_update(sc, belief, ct, bu, bt, noise, None, prev, impl=variant, nthreads=threads)
+        O.mppi_verify(sc, belief, dense, 0, 0, impl=variant, nthreads=threads)
+        O.mppi_verify(sc, belief, prev, 0, 1, impl=variant, nthreads=threads)
+    return time.perf_counter() - t0
+
+
 def run_reference(args) -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -963,16 +982,30 @@ def run_reference(args) -> None:
     if WL["kind"] == "pr":
         run_reference_pr(args)
         return
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O
+
+    drb = _package()
+    O.set_abi(drb.abi)
     scs = workload(0)
-    steps_ms = []
-    base = None
+    variant = _ref_variant(O)
+    if not O.ref_available(variant):
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference build oracle/_ref/libref_{variant}.so is missing (make -C oracle ref)"}),
+              flush=True)
+        return
+    threads = os.cpu_count() or 1
+    # the perturbations the reference's generateNoiseKernel would draw, made once before
+    # the timed steps (the CPU path has no noise kernel of its own)
+    noises = [O.mppi_noise(sc, 0) for sc in scs]
+    steps_s = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline_reference(scs, target_s=min(20.0, 120.0 / max(1, args.warmup + args.steps)), max_reps=1, fp64=False)
+        dt = reference_cpu_step(scs, variant, threads, noises)
         if i >= args.warmup:
-            steps_ms.append(r["ms_per_control_step"])
-        base = r
-    ms = statistics.mean(steps_ms)
+            steps_s.append(dt)
+    ms = statistics.mean(steps_s) * 1e3
     value = 1e3 / ms
+    sample = (f"the whole workload every step, no scaling: {AGENTS} agents x (rollout of K={_K()} samples x {N_THETA} hypotheses x {H} steps, "
+              f"update, verification of 2 plans x V={V} samples x {VERIF_H} steps); perturbations precomputed")
     line = {
         "impl": "reference",
         "metric": "control_steps_per_s",
@@ -988,8 +1021,8 @@ def run_reference(args) -> None:
         "dtype": "f32",
         "data": "synthetic (seeded tracks and states; no dataset)",
         "config": {"workload": _workload_name(), "agents": AGENTS, "K": _K(), "H": H, "n_theta": N_THETA, "n_opp": 1, "controls": "dense",
-                   "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": "host threads"},
-        "cpu_baseline": {"value": value, "unit": "control_steps/s", "cores": base["cores"], "kind": base["kind"], "sample": base["sample"]},
+                   "verif_samples": V, "verif_horizon": VERIF_H, "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": "control_steps/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "control steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_cuda": None if args.no_reference_cuda else reference_cuda_timing(scs),
     }

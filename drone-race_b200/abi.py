@@ -316,6 +316,7 @@ _PROTOS = {
     "dr_mppi_debug_rollout": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "dr_mppi_debug_update": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "dr_mppi_debug_verify": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "dr_mppi_debug_stage_timeout": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "dr_prmppi_create": (C.c_int, [C.POINTER(dr_env_config), C.POINTER(dr_prmppi_config), C.c_uint64, C.POINTER(C.c_float), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dr_prmppi_destroy": (C.c_int, [C.c_void_p]),
     "dr_prmppi_step": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_prmppi_info)]),

@@ -99,6 +99,8 @@ struct dr_mppi
     }
 
     // host tail of MPPIController::getControl (mppi_controller.cu:363-456)
+    int lastTimeouts = 0; // staging waits that gave up in the last finished step
+
     void finish(const float* belief, float* outAction, dr_mppi_info* info)
     {
         const unsigned char* r = hRes;
@@ -108,6 +110,7 @@ struct dr_mppi
         const float* nu = (const float*)(r + ((const unsigned char*)desc.nu - (const unsigned char*)desc.fail));
         const float* minCosts = (const float*)(r + ((const unsigned char*)desc.minCosts - (const unsigned char*)desc.fail));
         const int* stats = (const int*)(r + ((const unsigned char*)desc.stats - (const unsigned char*)desc.fail));
+        lastTimeouts = stats[1];
         fcNew.assign(fail, fail + T);
         fcOld.assign(fail + T, fail + 2 * T);
         if (cfg.verify)
@@ -461,9 +464,21 @@ struct dr_mppi_batch
         if (rc)
             return rc;
         CK(cudaStreamSynchronize(stream));
+        int timeouts = 0;
         for (int i = 0; i < n; i++)
+        {
             hs[i]->finish(beliefs + (size_t)i * beliefStride, actions + 2 * i, infos ? infos + i : nullptr);
-        return DR_OK;
+            timeouts += hs[i]->lastTimeouts;
+        }
+        return timeouts ? timedOut(timeouts) : DR_OK;
+    }
+
+    // A step whose kernels gave up a bounded wait has run to its end on defined values
+    // (timed-out rollout tiles cost infinity, timed-out verification tiles count no
+    // failures), but its result is not the control step's: report it.
+    static int timedOut(int n)
+    {
+        return fail(DR_ERR_TIMEOUT, "a bounded device wait gave up in " + std::to_string(n) + " CTA(s); the step's results are not valid");
     }
 
     // ---- sample-sharded step of a batch of one (dr_mppi_shard_*) ----
@@ -511,7 +526,7 @@ struct dr_mppi_batch
             return rc;
         CK(cudaStreamSynchronize(stream));
         hs[0]->finish(belief, action, info);
-        return DR_OK;
+        return hs[0]->lastTimeouts ? timedOut(hs[0]->lastTimeouts) : DR_OK;
     }
 
     void dropDevGraph()
@@ -610,6 +625,17 @@ struct dr_mppi_batch
         graph = nullptr;
     }
 
+    // Copies the controllers' device descriptors (host copies in dr_mppi::desc) to the
+    // batch's descriptor table; the caller has synchronised the stream.
+    int uploadDescs()
+    {
+        std::vector<MppiDev> descs;
+        for (auto* h : hs)
+            descs.push_back(h->desc);
+        CK(cudaMemcpy(dDesc, descs.data(), sizeof(MppiDev) * descs.size(), cudaMemcpyHostToDevice));
+        return DR_OK;
+    }
+
     // (Re)builds the gradient refinement job table from the controllers' settings.
     int setupGrad()
     {
@@ -618,10 +644,9 @@ struct dr_mppi_batch
         dropGraph();
         dropDevGraph();
         {
-            std::vector<MppiDev> descs;
-            for (auto* h : hs)
-                descs.push_back(h->desc);
-            CK(cudaMemcpy(dDesc, descs.data(), sizeof(MppiDev) * descs.size(), cudaMemcpyHostToDevice));
+            int rc = uploadDescs();
+            if (rc)
+                return rc;
         }
         std::vector<GradJob> jobs;
         gradSmemB = 0;
@@ -1695,6 +1720,19 @@ int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* bel
                          int32_t* fail_time, int32_t* thetas)
 {
     return debugVerify(h, state, belief, dense_plan, plan, fail_count, fail_time, thetas);
+}
+
+int dr_mppi_debug_stage_timeout(dr_mppi* h, int on, int polls)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    h->desc.cfg.dbgNoStage = on ? 1 : 0;
+    h->desc.cfg.waitPolls = polls > 0 ? polls : 0;
+    // the controller's own batch of one: re-upload its descriptor; its captured graph
+    // keeps pointers only, so it needs no rebuild
+    return h->self->uploadDescs();
 }
 
 int dr_gate_mppi_debug_verify(dr_mppi* h, const dr_gate_state* state, const float* belief, const float* dense_plan, int plan, uint32_t* fail_count,

@@ -68,6 +68,8 @@ struct dr_prmppi
 
     // host tail of PRMPPIController::getControl (prmppi_controller.cu:268-346); the
     // candidate choice and the safety decision were taken on the device.
+    int lastTimeouts = 0; // staging waits that gave up in the last finished step
+
     void finish(float* outAction, dr_prmppi_info* info)
     {
         const float* nom = at<float>(desc.nom);
@@ -77,6 +79,7 @@ struct dr_prmppi
         const float* full = at<float>(desc.candFull);
         const int* dec = at<int>(desc.decision);
         const int* stats = at<int>(desc.stats);
+        lastTimeouts = stats[1];
         resetNom = dec[0] != 0;
         useNomPlan = dec[1] != 0;
         hNom.assign(nom, nom + (size_t)T * 2);
@@ -226,9 +229,19 @@ struct dr_prmppi_batch
         if (rc)
             return rc;
         CK(cudaStreamSynchronize(stream));
+        int timeouts = 0;
         for (int i = 0; i < n; i++)
+        {
             hs[i]->finish(actions + 2 * i, infos ? infos + i : nullptr);
-        return DR_OK;
+            timeouts += hs[i]->lastTimeouts;
+        }
+        return timeouts ? timedOut(timeouts) : DR_OK;
+    }
+
+    // A step whose kernels gave up a bounded wait is reported, not returned as valid.
+    static int timedOut(int n)
+    {
+        return fail(DR_ERR_TIMEOUT, "a bounded device wait gave up in " + std::to_string(n) + " CTA(s); the step's results are not valid");
     }
 
     // ---- sample-sharded step of a batch of one (dr_prmppi_shard_*) ----
@@ -262,7 +275,7 @@ struct dr_prmppi_batch
             return rc;
         CK(cudaStreamSynchronize(stream));
         hs[0]->finish(action, info);
-        return DR_OK;
+        return hs[0]->lastTimeouts ? timedOut(hs[0]->lastTimeouts) : DR_OK;
     }
 
     void release()

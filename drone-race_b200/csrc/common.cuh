@@ -56,12 +56,18 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  : "memory");
 }
 
-// Waits for phase `parity` of `bar`, giving up after a bounded number of polls.
-// Returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+// Default poll limit of a bounded wait (each poll is one try_wait, which may suspend the
+// thread for a short, hardware-defined time).
+constexpr int WAIT_POLLS = 1 << 22;
+
+// Waits for phase `parity` of `bar`, giving up after `polls` polls (a non-positive value
+// means the default). Returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int polls = WAIT_POLLS)
 {
     uint32_t done = 0;
-    for (int it = 0; it < (1 << 22); it++)
+    if (polls <= 0)
+        polls = WAIT_POLLS;
+    for (int it = 0; it < polls; it++)
     {
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
                      : "=r"(done)

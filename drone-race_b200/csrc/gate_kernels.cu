@@ -91,15 +91,19 @@ __global__ void __launch_bounds__(GRB) gate_rollout(const MppiDev* __restrict__ 
     {
         mbar_init(bar, 1);
         mbar_expect_tx(bar, GATE_TRACK_FLOATS * 4 + knBytes + bBytes);
-        bulk_g2s(sTrack, D.gtrack, GATE_TRACK_FLOATS * 4, bar);
-        bulk_g2s(sKn, D.knots, knBytes, bar);
-        if (SPL)
-            bulk_g2s(sB, D.B, bBytes, bar);
+        if (!D.cfg.dbgNoStage)
+        {
+            bulk_g2s(sTrack, D.gtrack, GATE_TRACK_FLOATS * 4, bar);
+            bulk_g2s(sKn, D.knots, knBytes, bar);
+            if (SPL)
+                bulk_g2s(sB, D.B, bBytes, bar);
+        }
     }
     copyGate(sG, D.gate);
     __syncthreads();
-    if (!__syncthreads_and(mbar_wait(bar, 0)))
+    if (!__syncthreads_and(mbar_wait(bar, 0, D.cfg.waitPolls)))
     {
+        rolloutTileTimedOut<NTH>(D, I, tile, K);
         if (threadIdx.x == 0)
             atomicAdd(&D.stats[1], 1);
         return;
@@ -267,14 +271,17 @@ __global__ void __launch_bounds__(VERIFY_TILE, (gateVerifyMinBlocks<NTH>())) gat
     {
         mbar_init(bar, 1);
         mbar_expect_tx(bar, GATE_TRACK_FLOATS * 4 + planBytes);
-        bulk_g2s(sTrack, D.gtrack, GATE_TRACK_FLOATS * 4, bar);
-        bulk_g2s(sPlan, plan == 0 ? D.dense : D.prevDense, planBytes, bar);
+        if (!D.cfg.dbgNoStage)
+        {
+            bulk_g2s(sTrack, D.gtrack, GATE_TRACK_FLOATS * 4, bar);
+            bulk_g2s(sPlan, plan == 0 ? D.dense : D.prevDense, planBytes, bar);
+        }
     }
     copyGate(sG, D.gate);
     for (int i = threadIdx.x; i < T; i += blockDim.x)
         hist[i] = 0u;
     __syncthreads();
-    if (!__syncthreads_and(mbar_wait(bar, 0)))
+    if (!__syncthreads_and(mbar_wait(bar, 0, D.cfg.waitPolls)))
     {
         if (threadIdx.x == 0)
             atomicAdd(&D.stats[1], 1);

@@ -25,6 +25,12 @@ struct MppiCfgDev
     int verify;
     int gradSteps; // gradient refinement steps (0: off)
     int sLo, sHi;  // this process's samples when the controller is sample-sharded (else 0, K)
+    // Bounded-wait test switch (dr_mppi_debug_stage_timeout): when set, the rollout and
+    // verification CTAs announce their staging bytes on the mbarrier but issue no copy, so
+    // the barrier's phase never completes and the wait gives up after waitPolls polls (0:
+    // the default limit). Nothing is in flight when such a CTA returns.
+    int dbgNoStage;
+    int waitPolls;
 };
 
 // Per-step input of an MPPI instance (one H2D copy per step for the whole batch).
@@ -138,5 +144,33 @@ struct Tile
     int count;
     int aux;
 };
+
+// Branch record of a rollout sample: predTheta << 16 | (branchTime & 0xffff).
+__device__ __forceinline__ int packInfo(int pt, int bt)
+{
+    return (pt << 16) | (bt & 0xffff);
+}
+
+// Outputs of a rollout tile whose staging wait gave up: every sample gets an infinite
+// cost under every hypothesis and branch plan and the branch record of the initial
+// belief, so that the update reads defined values (the step then reports the timeout).
+template <int NTH> __device__ __forceinline__ void rolloutTileTimedOut(const MppiDev& D, const MppiIn& I, const Tile& tile, int K)
+{
+    const int th = threadIdx.x % NTH;
+    const int sl = threadIdx.x / NTH;
+    if (sl >= tile.count)
+        return;
+    const int s = tile.s0 + sl;
+    float belief0[NTH];
+#pragma unroll
+    for (int i = 0; i < NTH; i++)
+        belief0[i] = I.belief[i];
+    const int pt0 = findConfident<NTH>(belief0, D.cfg.minConf);
+    D.costsTrue[th * K + s] = INFINITY;
+    D.binfo[th * K + s] = packInfo(pt0, pt0 == 0 ? -1 : 0);
+    D.costs[(size_t)(th + 1) * K + s] = INFINITY;
+    if (th == 0)
+        D.costs[s] = INFINITY;
+}
 
 } // namespace dr

@@ -44,10 +44,6 @@ template <int NOPP, int NTH> constexpr int verifyMinBlocks()
 }
 constexpr int UB = 256; // update block size (the reference's reduction width)
 
-__device__ __forceinline__ int packInfo(int pt, int bt)
-{
-    return (pt << 16) | (bt & 0xffff);
-}
 __device__ __forceinline__ int infoPred(int v)
 {
     return v >> 16;
@@ -359,15 +355,21 @@ __global__ void __launch_bounds__(RB, 4) mppi_rollout(const MppiDev* __restrict_
             if (threadIdx.x == 0)
             {
                 mbar_expect_tx(bar, GRID_FLOATS * 4 + knBytes + bBytes);
-                bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
-                bulk_g2s(sKn, D.knots, knBytes, bar);
-                if (SPL)
-                    bulk_g2s(sB, D.B, bBytes, bar);
+                if (!D.cfg.dbgNoStage)
+                {
+                    bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
+                    bulk_g2s(sKn, D.knots, knBytes, bar);
+                    if (SPL)
+                        bulk_g2s(sB, D.B, bBytes, bar);
+                }
             }
             copyEnv(sE, &D.env);
             __syncthreads();
-            if (!__syncthreads_and(mbar_wait(bar, phase)))
+            if (!__syncthreads_and(mbar_wait(bar, phase, D.cfg.waitPolls)))
             {
+                // The staging did not complete within the poll limit: write the tile's
+                // defined timeout outputs, count the timeout for the host, return.
+                rolloutTileTimedOut<NTH>(D, I, tile, K);
                 if (threadIdx.x == 0)
                     atomicAdd(&D.stats[1], 1);
                 return;
@@ -827,8 +829,11 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
             if (threadIdx.x == 0)
             {
                 mbar_expect_tx(bar, GRID_FLOATS * 4 + planBytes);
-                bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
-                bulk_g2s(sPlan, plan == 0 ? D.dense : D.prevDense, planBytes, bar);
+                if (!D.cfg.dbgNoStage)
+                {
+                    bulk_g2s(sGrid, D.grids, GRID_FLOATS * 4, bar);
+                    bulk_g2s(sPlan, plan == 0 ? D.dense : D.prevDense, planBytes, bar);
+                }
             }
             copyEnv(sE, &D.env);
         }
@@ -837,7 +842,8 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
         __syncthreads();
         if (key != staged)
         {
-            if (!__syncthreads_and(mbar_wait(bar, phase)))
+            // on timeout the tile adds nothing to the histograms; the host reports it
+            if (!__syncthreads_and(mbar_wait(bar, phase, D.cfg.waitPolls)))
             {
                 if (threadIdx.x == 0)
                     atomicAdd(&D.stats[1], 1);

@@ -9,11 +9,14 @@
 // calls share it, so calls whose GPU work overlaps (on different streams or threads)
 // race on it and must be serialised by the caller. The first call on a device looks up
 // the array's device address (cudaGetSymbolAddress) with that device current; make that
-// first call before any CUDA stream capture.
+// first call before any CUDA stream capture. The address is kept per device and per CUDA
+// context, so a device reset (which reloads the module in a new context) is followed by a
+// fresh look-up instead of a stale address.
 #include <cstring>
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/drmppi.h"
@@ -30,19 +33,48 @@ static __device__ __align__(256) unsigned char g_noallocScratch[DR_NOALLOC_SCRAT
 
 constexpr int MAX_DEVICES = 64;
 
-// device address of g_noallocScratch per device, looked up once with the device current
+// The current CUDA context (driver cuCtxGetCurrent, reached through the runtime's entry
+// point query, so the library does not link the driver library), or null.
+CUcontext currentContext()
+{
+    using Fn = CUresult (*)(CUcontext*);
+    static Fn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+            return (Fn) nullptr;
+        return (Fn)p;
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS)
+        return nullptr;
+    return c;
+}
+
+// device address of g_noallocScratch per device, looked up with the device current the
+// first time the device is used in its current context
 unsigned char* scratchAddress(int& status)
 {
     static std::mutex mu;
     static unsigned char* addr[MAX_DEVICES] = {};
+    static CUcontext ctxOf[MAX_DEVICES] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
     {
         status = fail(DR_ERR_NO_DEVICE, "no current CUDA device");
         return nullptr;
     }
+    // makes the device's primary context current (cudaSetDevice initialises it) before the
+    // context is read
+    cudaError_t fe = cudaSetDevice(dev);
+    if (fe != cudaSuccess)
+    {
+        status = fail(DR_ERR_CUDA, std::string("CUDA context setup failed: ") + cudaGetErrorString(fe));
+        return nullptr;
+    }
+    const CUcontext ctx = currentContext();
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev])
+    if (!addr[dev] || ctxOf[dev] != ctx)
     {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
@@ -52,6 +84,7 @@ unsigned char* scratchAddress(int& status)
             return nullptr;
         }
         addr[dev] = (unsigned char*)p;
+        ctxOf[dev] = ctx;
     }
     status = DR_OK;
     return addr[dev];
@@ -167,5 +200,11 @@ extern "C" int dr_mppi_rollout_costs_noalloc(const dr_env_config* env, const dr_
     // host records may go out of scope; wait for the kernel so that the caller may read
     // costs_dev on any stream afterwards
     CK(cudaStreamSynchronize(s));
+    // the statistics words: [0] samples whose cost is not finite (left in costs_dev as
+    // they are), [1] rollout CTAs whose staging wait gave up (their samples cost infinity)
+    int stats[4] = {0, 0, 0, 0};
+    CK(cudaMemcpy(stats, base + oStats, sizeof(stats), cudaMemcpyDeviceToHost));
+    if (stats[1] > 0)
+        return fail(DR_ERR_TIMEOUT, "a bounded device wait gave up in " + std::to_string(stats[1]) + " rollout CTA(s); costs_dev is not valid");
     return DR_OK;
 }

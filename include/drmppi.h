@@ -178,7 +178,8 @@ typedef struct dr_mppi_info
     float nu;                    /* nu[branch_idx] */
     float inv_temperature;       /* temperature after this step's adaptation */
     int32_t nonfinite_costs;     /* number of samples whose cost was not finite */
-    int32_t verif_timeouts;      /* always 0 unless a bounded wait gave up */
+    int32_t verif_timeouts;      /* CTAs (rollout or verification) whose bounded staging wait gave up;
+                                    the step then returns DR_ERR_TIMEOUT */
     /* gradient refinement (dr_mppi_set_grad_refine; no counterpart in the reference) */
     float grad_cost_plain;       /* objective of the plain MPPI update */
     float grad_cost_refined;     /* objective of the plan kept (<= grad_cost_plain) */
@@ -435,6 +436,14 @@ int dr_mppi_debug_update(dr_mppi* h, const float* belief, const float* costs_tru
  * fail_time (optional, V entries): per-sample failure time or -1. thetas (optional): V. */
 int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* belief, const float* dense_plan, int plan,
                          uint32_t* fail_count, int32_t* fail_time, int32_t* thetas);
+/* Test switch for the bounded device waits (no counterpart in the reference, whose
+ * kernels have no device-side wait): while `on` is set, the rollout and verification CTAs
+ * of this controller's own steps (dr_mppi_step, the dr_mppi_debug_* hooks) announce their
+ * staging bytes but issue no copy, so each staging wait gives up after `polls` polls (<= 0:
+ * the default limit) with nothing in flight; the step then returns DR_ERR_TIMEOUT and
+ * info->verif_timeouts counts the CTAs that gave up. Batches the controller joined later
+ * keep their own copy of its settings. */
+int dr_mppi_debug_stage_timeout(dr_mppi* h, int on, int polls);
 
 /* ---- PR-MPPI controller (reference PRMPPIController) ---------------------------- */
 /* nominal: n_timesteps x DR_DIM or NULL (prmppi_controller.cu:24-37). */
@@ -476,9 +485,12 @@ int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float
  * array of DR_NOALLOC_SCRATCH_BYTES per GPU, held until the process exits; a problem
  * that does not fit (roughly 8 x n_theta x n_samples bytes plus the track and the
  * controls) is rejected with DR_ERR_INVALID_ARG. All calls share that array: calls
- * whose GPU work overlaps race on it. The first call on a device looks the array up
- * (cudaGetSymbolAddress) with that device current, so make it before any stream
- * capture. Returns after the work on `stream` (NULL: legacy default) has completed. */
+ * whose GPU work overlaps race on it. The first call on a device (and the first after
+ * the device's context was reset) looks the array up (cudaGetSymbolAddress) with that
+ * device current, so make it before any stream capture. The call is synchronous: it
+ * returns after the work on `stream` (NULL: legacy default) has completed. Samples whose
+ * cost is not finite keep that value in costs_dev; a rollout CTA whose bounded staging
+ * wait gave up makes the call return DR_ERR_TIMEOUT. */
 #define DR_NOALLOC_SCRATCH_BYTES (4u << 20)
 int dr_mppi_rollout_costs_noalloc(const dr_env_config* env, const dr_mppi_config* cfg, uint64_t seed, uint64_t step, const dr_sim_state* state,
                                   const float* belief, const float* knots_dev, float* costs_dev, void* stream);

@@ -34,6 +34,13 @@ def _types():
     return _abi
 
 
+def reference_dir() -> Path:
+    """The reference checkout: $DR_REFERENCE, else a directory named `reference` beside
+    the repository (the layout oracle/Makefile assumes too)."""
+    env = os.environ.get("DR_REFERENCE")
+    return Path(env) if env else ORACLE_DIR.parents[1] / "reference"
+
+
 def build(ref: bool = True) -> None:
     """Compile the oracle (make -C oracle). The reference variants need the reference
     sources, present only where the oracle is built (not on the GPU box, which uses the
@@ -41,7 +48,7 @@ def build(ref: bool = True) -> None:
     import subprocess
 
     targets = ["port"]
-    if ref and Path(os.environ.get("DR_REFERENCE", "/root/reference")).exists():
+    if ref and reference_dir().exists():
         targets += ["ref", "engine", "adapter_gate"]
     subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "-j4", *targets], check=True)
 

@@ -1132,7 +1132,7 @@ int refc_pr_candidates(const CEnv* ec, const dr_prmppi_config* c, const CState* 
     return st;
 }
 
-// Timing of the reference CUDA path on the GPU box, both figures SURVEY-style:
+// Timing of the reference CUDA path on a GPU, two figures:
 //  out[0] = kernels-only ms per control step (noise generation .. clamp, CUDA events,
 //           mppi_controller.cu:282-345, injected initial state, no host copies),
 //  out[1] = full MPPIController::getControl wall ms per step (stdout silenced).

@@ -40,7 +40,7 @@ def pytest_configure(config):
 def _ensure_oracle():
     if not O.PORT_LIB.exists():
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "port"], check=True)
-    ref_src = Path(os.environ.get("DR_REFERENCE", "/root/reference"))
+    ref_src = O.reference_dir()
     if ref_src.exists() and not all(O.ref_available(v) for v in ("nth2_spline", "nth2_dense", "nth8_spline")):
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "-j4", "ref"], check=True)
     if ref_src.exists() and not (O.REF_DIR / "libengine_dropin.so").exists() and drb.abi.LIB_PATH.exists():

@@ -13,7 +13,8 @@
   * gate_*.npz     the same for the gate race (the reference built with USE_ENV_DRONERACE).
   * cp.npz         Clopper-Pearson bounds from scipy.stats.beta.ppf.
 
-Run from the repository root with the reference at /root/reference:
+Run from the repository root, with the reference checkout in $DR_REFERENCE (default: a
+directory named reference beside the repository):
     python tests/golden/gen_golden.py
 """
 from __future__ import annotations
@@ -27,11 +28,12 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = Path("/root/reference")
 sys.path.insert(0, str(ROOT / "tests"))
 sys.path.insert(0, str(ROOT))
 
 from conftest import O, drb  # noqa: E402
+
+REF = O.reference_dir()
 
 S = drb.scenarios
 abi = drb.abi
