@@ -272,6 +272,7 @@ def uptr(a: np.ndarray) -> C.POINTER(C.c_uint32):
 
 PKG_DIR = Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "lib" / "libdrmppi.so"
+DR_PREDICT_RECORD = 5
 
 # name -> (restype, argtypes)
 _PROTOS = {
@@ -317,6 +318,12 @@ _PROTOS = {
     "dr_mppi_debug_update": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "dr_mppi_debug_verify": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "dr_mppi_debug_stage_timeout": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dr_mppi_set_verify_exact": (C.c_int, [C.c_void_p, C.c_int]),
+    "dr_mppi_predict": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                  C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    "dr_mppi_batch_predict_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "dr_prmppi_predict": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_float)]),
     "dr_prmppi_create": (C.c_int, [C.POINTER(dr_env_config), C.POINTER(dr_prmppi_config), C.c_uint64, C.POINTER(C.c_float), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dr_prmppi_destroy": (C.c_int, [C.c_void_p]),
     "dr_prmppi_step": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_prmppi_info)]),

@@ -19,7 +19,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "lib" / "libdrmppi.so"
 INCLUDE = PKG.parent / "include"
 
-SOURCES = ["mppi_kernels.cu", "gate_kernels.cu", "gate_pr_kernels.cu", "grad_kernels.cu", "finish_kernels.cu", "track_kernels.cu", "prmppi_kernels.cu", "api.cu", "api_pr.cu", "noalloc.cu"]
+SOURCES = ["mppi_kernels.cu", "gate_kernels.cu", "gate_pr_kernels.cu", "grad_kernels.cu", "finish_kernels.cu", "track_kernels.cu", "prmppi_kernels.cu", "api.cu", "api_pr.cu", "noalloc.cu", "predict_kernels.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "--expt-relaxed-constexpr", "-diag-suppress", "177,550"]
 

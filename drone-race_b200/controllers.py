@@ -21,6 +21,17 @@ def _state(s, gate: bool = False):
     raise TypeError(f"state must be a {want.__name__}")
 
 
+
+def _predict(call, rows: int, T: int, n_agents: int, what: str) -> dict:
+    """Runs a prediction entry point into fresh host arrays (layout of include/drmppi.h)."""
+    pos = np.zeros((rows, T, n_agents * 2), np.float32)
+    act = np.zeros((rows, T, 2), np.float32)
+    rec = np.zeros((rows, abi.DR_PREDICT_RECORD), np.int32)
+    cost = np.zeros(rows, np.float32)
+    check(call(pos, act, rec, cost), what)
+    return dict(positions=pos, actions=act, init_branch=rec[:, 0].copy(), branching_time=rec[:, 1].copy(), branch=rec[:, 2].copy(),
+                stop_reason=rec[:, 3].copy(), stop_time=rec[:, 4].copy(), cost=cost)
+
 class Controller:
     """include/controllers.h:12-21."""
 
@@ -51,6 +62,7 @@ class MPPIController(Controller):
                 raise ValueError(f"Invalid MPPI construction: expected nominal size {self.nbp * self.T * 2}, got {nominal.size}")
             nom = abi.fptr(nominal)
         self.gate = isinstance(env, abi.dr_gate_env_config)
+        self.n_agents = 2 if self.gate else int(env.n_opp) + 1
         create = lib().dr_gate_mppi_create if self.gate else lib().dr_mppi_create
         check(create(C.byref(env), C.byref(cfg), seed, nom, device, C.c_void_p(stream) if stream else None, C.byref(h)), "dr_mppi_create")
         self._h = h
@@ -64,6 +76,19 @@ class MPPIController(Controller):
     @property
     def handle(self) -> C.c_void_p:
         return self._h
+
+    def predict(self, state, belief) -> dict:
+        """The engine's prediction streaming for this controller (dr_mppi_predict): from the
+        state after the step, under every hypothesis, the plan the controller holds."""
+        bel = np.ascontiguousarray(belief, np.float32)
+        return _predict(lambda pos, act, rec, cost: lib().dr_mppi_predict(self._h, C.byref(state), abi.fptr(bel), abi.fptr(pos), abi.fptr(act),
+                                                                         abi.iptr(rec), abi.fptr(cost)),
+                        self.n_theta, self.T, self.n_agents, "dr_mppi_predict")
+
+    def set_verify_exact(self, on: bool = True) -> None:
+        """Verification flavour (dr_mppi_set_verify_exact): exact reproduces the CPU
+        oracle's per-sample results; the default fast flavour agrees in distribution."""
+        check(lib().dr_mppi_set_verify_exact(self._h, int(bool(on))), "dr_mppi_set_verify_exact")
 
     def close(self) -> None:
         if self._h:
@@ -155,12 +180,22 @@ class PRMPPIController(Controller):
                 raise ValueError(f"Invalid PRMPPI construction: expected nominal size {self.T * 2}, got {nominal.size}")
             nom = abi.fptr(nominal)
         self.gate = isinstance(env, abi.dr_gate_env_config)
+        self.n_theta = int(env.n_theta)
+        self.n_agents = 2 if self.gate else int(env.n_opp) + 1
         create = lib().dr_gate_prmppi_create if self.gate else lib().dr_prmppi_create
         check(create(C.byref(env), C.byref(cfg), seed, nom, device, C.c_void_p(stream) if stream else None, C.byref(h)), "dr_prmppi_create")
         self._h = h
         self.info = abi.dr_prmppi_info()
         self.min_nu = float(cfg.min_nu) or 0.0005
         self.max_nu = float(cfg.max_nu) or 0.001
+
+    def predict(self, prev_state) -> dict:
+        """The engine's prediction streaming for this controller (dr_prmppi_predict): from the
+        state before the step, the new nominal plan under every hypothesis, then the robust
+        plan under the last one."""
+        return _predict(lambda pos, act, rec, cost: lib().dr_prmppi_predict(self._h, C.byref(prev_state), abi.fptr(pos), abi.fptr(act), abi.iptr(rec),
+                                                                           abi.fptr(cost)),
+                        self.n_theta + 1, self.T, self.n_agents, "dr_prmppi_predict")
 
     @property
     def handle(self) -> C.c_void_p:

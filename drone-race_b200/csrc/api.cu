@@ -46,6 +46,9 @@ struct dr_mppi
     uint64_t seed = 0;
     int nth = 0, nopp = 0, K = 0, T = 0, M = 0, nbp = 0, V = 0, H = 0;
     bool spl = false;
+    // verification flavour: exact (per-sample parity with the oracle) or fast (default)
+    bool exactVerify = false;
+    DevScratch predBuf; // dr_mppi_predict's inputs and outputs on the device
     Arena arena;
     MppiDev desc{};
     unsigned char* hRes = nullptr; // pinned copy of the result block
@@ -245,6 +248,7 @@ struct dr_mppi_batch
         a.mppiIn = in;
         a.tiles = tiles;
         a.nTiles = n;
+        a.exactVerify = hs[0]->exactVerify ? 1 : 0; // equal across the batch (dr_mppi_batch_create)
         return a;
     }
 
@@ -735,9 +739,10 @@ int buildMppiBatch(dr_mppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     b->iMppi = hs[0]->iMppi;
     for (int i = 0; i < n; i++)
         if (!hs[i] || hs[i]->device != b->device || hs[i]->nopp != b->nopp || hs[i]->nth != b->nth || hs[i]->spl != b->spl ||
-            (hs[i]->cfg.verify != 0) != b->verify || hs[i]->envKind != b->envKind || hs[i]->iMppi != b->iMppi)
-            return fail(DR_ERR_INVALID_ARG,
-                        "a batch needs controllers on one device with equal environment kind, ego index, n_opp, n_theta, use_splines and verify");
+            (hs[i]->cfg.verify != 0) != b->verify || hs[i]->envKind != b->envKind || hs[i]->iMppi != b->iMppi ||
+            hs[i]->exactVerify != hs[0]->exactVerify)
+            return fail(DR_ERR_INVALID_ARG, "a batch needs controllers on one device with equal environment kind, ego index, n_opp, n_theta, "
+                                            "use_splines, verify and verification flavour");
     CK(cudaSetDevice(b->device));
     b->stream = stream;
     b->ownStream = ownStream;
@@ -1137,6 +1142,7 @@ int dr_mppi_destroy(dr_mppi* h)
     }
     cudaFree(h->dGradIn);
     cudaFree(h->dGradJobs);
+    h->predBuf.release();
     if (h->desc.cpFull)
         releaseCpTable(h->device, (uint32_t)h->V, h->cpBeta);
     h->arena.release();
@@ -1469,6 +1475,25 @@ int dr_mppi_batch_step_device(dr_mppi_batch* b, const void* states_dev, const fl
     return b->stepDevice(states_dev, beliefs_dev, actions_dev, infos_dev);
 }
 
+int dr_mppi_batch_predict_device(dr_mppi_batch* b, const void* states_dev, const float* beliefs_dev, float* positions_dev, float* actions_dev,
+                                 int32_t* records_dev, float* costs_dev, int t_stride)
+{
+    if (!b || !states_dev || !beliefs_dev || !positions_dev || !actions_dev || !records_dev || !costs_dev)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (b->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "predictions are built for the strategic race");
+    for (auto* h : b->hs)
+        if (h->T > t_stride)
+            return fail(DR_ERR_INVALID_ARG, "t_stride is below a controller's horizon");
+    if (!b->devCtl)
+        return fail(DR_ERR_STATE, "the batch's device records hold no step yet: step it with dr_mppi_batch_step_device first");
+    CK(cudaSetDevice(b->device));
+    PredictOut out{positions_dev, actions_dev, records_dev, costs_dev, t_stride};
+    CK(launchMppiPredict(b->stream, b->nopp, b->nth, b->dDesc, b->dIn, (const dr_sim_state*)states_dev, beliefs_dev, DR_MAX_THETA, out,
+                         (int)b->hs.size()));
+    return DR_OK;
+}
+
 int dr_mppi_batch_env_step_device(dr_mppi_batch* b, const int32_t* true_theta_dev, const float* actions_dev, void* states_dev, float* beliefs_dev,
                                   int update_belief, uint64_t seed, int32_t* terms_dev)
 {
@@ -1689,6 +1714,7 @@ static int debugVerify(dr_mppi* h, const St* state, const float* belief, const f
         a.mppiIn = dIn;
         a.tiles = dT;
         a.nTiles = (int)tiles.size();
+        a.exactVerify = h->exactVerify ? 1 : 0;
         e = h->envKind ? launchGateVerify(a, h->nth, h->iMppi, gateVerifySmem(h->nth, T), dFt, dTh)
                        : launchMppiVerify(a, h->nopp, h->nth, mppiVerifySmem(h->nth, T), dFt, dTh);
         std::vector<unsigned> fc(2 * T);
@@ -1720,6 +1746,51 @@ int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* bel
                          int32_t* fail_time, int32_t* thetas)
 {
     return debugVerify(h, state, belief, dense_plan, plan, fail_count, fail_time, thetas);
+}
+
+int dr_mppi_predict(dr_mppi* h, const dr_sim_state* state, const float* belief, float* positions, float* actions, int32_t* records, float* costs)
+{
+    if (!h || !state || !belief || !positions || !actions || !records || !costs)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "predictions are built for the strategic race");
+    CK(cudaSetDevice(h->device));
+    const int nth = h->nth, T = h->T, na = h->nopp + 1;
+    const size_t nPos = (size_t)nth * T * 2 * na, nAct = (size_t)nth * T * 2, nRec = (size_t)nth * PREDICT_RECORD;
+    const size_t oIn = 0, oSt = a256(sizeof(MppiIn)), oBel = oSt + a256(sizeof(dr_sim_state)), oPos = oBel + a256(DR_MAX_THETA * 4),
+                 oAct = oPos + a256(nPos * 4), oRec = oAct + a256(nAct * 4), oCost = oRec + a256(nRec * 4), total = oCost + a256((size_t)nth * 4);
+    CK(h->predBuf.reserve(total));
+    unsigned char* base = (unsigned char*)h->predBuf.p;
+    // the record carries the pending warm-start shift that the engine's h_nominal holds
+    MppiIn in = h->input(*state, belief);
+    float bel[DR_MAX_THETA] = {};
+    for (int i = 0; i < nth; i++)
+        bel[i] = belief[i];
+    CK(cudaMemcpyAsync(base + oIn, &in, sizeof(MppiIn), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(base + oSt, state, sizeof(dr_sim_state), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(base + oBel, bel, sizeof(bel), cudaMemcpyHostToDevice, h->stream));
+    PredictOut out{(float*)(base + oPos), (float*)(base + oAct), (int*)(base + oRec), (float*)(base + oCost), T};
+    CK(launchMppiPredict(h->stream, h->nopp, nth, h->self->dDesc, (const MppiIn*)(base + oIn), (const dr_sim_state*)(base + oSt),
+                         (const float*)(base + oBel), DR_MAX_THETA, out, 1));
+    CK(cudaMemcpyAsync(positions, base + oPos, nPos * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(actions, base + oAct, nAct * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(records, base + oRec, nRec * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(costs, base + oCost, (size_t)nth * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return DR_OK;
+}
+
+int dr_mppi_set_verify_exact(dr_mppi* h, int on)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    h->exactVerify = on != 0;
+    // the controller's own batch of one captured its verification kernels in its graphs
+    h->self->dropGraph();
+    h->self->dropDevGraph();
+    return DR_OK;
 }
 
 int dr_mppi_debug_stage_timeout(dr_mppi* h, int on, int polls)

@@ -41,6 +41,7 @@ struct dr_prmppi
     int shardWorld = 1;
     int sLo = 0, sHi = 0;
     int envKind = 0, iMppi = 0; // 1: the gate race, with the ego at index iMppi
+    DevScratch predBuf;         // dr_prmppi_predict's inputs and outputs on the device
 
     PrIn input(const dr_gate_state& s, const float* belief) const
     {
@@ -541,12 +542,37 @@ int dr_prmppi_destroy(dr_prmppi* h)
         h->self->release();
         delete h->self;
     }
+    h->predBuf.release();
     h->arena.release();
     if (h->hRes)
         cudaFreeHost(h->hRes);
     if (h->ownStream && h->stream)
         cudaStreamDestroy(h->stream);
     delete h;
+    return DR_OK;
+}
+
+int dr_prmppi_predict(dr_prmppi* h, const dr_sim_state* prev_state, float* positions, float* actions, int32_t* records, float* costs)
+{
+    if (!h || !prev_state || !positions || !actions || !records || !costs)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    if (h->envKind != 0)
+        return fail(DR_ERR_UNSUPPORTED, "predictions are built for the strategic race");
+    CK(cudaSetDevice(h->device));
+    const int rows = h->nth + 1, T = h->T, na = h->nopp + 1;
+    const size_t nPos = (size_t)rows * T * 2 * na, nAct = (size_t)rows * T * 2, nRec = (size_t)rows * PREDICT_RECORD;
+    const size_t oSt = 0, oPos = a256(sizeof(dr_sim_state)), oAct = oPos + a256(nPos * 4), oRec = oAct + a256(nAct * 4),
+                 oCost = oRec + a256(nRec * 4), total = oCost + a256((size_t)rows * 4);
+    CK(h->predBuf.reserve(total));
+    unsigned char* base = (unsigned char*)h->predBuf.p;
+    CK(cudaMemcpyAsync(base + oSt, prev_state, sizeof(dr_sim_state), cudaMemcpyHostToDevice, h->stream));
+    PredictOut out{(float*)(base + oPos), (float*)(base + oAct), (int*)(base + oRec), (float*)(base + oCost), T};
+    CK(launchPrPredict(h->stream, h->nopp, h->nth, h->self->dDesc, (const dr_sim_state*)(base + oSt), out, 1));
+    CK(cudaMemcpyAsync(positions, base + oPos, nPos * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(actions, base + oAct, nAct * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(records, base + oRec, nRec * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(costs, base + oCost, (size_t)rows * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return DR_OK;
 }
 

@@ -41,6 +41,33 @@ inline size_t a256(size_t x)
     return (x + 255) & ~(size_t)255;
 }
 
+// A device buffer that grows on demand (the prediction entry points' staging area).
+struct DevScratch
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t n)
+    {
+        if (n <= bytes)
+            return cudaSuccess;
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess)
+            bytes = n;
+        return e;
+    }
+    void release()
+    {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
 // Bump allocator over one cudaMalloc; every block is 256-byte aligned.
 struct Arena
 {

@@ -29,6 +29,9 @@ struct LaunchArgs
     // update / verification: launch as a programmatic dependent of the previous kernel of
     // the stream (its CTAs take SM slots as they free up and wait in the kernel)
     int pdl = 0;
+    // verification: 1 = the exact arithmetic flavour and noise source (per-sample parity
+    // with the oracle), 0 = the fast flavour (the default)
+    int exactVerify = 0;
 };
 
 inline int launchGrid(const LaunchArgs& a)
@@ -39,7 +42,10 @@ inline int launchGrid(const LaunchArgs& a)
 // Samples per verification CTA (one thread each). The CTA's warps step through the
 // horizon together (a barrier per step), so the warps sharing an SM sub-partition fetch
 // the same instructions; 512 threads, two CTAs per SM.
-constexpr int VERIFY_TILE = 512;
+#ifndef DR_VERIFY_TILE
+#define DR_VERIFY_TILE 512
+#endif
+constexpr int VERIFY_TILE = DR_VERIFY_TILE;
 
 bool mppiSupported(int nopp, int nth);
 int rolloutSamplesPerBlock(int nth);
@@ -106,6 +112,22 @@ cudaError_t launchPrShardApply(cudaStream_t stream, const PrDev* insts, const fl
 
 // Device tail of the control step and the batch's true-dynamics step (finish_kernels.cu).
 cudaError_t launchMppiFinish(cudaStream_t stream, const MppiDev* insts, MppiIn* in, float* actions, dr_mppi_info* infos, int nInst);
+
+// Prediction streaming (predict_kernels.cu). Row r of controller i is at (i * rows + r):
+// positions [tStride][2 (n_opp + 1)], actions [tStride][2], PREDICT_RECORD ints
+// (initial branch, branching time, branch, stop reason, stop time) and one cost.
+constexpr int PREDICT_RECORD = 5;
+struct PredictOut
+{
+    float* pos;
+    float* act;
+    int* rec;
+    float* cost;
+    int tStride;
+};
+cudaError_t launchMppiPredict(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, const dr_sim_state* states,
+                              const float* beliefs, int beliefStride, const PredictOut& out, int nInst);
+cudaError_t launchPrPredict(cudaStream_t stream, int nopp, int nth, const PrDev* insts, const dr_sim_state* prevStates, const PredictOut& out, int nInst);
 cudaError_t launchBatchEnvStep(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, const int* trueTheta,
                                const float* actions, dr_sim_state* states, float* beliefs, int updateBelief, uint32_t k0, uint32_t k1, int* terms);
 // Clopper-Pearson bounds of every failure count for verification size V and level beta,

@@ -20,6 +20,49 @@
 namespace dr
 {
 
+// Arithmetic of the model in two flavours. The exact flavour (F = false) is IEEE division
+// and square root and the CUDA math library's expf, the operations the reference's
+// kernels evaluate, so that results agree with them bit for bit. The fast flavour
+// (F = true) takes the hardware approximations (div.approx, sqrt.approx, rsqrt, ex2;
+// about 2 ulp): the Monte-Carlo verification uses it, whose agreement with the reference
+// is statistical because the reference draws its hypotheses and noise from curand.
+template <bool F> __device__ __forceinline__ float mdiv(float a, float b)
+{
+    if constexpr (F)
+        return __fdividef(a, b);
+    else
+        return a / b;
+}
+
+template <bool F> __device__ __forceinline__ float msqrt(float x)
+{
+    if constexpr (F)
+    {
+        float r;
+        asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+        return r;
+    }
+    else
+        return sqrtf(x);
+}
+
+// a / sqrt(x)
+template <bool F> __device__ __forceinline__ float mdivsqrt(float a, float x)
+{
+    if constexpr (F)
+        return a * rsqrtf(x);
+    else
+        return a / sqrtf(x);
+}
+
+template <bool F> __device__ __forceinline__ float mexp(float x)
+{
+    if constexpr (F)
+        return __expf(x);
+    else
+        return expf(x);
+}
+
 constexpr int NTS = 512;       // N_TRACK_SAMPLES (env_stratrace_defs.h:11)
 constexpr int WIN = 10;        // WINDOW_SIZE (env_stratrace_defs.h:40)
 constexpr float DECAY = 0.97f; // include/config.h:30
@@ -59,6 +102,14 @@ struct EnvParams
     // log-likelihood (env_stratrace.h:199-203), evaluated once per launch instead of
     // once per step with the same device logf.
     float logSqSigma[8][3];
+    // 1 / trackLength and 1 / dt (the fast flavour multiplies by them)
+    float invTrackLength, invDt;
+    // Hypotheses that give opponent o the same action as an earlier one: dupAll[th][o] is
+    // the first hypothesis j < th with the same s1, s2, s3 and speedScale (else -1), so
+    // j's action is th's whatever the state; dupNoBlock[th][o] the first j < th with the
+    // same s1, s2 and speedScale, so j's action is th's whenever the opponent blocks no
+    // one (s3 is read only by the blocking term, env_stratrace.h:357-372).
+    signed char dupAll[8][3], dupNoBlock[8][3];
 };
 
 constexpr int ENV_HOST_WORDS = (int)(offsetof(EnvParams, logSqSigma) / 4);
@@ -74,7 +125,26 @@ __device__ __forceinline__ float beliefSqSigma(float an)
 __device__ __forceinline__ void envDeviceTerms(EnvParams& dst, const EnvParams& src, int tid, int n)
 {
     for (int i = tid; i < 8 * 3; i += n)
-        dst.logSqSigma[i / 3][i % 3] = logf(beliefSqSigma(src.actionNoise[i / 3][i % 3]));
+    {
+        const int th = i / 3, o = i % 3;
+        dst.logSqSigma[th][o] = logf(beliefSqSigma(src.actionNoise[th][o]));
+        int all = -1, noBlock = -1;
+        for (int j = th - 1; j >= 0; j--)
+        {
+            const bool base = src.s1[j][o] == src.s1[th][o] && src.s2[j][o] == src.s2[th][o] && src.speedScale[j][o] == src.speedScale[th][o];
+            if (base)
+                noBlock = j;
+            if (base && src.s3[j][o] == src.s3[th][o])
+                all = j;
+        }
+        dst.dupAll[th][o] = (signed char)all;
+        dst.dupNoBlock[th][o] = (signed char)noBlock;
+    }
+    if (tid == 0)
+    {
+        dst.invTrackLength = 1.0f / src.trackLength;
+        dst.invDt = 1.0f / src.dt;
+    }
 }
 
 // Position on the sampled track (sampleTrackArray, env_stratrace.h:53-67, split into its
@@ -93,6 +163,21 @@ __device__ __forceinline__ TrackPos trackPos(float s, float L)
     float idx_f = s * NTS;
     int idx0 = (int)idx_f;
     return TrackPos{idx0, idx_f - idx0};
+}
+
+// trackPos in either flavour (the fast one multiplies by 1 / L)
+template <bool F> __device__ __forceinline__ TrackPos trackPosT(float s, float L, float invL)
+{
+    if constexpr (F)
+    {
+        s *= invL;
+        s = s - floorf(s);
+        float idx_f = s * NTS;
+        int idx0 = min((int)idx_f, NTS - 1);
+        return TrackPos{idx0, idx_f - idx0};
+    }
+    else
+        return trackPos(s, L);
 }
 
 template <int NA> struct DState
@@ -159,21 +244,28 @@ __device__ __forceinline__ float sqNorm(float x, float y)
     return x * x + y * y;
 }
 
-__device__ __forceinline__ void normalizedSpeed(const Track& tr, TrackPos q, float& o0, float& o1)
+template <bool F> __device__ __forceinline__ void normalizedSpeed(const Track& tr, TrackPos q, float& o0, float& o1)
 {
     sampleAt2(tr.t, q, o0, o1);
-    float invNorm = 1.0f / sqrtf(sqNorm(o0, o1));
+    float invNorm = mdivsqrt<F>(1.0f, sqNorm(o0, o1));
     o0 *= invNorm;
     o1 *= invNorm;
 }
 
 // fastProjectOnTrack<false> (env_stratrace.h:88-162): returns S, writes latDist and the
-// track position of S.
-__device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float px, float py, float prevS, float& latDist, TrackPos& tpS)
+// track position of S. The fast flavour takes the window's minimum on keys that pack the
+// squared distance (its low five mantissa bits dropped) with the sample's place in the
+// window, so one unsigned minimum per sample finds the first of the nearest samples; two
+// distances within 2^-18 relative of each other count as equal there.
+template <bool F>
+__device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float invL, float px, float py, float prevS, float& latDist, TrackPos& tpS)
 {
-    prevS /= L;
+    if constexpr (F)
+        prevS *= invL;
+    else
+        prevS /= L;
     prevS = prevS - floorf(prevS);
-    int idxPrev = (int)(prevS * NTS);
+    int idxPrev = (int)(prevS * NTS); // 512 when prevS rounds to 1: the padded grid holds that window
     const float* __restrict__ P = tr.p;
     const float2* __restrict__ P2 = reinterpret_cast<const float2*>(P);
     // Window idxPrev-10 .. idxPrev+10, first minimum of the squared distance wins (the
@@ -190,41 +282,72 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
     uint64_t pxx, pyy;
     asm("mov.b64 %0, {%1, %1};" : "=l"(pxx) : "f"(px));
     asm("mov.b64 %0, {%1, %1};" : "=l"(pyy) : "f"(py));
-    float bestSqDist = INFINITY;
     int bestJ = j0;
+    if constexpr (F)
+    {
+        uint32_t best = 0xffffffffu;
+        const uint32_t off = (uint32_t)(jp - j0); // place of the first pair's first sample
 #pragma unroll 5
-    for (int q = 0; q < WIN; q++)
-    {
-        const int j = jp + 2 * q;
-        float sqA, sqB;
-        asm("{\n\t.reg .b64 d0, d1, s;\n\t"
-            "sub.rn.f32x2 d0, %2, %4;\n\t"
-            "sub.rn.f32x2 d1, %3, %5;\n\t"
-            "mul.rn.f32x2 s, d0, d0;\n\t"
-            "fma.rn.f32x2 s, d1, d1, s;\n\t"
-            "mov.b64 {%0, %1}, s;\n\t}"
-            : "=f"(sqA), "=f"(sqB)
-            : "l"(PX2[j >> 1]), "l"(PY2[j >> 1]), "l"(pxx), "l"(pyy));
-        if (sqA < bestSqDist)
+        for (int q = 0; q < WIN; q++)
         {
-            bestSqDist = sqA;
-            bestJ = j;
+            const int j = jp + 2 * q;
+            float sqA, sqB;
+            asm("{\n\t.reg .b64 d0, d1, s;\n\t"
+                "sub.rn.f32x2 d0, %2, %4;\n\t"
+                "sub.rn.f32x2 d1, %3, %5;\n\t"
+                "mul.rn.f32x2 s, d0, d0;\n\t"
+                "fma.rn.f32x2 s, d1, d1, s;\n\t"
+                "mov.b64 {%0, %1}, s;\n\t}"
+                : "=f"(sqA), "=f"(sqB)
+                : "l"(PX2[j >> 1]), "l"(PY2[j >> 1]), "l"(pxx), "l"(pyy));
+            best = min(best, (__float_as_uint(sqA) & ~31u) | (off + 2u * q));
+            best = min(best, (__float_as_uint(sqB) & ~31u) | (off + 2u * q + 1u));
         }
-        if (sqB < bestSqDist)
         {
-            bestSqDist = sqB;
-            bestJ = j + 1;
+            float2 qs = P2[js];
+            float d0 = qs.x - px, d1 = qs.y - py;
+            float sq = d0 * d0 + d1 * d1;
+            best = min(best, (__float_as_uint(sq) & ~31u) | (uint32_t)(js - j0));
         }
+        bestJ = j0 + (int)(best & 31u);
     }
+    else
     {
-        float2 qs = P2[js];
-        float sq = 0.f;
-        float d0 = qs.x - px;
-        sq += d0 * d0;
-        float d1 = qs.y - py;
-        sq += d1 * d1;
-        if (sq < bestSqDist || (sq == bestSqDist && js < bestJ))
-            bestJ = js;
+        float bestSqDist = INFINITY;
+#pragma unroll 5
+        for (int q = 0; q < WIN; q++)
+        {
+            const int j = jp + 2 * q;
+            float sqA, sqB;
+            asm("{\n\t.reg .b64 d0, d1, s;\n\t"
+                "sub.rn.f32x2 d0, %2, %4;\n\t"
+                "sub.rn.f32x2 d1, %3, %5;\n\t"
+                "mul.rn.f32x2 s, d0, d0;\n\t"
+                "fma.rn.f32x2 s, d1, d1, s;\n\t"
+                "mov.b64 {%0, %1}, s;\n\t}"
+                : "=f"(sqA), "=f"(sqB)
+                : "l"(PX2[j >> 1]), "l"(PY2[j >> 1]), "l"(pxx), "l"(pyy));
+            if (sqA < bestSqDist)
+            {
+                bestSqDist = sqA;
+                bestJ = j;
+            }
+            if (sqB < bestSqDist)
+            {
+                bestSqDist = sqB;
+                bestJ = j + 1;
+            }
+        }
+        {
+            float2 qs = P2[js];
+            float sq = 0.f;
+            float d0 = qs.x - px;
+            sq += d0 * d0;
+            float d1 = qs.y - py;
+            sq += d1 * d1;
+            if (sq < bestSqDist || (sq == bestSqDist && js < bestJ))
+                bestJ = js;
+        }
     }
     const int bestInd = (bestJ + NTS) % NTS;
     float bestSegSqDist = INFINITY;
@@ -243,7 +366,7 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
         float t = 0.0f;
         if (sqAB > 1e-12f) // the reference compares with the double 1e-12; for floats the two tests agree
         {
-            t = ((px - ax) * abx + (py - ay) * aby) / sqAB;
+            t = mdiv<F>((px - ax) * abx + (py - ay) * aby, sqAB);
             t = fmaxf(0.0f, fminf(t, 1.0f));
         }
         float projx = ax + t * abx;
@@ -258,10 +381,10 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
         }
     }
     float tg0, tg1;
-    tpS = trackPos(bestS, L);
+    tpS = trackPosT<F>(bestS, L, invL);
     sampleAt2(tr.t, tpS, tg0, tg1);
     float cross = -tg1 * (px - closestX) + tg0 * (py - closestY);
-    latDist = copysignf(sqrtf(bestSegSqDist), cross);
+    latDist = copysignf(msqrt<F>(bestSegSqDist), cross);
     return bestS;
 }
 
@@ -274,17 +397,18 @@ template <int NA> struct AgentGeo
     float sdot[NA];         // computeSdot(a) (env_stratrace.h:302-315)
 };
 
-template <int NA> __device__ __forceinline__ void agentGeometry(const Track& tr, const EnvParams& E, const DState<NA>& s, AgentGeo<NA>& g)
+template <int NA, bool F = false>
+__device__ __forceinline__ void agentGeometry(const Track& tr, const EnvParams& E, const DState<NA>& s, AgentGeo<NA>& g)
 {
 #pragma unroll
     for (int a = 0; a < NA; a++)
     {
-        normalizedSpeed(tr, s.tp[a], g.tn0[a], g.tn1[a]);
+        normalizedSpeed<F>(tr, s.tp[a], g.tn0[a], g.tn1[a]);
         g.kap[a] = sampleAt1(tr.k, s.tp[a]);
         float metric = 1 - g.kap[a] * s.lat[a];
         if (fabsf(metric) < 1e-12f)
             metric = copysignf(1e-12f, metric);
-        g.sdot[a] = (g.tn0[a] * s.vel[2 * a] + g.tn1[a] * s.vel[2 * a + 1]) / metric;
+        g.sdot[a] = mdiv<F>(g.tn0[a] * s.vel[2 * a] + g.tn1[a] * s.vel[2 * a + 1], metric);
     }
 }
 
@@ -306,7 +430,7 @@ struct OppCommon
     bool brakePos, brakeNeg;
 };
 
-template <int NOPP>
+template <int NOPP, bool F = false>
 __device__ __forceinline__ void oppCommon(int iOpp, const Track& tr, const EnvParams& E, const DState<NOPP + 1>& s, const AgentGeo<NOPP + 1>& g,
                                           OppCommon& c)
 {
@@ -398,7 +522,7 @@ __device__ __forceinline__ void oppCommon(int iOpp, const Track& tr, const EnvPa
     if (fabsf(metric_actual) < 1e-6f)
         metric_actual = copysignf(1e-6f, metric_actual);
     c.metric_actual = metric_actual;
-    c.a_centripetal = c.v_t * c.v_t * c.kappa / metric_actual;
+    c.a_centripetal = mdiv<F>(c.v_t * c.v_t * c.kappa, metric_actual);
     c.a_lat_max = fmaxf(c.maxAccel - fabsf(c.a_centripetal), c.maxAccel * 0.2f);
     c.distPos = fmaxf(c.e_n_max - c.e_n, 0.001f);
     c.distNeg = fmaxf(c.e_n_max + c.e_n, 0.001f);
@@ -408,6 +532,7 @@ __device__ __forceinline__ void oppCommon(int iOpp, const Track& tr, const EnvPa
 
 // Hypothesis-dependent part: target lateral offset / speed goal and the resulting
 // acceleration of opponent iOpp under hypothesis th.
+template <bool F = false>
 __device__ __forceinline__ void oppAction(int iOpp, int th, const EnvParams& E, const OppCommon& c, float& out0, float& out1)
 {
     const float s1 = E.s1[th][iOpp - 1], s2 = E.s2[th][iOpp - 1], s3 = E.s3[th][iOpp - 1];
@@ -422,10 +547,10 @@ __device__ __forceinline__ void oppAction(int iOpp, int th, const EnvParams& E, 
         bool shouldOvertake = c.fasterThanJ[k] && (fabsf(deltaE) < s1);
         if (!c.shouldBlock[k] && !shouldOvertake)
             continue; // neither term uses the proximity factor
-        float factor = expf(-s2 * deltaS * deltaS);
+        float factor = mexp<F>(-s2 * deltaS * deltaS);
         if (c.shouldBlock[k])
         {
-            float blockTerm = c.latJ[k] * (1 - expf(-s3 * (c.sdotJ[k] + c.blockTol[k] - c.sdot_i))) * factor;
+            float blockTerm = c.latJ[k] * (1 - mexp<F>(-s3 * (c.sdotJ[k] + c.blockTol[k] - c.sdot_i))) * factor;
             latDis += blockTerm;
         }
         if (shouldOvertake)
@@ -437,7 +562,7 @@ __device__ __forceinline__ void oppAction(int iOpp, int th, const EnvParams& E, 
                 speedGoal = fminf(speedGoal, 0.7f * oppLongSpeed);
             else if (deltaS < 6 * E.droneRadius && s1 > 1e-6f) // double 1e-6 in the reference; same test for floats
             {
-                float latFactor = fabsf(deltaE) / s1;
+                float latFactor = mdiv<F>(fabsf(deltaE), s1);
                 speedGoal = fminf(speedGoal, latFactor * oppLongSpeed + (1.0f - latFactor) * baseSpeed);
             }
         }
@@ -454,13 +579,13 @@ __device__ __forceinline__ void oppAction(int iOpp, int th, const EnvParams& E, 
         a_n_cmd = a_lat_max;
     else if (fabsf(e_error) < 0.02f)
     {
-        float kp = a_lat_max / 0.02f;
-        a_n_cmd = kp * e_error - 2.0f * sqrtf(kp) * v_n;
+        float kp = F ? a_lat_max * 50.0f : a_lat_max / 0.02f;
+        a_n_cmd = kp * e_error - 2.0f * msqrt<F>(kp) * v_n;
         a_n_cmd = fmaxf(-a_lat_max, fminf(a_lat_max, a_n_cmd));
     }
     else
     {
-        float stopping_dist = v_n * v_n / (2.0f * a_lat_max);
+        float stopping_dist = mdiv<F>(v_n * v_n, 2.0f * a_lat_max);
         bool v_toward = (e_error > 0.0f && v_n > 0.0f) || (e_error < 0.0f && v_n < 0.0f);
         bool decel_phase = v_toward && stopping_dist >= fabsf(e_error) * 0.95f;
         a_n_cmd = (e_error > 0.0f) ? a_lat_max : -a_lat_max;
@@ -469,25 +594,25 @@ __device__ __forceinline__ void oppAction(int iOpp, int th, const EnvParams& E, 
         float v_n_next = v_n + a_n_cmd * dt;
         if (v_n_next > 0.0f)
         {
-            float v_safe = sqrtf(2.0f * a_lat_max * c.distPos);
+            float v_safe = msqrt<F>(2.0f * a_lat_max * c.distPos);
             if (v_n_next > v_safe)
-                a_n_cmd = (v_safe - v_n) / dt;
+                a_n_cmd = F ? (v_safe - v_n) * E.invDt : (v_safe - v_n) / dt;
         }
         else
         {
-            float v_safe = sqrtf(2.0f * a_lat_max * c.distNeg);
+            float v_safe = msqrt<F>(2.0f * a_lat_max * c.distNeg);
             if (-v_n_next > v_safe)
-                a_n_cmd = (-v_safe - v_n) / dt;
+                a_n_cmd = F ? (-v_safe - v_n) * E.invDt : (-v_safe - v_n) / dt;
         }
     }
     float a_n_total = fmaxf(-maxAccel, fminf(maxAccel, a_n_cmd + c.a_centripetal));
-    float a_t_max = sqrtf(fmaxf(c.maxAccelSq - a_n_total * a_n_total, 0.0f));
+    float a_t_max = msqrt<F>(fmaxf(c.maxAccelSq - a_n_total * a_n_total, 0.0f));
     float kappa = c.kappa;
-    float kappa_eff = kappa / (1.0f - kappa * latDisC + 1e-6f);
-    float pathSpeed = fminf(speedGoal, sqrtf(maxAccel / fmaxf(fabsf(kappa_eff), 1e-12f)));
+    float kappa_eff = mdiv<F>(kappa, 1.0f - kappa * latDisC + 1e-6f);
+    float pathSpeed = fminf(speedGoal, msqrt<F>(mdiv<F>(maxAccel, fmaxf(fabsf(kappa_eff), 1e-12f))));
     if (fabsf(a_n_cmd) > a_lat_max * 0.5f)
-        pathSpeed *= fmaxf(0.4f, 1.5f - fabsf(a_n_cmd) / a_lat_max);
-    float a_t_cmd = E.kV * (pathSpeed - c.v_t) - v_n * kappa * c.v_t / c.metric_actual;
+        pathSpeed *= fmaxf(0.4f, 1.5f - mdiv<F>(fabsf(a_n_cmd), a_lat_max));
+    float a_t_cmd = E.kV * (pathSpeed - c.v_t) - mdiv<F>(v_n * kappa * c.v_t, c.metric_actual);
     a_t_cmd = fmaxf(-a_t_max, fminf(a_t_max, a_t_cmd));
     out0 = a_t_cmd * c.tang0 + a_n_total * c.norm0;
     out1 = a_t_cmd * c.tang1 + a_n_total * c.norm1;
@@ -515,19 +640,28 @@ struct StepOut
 // environmentStep (env_stratrace.h:711-894).
 //   UPD: shouldUpdateBelief, BR: considerBranching, LOSE: loseOnOppWin,
 //   ALLTH: evaluate the opponent policy under every hypothesis (needed by the belief
-//   update) or only under the true one (the result is the same when UPD is false).
-template <int NOPP, int NTH, bool UPD, bool BR, bool LOSE, bool ALLTH>
+//   update) or only under the true one (the result is the same when UPD is false),
+//   F: the arithmetic flavour (exact or fast, see mdiv), RNG: the noise source.
+// Work whose result cannot change the step's outputs is not done:
+//   * a hypothesis whose policy parameters equal an earlier one's on every term the step
+//     evaluates (EnvParams::dupAll / dupNoBlock) takes that one's action;
+//   * with BR, once the sample has committed to a branch (predTheta != 0) its belief is
+//     read by nothing any more (the branch test runs only while predTheta == 0; the
+//     callers with BR return costs, branch records and failure times, never the belief),
+//     so the belief update and the other hypotheses' actions it needs are skipped.
+template <int NOPP, int NTH, bool UPD, bool BR, bool LOSE, bool ALLTH, bool F = false, class RNG = EnvNoise>
 __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr, const EnvParams& E, float ego0, float ego1, DState<NOPP + 1>& s,
-                                           BState<NTH>& bs, bool& branched, float minConf, EnvNoise& rng)
+                                           BState<NTH>& bs, bool& branched, float minConf, RNG& rng)
 {
     constexpr int NA = NOPP + 1;
     float prevS[NA];
 #pragma unroll
     for (int a = 0; a < NA; a++)
         prevS[a] = s.S[a];
+    const bool live = !BR || bs.predTheta == 0; // the belief is still read after this step
 
     AgentGeo<NA> g;
-    agentGeometry<NA>(tr, E, s, g);
+    agentGeometry<NA, F>(tr, E, s, g);
 
     float act0[NA], act1[NA];
     act0[0] = ego0;
@@ -537,14 +671,30 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     for (int o = 1; o <= NOPP; o++)
     {
         OppCommon c;
-        oppCommon<NOPP>(o, tr, E, s, g, c);
+        oppCommon<NOPP, F>(o, tr, E, s, g, c);
         float u0 = 0.f, u1 = 0.f;
         if constexpr (ALLTH)
         {
+            const bool blocks = c.shouldBlock[0] || c.shouldBlock[1];
 #pragma unroll
             for (int th = 0; th < NTH; th++)
             {
-                oppAction(o, th, E, c, nom0[th][o - 1], nom1[th][o - 1]);
+                if (!live && th != trueTheta)
+                    continue;
+                // an earlier hypothesis with the same action (all of them are evaluated
+                // while the belief is live, so that one's action is at hand)
+                const int src = live ? (blocks ? E.dupAll[th][o - 1] : E.dupNoBlock[th][o - 1]) : -1;
+                bool copied = false;
+#pragma unroll
+                for (int j = 0; j < th; j++)
+                    if (src == j)
+                    {
+                        nom0[th][o - 1] = nom0[j][o - 1];
+                        nom1[th][o - 1] = nom1[j][o - 1];
+                        copied = true;
+                    }
+                if (!copied)
+                    oppAction<F>(o, th, E, c, nom0[th][o - 1], nom1[th][o - 1]);
                 if (th == trueTheta)
                 {
                     u0 = nom0[th][o - 1];
@@ -554,7 +704,7 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
         }
         else
         {
-            oppAction(o, trueTheta, E, c, nom0[0][o - 1], nom1[0][o - 1]);
+            oppAction<F>(o, trueTheta, E, c, nom0[0][o - 1], nom1[0][o - 1]);
             u0 = nom0[0][o - 1];
             u1 = nom1[0][o - 1];
         }
@@ -578,7 +728,7 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
         float factor = 1.0f;
         float maxSq = E.maxAccel[a] * E.maxAccel[a];
         if (sq > maxSq)
-            factor = E.maxAccel[a] / sqrtf(sq);
+            factor = mdivsqrt<F>(E.maxAccel[a], sq);
         act0[a] *= factor;
         if (E.actionNoiseLevel != 0.0f)
             act0[a] += rng.next() * E.actionNoiseLevel;
@@ -611,7 +761,7 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
         float sqSpd = sqNorm(s.vel[2 * a], s.vel[2 * a + 1]);
         if (sqSpd > E.maxSpeed[a] * E.maxSpeed[a])
         {
-            float sc = E.maxSpeed[a] / sqrtf(sqSpd);
+            float sc = mdivsqrt<F>(E.maxSpeed[a], sqSpd);
             s.vel[2 * a] *= sc;
             s.vel[2 * a + 1] *= sc;
         }
@@ -633,7 +783,7 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     // 8. projection
 #pragma unroll
     for (int a = 0; a < NA; a++)
-        s.S[a] = projectOnTrack(tr, E.trackLength, s.pos[2 * a], s.pos[2 * a + 1], s.S[a], s.lat[a], s.tp[a]);
+        s.S[a] = projectOnTrack<F>(tr, E.trackLength, E.invTrackLength, s.pos[2 * a], s.pos[2 * a + 1], s.S[a], s.lat[a], s.tp[a]);
     // 9. laps
 #pragma unroll
     for (int a = 0; a < NA; a++)
@@ -646,45 +796,48 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     // 10. belief update (env_stratrace.h:166-222)
     if constexpr (UPD)
     {
-        float sum = 0.0f;
-#pragma unroll
-        for (int th = 0; th < NTH; th++)
+        if (live)
         {
-            float logLikelihood = 0.0f;
-#pragma unroll
-            for (int o = 0; o < NOPP; o++)
-            {
-                float n0 = nom0[th][o], n1 = nom1[th][o];
-                float sqAccel = 0.0f;
-                sqAccel += n0 * n0;
-                sqAccel += n1 * n1;
-                float scale = 1.0f;
-                if (sqAccel > E.maxAccel[o + 1] * E.maxAccel[o + 1])
-                    scale = E.maxAccel[o + 1] / sqrtf(sqAccel);
-                float sqDist = 0.0f;
-                float dx0 = act0[o + 1] - n0 * scale;
-                sqDist += dx0 * dx0;
-                float dx1 = act1[o + 1] - n1 * scale;
-                sqDist += dx1 * dx1;
-                float an = E.actionNoise[th][o];
-                float sqSigma = beliefSqSigma(an);
-                logLikelihood += -0.5f * sqDist / sqSigma - (float)2 * 0.5f * logf(2.0f * M_PIf32) - (float)2 * 0.5f * E.logSqSigma[th][o];
-            }
-            bs.belief[th] *= expf(logLikelihood);
-            sum += bs.belief[th];
-        }
-        if (sum < 1e-20f)
-        {
-            float uniform = 1.0f / NTH;
-#pragma unroll
-            for (int th = 0; th < NTH; ++th)
-                bs.belief[th] = uniform;
-        }
-        else
-        {
+            float sum = 0.0f;
 #pragma unroll
             for (int th = 0; th < NTH; th++)
-                bs.belief[th] /= sum;
+            {
+                float logLikelihood = 0.0f;
+#pragma unroll
+                for (int o = 0; o < NOPP; o++)
+                {
+                    float n0 = nom0[th][o], n1 = nom1[th][o];
+                    float sqAccel = 0.0f;
+                    sqAccel += n0 * n0;
+                    sqAccel += n1 * n1;
+                    float scale = 1.0f;
+                    if (sqAccel > E.maxAccel[o + 1] * E.maxAccel[o + 1])
+                        scale = mdivsqrt<F>(E.maxAccel[o + 1], sqAccel);
+                    float sqDist = 0.0f;
+                    float dx0 = act0[o + 1] - n0 * scale;
+                    sqDist += dx0 * dx0;
+                    float dx1 = act1[o + 1] - n1 * scale;
+                    sqDist += dx1 * dx1;
+                    float an = E.actionNoise[th][o];
+                    float sqSigma = beliefSqSigma(an);
+                    logLikelihood += mdiv<F>(-0.5f * sqDist, sqSigma) - (float)2 * 0.5f * logf(2.0f * M_PIf32) - (float)2 * 0.5f * E.logSqSigma[th][o];
+                }
+                bs.belief[th] *= mexp<F>(logLikelihood);
+                sum += bs.belief[th];
+            }
+            if (sum < 1e-20f)
+            {
+                float uniform = 1.0f / NTH;
+#pragma unroll
+                for (int th = 0; th < NTH; ++th)
+                    bs.belief[th] = uniform;
+            }
+            else
+            {
+#pragma unroll
+                for (int th = 0; th < NTH; th++)
+                    bs.belief[th] = mdiv<F>(bs.belief[th], sum);
+            }
         }
     }
     if constexpr (BR)
@@ -708,7 +861,7 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
 #pragma unroll
     for (int o = 1; o <= NOPP; o++)
         minSq = fminf(minSq, sqNorm(s.pos[2 * o] - s.pos[0], s.pos[2 * o + 1] - s.pos[1]));
-    float bdRaw = fminf(sqrtf(minSq) - E.droneRadius, E.trackWidth - fabsf(s.lat[0]));
+    float bdRaw = fminf(msqrt<F>(minSq) - E.droneRadius, E.trackWidth - fabsf(s.lat[0]));
     bool winner = s.laps[0] >= E.nWinLaps;
 #pragma unroll
     for (int o = 1; o <= NOPP; o++)

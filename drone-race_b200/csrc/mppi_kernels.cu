@@ -20,6 +20,7 @@
 //   mppi_verify     Monte-Carlo failure counts of the new and the previous plan
 //                   (verifyNominalFailureKernel, kernels.cu:488-551), both plans in one grid.
 #include <cstdio>
+#include <type_traits>
 
 #include "common.cuh"
 #include "instance.cuh"
@@ -793,7 +794,9 @@ __global__ void __launch_bounds__(UB) mppi_shard_apply(const MppiDev* __restrict
 // ---------------------------------------------------------------------------------------
 // verification
 // ---------------------------------------------------------------------------------------
-template <int NOPP, int NTH, bool PQ>
+// FAST: the fast arithmetic flavour and noise source (the default; the exact flavour
+// reproduces the oracle's per-sample results and serves parity tests).
+template <int NOPP, int NTH, bool PQ, bool FAST>
 __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) mppi_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
                                                   int nTiles, unsigned* __restrict__ queue, int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
 {
@@ -895,7 +898,8 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
                     }
                 }
             }
-            EnvNoise rng(k0, k1, (uint32_t)v, (uint32_t)plan << 16, step, S_VERIF_ENV);
+            using Noise = typename std::conditional<FAST, FastNoise, EnvNoise>::type;
+            Noise rng(k0, k1, (uint32_t)v, (uint32_t)plan << 16, step, S_VERIF_ENV);
             int tOrigin = 0, t = 0, tEnd = H;
             bool failed = false;
             for (; t < H; t++)
@@ -911,7 +915,7 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
                 int b = bs.predTheta;
                 float e0 = sPlan[(b * T + local) * 2], e1 = sPlan[(b * T + local) * 2 + 1];
                 bool branched = false;
-                StepOut o = envStep<NOPP, NTH, true, true, false, true>(t, theta, tr, E, e0, e1, st, bs, branched, minConf, rng);
+                StepOut o = envStep<NOPP, NTH, true, true, false, true, FAST>(t, theta, tr, E, e0, e1, st, bs, branched, minConf, rng);
                 if (branched)
                     tOrigin = t + 1;
                 if (o.term == TERM_LOSE)
@@ -989,7 +993,8 @@ template <int NOPP, int NTH> static cudaError_t launchRolloutT(const LaunchArgs&
 
 template <int NOPP, int NTH> static cudaError_t launchVerifyT(const LaunchArgs& a, size_t smem, int* ft, int* th)
 {
-    auto k = a.queue ? mppi_verify<NOPP, NTH, true> : mppi_verify<NOPP, NTH, false>;
+    auto k = a.exactVerify ? (a.queue ? mppi_verify<NOPP, NTH, true, false> : mppi_verify<NOPP, NTH, false, false>)
+                           : (a.queue ? mppi_verify<NOPP, NTH, true, true> : mppi_verify<NOPP, NTH, false, true>);
     ensureSmem(k, smem);
     return launchMaybePdl(a.pdl != 0, k, dim3(launchGrid(a)), dim3(VERIFY_TILE), smem, a.stream, a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue, ft, th);
 }
@@ -1001,8 +1006,8 @@ template <int NOPP, int NTH> static int residentT(bool verify, bool spl, size_t 
     int n = 0;
     if (verify)
     {
-        ensureSmem(mppi_verify<NOPP, NTH, true>, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_verify<NOPP, NTH, true>, VERIFY_TILE, smem);
+        ensureSmem(mppi_verify<NOPP, NTH, true, true>, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mppi_verify<NOPP, NTH, true, true>, VERIFY_TILE, smem);
     }
     else if (spl)
     {

@@ -14,6 +14,7 @@
 //   MPPI rollout env noise   c0 = sample, c1 = theta << 16 | t, normal j: sub j>>2, word j&3
 //   verification theta draw  c0 = sample, c1 = plan, word 0 (uniform)
 //   verification env noise   c0 = sample, c1 = plan << 16 | t
+//     (fast flavour)         c0 = sample, c1 = plan << 16, sub = 0x400000 | block (FastNoise)
 //   PR-MPPI perturbation     c0 = sample, c1 = t, words 0..1
 //   PR-MPPI theta draw       c0 = p, c1 = 0, word 0 (uniform)
 //   PR-MPPI rollout env      c0 = sample, c1 = ((robust << 8 | p) << 16) | t
@@ -203,6 +204,61 @@ struct EnvNoise
         const uint32_t w0 = lo ? cur.x : cur.z, w1 = lo ? cur.y : cur.w;
         j += 2;
         return normal_pair_ool(w0, w1);
+    }
+};
+
+// A pair of normal variates from two Philox words by the Box-Muller transform (Box and
+// Muller, "A note on the generation of random normal deviates", 1958):
+// r = sqrt(-2 ln u1), (r cos 2 pi u2, r sin 2 pi u2), with the hardware's approximate
+// log, square root, sine and cosine (the angle is taken in (-pi, pi), where the
+// approximate sine and cosine are accurate). u1 is at least 2^-24, so |z| < 5.8.
+__device__ __forceinline__ float2 box_muller_fast(uint32_t w0, uint32_t w1)
+{
+    const float u1 = uniform_from_word(w0);
+    const float u2 = uniform_from_word(w1);
+    // the approximate log of a u1 just below 1 may come out just above 0
+    float r2 = fmaxf(-2.0f * __logf(u1), 0.0f);
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(r2));
+    float sn, cs;
+    __sincosf(6.28318531f * (u2 - 0.5f), &sn, &cs);
+    return make_float2(r * cs, r * sn);
+}
+
+// Normal source of the Monte-Carlo verification's fast flavour: Box-Muller pairs from
+// the words of one Philox stream per sample, taken in sequence across its steps (a block
+// of four words gives two pairs: one returned at once, one kept for the next call),
+// counter = (c0, c1, step, stream << 24 | 0x400000 | block). Its draws differ from
+// EnvNoise's; the distribution is the same.
+struct FastNoise
+{
+    uint32_t k0, k1, c0, c1, step, stream;
+    uint32_t block; // next Philox block
+    bool have;      // spare holds the second pair of the last block
+    float2 spare;
+    __device__ __forceinline__ FastNoise(uint32_t k0_, uint32_t k1_, uint32_t c0_, uint32_t c1_, uint32_t step_, uint32_t stream_)
+        : k0(k0_), k1(k1_), c0(c0_), c1(c1_), step(step_), stream(stream_), block(0), have(false), spare{0.f, 0.f}
+    {
+    }
+    __device__ __forceinline__ void begin_step(uint32_t)
+    {
+    }
+    __device__ __forceinline__ float2 next2()
+    {
+        if (have)
+        {
+            have = false;
+            return spare;
+        }
+        const U4 r = draw(k0, k1, c0, c1, step, stream, 0x400000u | block);
+        block++;
+        spare = box_muller_fast(r.z, r.w);
+        have = true;
+        return box_muller_fast(r.x, r.y);
+    }
+    __device__ __forceinline__ float next()
+    {
+        return next2().x;
     }
 };
 

@@ -436,6 +436,15 @@ int dr_mppi_debug_update(dr_mppi* h, const float* belief, const float* costs_tru
  * fail_time (optional, V entries): per-sample failure time or -1. thetas (optional): V. */
 int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* belief, const float* dense_plan, int plan,
                          uint32_t* fail_count, int32_t* fail_time, int32_t* thetas);
+/* Arithmetic flavour of this controller's Monte-Carlo verification (no counterpart in the
+ * reference, whose verifyNominalFailureKernel, kernels.cu:488-551, draws its hypotheses and
+ * noise from curand, so that its failure counts are reproducible only in distribution).
+ * on = 0 (the default): the fast flavour, with the hardware's approximate division, square
+ * root and exponential and Box-Muller normals; on = 1: the exact flavour, the reference's
+ * IEEE arithmetic and the library's inverse-CDF normals, whose per-sample failure times
+ * equal the CPU oracle's. Controllers of one batch need the same flavour, so set it before
+ * batching the controller. */
+int dr_mppi_set_verify_exact(dr_mppi* h, int on);
 /* Test switch for the bounded device waits (no counterpart in the reference, whose
  * kernels have no device-side wait): while `on` is set, the rollout and verification CTAs
  * of this controller's own steps (dr_mppi_step, the dr_mppi_debug_* hooks) announce their
@@ -472,6 +481,41 @@ int dr_prmppi_debug_noise(dr_prmppi* h, const float* belief, float* noise, size_
 /* Rollout of the next step (prmppi_kernels.cu:55-130): cost_nom/cost_rob [P][K][2]
  * (running cost, safety cost), before averaging. The nominals are the shifted ones. */
 int dr_prmppi_debug_rollout(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* cost_nom, float* cost_rob);
+
+/* ---- prediction streaming (the engine's sendState, src/engine.cpp:55-264) --------
+ * After each closed-loop step the reference engine re-simulates the controller's plan on
+ * the host, with noise off, and streams the predicted trajectories in MSG_STATE. These
+ * entry points run that re-simulation on the device. Output rows (one per hypothesis for
+ * MPPI; for PR-MPPI one per hypothesis with the nominal plan, then the robust plan under
+ * the last hypothesis) hold, with T the horizon (or t_stride):
+ *   positions [rows][T][(n_opp + 1) * DR_DIM]  every agent's position after each step,
+ *                                              the last one repeated after a terminal step
+ *                                              (Env::pushPredictions, env_stratrace.cpp:70-78)
+ *   actions   [rows][T][DR_DIM]                the ego actions taken, zero after the stop
+ *   records   [rows][DR_PREDICT_RECORD]        initial branch, branching time, branch (MPPI;
+ *                                              0, -1, 0 for PR-MPPI), stop reason (EventType:
+ *                                              0 outside, 1 winner, 2 opponent winner,
+ *                                              3 truncated), stop time (-1: none)
+ *   costs     [rows]                           MPPI: the discounted running + terminal cost
+ *                                              (engine.cpp:131-141); PR-MPPI: running +
+ *                                              terminal + safety weight if unsafe, on the
+ *                                              predicted states (the engine prints these,
+ *                                              evaluated on the current state, 221-222). */
+#define DR_PREDICT_RECORD 5
+/* MPPI (engine.cpp:73-166): from `state` (the state after the step) and `belief`, under
+ * every hypothesis, the controller's plan as the engine holds it (the chosen plan with the
+ * warm-start shift of the sent branch), belief update and branching on. Host buffers. */
+int dr_mppi_predict(dr_mppi* h, const dr_sim_state* state, const float* belief, float* positions, float* actions, int32_t* records, float* costs);
+/* The same for every controller of a batch stepped on the device (dr_mppi_batch_step_device,
+ * which leaves each controller's pending shift in the batch's device records), from device
+ * states and beliefs (DR_MAX_THETA per controller) into device outputs: controller i's rows
+ * start at row i * n_theta, each of t_stride steps (at least every controller's horizon).
+ * Enqueued on the batch's stream. DR_ERR_STATE before the first device step. */
+int dr_mppi_batch_predict_device(dr_mppi_batch* b, const void* states_dev, const float* beliefs_dev, float* positions_dev, float* actions_dev,
+                                 int32_t* records_dev, float* costs_dev, int t_stride);
+/* PR-MPPI (engine.cpp:167-240): from `prev_state` (the state before the step), the new
+ * nominal plan under every hypothesis and the robust plan under the last one. */
+int dr_prmppi_predict(dr_prmppi* h, const dr_sim_state* prev_state, float* positions, float* actions, int32_t* records, float* costs);
 
 /* ---- allocation-free rollout ------------------------------------------------------
  * No counterpart in the reference: an entry point for callers that cannot call

@@ -37,8 +37,13 @@ def small_mppi(use_splines: bool, K=512, T=40, M=10, n_verif=1024, seed=7, noise
     return sc
 
 
-def mppi_ctl(sc, nominal=None):
-    return drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed, nominal=nominal)
+def mppi_ctl(sc, nominal=None, exact_verify=False):
+    """exact_verify: the verification's exact flavour, whose per-sample results equal the
+    oracle's (tests that compare a step's plan choice or failure counts with the oracle)."""
+    ctl = drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed, nominal=nominal)
+    if exact_verify:
+        ctl.set_verify_exact(True)
+    return ctl
 
 
 def random_nominal(sc, rng, scale=0.8):

@@ -39,7 +39,7 @@ def test_longest_horizon_most_knots_ragged_tiles(gpu, spl):
     frac, bfrac = _rollout_agreement(sc, ctl, spl)
     print(f"spl={spl}: rollout agreement {frac:.4f}, branch bookkeeping {bfrac:.4f}")
     assert frac >= 0.97 and bfrac >= 0.97
-    ctl2 = mppi_ctl(sc, nominal=nominal)
+    ctl2 = mppi_ctl(sc, nominal=nominal, exact_verify=True)
     ctl2.engine = object()
     ref = OracleMPPI(sc, nominal=nominal)
     a = ctl2.getControl(sc.state)
@@ -53,7 +53,7 @@ def test_single_sample_single_verification_sample(gpu):
     ctl = mppi_ctl(sc)
     frac, _ = _rollout_agreement(sc, ctl, False)
     assert frac == 1.0
-    ctl2 = mppi_ctl(sc)
+    ctl2 = mppi_ctl(sc, exact_verify=True)
     ctl2.engine = object()
     ref = OracleMPPI(sc)
     for _ in range(3):

@@ -144,7 +144,7 @@ def test_rollout_matches_oracle_with_env_noise(gpu, spl):
 def test_verification_matches_oracle(gpu):
     sc = small_mppi(False, K=256, T=40, n_verif=4096, noise=True)
     rng = np.random.default_rng(4)
-    ctl = mppi_ctl(sc)
+    ctl = mppi_ctl(sc, exact_verify=True)
     plan = random_nominal(sc, rng, 1.0)
     belief = sc.belief()
     fc = np.zeros(sc.mppi.n_timesteps, np.uint32)
@@ -167,7 +167,7 @@ def test_full_steps_match_oracle(gpu):
     sc = small_mppi(True, K=1024, T=40, n_verif=2048, noise=True)
     rng = np.random.default_rng(5)
     nominal = random_nominal(sc, rng, 0.3)
-    ctl = mppi_ctl(sc, nominal=nominal)
+    ctl = mppi_ctl(sc, nominal=nominal, exact_verify=True)
     ctl.engine = object()
     ref = OracleMPPI(sc, nominal=nominal)
     belief = sc.belief()
