@@ -947,6 +947,217 @@ def run_ours_races(args) -> None:
         dist.destroy_process_group()
 
 
+def run_ours_mixed(args) -> None:
+    """--workload races: the batched uneven workload of mixed controller kinds
+    (scenarios.mixed_races: 256 races of U{1..8} agents, plain MPPI, gradient-refined MPPI
+    and PR-MPPI with B in {2, 4, 8}). Controllers of one kind and compile-time shape share a
+    batch (MPPI: plain and gradient-refined together, one batch per control mode; PR-MPPI:
+    one batch per B), each batch on its own stream, all stepped from device-resident inputs;
+    one control step = every agent of every race advanced once. Reported: aggregate agent
+    control steps/s and rollout-steps/s (steps pipelined), and the per-agent control-step
+    latency (p50 / p99 over agents x steps of the time from a step's start, all batches
+    launched together, to the end of the agent's batch)."""
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    drb = _package()
+    import drone_race_b200.controllers as ctl_mod
+
+    abi = drb.abi
+    scs = drb.scenarios.mixed_races(N_RACES, seed=rank, n_verif=V_RACES)
+    groups = []
+    for spl in (False, True):
+        g = [s for s in scs if s.kind in ("plain", "grad") and bool(s.mppi.use_splines) == spl]
+        if g:
+            groups.append(("mppi", g))
+    for B in (2, 4, 8):
+        g = [s for s in scs if s.kind == "pr" and s.n_theta == B]
+        if g:
+            groups.append(("pr", g))
+    runs = []
+    for kind, g in groups:
+        stream = torch.cuda.Stream()
+        n = len(g)
+        states = [s.state for s in g]
+        st_dev = torch.frombuffer(bytearray(bytes((type(states[0]) * n)(*states))), dtype=torch.uint8).to("cuda")
+        bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+        for i, s in enumerate(g):
+            bel[i, : s.n_theta] = s.belief()
+        r = {"kind": kind, "stream": stream, "scs": g, "st": st_dev, "bel": torch.from_numpy(bel).to("cuda")}
+        if kind == "mppi":
+            ctls = [ctl_mod.MPPIController(s.env, s.mppi, s.seed, device=local, stream=stream.cuda_stream) for s in g]
+            for c, s in zip(ctls, g):
+                if s.kind == "grad":
+                    c.set_grad_refine(GRAD_STEPS, GRAD_STEP_SIZE, 0)
+            r["batch"] = ctl_mod.MPPIBatch(ctls, stream=stream.cuda_stream)
+            r["act"] = torch.zeros((n, 2), dtype=torch.float32, device="cuda")
+            r["info"] = torch.zeros(C.sizeof(abi.dr_mppi_info) * n, dtype=torch.uint8, device="cuda")
+        else:
+            ctls = [ctl_mod.PRMPPIController(s.env, s.prmppi, s.seed, device=local, stream=stream.cuda_stream) for s in g]
+            r["batch"] = ctl_mod.PRMPPIBatch(ctls, stream=stream.cuda_stream)
+        r["ctls"] = ctls
+        runs.append(r)
+    torch.cuda.synchronize()
+    n_agents = len(scs)
+
+    def run_step(r):
+        if r["kind"] == "mppi":
+            r["batch"].step_device(r["st"].data_ptr(), r["bel"].data_ptr(), r["act"].data_ptr(), r["info"].data_ptr())
+        else:
+            r["batch"].step_dev(r["st"].data_ptr(), r["bel"].data_ptr())
+
+    def dev_step():
+        for r in runs:
+            run_step(r)
+
+    s0 = runs[0]["stream"]
+
+    def timed(steps: int) -> float:
+        torch.cuda.synchronize()
+        _barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s0)
+        for r in runs[1:]:
+            r["stream"].wait_event(e0)
+        for _ in range(steps):
+            dev_step()
+        for r in runs[1:]:
+            ev = torch.cuda.Event()
+            ev.record(r["stream"])
+            s0.wait_event(ev)
+        e1.record(s0)
+        torch.cuda.synchronize()
+        _barrier(world)
+        return _max_over_ranks(e0.elapsed_time(e1), world)
+
+    for _ in range(10):
+        dev_step()
+    torch.cuda.synchronize()
+    tune = [r["batch"].autotune(5) if r["kind"] == "mppi" else None for r in runs]
+    for _ in range(max(args.warmup, 3)):
+        dev_step()
+    clocks = Clocks(local)
+    clocks.start()
+    ms = timed(args.steps)
+    clk = clocks.stop()
+    ms_per_step = ms / args.steps
+    # per-step latency: each step starts when the previous one has ended everywhere
+    lat_steps = max(5, min(30, args.steps))
+    marks = []
+    torch.cuda.synchronize()
+    for _ in range(lat_steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record(s0)
+        ends = []
+        for r in runs:
+            r["stream"].wait_event(e0)
+            run_step(r)
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(r["stream"])
+            ends.append(e)
+        for e in ends:
+            s0.wait_event(e)
+        marks.append((e0, ends))
+    torch.cuda.synchronize()
+    per_agent = []
+    step_ms = []
+    for e0, ends in marks:
+        t = [e0.elapsed_time(e) for e in ends]
+        step_ms.append(max(t))
+        for r, tr in zip(runs, t):
+            per_agent += [tr] * len(r["scs"])
+    per_agent = np.array(per_agent)
+    latency = {"p50_ms": float(np.percentile(per_agent, 50)), "p99_ms": float(np.percentile(per_agent, 99)), "max_ms": float(per_agent.max()),
+               "step_ms_median": float(np.median(step_ms)), "samples": int(per_agent.size),
+               "what": "per agent and step: from the step's start (all batches launched together) to the end of the agent's batch"}
+    # per-kernel device times
+    for r in runs:
+        r["batch"].set_profiling(True)
+    for _ in range(3):
+        dev_step()
+    torch.cuda.synchronize()
+    kts = [r["batch"].kernel_times() for r in runs]
+    for r in runs:
+        r["batch"].set_profiling(False)
+    # end to end through the C ABI with host buffers, one batch after the other
+    e2e = None
+    if not args.quick:
+        for r in runs:
+            for c in r["ctls"]:
+                c.engine = object()
+        host = [([s.state for s in r["scs"]], np.stack([s.belief() for s in r["scs"]])) for r in runs]
+        for _ in range(2):
+            for r, (st, be) in zip(runs, host):
+                r["batch"].step(st, be)
+        torch.cuda.synchronize()
+        e2e_steps = max(3, min(10, args.steps))
+        _barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for r, (st, be) in zip(runs, host):
+                r["batch"].step(st, be)
+        t1 = time.perf_counter()
+        _barrier(world)
+        e2e_s = _max_over_ranks(t1 - t0, world)
+        h2d = d2h = 0
+        for r in runs:
+            fn = abi.lib().dr_mppi_io_bytes if r["kind"] == "mppi" else abi.lib().dr_prmppi_io_bytes
+            for c in r["ctls"]:
+                a, b = C.c_size_t(), C.c_size_t()
+                fn(c.handle, C.byref(a), C.byref(b))
+                h2d += a.value
+                d2h += b.value
+        e2e = {"value": world * n_agents * e2e_steps / e2e_s, "unit": "agent control steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e2e_s / e2e_steps * 1e3}
+    mppi_scs = [s for s in scs if s.kind != "pr"]
+    pr_scs = [s for s in scs if s.kind == "pr"]
+    rollout_units = sum(s.mppi.n_samples * s.n_theta * s.mppi.n_timesteps for s in mppi_scs)
+    verify_units = sum(2 * V_RACES * min(40, s.mppi.n_timesteps) for s in mppi_scs)
+    pr_units = sum(2 * s.prmppi.P * s.prmppi.n_samples * s.prmppi.n_timesteps for s in pr_scs)
+    roof = None
+    if clk.get("sm_mhz"):
+        peak = 2 * 128 * 148 * clk["sm_mhz"] * 1e6 / 1e12
+        ach = (rollout_units * FLOPS_PER_ROLLOUT_STEP + verify_units * FLOPS_PER_VERIFY_STEP + pr_units * PR_FLOPS_PER_ROLLOUT_STEP) / (ms_per_step / 1e3) / 1e12
+        roof = {"bound": "fp32", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                "scope": "FP32 work of the MPPI rollouts and verifications and the PR-MPPI rollouts of one control step of every agent (dense-control "
+                         "FLOP counts; spline evaluation, updates, gradient refinement and candidate re-checks not counted) / device step time",
+                "peak_source": "FP32 FMA rate of 148 SMs x 128 lanes at the median SM clock sampled during the timed region"}
+    kinds = {k: sum(1 for s in scs if s.kind == k) for k in ("plain", "grad", "pr")}
+    line = {
+        "metric": "agent_control_steps_per_s",
+        "value": world * n_agents / (ms_per_step / 1e3),
+        "unit": f"agent control steps/s ({N_RACES} races, {n_agents} agents of uneven K/H and mixed kinds, every agent advanced once per step)",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uneven races of mixed controller kinds; no dataset)",
+        "config": {"workload": f"mixed_races_{N_RACES}", "agents": n_agents, "kinds": kinds,
+                   "pr_branches": {str(B): sum(1 for s in pr_scs if s.n_theta == B) for B in (2, 4, 8)},
+                   "K_total": sum(s.mppi.n_samples if s.mppi else s.prmppi.n_samples for s in scs),
+                   "H": sorted({(s.mppi or s.prmppi).n_timesteps for s in scs}), "verif_samples": V_RACES, "grad_steps": GRAD_STEPS,
+                   "batches": [f"{r['kind']}:{len(r['scs'])}" for r in runs], "parallelism": f"replicas x{world}",
+                   "l2": "working set per step > L2 (costs and plans of all agents)"},
+        "latency": latency,
+        "rollout_steps_per_s": world * (rollout_units + pr_units) / (ms_per_step / 1e3),
+        "kernel_ms": kts,
+        "autotune": [None if t is None else {k: t[k] for k in ("rollout_ctas_per_sm", "rollout_lockstep", "verify_ctas_per_sm", "grad_ckpt")} for t in tune],
+        "e2e": e2e,
+        "gpu_launches": sum(len(kt) for kt in kts) * args.steps,
+        "roofline": roof,
+        "cpu_baseline": None,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for r in runs:
+        r["batch"].close()
+        for c in r["ctls"]:
+            c.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
 def reference_cpu_step(scs, variant: str, threads: int, noises) -> float:
     """One control step of the 4-agent workload on the reference's own CPU path (its
     model functions in host loops, oracle/_ref, OpenMP over `threads`): per agent the
@@ -971,9 +1182,9 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    if WL["kind"] == "races":
+    if WL["kind"] in ("races", "races_mppi"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference steps one controller per getControl call and has no multi-race batch; "
-                                                              "its per-controller rate is the strat workload's reference arm"}), flush=True)
+                                                              "its per-controller rate is the strat and pr workloads' reference arm"}), flush=True)
         return
     if WL["kind"] == "grad":
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no gradient-refined MPPI; its plain MPPI arm is --workload strat"}),
@@ -1037,11 +1248,12 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e, no CPU baseline): for profiler runs")
     ap.add_argument("--no-overlap", action="store_true", help="run the previous plan's verification after the rollout instead of beside it")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="strat", choices=["strat", "gates", "grad", "pr", "races"],
+    ap.add_argument("--workload", default="strat", choices=["strat", "gates", "grad", "pr", "races", "races_mppi"],
                     help="strat: the strategic race (the headline workload); gates: the gate race (EnvDroneRace); "
                          "grad: gradient-refined MPPI at K=1024 with a closed-loop comparison against plain MPPI at K=4096; "
                          "pr: PR-MPPI, 4 agents x 8 hypotheses x K=2048; "
-                         "races: 256 independent races of uneven K/H in one batch per control mode")
+                         "races: 256 independent races of uneven K/H and mixed kinds (plain, gradient-refined and PR-MPPI); "
+                         "races_mppi: the same races with plain MPPI only, one batch per control mode")
     ap.add_argument("--side-verify", type=int, default=None,
                     help="CTAs per SM of the previous plan's verification beside the rollout (0: one per tile; default: the library's)")
     ap.add_argument("--pdl", action="store_true", help="programmatic dependent launches of the update and the new plan's verification")
@@ -1058,6 +1270,8 @@ def main():
     elif WL["kind"] == "pr":
         run_ours_pr(args)
     elif WL["kind"] == "races":
+        run_ours_mixed(args)
+    elif WL["kind"] == "races_mppi":
         run_ours_races(args)
     else:
         run_ours(args)

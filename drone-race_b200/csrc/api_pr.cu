@@ -141,6 +141,10 @@ struct dr_prmppi_batch
     int runs = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
+    // dr_prmppi_batch_step_dev: the device-input step as one graph, per (states, beliefs)
+    cudaGraph_t devGraph = nullptr;
+    cudaGraphExec_t devGraphExec = nullptr;
+    const void* devKey[2] = {nullptr, nullptr};
 
     LaunchArgs args(const Tile* tiles, int n, const PrIn* in) const
     {
@@ -279,8 +283,61 @@ struct dr_prmppi_batch
         return hs[0]->lastTimeouts ? timedOut(hs[0]->lastTimeouts) : DR_OK;
     }
 
+    void dropDevGraph()
+    {
+        if (devGraphExec)
+            cudaGraphExecDestroy(devGraphExec);
+        if (devGraph)
+            cudaGraphDestroy(devGraph);
+        devGraphExec = nullptr;
+        devGraph = nullptr;
+    }
+
+    // The step from device-resident states and beliefs (dr_prmppi_batch_step_dev): the
+    // input records (filled on the host with the controllers' temperatures and step
+    // counters, which this step does not advance) and the per-controller state and belief
+    // copies, then the kernels; replayed from a graph unless profiling.
+    int stepDev(const dr_sim_state* states, const float* beliefs)
+    {
+        const int n = (int)hs.size();
+        CK(cudaSetDevice(device));
+        std::vector<float> zero(DR_MAX_THETA, 0.0f);
+        for (int i = 0; i < n; i++)
+            hIn[i] = hs[i]->input(dr_sim_state{}, zero.data());
+        auto body = [&](bool profile) -> int {
+            CK(cudaMemcpyAsync(dIn, hIn, sizeof(PrIn) * n, cudaMemcpyHostToDevice, stream));
+            for (int i = 0; i < n; i++)
+            {
+                CK(cudaMemcpyAsync(&dIn[i].state, states + i, sizeof(dr_sim_state), cudaMemcpyDeviceToDevice, stream));
+                CK(cudaMemcpyAsync(&dIn[i].belief, beliefs + (size_t)i * DR_MAX_THETA, DR_MAX_THETA * 4, cudaMemcpyDeviceToDevice, stream));
+            }
+            return launchAll(dIn, profile, &timer);
+        };
+        if (profiling || !useGraph)
+            return body(profiling);
+        const void* key[2] = {states, beliefs};
+        if (devGraphExec && std::memcmp(key, devKey, sizeof(key)) != 0)
+            dropDevGraph();
+        if (!devGraphExec)
+        {
+            CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            int rc = body(false);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(stream, &g);
+            if (rc)
+                return rc;
+            CK(e);
+            devGraph = g;
+            CK(cudaGraphInstantiate(&devGraphExec, devGraph, 0));
+            std::memcpy(devKey, key, sizeof(key));
+        }
+        CK(cudaGraphLaunch(devGraphExec, stream));
+        return DR_OK;
+    }
+
     void release()
     {
+        dropDevGraph();
         if (graphExec)
             cudaGraphExecDestroy(graphExec);
         if (graph)
@@ -733,18 +790,7 @@ int dr_prmppi_batch_step_dev(dr_prmppi_batch* b, const dr_sim_state* states_dev,
 {
     if (!b || !states_dev || !beliefs_dev)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
-    CK(cudaSetDevice(b->device));
-    const int n = (int)b->hs.size();
-    std::vector<float> zero(DR_MAX_THETA, 0.0f);
-    for (int i = 0; i < n; i++)
-        b->hIn[i] = b->hs[i]->input(dr_sim_state{}, zero.data());
-    CK(cudaMemcpyAsync(b->dIn, b->hIn, sizeof(PrIn) * n, cudaMemcpyHostToDevice, b->stream));
-    for (int i = 0; i < n; i++)
-    {
-        CK(cudaMemcpyAsync(&b->dIn[i].state, states_dev + i, sizeof(dr_sim_state), cudaMemcpyDeviceToDevice, b->stream));
-        CK(cudaMemcpyAsync(&b->dIn[i].belief, beliefs_dev + (size_t)i * DR_MAX_THETA, DR_MAX_THETA * 4, cudaMemcpyDeviceToDevice, b->stream));
-    }
-    return b->launchAll(b->dIn, b->profiling, &b->timer);
+    return b->stepDev(states_dev, beliefs_dev);
 }
 
 int dr_prmppi_debug_noise(dr_prmppi* h, const float* belief, float* noise, size_t n, int32_t* thetas)

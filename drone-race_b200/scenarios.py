@@ -47,6 +47,8 @@ class Scenario:
     seed: int = 42
     name: str = ""
     keep: list = field(default_factory=list)
+    # controller kind in a mixed batch: "plain" MPPI, "grad" (gradient-refined MPPI) or "pr"
+    kind: str = "plain"
 
     @property
     def n_theta(self) -> int:
@@ -290,12 +292,44 @@ def uneven_races(n_races: int = 256, seed: int = 0, n_verif: int = 4096) -> list
     return out
 
 
-def robust_race(agent: int = 0, seed: int = 0, K: int = 2048, T: int = 64, P: int = 8, n_theta: int = 8) -> Scenario:
+def mixed_races(n_races: int = 256, seed: int = 0, n_verif: int = 4096) -> list[Scenario]:
+    """The batched uneven workload of many independent races of mixed controller kinds, one
+    scenario per agent: per race U{1..8} agents on a track through U{6..16} control points
+    jittered around a 40 m circle and one kind (`Scenario.kind`): plain MPPI (about half the
+    races, dense or spline controls alternating), gradient-refined MPPI (about a quarter: one
+    projected gradient step after each update) or PR-MPPI with B in {2, 4, 8} belief
+    branches (about a quarter: B opponent hypotheses under a Dirichlet(1) belief, P = B
+    sampled hypotheses). Per agent K log-uniform in [256, 16384] and H in {32, 48, 64, 96};
+    MPPI verification of n_verif samples over min(40, H) steps."""
+    rng = np.random.default_rng(60_000 + seed)
+    out = []
+    for race in range(n_races):
+        n_agents = int(rng.integers(1, 9))
+        n_points = int(rng.integers(6, 17))
+        u = float(rng.uniform())
+        kind = "plain" if u < 0.5 else ("grad" if u < 0.75 else "pr")
+        B = int(rng.choice([2, 4, 8]))
+        spl = bool(race % 2)
+        for a in range(n_agents):
+            K = int(round(float(np.exp(rng.uniform(np.log(256), np.log(16384))))))
+            T = int(rng.choice([32, 48, 64, 96]))
+            if kind == "pr":
+                sc = robust_race(agent=a, seed=seed * 100_000 + race, K=K, T=T, P=B, n_theta=B, n_points=n_points)
+            else:
+                sc = circle_race(agent=a, seed=seed * 100_000 + race, K=K, T=T, use_splines=spl, n_verif=n_verif, n_points=n_points)
+            sc.kind = kind
+            sc.name = f"race{race}/agent{a}"
+            out.append(sc)
+    return out
+
+
+def robust_race(agent: int = 0, seed: int = 0, K: int = 2048, T: int = 64, P: int = 8, n_theta: int = 8, n_points: int = 12) -> Scenario:
     """Per-agent PR-MPPI workload: n_theta opponent hypotheses (speed scale U(0.8,1.2),
-    lateral aggressiveness s1 U(0,2) m), belief ~ Dirichlet(1), P sampled hypotheses."""
+    lateral aggressiveness s1 U(0,2) m), belief ~ Dirichlet(1), P sampled hypotheses, on a
+    track through n_points control points jittered around a 40 m circle."""
     r = 0.5
     rng = np.random.default_rng(10_000 + seed * 100 + agent)
-    grids = track_grids(catmull_rom_closed(jittered_circle_points(seed, 12)))
+    grids = _circle_grids(seed, n_points)
     presets = []
     for th in range(n_theta):
         presets.append(opp_preset(r, s1=float(rng.uniform(0, 2)), s3="default" if th % 2 == 0 else "no-block", speed_scale=float(rng.uniform(0.8, 1.2))))
