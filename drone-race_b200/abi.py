@@ -307,9 +307,9 @@ _PROTOS = {
     "dr_mppi_batch_set_side_verify": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_batch_set_pdl": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_prmppi_set_shard": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dr_prmppi_shard_words": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "dr_prmppi_shard_begin": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
-    "dr_prmppi_shard_sums": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
-    "dr_prmppi_shard_finish": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dr_prmppi_shard_finish": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "dr_mppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "dr_prmppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_prmppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
@@ -349,9 +349,9 @@ _PROTOS = {
                                        C.c_void_p, C.c_int, C.c_void_p]),
     "dr_mppi_set_grad_refine": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_int]),
     "dr_mppi_set_shard": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dr_mppi_shard_words": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "dr_mppi_shard_begin": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_void_p]),
-    "dr_mppi_shard_sums": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
-    "dr_mppi_shard_update": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dr_mppi_shard_update": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "dr_mppi_shard_finish": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_mppi_info)]),
     "dr_mppi_batch_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dr_mppi_batch_env_step_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint64, C.c_void_p]),

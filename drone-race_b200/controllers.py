@@ -21,7 +21,6 @@ def _state(s, gate: bool = False):
     raise TypeError(f"state must be a {want.__name__}")
 
 
-
 def _predict(call, rows: int, T: int, n_agents: int, what: str) -> dict:
     """Runs a prediction entry point into fresh host arrays (layout of include/drmppi.h)."""
     pos = np.zeros((rows, T, n_agents * 2), np.float32)
@@ -31,6 +30,7 @@ def _predict(call, rows: int, T: int, n_agents: int, what: str) -> dict:
     check(call(pos, act, rec, cost), what)
     return dict(positions=pos, actions=act, init_branch=rec[:, 0].copy(), branching_time=rec[:, 1].copy(), branch=rec[:, 2].copy(),
                 stop_reason=rec[:, 3].copy(), stop_time=rec[:, 4].copy(), cost=cost)
+
 
 class Controller:
     """include/controllers.h:12-21."""
@@ -257,92 +257,113 @@ def _kernel_times(fn, h) -> dict[str, float]:
     return {names[i].decode(): float(ms[i]) for i in range(cnt.value)}
 
 
-class ShardedMPPIController(MPPIController):
+class _Sharded:
+    """The exchange of a sample-sharded controller: its partial results gathered from
+    every process of a torch.distributed group, on the controller's own stream (a torch
+    stream handed to the library), so the library's kernels, the collectives and the next
+    kernels run in order with no host synchronisation until the step's tail. With NCCL the
+    tensors stay on the device; with gloo they travel through host memory."""
+
+    def _setup(self, words: int, device: int, group):
+        import torch
+
+        self.group = group
+        dev = torch.device("cuda", device)
+        self._partial = torch.empty(words, dtype=torch.float32, device=dev)
+        self._gathered = None
+        self._words = words
+
+    def _all_gather(self):
+        import torch
+        import torch.distributed as dist
+
+        world = dist.get_world_size(self.group)
+        with torch.cuda.stream(self._tstream):
+            if self._gathered is None:
+                self._gathered = torch.empty(world * self._words, dtype=torch.float32, device=self._partial.device)
+            if dist.get_backend(self.group) == "gloo":
+                parts = [torch.empty(self._words, dtype=torch.float32) for _ in range(world)]
+                dist.all_gather(parts, self._partial.cpu(), group=self.group)
+                self._gathered.copy_(torch.cat(parts))
+            else:
+                dist.all_gather_into_tensor(self._gathered, self._partial, group=self.group)
+        return world
+
+    def _all_reduce_sum(self, t):
+        import torch
+        import torch.distributed as dist
+
+        with torch.cuda.stream(self._tstream):
+            if dist.get_backend(self.group) == "gloo":
+                x = t.cpu()
+                dist.all_reduce(x, op=dist.ReduceOp.SUM, group=self.group)
+                t.copy_(x)
+            else:
+                dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+
+
+class ShardedMPPIController(_Sharded, MPPIController):
     """One MPPI controller whose samples are split across the processes of a
     torch.distributed group (one process per GPU): this process rolls out and verifies its
-    share, and the partial minima, weighted sums and failure histograms are combined with
-    three all-reduces per step (dr_mppi_set_shard / dr_mppi_shard_*). With the gloo
-    backend the partials travel through host memory; with NCCL they stay on the device."""
+    share; one all-gather of the partial minima, weighted sums and previous-plan failure
+    histograms and one all-reduce of the new plan's histograms per step
+    (dr_mppi_set_shard / dr_mppi_shard_*)."""
 
     def __init__(self, env, cfg: abi.dr_mppi_config, seed: int, rank: int, world: int, group=None, nominal: np.ndarray | None = None,
                  device: int = 0):
         import torch
 
-        super().__init__(env, cfg, seed, nominal=nominal, device=device)
+        self._tstream = torch.cuda.Stream(device=device)
+        super().__init__(env, cfg, seed, nominal=nominal, device=device, stream=self._tstream.cuda_stream)
         check(lib().dr_mppi_set_shard(self._h, int(rank), int(world)), "dr_mppi_set_shard")
-        self.group = group
-        M = int(cfg.n_knots) if cfg.use_splines else self.T
-        dev = torch.device("cuda", device)
-        self._mins = torch.empty(self.nbp * M, dtype=torch.float32, device=dev)
-        self._sums = torch.empty(self.nbp * M * 3, dtype=torch.float32, device=dev)
-        self._hist = torch.empty(2 * self.T, dtype=torch.int32, device=dev)
-
-    def _all_reduce(self, t, op) -> None:
-        import torch
-        import torch.distributed as dist
-
-        if dist.get_backend(self.group) == "gloo":
-            x = t.cpu()
-            dist.all_reduce(x, op=op, group=self.group)
-            t.copy_(x)
-        else:
-            dist.all_reduce(t, op=op, group=self.group)
-        torch.cuda.current_stream(t.device).synchronize()
+        n = C.c_size_t()
+        check(lib().dr_mppi_shard_words(self._h, C.byref(n)), "dr_mppi_shard_words")
+        self._setup(int(n.value), device, group)
+        self._hist = torch.empty(self.T, dtype=torch.int32, device=torch.device("cuda", device))
 
     def getControl(self, state) -> np.ndarray:  # noqa: N802
-        import torch.distributed as dist
-
         if self.engine is None:
             raise RuntimeError("MPPI: engine not set")
         P = lambda t: C.c_void_p(t.data_ptr())
         bel = abi.fptr(self.h_belief)
         st = C.byref(_state(state, False))
-        check(lib().dr_mppi_shard_begin(self._h, st, bel, P(self._mins)), "dr_mppi_shard_begin")
-        self._all_reduce(self._mins, dist.ReduceOp.MIN)
-        check(lib().dr_mppi_shard_sums(self._h, P(self._mins), P(self._sums)), "dr_mppi_shard_sums")
-        self._all_reduce(self._sums, dist.ReduceOp.SUM)
-        check(lib().dr_mppi_shard_update(self._h, P(self._mins), P(self._sums), P(self._hist)), "dr_mppi_shard_update")
-        self._all_reduce(self._hist, dist.ReduceOp.SUM)
+        check(lib().dr_mppi_shard_begin(self._h, st, bel, P(self._partial)), "dr_mppi_shard_begin")
+        world = self._all_gather()
+        check(lib().dr_mppi_shard_update(self._h, P(self._gathered), world, P(self._hist)), "dr_mppi_shard_update")
+        self._all_reduce_sum(self._hist)
         out = np.zeros(2, np.float32)
         check(lib().dr_mppi_shard_finish(self._h, P(self._hist), bel, abi.fptr(out), C.byref(self.info)), "dr_mppi_shard_finish")
         self._pull()
         return out
 
 
-class ShardedPRMPPIController(PRMPPIController):
+class ShardedPRMPPIController(_Sharded, PRMPPIController):
     """One PR-MPPI controller whose samples are split across the processes of a
     torch.distributed group: this process rolls out its share of the samples under every
-    hypothesis, and the three minima and the weighted sums are combined with two
-    all-reduces per step (dr_prmppi_set_shard / dr_prmppi_shard_*); the candidates'
-    re-check runs on every process."""
+    hypothesis; one all-gather of the partial minima and weighted sums per step
+    (dr_prmppi_set_shard / dr_prmppi_shard_*); the candidates' re-check runs on every
+    process."""
 
     def __init__(self, env, cfg: abi.dr_prmppi_config, seed: int, rank: int, world: int, group=None, nominal: np.ndarray | None = None,
                  device: int = 0):
         import torch
 
-        super().__init__(env, cfg, seed, nominal=nominal, device=device)
+        self._tstream = torch.cuda.Stream(device=device)
+        super().__init__(env, cfg, seed, nominal=nominal, device=device, stream=self._tstream.cuda_stream)
         check(lib().dr_prmppi_set_shard(self._h, int(rank), int(world)), "dr_prmppi_set_shard")
-        self.group = group
-        dev = torch.device("cuda", device)
-        self._mins = torch.empty(3, dtype=torch.float32, device=dev)
-        self._sums = torch.empty(3 * self.T * 3, dtype=torch.float32, device=dev)
-
-    _all_reduce = ShardedMPPIController._all_reduce
+        n = C.c_size_t()
+        check(lib().dr_prmppi_shard_words(self._h, C.byref(n)), "dr_prmppi_shard_words")
+        self._setup(int(n.value), device, group)
 
     def getControl(self, state) -> np.ndarray:  # noqa: N802
-        import torch.distributed as dist
-
         if self.engine is None:
             raise RuntimeError("PRMPPI: engine not set")
         P = lambda t: C.c_void_p(t.data_ptr())
-        check(lib().dr_prmppi_shard_begin(self._h, C.byref(_state(state)), abi.fptr(self.h_belief), P(self._mins)), "dr_prmppi_shard_begin")
-        self._all_reduce(self._mins, dist.ReduceOp.MIN)
-        check(lib().dr_prmppi_shard_sums(self._h, P(self._mins), P(self._sums)), "dr_prmppi_shard_sums")
-        self._all_reduce(self._sums, dist.ReduceOp.SUM)
+        check(lib().dr_prmppi_shard_begin(self._h, C.byref(_state(state)), abi.fptr(self.h_belief), P(self._partial)), "dr_prmppi_shard_begin")
+        world = self._all_gather()
         out = np.zeros(2, np.float32)
-        check(lib().dr_prmppi_shard_finish(self._h, P(self._mins), P(self._sums), abi.fptr(out), C.byref(self.info)), "dr_prmppi_shard_finish")
+        check(lib().dr_prmppi_shard_finish(self._h, P(self._gathered), world, abi.fptr(out), C.byref(self.info)), "dr_prmppi_shard_finish")
         return out
-
 
 class MPPIBatch:
     """Several MPPI controllers (one per agent) advanced by one launch sequence."""

@@ -486,45 +486,54 @@ struct dr_mppi_batch
     }
 
     // ---- sample-sharded step of a batch of one (dr_mppi_shard_*) ----
-    int shardBegin(const MppiIn& hin, float* mins)
+    // The phases only enqueue work on the stream; the caller's collectives order after
+    // them on the same stream, and only the tail synchronises.
+    DevScratch shardBuf; // merged minima and sums of the update
+
+    int shardWords() const
+    {
+        const dr_mppi* h = hs[0];
+        return h->nbp * h->M * 4 + h->T;
+    }
+
+    int shardBegin(const MppiIn& hin, float* partial)
     {
         CK(cudaSetDevice(device));
+        dr_mppi* h = hs[0];
         hIn[0] = hin;
         CK(cudaMemcpyAsync(dIn, hIn, sizeof(MppiIn), cudaMemcpyHostToDevice, stream));
         CK(launchMppiPrologue(args(nullptr, 0, dIn), 1, proSmem));
         if (verify && nVerOld > 0)
             CK(launchVerify(args(dVerOld, nVerOld, dIn)));
         CK(launchRollout(args(dRoll, nRoll, dIn)));
-        CK(launchShardMin(args(dUpd, nUpd, dIn), nth, mins));
-        CK(cudaStreamSynchronize(stream));
+        CK(launchShardLocal(args(dUpd, nUpd, dIn), nth, partial));
+        // the previous plan's failure histogram of this process's verification samples
+        CK(cudaMemcpyAsync(partial + (size_t)h->nbp * h->M * 4, h->desc.fail + h->T, sizeof(uint32_t) * h->T, cudaMemcpyDeviceToDevice, stream));
         return DR_OK;
     }
 
-    int shardSums(const float* mins, float* sums)
+    int shardUpdate(const float* gathered, int world, uint32_t* hist)
     {
         CK(cudaSetDevice(device));
-        CK(launchShardSums(args(dUpd, nUpd, dIn), nth, mins, sums));
-        CK(cudaStreamSynchronize(stream));
-        return DR_OK;
-    }
-
-    int shardUpdate(const float* mins, const float* sums, uint32_t* hist)
-    {
-        CK(cudaSetDevice(device));
+        dr_mppi* h = hs[0];
+        const size_t nv = (size_t)h->nbp * h->M;
+        CK(shardBuf.reserve(nv * 4 * sizeof(float)));
+        float* mins = (float*)shardBuf.p;
+        float* sums = mins + nv;
+        CK(launchShardMerge(stream, dDesc, dIn, gathered, shardWords(), world, mins, sums));
         CK(launchShardApply(stream, dDesc, 1, nth, mins, sums));
         if (nGrad > 0)
             CK(launchGradNominal(stream, dGrad, nGrad, nopp, nth, spl, gradSmemB));
         if (verify && nVerNew > 0)
             CK(launchVerify(args(dVerNew, nVerNew, dIn)));
-        CK(cudaMemcpyAsync(hist, hs[0]->desc.fail, sizeof(uint32_t) * 2 * hs[0]->T, cudaMemcpyDeviceToDevice, stream));
-        CK(cudaStreamSynchronize(stream));
+        CK(cudaMemcpyAsync(hist, h->desc.fail, sizeof(uint32_t) * h->T, cudaMemcpyDeviceToDevice, stream));
         return DR_OK;
     }
 
     int shardFinish(const uint32_t* hist, const float* belief, float* action, dr_mppi_info* info)
     {
         CK(cudaSetDevice(device));
-        CK(cudaMemcpyAsync(hs[0]->desc.fail, hist, sizeof(uint32_t) * 2 * hs[0]->T, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(hs[0]->desc.fail, hist, sizeof(uint32_t) * hs[0]->T, cudaMemcpyDeviceToDevice, stream));
         int rc = copyResults();
         if (rc)
             return rc;
@@ -687,6 +696,7 @@ struct dr_mppi_batch
     {
         dropGraph();
         dropDevGraph();
+        shardBuf.release();
         cudaFree(dGrad);
         dGrad = nullptr;
         cudaFree(dDesc);
@@ -1259,27 +1269,30 @@ int dr_mppi_set_shard(dr_mppi* h, int rank, int world)
     return buildMppiBatch(&raw, 1, h->stream, false, &h->self);
 }
 
-int dr_mppi_shard_begin(dr_mppi* h, const dr_sim_state* state, const float* belief, float* mins_dev)
+int dr_mppi_shard_words(const dr_mppi* h, size_t* words)
 {
-    if (!h || !state || !belief || !mins_dev)
+    if (!h || !words)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    *words = (size_t)h->self->shardWords();
+    return DR_OK;
+}
+
+int dr_mppi_shard_begin(dr_mppi* h, const dr_sim_state* state, const float* belief, float* partial_dev)
+{
+    if (!h || !state || !belief || !partial_dev)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
     if (h->envKind != 0)
         return fail(DR_ERR_UNSUPPORTED, "sample sharding is built for the strategic race");
-    return h->self->shardBegin(h->input(*state, belief), mins_dev);
+    return h->self->shardBegin(h->input(*state, belief), partial_dev);
 }
 
-int dr_mppi_shard_sums(dr_mppi* h, const float* mins_dev, float* sums_dev)
+int dr_mppi_shard_update(dr_mppi* h, const float* gathered_dev, int world, uint32_t* hist_dev)
 {
-    if (!h || !mins_dev || !sums_dev)
+    if (!h || !gathered_dev || !hist_dev)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
-    return h->self->shardSums(mins_dev, sums_dev);
-}
-
-int dr_mppi_shard_update(dr_mppi* h, const float* mins_dev, const float* sums_dev, uint32_t* hist_dev)
-{
-    if (!h || !mins_dev || !sums_dev || !hist_dev)
-        return fail(DR_ERR_INVALID_ARG, "NULL argument");
-    return h->self->shardUpdate(mins_dev, sums_dev, hist_dev);
+    if (world != h->shardWorld)
+        return fail(DR_ERR_INVALID_ARG, "world differs from dr_mppi_set_shard's");
+    return h->self->shardUpdate(gathered_dev, world, hist_dev);
 }
 
 int dr_mppi_shard_finish(dr_mppi* h, const uint32_t* hist_dev, const float* belief, float* out_action, dr_mppi_info* info)

@@ -250,29 +250,33 @@ struct dr_prmppi_batch
     }
 
     // ---- sample-sharded step of a batch of one (dr_prmppi_shard_*) ----
-    int shardBegin(const PrIn& hin, float* mins)
+    // Begin only enqueues work; the caller's all-gather follows on the same stream.
+    DevScratch shardBuf; // merged minima and sums
+
+    int shardWords() const
+    {
+        return 3 + 9 * hs[0]->T;
+    }
+
+    int shardBegin(const PrIn& hin, float* partial)
     {
         CK(cudaSetDevice(device));
         hIn[0] = hin;
         CK(cudaMemcpyAsync(dIn, hIn, sizeof(PrIn), cudaMemcpyHostToDevice, stream));
         CK(launchPrPrologue(args(nullptr, 0, dIn), 1));
         CK(launchPrRollout(args(dRoll, nRoll, dIn), nopp, nth, rollSmem));
-        CK(launchPrShardMin(stream, dDesc, mins));
-        CK(cudaStreamSynchronize(stream));
+        CK(launchPrShardMin(stream, dDesc, partial));
+        CK(launchPrShardSums(stream, dDesc, dIn, hs[0]->T, partial, partial + 3));
         return DR_OK;
     }
 
-    int shardSums(const float* mins, float* sums)
+    int shardFinish(const float* gathered, int world, float* action, dr_prmppi_info* info)
     {
         CK(cudaSetDevice(device));
-        CK(launchPrShardSums(stream, dDesc, dIn, hs[0]->T, mins, sums));
-        CK(cudaStreamSynchronize(stream));
-        return DR_OK;
-    }
-
-    int shardFinish(const float* mins, const float* sums, float* action, dr_prmppi_info* info)
-    {
-        CK(cudaSetDevice(device));
+        CK(shardBuf.reserve((size_t)shardWords() * sizeof(float)));
+        float* mins = (float*)shardBuf.p;
+        float* sums = mins + 3;
+        CK(launchPrShardMerge(stream, dDesc, dIn, gathered, shardWords(), world, mins, sums));
         CK(launchPrShardApply(stream, dDesc, mins, sums));
         CK(launchPrCandidates(args(nullptr, 0, dIn), nopp, nth, 1, maxT, 0));
         int rc = copyResults();
@@ -338,6 +342,7 @@ struct dr_prmppi_batch
     void release()
     {
         dropDevGraph();
+        shardBuf.release();
         if (graphExec)
             cudaGraphExecDestroy(graphExec);
         if (graph)
@@ -678,25 +683,28 @@ int dr_prmppi_set_shard(dr_prmppi* h, int rank, int world)
     return buildPrBatch(&raw, 1, h->stream, false, &h->self);
 }
 
-int dr_prmppi_shard_begin(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* mins_dev)
+int dr_prmppi_shard_words(const dr_prmppi* h, size_t* words)
 {
-    if (!h || !state || !belief || !mins_dev)
+    if (!h || !words)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
-    return h->self->shardBegin(h->input(*state, belief), mins_dev);
+    *words = (size_t)h->self->shardWords();
+    return DR_OK;
 }
 
-int dr_prmppi_shard_sums(dr_prmppi* h, const float* mins_dev, float* sums_dev)
+int dr_prmppi_shard_begin(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* partial_dev)
 {
-    if (!h || !mins_dev || !sums_dev)
+    if (!h || !state || !belief || !partial_dev)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
-    return h->self->shardSums(mins_dev, sums_dev);
+    return h->self->shardBegin(h->input(*state, belief), partial_dev);
 }
 
-int dr_prmppi_shard_finish(dr_prmppi* h, const float* mins_dev, const float* sums_dev, float* out_action, dr_prmppi_info* info)
+int dr_prmppi_shard_finish(dr_prmppi* h, const float* gathered_dev, int world, float* out_action, dr_prmppi_info* info)
 {
-    if (!h || !mins_dev || !sums_dev || !out_action)
+    if (!h || !gathered_dev || !out_action)
         return fail(DR_ERR_INVALID_ARG, "NULL argument");
-    return h->self->shardFinish(mins_dev, sums_dev, out_action, info);
+    if (world != h->shardWorld)
+        return fail(DR_ERR_INVALID_ARG, "world differs from dr_prmppi_set_shard's");
+    return h->self->shardFinish(gathered_dev, world, out_action, info);
 }
 
 int dr_prmppi_get_nominals(const dr_prmppi* h, float* nom, float* rob, size_t n)

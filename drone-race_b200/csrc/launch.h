@@ -56,8 +56,9 @@ cudaError_t launchMppiRollout(const LaunchArgs& a, int nopp, int nth, bool spl, 
 cudaError_t launchMppiUpdate(const LaunchArgs& a, int nth);
 cudaError_t launchMppiAggregate(const LaunchArgs& a, int nth, int K);
 // sample-sharded update phases (one controller's samples split across processes)
-cudaError_t launchShardMin(const LaunchArgs& a, int nth, float* mins);
-cudaError_t launchShardSums(const LaunchArgs& a, int nth, const float* mins, float* sums);
+cudaError_t launchShardLocal(const LaunchArgs& a, int nth, float* partial);
+cudaError_t launchShardMerge(cudaStream_t stream, const MppiDev* insts, const MppiIn* in, const float* gathered, int words, int world, float* mins,
+                             float* sums);
 cudaError_t launchShardApply(cudaStream_t stream, const MppiDev* insts, int nInst, int nth, const float* mins, const float* sums);
 cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem, int* dbgFailTime, int* dbgTheta);
 // CTAs per SM of the persistent rollout (verify = false) or verification kernel
@@ -109,6 +110,8 @@ cudaError_t launchGatePrCandidates(const LaunchArgs& a, int nth, int me, int nIn
 cudaError_t launchPrShardMin(cudaStream_t stream, const PrDev* insts, float* mins);
 cudaError_t launchPrShardSums(cudaStream_t stream, const PrDev* insts, const PrIn* in, int T, const float* mins, float* sums);
 cudaError_t launchPrShardApply(cudaStream_t stream, const PrDev* insts, const float* mins, const float* sums);
+cudaError_t launchPrShardMerge(cudaStream_t stream, const PrDev* insts, const PrIn* in, const float* gathered, int words, int world, float* mins,
+                               float* sums);
 
 // Device tail of the control step and the batch's true-dynamics step (finish_kernels.cu).
 cudaError_t launchMppiFinish(cudaStream_t stream, const MppiDev* insts, MppiIn* in, float* actions, dr_mppi_info* infos, int nInst);

@@ -609,15 +609,20 @@ template <int NTH> __global__ void __launch_bounds__(UB) mppi_update(const MppiD
 
 // ---------------------------------------------------------------------------------------
 // sample-sharded update: one controller's samples split across processes (one per GPU),
-// the partial results combined by the caller's collectives between the three phases
+// the processes' partial results exchanged once per step by the caller's all-gather
 // ---------------------------------------------------------------------------------------
-// phase 1: masked minimum over this process's samples [sLo, sHi) per (branch plan, knot)
-// (computeMaskedMinCostsKernel, kernels.cu:221-301); the caller takes the minimum over
-// the processes
-template <int NTH> __global__ void __launch_bounds__(UB) mppi_shard_min(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in,
-                                                                        const Tile* __restrict__ tiles, float* __restrict__ mins)
+// One exchange per step for a sample-sharded controller: this process's masked minimum
+// per (branch plan, knot) over its own samples and its weighted sums of the regenerated
+// perturbations taken with that local minimum, partial[(b, k)] = (m_r, sum w coeff eps0,
+// sum w coeff eps1, sum w coeff), w = exp(-(c - m_r) / lambda). The processes all-gather
+// the partials; mppi_shard_merge brings them to the global minimum m with the factor
+// exp(-(m_r - m) / lambda) (the weight of a sample relative to m is its weight relative to
+// m_r times that factor), so no second exchange is needed for the sums.
+template <int NTH> __global__ void __launch_bounds__(UB) mppi_shard_local(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in,
+                                                                          const Tile* __restrict__ tiles, float* __restrict__ partial)
 {
     __shared__ float sMin[UB / 32];
+    __shared__ float sNum0[UB], sNum1[UB], sDen[UB];
     const Tile tile = tiles[blockIdx.x];
     const MppiDev& D = insts[tile.inst];
     const MppiIn& I = in[tile.inst];
@@ -647,37 +652,10 @@ template <int NTH> __global__ void __launch_bounds__(UB) mppi_shard_min(const Mp
     if ((tid & 31) == 0)
         sMin[tid >> 5] = mn;
     __syncthreads();
-    if (tid == 0)
-    {
-        float minC = sMin[0];
+    float minC = sMin[0];
 #pragma unroll
-        for (int w = 1; w < UB / 32; w++)
-            minC = fminf(minC, sMin[w]);
-        mins[b * M + k] = minC;
-    }
-}
-
-// phase 2: this process's weighted sums of the regenerated perturbations with the
-// minimum over all processes (weightedAverageKernelUnified, kernels.cu:307-408):
-// sums[(b, k)] = (sum w coeff eps0, sum w coeff eps1, sum w coeff); the caller adds them up
-template <int NTH> __global__ void __launch_bounds__(UB) mppi_shard_sums(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in,
-                                                                         const Tile* __restrict__ tiles, const float* __restrict__ mins,
-                                                                         float* __restrict__ sums)
-{
-    __shared__ float sNum0[UB], sNum1[UB], sDen[UB];
-    const Tile tile = tiles[blockIdx.x];
-    const MppiDev& D = insts[tile.inst];
-    const MppiIn& I = in[tile.inst];
-    const int K = D.cfg.K, T = D.cfg.T, M = D.cfg.M, sLo = D.cfg.sLo, sHi = D.cfg.sHi;
-    const bool spl = D.cfg.useSplines != 0;
-    const int b = tile.s0 / M, k = tile.s0 % M;
-    const int tid = threadIdx.x;
-    float belief[NTH];
-#pragma unroll
-    for (int i = 0; i < NTH; i++)
-        belief[i] = I.belief[i];
-    const float* costs = D.costs + (size_t)b * K;
-    const float minC = mins[b * M + k];
+    for (int w = 1; w < UB / 32; w++)
+        minC = fminf(minC, sMin[w]);
     const float lambda = I.lambda;
     const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
     float num0 = 0.0f, num1 = 0.0f, den = 0.0f;
@@ -724,15 +702,58 @@ template <int NTH> __global__ void __launch_bounds__(UB) mppi_shard_sums(const M
         }
         if (tid == 0)
         {
-            float* o = sums + (size_t)(b * M + k) * 3;
-            o[0] = a0;
-            o[1] = a1;
-            o[2] = dd;
+            float* o = partial + (size_t)(b * M + k) * 4;
+            o[0] = minC;
+            o[1] = a0;
+            o[2] = a1;
+            o[3] = dd;
         }
     }
 }
 
-// phase 3: the update from the sums over all processes, then interpolateSplineKernel and
+// The partials of all processes (gathered[r * words + ...], rank order), merged the same
+// way on every process: the global minimum and the rescaled sums per (branch plan, knot)
+// into mins / sums (the layout mppi_shard_apply reads), and the previous plan's failure
+// histograms summed into the controller's fail[T .. 2T).
+__global__ void __launch_bounds__(UB) mppi_shard_merge(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const float* __restrict__ gathered,
+                                                       int words, int world, float* __restrict__ mins, float* __restrict__ sums)
+{
+    const MppiDev& D = insts[0];
+    const int T = D.cfg.T, M = D.cfg.M, nbp = D.cfg.nth + 1;
+    const float lambda = in[0].lambda;
+    for (int v = threadIdx.x; v < nbp * M; v += blockDim.x)
+    {
+        float m = INFINITY;
+        for (int r = 0; r < world; r++)
+            m = fminf(m, gathered[(size_t)r * words + v * 4]);
+        float a0 = 0.0f, a1 = 0.0f, dd = 0.0f;
+        if (!isinf(m))
+            for (int r = 0; r < world; r++)
+            {
+                const float* p = gathered + (size_t)r * words + v * 4;
+                if (isinf(p[0]))
+                    continue; // no sample of process r contributes
+                const float f = expf(-(p[0] - m) / lambda);
+                a0 += p[1] * f;
+                a1 += p[2] * f;
+                dd += p[3] * f;
+            }
+        mins[v] = m;
+        sums[v * 3] = a0;
+        sums[v * 3 + 1] = a1;
+        sums[v * 3 + 2] = dd;
+    }
+    const int hOff = nbp * M * 4;
+    for (int t = threadIdx.x; t < T; t += blockDim.x)
+    {
+        unsigned h = 0u;
+        for (int r = 0; r < world; r++)
+            h += __float_as_uint(gathered[(size_t)r * words + hOff + t]);
+        D.fail[T + t] = h;
+    }
+}
+
+// the update from the merged sums of all processes, then interpolateSplineKernel and
 // clampNominalKernel (kernels.cu:411-456); one block per instance
 __global__ void __launch_bounds__(UB) mppi_shard_apply(const MppiDev* __restrict__ insts, int nbp, const float* __restrict__ mins,
                                                        const float* __restrict__ sums)
@@ -1077,29 +1098,23 @@ cudaError_t launchMppiUpdate(const LaunchArgs& a, int nth)
     }
 }
 
-cudaError_t launchShardMin(const LaunchArgs& a, int nth, float* mins)
+cudaError_t launchShardLocal(const LaunchArgs& a, int nth, float* partial)
 {
     switch (nth)
     {
-    case 1: mppi_shard_min<1><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins); break;
-    case 2: mppi_shard_min<2><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins); break;
-    case 4: mppi_shard_min<4><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins); break;
-    case 8: mppi_shard_min<8><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins); break;
+    case 1: mppi_shard_local<1><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, partial); break;
+    case 2: mppi_shard_local<2><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, partial); break;
+    case 4: mppi_shard_local<4><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, partial); break;
+    case 8: mppi_shard_local<8><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, partial); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
-cudaError_t launchShardSums(const LaunchArgs& a, int nth, const float* mins, float* sums)
+cudaError_t launchShardMerge(cudaStream_t stream, const MppiDev* insts, const MppiIn* in, const float* gathered, int words, int world, float* mins,
+                             float* sums)
 {
-    switch (nth)
-    {
-    case 1: mppi_shard_sums<1><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins, sums); break;
-    case 2: mppi_shard_sums<2><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins, sums); break;
-    case 4: mppi_shard_sums<4><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins, sums); break;
-    case 8: mppi_shard_sums<8><<<a.nTiles, UB, 0, a.stream>>>(a.mppi, a.mppiIn, a.tiles, mins, sums); break;
-    default: return cudaErrorInvalidValue;
-    }
+    mppi_shard_merge<<<1, UB, 0, stream>>>(insts, in, gathered, words, world, mins, sums);
     return cudaGetLastError();
 }
 

@@ -316,10 +316,11 @@ __global__ void __launch_bounds__(PUB) pr_weighted(const PrDev* __restrict__ ins
 // ---------------------------------------------------------------------------------------
 // sample-sharded update of one controller (dr_prmppi_shard_*): this process holds samples
 // [sLo, sHi) of every hypothesis. pr_shard_min: the three minima (nominal + full cost,
-// robust + full cost, robust + safety cost) over its samples, which the caller all-reduces
-// with MIN; pr_shard_sums: its weighted sums of the absolute controls with the global
-// minima (per (which, t): sum w u0, sum w u1, sum w), all-reduced with SUM; pr_shard_apply:
-// the weighted averages from the summed sums, as pr_weighted writes them.
+// robust + full cost, robust + safety cost) over its samples; pr_shard_sums: its weighted
+// sums of the absolute controls with those local minima (per (which, t): sum w u0,
+// sum w u1, sum w); the processes all-gather both (one exchange), and pr_shard_merge takes
+// the global minima and rescales every process's sums to them by exp(-(m_r - m) / lambda);
+// pr_shard_apply: the weighted averages from the merged sums, as pr_weighted writes them.
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ const float* prArr(const PrDev& D, int which)
 {
@@ -430,6 +431,52 @@ __global__ void __launch_bounds__(PUB) pr_shard_apply(const PrDev* __restrict__ 
             D.minCosts[which] = mins[which];
         }
     }
+}
+
+// gathered[r * words + ...] = process r's (3 minima, 3 x T x 3 sums), rank order
+__global__ void __launch_bounds__(PUB) pr_shard_merge(const PrDev* __restrict__ insts, const PrIn* __restrict__ in, const float* __restrict__ gathered,
+                                                      int words, int world, float* __restrict__ mins, float* __restrict__ sums)
+{
+    const PrDev& D = insts[0];
+    const int T = D.cfg.T;
+    __shared__ float sMin[3];
+    if (threadIdx.x < 3)
+    {
+        float m = INFINITY;
+        for (int r = 0; r < world; r++)
+            m = fminf(m, gathered[(size_t)r * words + threadIdx.x]);
+        sMin[threadIdx.x] = m;
+        mins[threadIdx.x] = m;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * T; i += blockDim.x)
+    {
+        const int which = i / T;
+        const float m = sMin[which], invTemp = in[0].lambda[which];
+        float a0 = 0.0f, a1 = 0.0f, dd = 0.0f;
+        if (!isinf(m))
+            for (int r = 0; r < world; r++)
+            {
+                const float* g = gathered + (size_t)r * words;
+                if (isinf(g[which]))
+                    continue;
+                const float f = expf(-(g[which] - m) / invTemp);
+                const float* p = g + 3 + (size_t)i * 3;
+                a0 += p[0] * f;
+                a1 += p[1] * f;
+                dd += p[2] * f;
+            }
+        sums[i * 3] = a0;
+        sums[i * 3 + 1] = a1;
+        sums[i * 3 + 2] = dd;
+    }
+}
+
+cudaError_t launchPrShardMerge(cudaStream_t stream, const PrDev* insts, const PrIn* in, const float* gathered, int words, int world, float* mins,
+                               float* sums)
+{
+    pr_shard_merge<<<1, PUB, 0, stream>>>(insts, in, gathered, words, world, mins, sums);
+    return cudaGetLastError();
 }
 
 cudaError_t launchPrShardMin(cudaStream_t stream, const PrDev* insts, float* mins)

@@ -370,48 +370,55 @@ int dr_mppi_set_grad_refine(dr_mppi* h, int steps, float step_size, int ckpt_str
  * No counterpart in the reference. Process `rank` of `world` rolls out the samples
  * [rank K / world, (rank+1) K / world) and verifies [rank V / world, (rank+1) V / world),
  * with every random stream keyed by the global sample index, so the union over the
- * processes is the single-process workload. A step is four calls, with the caller's
- * collectives (e.g. torch.distributed over NCCL) in between, on device buffers it owns:
+ * processes is the single-process workload. Each process reduces its share with its own
+ * minimum cost m_r; one all-gather exchanges these partials, and every process merges them
+ * the same way, rescaling process r's weighted sums by exp(-(m_r - m) / lambda) to the
+ * global minimum m. A step is three calls with two collectives of the caller (e.g.
+ * torch.distributed over NCCL, on the controller's stream) in between, on device buffers
+ * it owns:
  *   dr_mppi_shard_begin   prologue, previous-plan verification, rollout, and this
- *                         process's masked minimum per (branch plan, knot) -> mins_dev
- *                         ((n_theta+1) x M floats)         caller: all-reduce MIN
- *   dr_mppi_shard_sums    this process's weighted sums with the global minima
- *                         -> sums_dev ((n_theta+1) x M x 3) caller: all-reduce SUM
- *   dr_mppi_shard_update  the update from the summed sums (then interpolation, clamp,
- *                         gradient refinement if set), new-plan verification
- *                         -> hist_dev (2 x n_timesteps u32: new, previous plan)
- *                                                            caller: all-reduce SUM
+ *                         process's partial -> partial_dev (dr_mppi_shard_words words:
+ *                         per (branch plan, knot) its masked minimum and its sums
+ *                         (w coeff eps0, w coeff eps1, w coeff) with that minimum, then the
+ *                         previous plan's failure histogram, T u32)
+ *                                         caller: all-gather -> gathered_dev [world][words]
+ *   dr_mppi_shard_update  the merge, the update (interpolation, clamp, gradient refinement
+ *                         if set), the new-plan verification -> hist_dev (T u32)
+ *                                         caller: all-reduce SUM of hist_dev
  *   dr_mppi_shard_finish  the host tail on the summed histograms -> action, info
- * Each call returns after its work on the controller's stream has completed. The
- * results equal the single-process step's up to the order of the floating-point sums
- * (the per-process partial sums are added in rank order). dr_mppi_step is refused on a
- * sharded controller. */
+ * Begin and update only enqueue work on the controller's stream (the caller's
+ * collectives must follow it on that stream); finish synchronises. The minima equal the
+ * single-process step's; the updated controls agree with it to FP32 rounding (the
+ * rescaling rounds differently); every process computes identical results.
+ * dr_mppi_step is refused on a sharded controller. */
 int dr_mppi_set_shard(dr_mppi* h, int rank, int world);
-int dr_mppi_shard_begin(dr_mppi* h, const dr_sim_state* state, const float* belief, float* mins_dev);
-int dr_mppi_shard_sums(dr_mppi* h, const float* mins_dev, float* sums_dev);
-int dr_mppi_shard_update(dr_mppi* h, const float* mins_dev, const float* sums_dev, uint32_t* hist_dev);
+int dr_mppi_shard_words(const dr_mppi* h, size_t* words);
+int dr_mppi_shard_begin(dr_mppi* h, const dr_sim_state* state, const float* belief, float* partial_dev);
+int dr_mppi_shard_update(dr_mppi* h, const float* gathered_dev, int world, uint32_t* hist_dev);
 int dr_mppi_shard_finish(dr_mppi* h, const uint32_t* hist_dev, const float* belief, float* out_action, dr_mppi_info* info);
 
 /* Sample sharding of one PR-MPPI controller across processes (the reference's
  * PRMPPIController::getControl, prmppi_controller.cu:180-346, split at its reductions).
  * dr_prmppi_set_shard gives process `rank` the samples [rank K / world, (rank+1) K / world)
  * of every hypothesis (all P hypotheses of a sample stay together, so the per-sample
- * averaging over hypotheses is local). Per step:
+ * averaging over hypotheses is local). Per step, one exchange:
  *   dr_prmppi_shard_begin   prologue (hypotheses drawn alike on every process), rollout of
- *                           this process's samples -> mins_dev (3 floats: nominal + full
- *                           cost, robust + full cost, robust + safety)   caller: MIN
- *   dr_prmppi_shard_sums    weighted sums with the global minima -> sums_dev (3 x T x 3
- *                           floats: sum w u0, sum w u1, sum w)           caller: SUM
- *   dr_prmppi_shard_finish  the weighted averages from the summed sums, the candidates'
- *                           re-check and choice (replicated on every process) and the
- *                           host tail -> action, info
- * Each call returns after its work has completed. Results equal the single-process
- * step's up to the order of the floating-point sums; info->nonfinite_costs counts this
- * process's samples. dr_prmppi_step is refused on a sharded controller. */
+ *                           this process's samples, its three minima (nominal + full cost,
+ *                           robust + full cost, robust + safety) and its weighted sums of
+ *                           the absolute controls with them -> partial_dev
+ *                           (dr_prmppi_shard_words = 3 + 3 x T x 3 floats)
+ *                                         caller: all-gather -> gathered_dev [world][words]
+ *   dr_prmppi_shard_finish  the merge (as for MPPI), the weighted averages, the
+ *                           candidates' re-check and choice (replicated on every process)
+ *                           and the host tail -> action, info
+ * Begin only enqueues work on the controller's stream; finish synchronises. The minima
+ * equal the single-process step's, the plans agree with it to FP32 rounding;
+ * info->nonfinite_costs counts this process's samples. dr_prmppi_step is refused on a
+ * sharded controller. */
 int dr_prmppi_set_shard(dr_prmppi* h, int rank, int world);
-int dr_prmppi_shard_begin(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* mins_dev);
-int dr_prmppi_shard_sums(dr_prmppi* h, const float* mins_dev, float* sums_dev);
-int dr_prmppi_shard_finish(dr_prmppi* h, const float* mins_dev, const float* sums_dev, float* out_action, dr_prmppi_info* info);
+int dr_prmppi_shard_words(const dr_prmppi* h, size_t* words);
+int dr_prmppi_shard_begin(dr_prmppi* h, const dr_sim_state* state, const float* belief, float* partial_dev);
+int dr_prmppi_shard_finish(dr_prmppi* h, const float* gathered_dev, int world, float* out_action, dr_prmppi_info* info);
 
 /* ---- MPPI test hooks (component parity against the reference kernels) ----------- */
 /* Clopper-Pearson bounds (state.h:134-151) of n counts k out of N at level alpha, as the

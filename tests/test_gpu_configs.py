@@ -34,8 +34,8 @@ def _c1(n_verif=4096, verify=False):
 
 # FP32 costs against FP64 costs of the same 1024 x 2 rollouts, through exp weights with
 # lambda 1: a cost error of 1e-6 relative on costs of order 1e3 moves the weights by about
-# 1e-3 relative, and the action (of order maxAccel 6) by a few 1e-3
-C1_ACTION_ATOL = 5e-3
+# 1e-3 relative, and the action by about 1e-3 (measured 8e-4)
+C1_ACTION_ATOL = 2e-3
 
 
 def test_c1_first_step_with_verification_against_fp64_oracle(gpu):

@@ -20,7 +20,7 @@ import struct
 import numpy as np
 import pytest
 
-from conftest import drb
+from conftest import O, drb
 from test_gpu_engine import Rd, run_episode, to_state
 
 pytestmark = pytest.mark.gpu
@@ -72,8 +72,13 @@ def _close(a, b):
     return np.all(np.abs(a - b) <= TOL * np.maximum(1.0, np.abs(b)))
 
 
-def test_mppi_predictions_match_reference_engine(gpu):
+@pytest.mark.parametrize("gap", [None, 1.2])
+def test_mppi_predictions_match_reference_engine(gpu, gap):
+    """gap: start the ego that many metres of arc behind the opponent, close enough for the
+    opponent's blocking to tell the hypotheses apart, so that the predictions branch."""
     sc = S.strat_race(use_splines=True, K=2048, T=40, n_verif=4096)
+    if gap is not None:
+        sc.state = S.initial_state(sc.grids, S._start_indices(sc.grids, 3.0, gap, 0), 1)
     frames = _frames_mppi(run_episode(sc, sc.mppi, 12), 2)
     assert len(frames) >= 3
     ctl = drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed)
@@ -96,6 +101,55 @@ def test_mppi_predictions_match_reference_engine(gpu):
             worst = max(worst, float(np.max(np.abs(pred["positions"][th] - ref["pos"]))))
             n_branch += int(ref["pt"] != 0)
     print(f"{len(frames)} frames x {len(frames[0]['pred'])} hypotheses; largest position difference {worst:.2e}; rows that branched {n_branch}")
+
+
+def test_mppi_prediction_branches_like_reference_host_model(gpu):
+    """The engine's MPPI prediction loop (engine.cpp:96-166) restated here over the
+    reference's own host model (environmentStep, oracle/_ref), on a plan that pushes the ego
+    at an opponent 1.2 m ahead, so that the hypotheses separate and the predictions branch:
+    dr_mppi_predict gives the same branch, branching time, stop reason and time and ego
+    actions, and positions within FP32 rounding."""
+    sc = S.strat_race(use_splines=False, K=512, T=40, n_verif=1024)
+    sc.state = S.initial_state(sc.grids, S._start_indices(sc.grids, 3.0, 1.2, 0), 1)
+    c = sc.mppi
+    T, nth, nbp = c.n_timesteps, sc.n_theta, sc.n_theta + 1
+    st0 = sc.state
+    d = np.array([st0.pos[2] - st0.pos[0], st0.pos[3] - st0.pos[1]], np.float64)
+    plan = np.broadcast_to(d / np.linalg.norm(d) * 4.0, (nbp, T, 2)).astype(np.float32).copy()
+    ctl = drb.controllers.MPPIController(sc.env, c, sc.seed, nominal=plan)
+    belief = sc.belief()
+    pred = ctl.predict(sc.state, belief)
+    ref = O.ref(O.ref_variant_name(nth, False))
+    minc = float(np.float32(c.min_confidence))
+    branched = 0
+    for th in range(nth):
+        st = drb.abi.dr_sim_state.from_buffer_copy(sc.state)
+        bel = np.zeros(drb.abi.DR_MAX_THETA, np.float32)
+        bel[:nth] = belief
+        first = next((k + 1 for k in range(nth) if bel[k] > np.float32(minc)), 0)
+        pt, bt, t_origin = first, (-1 if first == 0 else 0), 0
+        stop_reason, stop_time = 3, -1
+        pos = np.zeros((T, 4), np.float32)
+        acts = np.zeros((T, 2), np.float32)
+        for t in range(T):
+            a = plan[pt, t - t_origin].copy()
+            acts[t] = a
+            term = ref.refh_env_step(C.byref(sc.env), th, O._f(a), C.byref(st), O._f(bel), 1, 0, minc, 0, 0, sc.seed, 0, t)
+            npt = next((k + 1 for k in range(nth) if bel[k] > np.float32(minc)), 0)
+            if pt == 0 and npt != 0:
+                pt, bt, t_origin = npt, t + 1, t + 1
+            pos[t] = np.array(st.pos[:4], np.float32)
+            if term != 0:
+                stop_reason, stop_time = {1: 0, 2: 1, 3: 2}[term], t
+                pos[t + 1:] = pos[t]
+                break
+        branched += int(pt != 0)
+        assert pred["branch"][th] == pt and pred["branching_time"][th] == bt, (th, pred["branch"][th], pt, pred["branching_time"][th], bt)
+        assert pred["stop_reason"][th] == stop_reason and pred["stop_time"][th] == stop_time, th
+        assert np.array_equal(pred["actions"][th], acts), th
+        assert _close(pred["positions"][th], pos), (th, np.max(np.abs(pred["positions"][th] - pos)))
+    assert branched > 0, "the case must branch"
+    print(f"hypotheses that branched {branched} of {nth}; branching times {pred['branching_time']}")
 
 
 def test_prmppi_predictions_match_reference_engine(gpu):

@@ -1,7 +1,8 @@
 """Sample sharding of one controller across processes (dr_mppi_set_shard /
 dr_mppi_shard_*): two processes, each with half of the samples and half of the
-verification samples, combining their partial minima, weighted sums and failure
-histograms by all-reduces, against one process stepping the whole controller.
+verification samples, exchanging their partial minima, weighted sums (taken with their own
+minima) and previous-plan failure histograms by one all-gather and the new plan's
+histograms by one all-reduce, against one process stepping the whole controller.
 
 The processes share the one GPU of the test box; their kernels never wait on one
 another (the exchange happens on the host between the phases, over gloo), so this is
@@ -88,9 +89,9 @@ def test_two_shards_equal_one_controller(gpu, spl):
         nom = ctl.h_nominal
         for r in (0, 1):
             acts, noms, fcs, infos = res[r]
-            # the two shards agree with each other exactly (same summed partials)
+            # the two shards agree with each other exactly (same gathered partials, merged alike)
             assert np.array_equal(acts[k], res[0][0][k]) and np.array_equal(noms[k], res[0][1][k])
-            # and with the single process up to the order of the floating-point sums
+            # and with the single process to FP32 rounding (the rescaled sums round differently)
             np.testing.assert_allclose(acts[k], a, rtol=1e-4, atol=1e-5)
             np.testing.assert_allclose(noms[k], nom, rtol=1e-4, atol=1e-5)
             assert infos[k][0] == ctl.info.use_new_plan

@@ -1,7 +1,7 @@
 """Sample sharding of one PR-MPPI controller across processes (dr_prmppi_set_shard /
 dr_prmppi_shard_*): two processes, each with half of the samples under every hypothesis,
-combining their minima and weighted sums by all-reduces, against one process stepping the
-whole controller.
+exchanging their minima and weighted sums (taken with their own minima) by one all-gather,
+against one process stepping the whole controller.
 
 The processes share the one GPU of the test box; their kernels never wait on one
 another (the exchange happens on the host between the phases, over gloo), so this is
@@ -96,9 +96,9 @@ def test_two_pr_shards_equal_one_controller(gpu):
         rec = _record(ctl)
         for r in (0, 1):
             acts, noms, recs = res[r]
-            # the shards agree with each other exactly (same summed partials)
+            # the shards agree with each other exactly (same gathered partials, merged alike)
             assert np.array_equal(acts[k], res[0][0][k]) and np.array_equal(noms[k], res[0][1][k]) and recs[k] == res[0][2][k]
-            # and with the single process up to the order of the floating-point sums
+            # and with the single process to FP32 rounding (the rescaled sums round differently)
             np.testing.assert_allclose(acts[k], a, rtol=1e-4, atol=1e-5)
             np.testing.assert_allclose(noms[k], nom, rtol=1e-4, atol=1e-5)
             assert recs[k][0] == rec[0] and recs[k][1] == rec[1]
