@@ -48,6 +48,13 @@ struct dr_mppi
     bool spl = false;
     // verification flavour: exact (per-sample parity with the oracle) or fast (default)
     bool exactVerify = false;
+
+    // The fast verification takes the ego's moves from the ego tables: they exist and no
+    // noise of the environment moves the ego.
+    bool egoTableUsable() const
+    {
+        return !exactVerify && desc.egoTab && env.action_noise_level == 0.0f && env.pos_noise_level == 0.0f && env.speed_noise_level == 0.0f;
+    }
     DevScratch predBuf; // dr_mppi_predict's inputs and outputs on the device
     Arena arena;
     MppiDev desc{};
@@ -249,7 +256,24 @@ struct dr_mppi_batch
         a.tiles = tiles;
         a.nTiles = n;
         a.exactVerify = hs[0]->exactVerify ? 1 : 0; // equal across the batch (dr_mppi_batch_create)
+        a.egoTable = egoTable() ? 1 : 0;
         return a;
+    }
+
+    // every controller's verification reads its ego tables (filled before each verification)
+    bool egoTable() const
+    {
+        if (envKind != 0 || !verify)
+            return false;
+        for (auto* h : hs)
+            if (!h->egoTableUsable())
+                return false;
+        return true;
+    }
+
+    cudaError_t launchEgo(cudaStream_t s, const MppiIn* in, int plans) const
+    {
+        return egoTable() ? launchEgoTable(s, nopp, nth, dDesc, in, (int)hs.size(), plans) : cudaSuccess;
     }
 
     cudaError_t launchRollout(const LaunchArgs& a) const
@@ -352,8 +376,11 @@ struct dr_mppi_batch
             if (profile)
             {
                 timerSide.begin();
-                timerSide.mark("verify_old", sideStream);
+                timerSide.mark("ego_table_old", sideStream);
             }
+            CK(launchEgo(sideStream, in, 1));
+            if (profile)
+                timerSide.mark("verify_old", sideStream);
             CK(launchQueued(qargs(dVerOld, nVerOld, in, Q_VER_OLD, sidePerSm, sideStream), true));
             if (profile)
             {
@@ -380,6 +407,9 @@ struct dr_mppi_batch
         }
         if (verify && nVerNew > 0)
         {
+            if (profile)
+                timer->mark("ego_table", ex);
+            CK(launchEgo(ex, in, side ? 0 : 2));
             if (profile)
                 timer->mark(side ? "verify_new" : "verify", ex);
             LaunchArgs va = side ? qargs(dVerNew, nVerNew, in, Q_VER_NEW, verPerSm, ex) : qargs(dVer, nVer, in, Q_VER_ALL, verPerSm, ex);
@@ -504,7 +534,10 @@ struct dr_mppi_batch
         CK(cudaMemcpyAsync(dIn, hIn, sizeof(MppiIn), cudaMemcpyHostToDevice, stream));
         CK(launchMppiPrologue(args(nullptr, 0, dIn), 1, proSmem));
         if (verify && nVerOld > 0)
+        {
+            CK(launchEgo(stream, dIn, 1));
             CK(launchVerify(args(dVerOld, nVerOld, dIn)));
+        }
         CK(launchRollout(args(dRoll, nRoll, dIn)));
         CK(launchShardLocal(args(dUpd, nUpd, dIn), nth, partial));
         // the previous plan's failure histogram of this process's verification samples
@@ -525,7 +558,10 @@ struct dr_mppi_batch
         if (nGrad > 0)
             CK(launchGradNominal(stream, dGrad, nGrad, nopp, nth, spl, gradSmemB));
         if (verify && nVerNew > 0)
+        {
+            CK(launchEgo(stream, dIn, 0));
             CK(launchVerify(args(dVerNew, nVerNew, dIn)));
+        }
         CK(cudaMemcpyAsync(hist, h->desc.fail, sizeof(uint32_t) * h->T, cudaMemcpyDeviceToDevice, stream));
         return DR_OK;
     }
@@ -1023,6 +1059,11 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     A.add(counter, 16);
     double* cpTab;
     A.add(cpTab, sizeof(double) * 3 * CP_TAB);
+    // the ego tables of the fast verification (strategic race), when they stay small
+    EgoRow* egoTab = nullptr;
+    const size_t egoBytes = (size_t)2 * egoRows(nth, h->H) * h->H * sizeof(EgoRow);
+    if (env && cfg->verify && egoBytes <= EGO_TABLE_MAX_BYTES)
+        A.add(egoTab, egoBytes);
 
     // result block, one contiguous range
     size_t oFail = 0, oDense = a16(oFail + (size_t)2 * T * 4), oPrev = oDense + a16((size_t)nbp * T * 2 * 4), oNu = oPrev + a16((size_t)nbp * T * 2 * 4),
@@ -1062,6 +1103,7 @@ static int createMppi(const dr_env_config* env, const dr_gate_env_config* genv, 
     D.nu = nu;
     D.minCosts = minCosts;
     D.stats = stats;
+    D.egoTab = egoTab;
     D.resBytes = resBytes;
     if (env)
     {
@@ -1728,7 +1770,11 @@ static int debugVerify(dr_mppi* h, const St* state, const float* belief, const f
         a.tiles = dT;
         a.nTiles = (int)tiles.size();
         a.exactVerify = h->exactVerify ? 1 : 0;
-        e = h->envKind ? launchGateVerify(a, h->nth, h->iMppi, gateVerifySmem(h->nth, T), dFt, dTh)
+        a.egoTable = h->envKind == 0 && h->egoTableUsable() ? 1 : 0;
+        if (a.egoTable)
+            e = launchEgoTable(h->stream, h->nopp, h->nth, dD, dIn, 1, plan);
+        if (e == cudaSuccess)
+            e = h->envKind ? launchGateVerify(a, h->nth, h->iMppi, gateVerifySmem(h->nth, T), dFt, dTh)
                        : launchMppiVerify(a, h->nopp, h->nth, mppiVerifySmem(h->nth, T), dFt, dTh);
         std::vector<unsigned> fc(2 * T);
         if (e == cudaSuccess)

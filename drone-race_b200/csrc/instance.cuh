@@ -79,10 +79,20 @@ struct MppiDev
     // the same three bounds for every count, [which][k] for k <= max(V, 1), computed on the
     // device once per (device, V, beta) and shared by the controllers that have them (or null)
     const double* cpFull;
+    // The ego's moves under each plan (new = 0, previous = 1), shared by the verification
+    // samples (EgoRow): [plan][row][H], row 0 = no branch (or the branch of a confident
+    // initial belief), row 1 + (b - 1) H + tb = branch b taken at step tb; or null
+    EgoRow* egoTab;
     size_t resBytes;
 };
 
 constexpr int CP_TAB = 1024;
+
+// rows of a plan's ego table
+__host__ __device__ __forceinline__ int egoRows(int nth, int H)
+{
+    return 1 + nth * H;
+}
 
 struct PrCfgDev
 {

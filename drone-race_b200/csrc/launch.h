@@ -32,6 +32,9 @@ struct LaunchArgs
     // verification: 1 = the exact arithmetic flavour and noise source (per-sample parity
     // with the oracle), 0 = the fast flavour (the default)
     int exactVerify = 0;
+    // fast verification: 1 = the ego's moves come from the instances' ego tables
+    // (mppi_ego_table must have filled them for the plans verified)
+    int egoTable = 0;
 };
 
 inline int launchGrid(const LaunchArgs& a)
@@ -42,6 +45,13 @@ inline int launchGrid(const LaunchArgs& a)
 // Samples per verification CTA (one thread each). The CTA's warps step through the
 // horizon together (a barrier per step), so the warps sharing an SM sub-partition fetch
 // the same instructions; 512 threads, two CTAs per SM.
+// Largest ego tables (both plans) a controller holds; larger ones (many hypotheses and a
+// long verification horizon) are not built and the verification moves the ego itself.
+#ifndef DR_EGO_TABLE_MAX_BYTES
+#define DR_EGO_TABLE_MAX_BYTES (16u << 20)
+#endif
+constexpr size_t EGO_TABLE_MAX_BYTES = DR_EGO_TABLE_MAX_BYTES;
+
 #ifndef DR_VERIFY_TILE
 #define DR_VERIFY_TILE 512
 #endif
@@ -61,6 +71,9 @@ cudaError_t launchShardMerge(cudaStream_t stream, const MppiDev* insts, const Mp
                              float* sums);
 cudaError_t launchShardApply(cudaStream_t stream, const MppiDev* insts, int nInst, int nth, const float* mins, const float* sums);
 cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem, int* dbgFailTime, int* dbgTheta);
+// fills the ego tables (MppiDev::egoTab) of plan `plan` (0 new, 1 previous, 2 both) of
+// every instance
+cudaError_t launchEgoTable(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, int plan);
 // CTAs per SM of the persistent rollout (verify = false) or verification kernel
 int mppiResident(int nopp, int nth, bool verify, bool spl, size_t smem);
 cudaError_t launchMppiNoise(const LaunchArgs& a, size_t n, float* out);

@@ -397,11 +397,11 @@ template <int NA> struct AgentGeo
     float sdot[NA];         // computeSdot(a) (env_stratrace.h:302-315)
 };
 
-template <int NA, bool F = false>
+template <int NA, bool F = false, int A0 = 0>
 __device__ __forceinline__ void agentGeometry(const Track& tr, const EnvParams& E, const DState<NA>& s, AgentGeo<NA>& g)
 {
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = A0; a < NA; a++)
     {
         normalizedSpeed<F>(tr, s.tp[a], g.tn0[a], g.tn1[a]);
         g.kap[a] = sampleAt1(tr.k, s.tp[a]);
@@ -629,6 +629,73 @@ template <int NTH> __device__ __forceinline__ int findConfident(const float (&be
     return pt;
 }
 
+// One step of the ego (agent 0) as the environment step moves it: its geometry before the
+// step (unit tangent, ds/dt) and its state after it. The ego's motion depends on its own
+// action only (the opponents enter its costs and terminal tests, not its dynamics), so when
+// the ego draws no noise every Monte-Carlo verification sample that has taken the same
+// branch at the same step moves the ego identically; mppi_ego_table computes these rows once
+// per plan, and envStep<..., EGO = true> reads them instead of moving the ego itself.
+struct __align__(16) EgoRow
+{
+    float tn0, tn1, sdot;       // before the step
+    float pos0, pos1, vel0, vel1; // after the step
+    float S, lat, w;            // after the step: arc length, lateral offset, TrackPos weight
+    int laps, i0;               // after the step: laps, TrackPos index
+};
+
+// The ego's part of envStep (geometry, clamp, position, arc length, velocity, speed cap,
+// projection, laps; the same expressions), for an ego that draws no noise.
+template <bool F> __device__ __forceinline__ void egoStep(const Track& tr, const EnvParams& E, float ego0, float ego1, DState<1>& s, EgoRow& row)
+{
+    AgentGeo<1> g;
+    agentGeometry<1, F>(tr, E, s, g);
+    row.tn0 = g.tn0[0];
+    row.tn1 = g.tn1[0];
+    row.sdot = g.sdot[0];
+    const float prevS = s.S[0];
+    float sq = 0.0f;
+    sq += ego0 * ego0;
+    sq += ego1 * ego1;
+    float factor = 1.0f;
+    float maxSq = E.maxAccel[0] * E.maxAccel[0];
+    if (sq > maxSq)
+        factor = mdivsqrt<F>(E.maxAccel[0], sq);
+    ego0 *= factor;
+    ego1 *= factor;
+    s.pos[0] += E.dt * s.vel[0];
+    s.pos[1] += E.dt * s.vel[1];
+    s.S[0] += E.dt * g.sdot[0];
+    s.vel[0] += E.dt * ego0;
+    s.vel[1] += E.dt * ego1;
+    float sqSpd = sqNorm(s.vel[0], s.vel[1]);
+    if (sqSpd > E.maxSpeed[0] * E.maxSpeed[0])
+    {
+        float sc = mdivsqrt<F>(E.maxSpeed[0], sqSpd);
+        s.vel[0] *= sc;
+        s.vel[1] *= sc;
+    }
+    s.S[0] = projectOnTrack<F>(tr, E.trackLength, E.invTrackLength, s.pos[0], s.pos[1], s.S[0], s.lat[0], s.tp[0]);
+    if (s.S[0] < prevS - E.trackLength * 0.5f)
+        s.laps[0]++;
+    if (s.S[0] > prevS + E.trackLength * 0.5f)
+        s.laps[0]--;
+    row.pos0 = s.pos[0];
+    row.pos1 = s.pos[1];
+    row.vel0 = s.vel[0];
+    row.vel1 = s.vel[1];
+    row.S = s.S[0];
+    row.lat = s.lat[0];
+    row.w = s.tp[0].w;
+    row.laps = s.laps[0];
+    row.i0 = s.tp[0].i0;
+}
+
+// The environment noise of every agent is off: no draw of envStep moves the ego.
+__device__ __forceinline__ bool egoNoiseFree(const EnvParams& E)
+{
+    return E.actionNoiseLevel == 0.0f && E.posNoise == 0.0f && E.speedNoise == 0.0f;
+}
+
 struct StepOut
 {
     int term;
@@ -641,7 +708,9 @@ struct StepOut
 //   UPD: shouldUpdateBelief, BR: considerBranching, LOSE: loseOnOppWin,
 //   ALLTH: evaluate the opponent policy under every hypothesis (needed by the belief
 //   update) or only under the true one (the result is the same when UPD is false),
-//   F: the arithmetic flavour (exact or fast, see mdiv), RNG: the noise source.
+//   F: the arithmetic flavour (exact or fast, see mdiv), RNG: the noise source,
+//   EGO: the ego's geometry and its move come from *ego (an EgoRow; only for an ego that
+//   draws no noise, egoNoiseFree), the step computes the opponents only.
 // Work whose result cannot change the step's outputs is not done:
 //   * a hypothesis whose policy parameters equal an earlier one's on every term the step
 //     evaluates (EnvParams::dupAll / dupNoBlock) takes that one's action;
@@ -649,11 +718,12 @@ struct StepOut
 //     read by nothing any more (the branch test runs only while predTheta == 0; the
 //     callers with BR return costs, branch records and failure times, never the belief),
 //     so the belief update and the other hypotheses' actions it needs are skipped.
-template <int NOPP, int NTH, bool UPD, bool BR, bool LOSE, bool ALLTH, bool F = false, class RNG = EnvNoise>
+template <int NOPP, int NTH, bool UPD, bool BR, bool LOSE, bool ALLTH, bool F = false, class RNG = EnvNoise, bool EGO = false>
 __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr, const EnvParams& E, float ego0, float ego1, DState<NOPP + 1>& s,
-                                           BState<NTH>& bs, bool& branched, float minConf, RNG& rng)
+                                           BState<NTH>& bs, bool& branched, float minConf, RNG& rng, const EgoRow* ego = nullptr)
 {
     constexpr int NA = NOPP + 1;
+    constexpr int A0 = EGO ? 1 : 0; // first agent this step moves itself
     float prevS[NA];
 #pragma unroll
     for (int a = 0; a < NA; a++)
@@ -661,7 +731,14 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     const bool live = !BR || bs.predTheta == 0; // the belief is still read after this step
 
     AgentGeo<NA> g;
-    agentGeometry<NA, F>(tr, E, s, g);
+    if constexpr (EGO)
+    {
+        g.tn0[0] = ego->tn0;
+        g.tn1[0] = ego->tn1;
+        g.sdot[0] = ego->sdot;
+        g.kap[0] = 0.0f; // read by nothing for the ego
+    }
+    agentGeometry<NA, F, A0>(tr, E, s, g);
 
     float act0[NA], act1[NA];
     act0[0] = ego0;
@@ -720,7 +797,7 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     }
     // 2. clamp + action noise
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = A0; a < NA; a++)
     {
         float sq = 0.0f;
         sq += act0[a] * act0[a];
@@ -738,25 +815,25 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     }
     // 3. position
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = A0; a < NA; a++)
     {
         s.pos[2 * a] += E.dt * s.vel[2 * a];
         s.pos[2 * a + 1] += E.dt * s.vel[2 * a + 1];
     }
     // 4. arc length (ds/dt of the pre-step state)
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = A0; a < NA; a++)
         s.S[a] += E.dt * g.sdot[a];
     // 5. velocity
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = A0; a < NA; a++)
     {
         s.vel[2 * a] += E.dt * act0[a];
         s.vel[2 * a + 1] += E.dt * act1[a];
     }
     // 6. speed cap
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = A0; a < NA; a++)
     {
         float sqSpd = sqNorm(s.vel[2 * a], s.vel[2 * a + 1]);
         if (sqSpd > E.maxSpeed[a] * E.maxSpeed[a])
@@ -770,7 +847,7 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     if (E.posNoise != 0.0f || E.speedNoise != 0.0f)
     {
 #pragma unroll
-        for (int a = 0; a < NA; a++)
+        for (int a = A0; a < NA; a++)
 #pragma unroll
             for (int d = 0; d < 2; d++)
             {
@@ -782,16 +859,27 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     }
     // 8. projection
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = A0; a < NA; a++)
         s.S[a] = projectOnTrack<F>(tr, E.trackLength, E.invTrackLength, s.pos[2 * a], s.pos[2 * a + 1], s.S[a], s.lat[a], s.tp[a]);
     // 9. laps
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = A0; a < NA; a++)
     {
         if (s.S[a] < prevS[a] - E.trackLength * 0.5f)
             s.laps[a]++;
         if (s.S[a] > prevS[a] + E.trackLength * 0.5f)
             s.laps[a]--;
+    }
+    if constexpr (EGO)
+    {
+        s.pos[0] = ego->pos0;
+        s.pos[1] = ego->pos1;
+        s.vel[0] = ego->vel0;
+        s.vel[1] = ego->vel1;
+        s.S[0] = ego->S;
+        s.lat[0] = ego->lat;
+        s.laps[0] = ego->laps;
+        s.tp[0] = TrackPos{ego->i0, ego->w};
     }
     // 10. belief update (env_stratrace.h:166-222)
     if constexpr (UPD)

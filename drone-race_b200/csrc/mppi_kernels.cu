@@ -815,9 +815,72 @@ __global__ void __launch_bounds__(UB) mppi_shard_apply(const MppiDev* __restrict
 // ---------------------------------------------------------------------------------------
 // verification
 // ---------------------------------------------------------------------------------------
+// The ego tables of a plan (EgoRow; plan 0 the new one, 1 the previous one, 2 both): one
+// block per instance, the track staged in shared memory, one thread per row (the
+// trajectory with no branch, and one per branch and branching step), each moving the ego
+// alone through the verification horizon with the fast arithmetic of the verification.
+template <int NTH>
+__global__ void __launch_bounds__(128) mppi_ego_table(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, int nInst, int plans)
+{
+    __shared__ float sg[GRID_FLOATS];
+    __shared__ EnvParams sE;
+    const int inst = blockIdx.x;
+    if (inst >= nInst)
+        return;
+    const MppiDev& D = insts[inst];
+    const MppiIn& I = in[inst];
+    if (!D.egoTab)
+        return;
+    for (int i = threadIdx.x; i < GRID_FLOATS; i += blockDim.x)
+        sg[i] = D.grids[i];
+    copyEnv(&sE, &D.env);
+    __syncthreads();
+    const EnvParams& E = sE;
+    if (!egoNoiseFree(E))
+        return;
+    const Track tr = trackIn(sg);
+    const int H = D.cfg.H, T = D.cfg.T, rows = egoRows(NTH, H);
+    float belief[NTH];
+#pragma unroll
+    for (int i = 0; i < NTH; i++)
+        belief[i] = I.belief[i];
+    const int pt0 = findConfident<NTH>(belief, D.cfg.minConf);
+    const int p0 = plans == 1 ? 1 : 0, p1 = plans == 0 ? 0 : 1;
+    for (int plan = p0; plan <= p1; plan++)
+    {
+        const float* P = plan == 0 ? D.dense : D.prevDense;
+        EgoRow* tab = D.egoTab + (size_t)plan * rows * H;
+        for (int r = threadIdx.x; r < rows; r += blockDim.x)
+        {
+            if (r > 0 && pt0 != 0)
+                break; // a confident initial belief never branches
+            const int bb = r > 0 ? 1 + (r - 1) / H : 0, tb = r > 0 ? (r - 1) % H : H;
+            DState<1> s;
+            s.pos[0] = I.state.pos[0];
+            s.pos[1] = I.state.pos[1];
+            s.vel[0] = I.state.vel[0];
+            s.vel[1] = I.state.vel[1];
+            s.S[0] = I.state.S[0];
+            s.lat[0] = I.state.lat_dist[0];
+            s.laps[0] = I.state.laps[0];
+            s.locate(E.trackLength);
+            for (int t = 0; t < H; t++)
+            {
+                // the verification's plan index: branch pt0 before any branching, then the
+                // branch taken, its clock restarting after the branching step
+                const int b = t <= tb ? pt0 : bb, local = t <= tb ? t : t - tb - 1;
+                EgoRow row;
+                egoStep<true>(tr, E, P[(b * T + local) * 2], P[(b * T + local) * 2 + 1], s, row);
+                tab[(size_t)r * H + t] = row;
+            }
+        }
+    }
+}
+
 // FAST: the fast arithmetic flavour and noise source (the default; the exact flavour
-// reproduces the oracle's per-sample results and serves parity tests).
-template <int NOPP, int NTH, bool PQ, bool FAST>
+// reproduces the oracle's per-sample results and serves parity tests). EGO (with FAST):
+// the ego's moves come from the instance's ego table of the plan (mppi_ego_table).
+template <int NOPP, int NTH, bool PQ, bool FAST, bool EGO = false>
 __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) mppi_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
                                                   int nTiles, unsigned* __restrict__ queue, int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
 {
@@ -901,6 +964,8 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
                 bs.belief[i] = I.belief[i];
             bs.predTheta = findConfident<NTH>(bs.belief, minConf);
             bs.branchingTime = bs.predTheta == 0 ? -1 : 0;
+            const int pt0 = bs.predTheta;
+            const EgoRow* egoTab = EGO ? D.egoTab + (size_t)plan * egoRows(NTH, H) * H : nullptr;
             // sampleModelFromBelief (state.h:118-131) on a Philox uniform
             const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
             float u = uniform_from_word(draw(k0, k1, (uint32_t)v, (uint32_t)plan, step, S_VERIF_THETA, 0).x);
@@ -936,7 +1001,15 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
                 int b = bs.predTheta;
                 float e0 = sPlan[(b * T + local) * 2], e1 = sPlan[(b * T + local) * 2 + 1];
                 bool branched = false;
-                StepOut o = envStep<NOPP, NTH, true, true, false, true, FAST>(t, theta, tr, E, e0, e1, st, bs, branched, minConf, rng);
+                StepOut o;
+                if constexpr (EGO)
+                {
+                    const int row = (bs.predTheta == 0 || pt0 != 0) ? 0 : 1 + (bs.predTheta - 1) * H + (tOrigin - 1);
+                    const EgoRow er = egoTab[(size_t)row * H + t];
+                    o = envStep<NOPP, NTH, true, true, false, true, FAST, Noise, true>(t, theta, tr, E, e0, e1, st, bs, branched, minConf, rng, &er);
+                }
+                else
+                    o = envStep<NOPP, NTH, true, true, false, true, FAST>(t, theta, tr, E, e0, e1, st, bs, branched, minConf, rng);
                 if (branched)
                     tOrigin = t + 1;
                 if (o.term == TERM_LOSE)
@@ -1015,6 +1088,7 @@ template <int NOPP, int NTH> static cudaError_t launchRolloutT(const LaunchArgs&
 template <int NOPP, int NTH> static cudaError_t launchVerifyT(const LaunchArgs& a, size_t smem, int* ft, int* th)
 {
     auto k = a.exactVerify ? (a.queue ? mppi_verify<NOPP, NTH, true, false> : mppi_verify<NOPP, NTH, false, false>)
+             : a.egoTable  ? (a.queue ? mppi_verify<NOPP, NTH, true, true, true> : mppi_verify<NOPP, NTH, false, true, true>)
                            : (a.queue ? mppi_verify<NOPP, NTH, true, true> : mppi_verify<NOPP, NTH, false, true>);
     ensureSmem(k, smem);
     return launchMaybePdl(a.pdl != 0, k, dim3(launchGrid(a)), dim3(VERIFY_TILE), smem, a.stream, a.mppi, a.mppiIn, a.tiles, a.nTiles, a.queue, ft, th);
@@ -1150,6 +1224,20 @@ cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem
 #define CALL(P, Q) launchVerifyT<P, Q>(a, smem, dbgFailTime, dbgTheta)
     DR_DISPATCH(nopp, nth, CALL)
 #undef CALL
+}
+
+cudaError_t launchEgoTable(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, int plan)
+{
+    (void)nopp; // the ego's moves do not depend on the opponents
+    switch (nth)
+    {
+    case 1: mppi_ego_table<1><<<nInst, 128, 0, stream>>>(insts, in, nInst, plan); break;
+    case 2: mppi_ego_table<2><<<nInst, 128, 0, stream>>>(insts, in, nInst, plan); break;
+    case 4: mppi_ego_table<4><<<nInst, 128, 0, stream>>>(insts, in, nInst, plan); break;
+    case 8: mppi_ego_table<8><<<nInst, 128, 0, stream>>>(insts, in, nInst, plan); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launchMppiNoise(const LaunchArgs& a, size_t n, float* out)
