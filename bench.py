@@ -52,8 +52,13 @@ VERIF_H = 40
 # mul, div, sqrt, exp, log, pow, min/max/abs/floor/copysign = 1 FLOP, comparisons not
 # counted, and an operation repeated on the same operands within one step counted once
 # (the reference evaluates 1323 ops per step as written; 652 / 571 are distinct).
+# The verification shares the ego's moves across its samples (the ego draws no noise in
+# this workload, so samples that took the same branch at the same step move it alike;
+# mppi_ego_table computes them once per plan): counting each distinct operation once per
+# step index over the samples (opcount dedup mode 2) leaves 337 FLOPs per sample-step,
+# the work the verification kernel has to do; 571 is a sample's own work in isolation.
 FLOPS_PER_ROLLOUT_STEP = 652.0    # MPPI rollout step (belief update over 2 hypotheses)
-FLOPS_PER_VERIFY_STEP = 571.0     # verification step (noise-free ego plan)
+FLOPS_PER_VERIFY_STEP = 337.0     # verification step, ego moves shared across samples
 
 # --workload gates: the same control step on the gate race (the reference's EnvDroneRace:
 # one PID opponent with 2 hypotheses, 8 gates on a 30 x 20 m ellipse, 2 racelines), FLOPs
@@ -530,6 +535,7 @@ def run_ours(args) -> None:
         "rollout_steps_per_s": world * rollout_steps * args.steps / (ms / 1e3),
         "verify_steps_per_s": world * AGENTS * 2 * V * VERIF_H * args.steps / (ms / 1e3),
         "kernel_ms": kt,
+        "kernel_ms_serial": kt_serial,
         "e2e": None if args.quick else {"value": world * args.steps / e2e_s, "unit": "control steps/s", "h2d_bytes_per_step": h2d,
                                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s / args.steps * 1e3},
         "gpu_launches": len(kt) * args.steps,

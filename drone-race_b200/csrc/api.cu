@@ -273,7 +273,12 @@ struct dr_mppi_batch
 
     cudaError_t launchEgo(cudaStream_t s, const MppiIn* in, int plans) const
     {
-        return egoTable() ? launchEgoTable(s, nopp, nth, dDesc, in, (int)hs.size(), plans) : cudaSuccess;
+        if (!egoTable())
+            return cudaSuccess;
+        int maxH = 1;
+        for (auto* h : hs)
+            maxH = std::max(maxH, h->H);
+        return launchEgoTable(s, nopp, nth, dDesc, in, (int)hs.size(), plans, maxH);
     }
 
     cudaError_t launchRollout(const LaunchArgs& a) const
@@ -1772,7 +1777,7 @@ static int debugVerify(dr_mppi* h, const St* state, const float* belief, const f
         a.exactVerify = h->exactVerify ? 1 : 0;
         a.egoTable = h->envKind == 0 && h->egoTableUsable() ? 1 : 0;
         if (a.egoTable)
-            e = launchEgoTable(h->stream, h->nopp, h->nth, dD, dIn, 1, plan);
+            e = launchEgoTable(h->stream, h->nopp, h->nth, dD, dIn, 1, plan, h->H);
         if (e == cudaSuccess)
             e = h->envKind ? launchGateVerify(a, h->nth, h->iMppi, gateVerifySmem(h->nth, T), dFt, dTh)
                        : launchMppiVerify(a, h->nopp, h->nth, mppiVerifySmem(h->nth, T), dFt, dTh);

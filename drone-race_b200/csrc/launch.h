@@ -72,8 +72,8 @@ cudaError_t launchShardMerge(cudaStream_t stream, const MppiDev* insts, const Mp
 cudaError_t launchShardApply(cudaStream_t stream, const MppiDev* insts, int nInst, int nth, const float* mins, const float* sums);
 cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem, int* dbgFailTime, int* dbgTheta);
 // fills the ego tables (MppiDev::egoTab) of plan `plan` (0 new, 1 previous, 2 both) of
-// every instance
-cudaError_t launchEgoTable(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, int plan);
+// every instance; maxH: the longest verification horizon of the instances
+cudaError_t launchEgoTable(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, int plan, int maxH);
 // CTAs per SM of the persistent rollout (verify = false) or verification kernel
 int mppiResident(int nopp, int nth, bool verify, bool spl, size_t smem);
 cudaError_t launchMppiNoise(const LaunchArgs& a, size_t n, float* out);

@@ -252,6 +252,51 @@ template <bool F> __device__ __forceinline__ void normalizedSpeed(const Track& t
     o1 *= invNorm;
 }
 
+// The part of fastProjectOnTrack after the window scan: exact projection onto the two
+// segments at the nearest sample bestJ, then the signed lateral distance.
+template <bool F>
+__device__ __forceinline__ float projectSegments(const Track& tr, float L, float invL, float px, float py, int bestJ, float& latDist, TrackPos& tpS)
+{
+    const float2* __restrict__ P2 = reinterpret_cast<const float2*>(tr.p);
+    const int bestInd = (bestJ + NTS) % NTS;
+    float bestSegSqDist = INFINITY;
+    float bestS = 0.0f;
+    float closestX = 0.0f, closestY = 0.0f;
+#pragma unroll
+    for (int seg = -1; seg <= 0; ++seg)
+    {
+        const int aj = bestInd + seg;  // -1 .. 511; the padded grid holds p[-1] and p[512]
+        const int a = aj < 0 ? aj + NTS : aj;
+        const float2 qa = P2[aj], qb = P2[aj + 1];
+        float ax = qa.x, ay = qa.y;
+        float abx = qb.x - ax;
+        float aby = qb.y - ay;
+        float sqAB = sqNorm(abx, aby);
+        float t = 0.0f;
+        if (sqAB > 1e-12f) // the reference compares with the double 1e-12; for floats the two tests agree
+        {
+            t = mdiv<F>((px - ax) * abx + (py - ay) * aby, sqAB);
+            t = fmaxf(0.0f, fminf(t, 1.0f));
+        }
+        float projx = ax + t * abx;
+        float projy = ay + t * aby;
+        float sqDist = sqNorm(px - projx, py - projy);
+        if (sqDist < bestSegSqDist)
+        {
+            bestSegSqDist = sqDist;
+            bestS = ((float)a + t) / NTS * L;
+            closestX = projx;
+            closestY = projy;
+        }
+    }
+    float tg0, tg1;
+    tpS = trackPosT<F>(bestS, L, invL);
+    sampleAt2(tr.t, tpS, tg0, tg1);
+    float cross = -tg1 * (px - closestX) + tg0 * (py - closestY);
+    latDist = copysignf(msqrt<F>(bestSegSqDist), cross);
+    return bestS;
+}
+
 // fastProjectOnTrack<false> (env_stratrace.h:88-162): returns S, writes latDist and the
 // track position of S. The fast flavour takes the window's minimum on keys that pack the
 // squared distance (its low five mantissa bits dropped) with the sample's place in the
@@ -304,9 +349,10 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
             best = min(best, (__float_as_uint(sqB) & ~31u) | (off + 2u * q + 1u));
         }
         {
+            // rounded like each lane of the pairs above
             float2 qs = P2[js];
-            float d0 = qs.x - px, d1 = qs.y - py;
-            float sq = d0 * d0 + d1 * d1;
+            float d0 = __fsub_rn(qs.x, px), d1 = __fsub_rn(qs.y, py);
+            float sq = __fmaf_rn(d1, d1, __fmul_rn(d0, d0));
             best = min(best, (__float_as_uint(sq) & ~31u) | (uint32_t)(js - j0));
         }
         bestJ = j0 + (int)(best & 31u);
@@ -349,43 +395,30 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
                 bestJ = js;
         }
     }
-    const int bestInd = (bestJ + NTS) % NTS;
-    float bestSegSqDist = INFINITY;
-    float bestS = 0.0f;
-    float closestX = 0.0f, closestY = 0.0f;
-#pragma unroll
-    for (int seg = -1; seg <= 0; ++seg)
+    return projectSegments<F>(tr, L, invL, px, py, bestJ, latDist, tpS);
+}
+
+// projectOnTrack<true> with the window scan spread over the 32 lanes of a warp, all of
+// which hold the same position and take part: lane j < 21 evaluates window sample j and one
+// warp-wide unsigned minimum of the packed (squared distance, place) keys finds the nearest;
+// every lane returns projectOnTrack<true>'s result.
+__device__ __forceinline__ float projectOnTrackWarp(const Track& tr, float L, float invL, float px, float py, float prevS, float& latDist, TrackPos& tpS)
+{
+    prevS *= invL;
+    prevS = prevS - floorf(prevS);
+    const int idxPrev = (int)(prevS * NTS);
+    const int j0 = idxPrev - WIN;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t key = 0xffffffffu;
+    if (lane <= 2 * WIN)
     {
-        const int aj = bestInd + seg;  // -1 .. 511; the padded grid holds p[-1] and p[512]
-        const int a = aj < 0 ? aj + NTS : aj;
-        const float2 qa = P2[aj], qb = P2[aj + 1];
-        float ax = qa.x, ay = qa.y;
-        float abx = qb.x - ax;
-        float aby = qb.y - ay;
-        float sqAB = sqNorm(abx, aby);
-        float t = 0.0f;
-        if (sqAB > 1e-12f) // the reference compares with the double 1e-12; for floats the two tests agree
-        {
-            t = mdiv<F>((px - ax) * abx + (py - ay) * aby, sqAB);
-            t = fmaxf(0.0f, fminf(t, 1.0f));
-        }
-        float projx = ax + t * abx;
-        float projy = ay + t * aby;
-        float sqDist = sqNorm(px - projx, py - projy);
-        if (sqDist < bestSegSqDist)
-        {
-            bestSegSqDist = sqDist;
-            bestS = ((float)a + t) / NTS * L;
-            closestX = projx;
-            closestY = projy;
-        }
+        const int j = j0 + (int)lane;
+        const float d0 = __fsub_rn(tr.px[j], px), d1 = __fsub_rn(tr.py[j], py);
+        const float sq = __fmaf_rn(d1, d1, __fmul_rn(d0, d0));
+        key = (__float_as_uint(sq) & ~31u) | lane;
     }
-    float tg0, tg1;
-    tpS = trackPosT<F>(bestS, L, invL);
-    sampleAt2(tr.t, tpS, tg0, tg1);
-    float cross = -tg1 * (px - closestX) + tg0 * (py - closestY);
-    latDist = copysignf(msqrt<F>(bestSegSqDist), cross);
-    return bestS;
+    key = __reduce_min_sync(0xffffffffu, key);
+    return projectSegments<true>(tr, L, invL, px, py, j0 + (int)(key & 31u), latDist, tpS);
 }
 
 // ---- per-step agent quantities -------------------------------------------------------
@@ -644,8 +677,10 @@ struct __align__(16) EgoRow
 };
 
 // The ego's part of envStep (geometry, clamp, position, arc length, velocity, speed cap,
-// projection, laps; the same expressions), for an ego that draws no noise.
-template <bool F> __device__ __forceinline__ void egoStep(const Track& tr, const EnvParams& E, float ego0, float ego1, DState<1>& s, EgoRow& row)
+// projection, laps; the same expressions), for an ego that draws no noise. WARP (fast
+// flavour only): all 32 lanes of the warp hold the same ego and share the projection's scan.
+template <bool F, bool WARP = false>
+__device__ __forceinline__ void egoStep(const Track& tr, const EnvParams& E, float ego0, float ego1, DState<1>& s, EgoRow& row)
 {
     AgentGeo<1> g;
     agentGeometry<1, F>(tr, E, s, g);
@@ -674,7 +709,10 @@ template <bool F> __device__ __forceinline__ void egoStep(const Track& tr, const
         s.vel[0] *= sc;
         s.vel[1] *= sc;
     }
-    s.S[0] = projectOnTrack<F>(tr, E.trackLength, E.invTrackLength, s.pos[0], s.pos[1], s.S[0], s.lat[0], s.tp[0]);
+    if constexpr (WARP)
+        s.S[0] = projectOnTrackWarp(tr, E.trackLength, E.invTrackLength, s.pos[0], s.pos[1], s.S[0], s.lat[0], s.tp[0]);
+    else
+        s.S[0] = projectOnTrack<F>(tr, E.trackLength, E.invTrackLength, s.pos[0], s.pos[1], s.S[0], s.lat[0], s.tp[0]);
     if (s.S[0] < prevS - E.trackLength * 0.5f)
         s.laps[0]++;
     if (s.S[0] > prevS + E.trackLength * 0.5f)

@@ -816,13 +816,18 @@ __global__ void __launch_bounds__(UB) mppi_shard_apply(const MppiDev* __restrict
 // verification
 // ---------------------------------------------------------------------------------------
 // The ego tables of a plan (EgoRow; plan 0 the new one, 1 the previous one, 2 both): one
-// block per instance, the track staged in shared memory, one thread per row (the
-// trajectory with no branch, and one per branch and branching step), each moving the ego
-// alone through the verification horizon with the fast arithmetic of the verification.
+// warp per row (the trajectory with no branch, and one per branch and branching step)
+// moves the ego alone through the verification horizon with the fast arithmetic of the
+// verification, its lanes sharing the projection's window scan; each CTA of
+// EGO_WARPS warps stages the track, the environment and the plan in shared memory. The
+// rows are independent, so the kernel's time is one trajectory's: H steps of one warp.
+constexpr int EGO_WARPS = 4;
+
 template <int NTH>
-__global__ void __launch_bounds__(128) mppi_ego_table(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, int nInst, int plans)
+__global__ void __launch_bounds__(EGO_WARPS * 32) mppi_ego_table(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, int nInst, int plans)
 {
     __shared__ float sg[GRID_FLOATS];
+    __shared__ __align__(16) float sPlan[(DR_MAX_THETA + 1) * DR_MAX_T * 2];
     __shared__ EnvParams sE;
     const int inst = blockIdx.x;
     if (inst >= nInst)
@@ -831,15 +836,13 @@ __global__ void __launch_bounds__(128) mppi_ego_table(const MppiDev* __restrict_
     const MppiIn& I = in[inst];
     if (!D.egoTab)
         return;
+    const int H = D.cfg.H, T = D.cfg.T, rows = egoRows(NTH, H), nbp = NTH + 1;
+    const int warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < GRID_FLOATS; i += blockDim.x)
         sg[i] = D.grids[i];
     copyEnv(&sE, &D.env);
-    __syncthreads();
     const EnvParams& E = sE;
-    if (!egoNoiseFree(E))
-        return;
     const Track tr = trackIn(sg);
-    const int H = D.cfg.H, T = D.cfg.T, rows = egoRows(NTH, H);
     float belief[NTH];
 #pragma unroll
     for (int i = 0; i < NTH; i++)
@@ -849,8 +852,14 @@ __global__ void __launch_bounds__(128) mppi_ego_table(const MppiDev* __restrict_
     for (int plan = p0; plan <= p1; plan++)
     {
         const float* P = plan == 0 ? D.dense : D.prevDense;
+        __syncthreads(); // the previous plan's rows are done with sPlan
+        for (int i = threadIdx.x; i < nbp * T * 2; i += blockDim.x)
+            sPlan[i] = P[i];
+        __syncthreads();
+        if (!egoNoiseFree(E))
+            continue; // uniform: the verification moves the ego itself
         EgoRow* tab = D.egoTab + (size_t)plan * rows * H;
-        for (int r = threadIdx.x; r < rows; r += blockDim.x)
+        for (int r = blockIdx.y * EGO_WARPS + warp; r < rows; r += gridDim.y * EGO_WARPS)
         {
             if (r > 0 && pt0 != 0)
                 break; // a confident initial belief never branches
@@ -870,8 +879,9 @@ __global__ void __launch_bounds__(128) mppi_ego_table(const MppiDev* __restrict_
                 // branch taken, its clock restarting after the branching step
                 const int b = t <= tb ? pt0 : bb, local = t <= tb ? t : t - tb - 1;
                 EgoRow row;
-                egoStep<true>(tr, E, P[(b * T + local) * 2], P[(b * T + local) * 2 + 1], s, row);
-                tab[(size_t)r * H + t] = row;
+                egoStep<true, true>(tr, E, sPlan[(b * T + local) * 2], sPlan[(b * T + local) * 2 + 1], s, row);
+                if ((threadIdx.x & 31) == 0)
+                    tab[(size_t)r * H + t] = row;
             }
         }
     }
@@ -1226,15 +1236,17 @@ cudaError_t launchMppiVerify(const LaunchArgs& a, int nopp, int nth, size_t smem
 #undef CALL
 }
 
-cudaError_t launchEgoTable(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, int plan)
+cudaError_t launchEgoTable(cudaStream_t stream, int nopp, int nth, const MppiDev* insts, const MppiIn* in, int nInst, int plan, int maxH)
 {
     (void)nopp; // the ego's moves do not depend on the opponents
+    // blocks per instance: enough warps for the rows of the longest horizon of the batch
+    const dim3 grid(nInst, (unsigned)((egoRows(nth, maxH) + EGO_WARPS - 1) / EGO_WARPS));
     switch (nth)
     {
-    case 1: mppi_ego_table<1><<<nInst, 128, 0, stream>>>(insts, in, nInst, plan); break;
-    case 2: mppi_ego_table<2><<<nInst, 128, 0, stream>>>(insts, in, nInst, plan); break;
-    case 4: mppi_ego_table<4><<<nInst, 128, 0, stream>>>(insts, in, nInst, plan); break;
-    case 8: mppi_ego_table<8><<<nInst, 128, 0, stream>>>(insts, in, nInst, plan); break;
+    case 1: mppi_ego_table<1><<<grid, EGO_WARPS * 32, 0, stream>>>(insts, in, nInst, plan); break;
+    case 2: mppi_ego_table<2><<<grid, EGO_WARPS * 32, 0, stream>>>(insts, in, nInst, plan); break;
+    case 4: mppi_ego_table<4><<<grid, EGO_WARPS * 32, 0, stream>>>(insts, in, nInst, plan); break;
+    case 8: mppi_ego_table<8><<<grid, EGO_WARPS * 32, 0, stream>>>(insts, in, nInst, plan); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

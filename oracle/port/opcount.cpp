@@ -4,10 +4,15 @@
 // (model.hpp, the restatement of env_stratrace.h / costs.cuh) with an operation-counting
 // scalar. Every floating-point operation is counted once: add/sub, mul, div, sqrt, exp,
 // log, pow, min/max/abs/floor/copysign; comparisons are counted separately and are not
-// FLOPs. With `dedup` set, an operation whose opcode and operands were already seen in
+// FLOPs. With `dedup` = 1, an operation whose opcode and operands were already seen in
 // the same environment step is not counted again: the work of an implementation that
 // evaluates each distinct expression once per step (the reference re-evaluates some
-// track quantities several times per step; the CUDA kernels share them).
+// track quantities several times per step; the CUDA kernels share them). With `dedup` = 2
+// an operation is counted once per step index over all the samples counted: the work of an
+// implementation that also shares what samples have in common at the same step (the
+// verification's ego moves, identical for samples that took the same branch at the same
+// step when the ego draws no noise).
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <unordered_set>
@@ -29,6 +34,7 @@ struct CountCtx
     OpStats s;
     bool dedup = false;
     std::unordered_set<uint64_t> seen;
+    std::vector<std::unordered_set<uint64_t>> seenAt; // dedup 2: per step index
 };
 
 inline thread_local CountCtx* g_ctx = nullptr;
@@ -196,6 +202,8 @@ static int countOps(const EnvT& env, const dr_mppi_config* mc, const S0* s0, con
 {
     CountCtx ctx;
     ctx.dedup = dedup != 0;
+    if (dedup == 2)
+        ctx.seenAt.resize((size_t)std::max(mc->n_timesteps, mc->verif_horizon) + 1);
     const int K = mc->n_samples, T = mc->n_timesteps, nth = env.nth;
     const CF minConf = mc->min_confidence;
     MppiCosts<CF> cc{mc->coll_dist_factor, mc->boundary_cost, mc->boundary_threshold_factor, mc->outside_cost,
@@ -243,7 +251,10 @@ static int countOps(const EnvT& env, const dr_mppi_config* mc, const S0* s0, con
             int H = kind == 0 ? T : mc->verif_horizon;
             for (int t = 0; t < H && !stop; t++)
             {
-                ctx.seen.clear();
+                if (dedup == 2)
+                    std::swap(ctx.seen, ctx.seenAt[t]); // the set of step t over the samples so far
+                else
+                    ctx.seen.clear();
                 g_ctx = nullptr;
                 rng.begin_step((uint32_t)t);
                 int local = t - tOrigin;
@@ -271,6 +282,8 @@ static int countOps(const EnvT& env, const dr_mppi_config* mc, const S0* s0, con
                 else if (term == TERM_LOSE || term == TERM_WIN || term == TERM_OPP_WIN)
                     stop = true;
                 g_ctx = nullptr;
+                if (dedup == 2)
+                    std::swap(ctx.seen, ctx.seenAt[t]);
                 steps += 1;
             }
         }
