@@ -150,14 +150,71 @@ def workload(rank: int):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clocks and clock-event reasons sampled during the timed region: NVML read by a
+    thread every few milliseconds, with one sample taken when the region starts and one when
+    it ends, so that even a short region has samples (nvidia-smi polling as the fallback)."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"), ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"), ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.nv = None
         self.path = Path(f"/tmp/dr_clocks_{os.getpid()}.csv")
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = self._handle(pynvml, index)
+            self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.bits = {name: getattr(pynvml, attr) for name, attr in self.REASONS}
+        except Exception:
+            self.nv = None
+
+    @staticmethod
+    def _handle(pynvml, index: int):
+        """The NVML device of CUDA device `index` (matched by PCI bus id when torch has it)."""
+        try:
+            import torch
+
+            bus = getattr(torch.cuda.get_device_properties(index), "pci_bus_id", None)
+            dom = getattr(torch.cuda.get_device_properties(index), "pci_domain_id", 0)
+            dev = getattr(torch.cuda.get_device_properties(index), "pci_device_id", None)
+            if bus is not None and dev is not None:
+                return pynvml.nvmlDeviceGetHandleByPciBusId(f"{dom:08x}:{bus:02x}:{dev:02x}.0")
+        except Exception:
+            pass
+        return pynvml.nvmlDeviceGetHandleByIndex(index)
+
+    def _sample(self):
+        nv = self.nv
+        sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+        r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+        self.samples.append((sm, {name for name, bit in self.bits.items() if r & bit}))
+
+    def _loop(self):
+        while not self.done.wait(0.005):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def start(self):
+        if self.nv is not None:
+            import threading
+
+            self.samples = []
+            self.done = threading.Event()
+            try:
+                self._sample()
+            except Exception:
+                self.nv = None
+            else:
+                self.thread = threading.Thread(target=self._loop, daemon=True)
+                self.thread.start()
+                return
         q = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
         try:
             self.f = open(self.path, "w")
@@ -167,6 +224,16 @@ class Clocks:
             self.proc = None
 
     def stop(self) -> dict:
+        if self.nv is not None:
+            self.done.set()
+            self.thread.join(timeout=5)
+            try:
+                self._sample()
+            except Exception:
+                pass
+            sm = [x for x, _ in self.samples]
+            reasons = set().union(*(r for _, r in self.samples)) if self.samples else set()
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.mx, "reasons": sorted(reasons), "samples": len(sm), "source": "nvml"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -194,7 +261,7 @@ class Clocks:
             pass
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def _dist():
@@ -432,7 +499,6 @@ def run_ours(args) -> None:
     for _ in range(args.warmup):
         dev_step()
     torch.cuda.synchronize()
-    batch.set_profiling(True)
     _barrier(world)
     torch.cuda.synchronize()
     clocks = Clocks(local)
@@ -448,7 +514,14 @@ def run_ours(args) -> None:
     _barrier(world)
     ms = e0.elapsed_time(e1)
     ms = _max_over_ranks(ms, world)
+    # per-kernel times and the two streams' schedule: a pass after the timed region with
+    # CUDA events between the kernels (launched directly, not replayed from the graph)
+    batch.set_profiling(True)
+    for _ in range(args.steps):
+        dev_step()
+    torch.cuda.synchronize()
     kt = batch.kernel_times()
+    timeline = {k: [round(a, 4), round(b, 4)] for k, (a, b) in batch.kernel_timeline().items()}
     batch.set_profiling(False)
     ms_per_step = ms / args.steps
     value = world * args.steps / (ms / 1e3)
@@ -535,6 +608,7 @@ def run_ours(args) -> None:
         "rollout_steps_per_s": world * rollout_steps * args.steps / (ms / 1e3),
         "verify_steps_per_s": world * AGENTS * 2 * V * VERIF_H * args.steps / (ms / 1e3),
         "kernel_ms": kt,
+        "kernel_timeline_ms": timeline,
         "kernel_ms_serial": kt_serial,
         "e2e": None if args.quick else {"value": world * args.steps / e2e_s, "unit": "control steps/s", "h2d_bytes_per_step": h2d,
                                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s / args.steps * 1e3},
@@ -661,7 +735,6 @@ def run_ours_pr(args) -> None:
     for _ in range(args.warmup):
         batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
     torch.cuda.synchronize()
-    batch.set_profiling(True)
     _barrier(world)
     torch.cuda.synchronize()
     clocks = Clocks(local)
@@ -676,6 +749,11 @@ def run_ours_pr(args) -> None:
     clk = clocks.stop()
     _barrier(world)
     ms = _max_over_ranks(e0.elapsed_time(e1), world)
+    # per-kernel times: a pass after the timed region with CUDA events between the kernels
+    batch.set_profiling(True)
+    for _ in range(args.steps):
+        batch.step_dev(st_dev.data_ptr(), bel_dev.data_ptr())
+    torch.cuda.synchronize()
     kt = batch.kernel_times()
     batch.set_profiling(False)
     ms_per_step = ms / args.steps

@@ -311,6 +311,7 @@ _PROTOS = {
     "dr_prmppi_shard_begin": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dr_prmppi_shard_finish": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "dr_mppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
+    "dr_mppi_batch_get_kernel_timeline": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "dr_prmppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_prmppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "dr_mppi_debug_noise": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_size_t]),
@@ -319,6 +320,7 @@ _PROTOS = {
     "dr_mppi_debug_verify": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "dr_mppi_debug_stage_timeout": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "dr_mppi_set_verify_exact": (C.c_int, [C.c_void_p, C.c_int]),
+    "dr_mppi_set_ego_table": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_predict": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
                                   C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "dr_mppi_batch_predict_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),

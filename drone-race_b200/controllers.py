@@ -90,6 +90,11 @@ class MPPIController(Controller):
         oracle's per-sample results; the default fast flavour agrees in distribution."""
         check(lib().dr_mppi_set_verify_exact(self._h, int(bool(on))), "dr_mppi_set_verify_exact")
 
+    def set_ego_table(self, on: bool = True) -> None:
+        """Whether the fast verification reads the ego from the shared ego tables
+        (dr_mppi_set_ego_table; the default) or moves it in every sample."""
+        check(lib().dr_mppi_set_ego_table(self._h, int(bool(on))), "dr_mppi_set_ego_table")
+
     def close(self) -> None:
         if self._h:
             lib().dr_mppi_destroy(self._h)
@@ -375,17 +380,22 @@ class MPPIBatch:
         check(lib().dr_mppi_batch_create(arr, len(controllers), C.c_void_p(stream) if stream else None, C.byref(b)), "dr_mppi_batch_create")
         self._b = b
         self.infos = (abi.dr_mppi_info * len(controllers))()
+        # per-call buffers, allocated once (the call sits in closed control loops)
+        n = len(controllers)
+        gate = controllers[0].gate
+        self._st = ((abi.dr_gate_state if gate else abi.dr_sim_state) * n)()
+        self._bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+        self._out = np.zeros((n, 2), np.float32)
+        self._step = lib().dr_gate_mppi_batch_step if gate else lib().dr_mppi_batch_step
+        self._args = (self._st, abi.fptr(self._bel), abi.fptr(self._out), self.infos)
 
     def step(self, states, beliefs: np.ndarray) -> np.ndarray:
-        n = len(self.ctls)
-        gate = self.ctls[0].gate
-        st = ((abi.dr_gate_state if gate else abi.dr_sim_state) * n)(*states)
-        bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
-        bel[:, : beliefs.shape[1]] = beliefs
-        out = np.zeros((n, 2), np.float32)
-        step = lib().dr_gate_mppi_batch_step if gate else lib().dr_mppi_batch_step
-        check(step(self._b, st, abi.fptr(bel), abi.fptr(out), self.infos), "dr_mppi_batch_step")
-        return out
+        for i, s in enumerate(states):
+            self._st[i] = s
+        self._bel[:, : beliefs.shape[1]] = beliefs
+        self._bel[:, beliefs.shape[1]:] = 0.0
+        check(self._step(self._b, *self._args), "dr_mppi_batch_step")
+        return self._out.copy()
 
     def set_graph(self, on: bool) -> None:
         check(lib().dr_mppi_batch_set_graph(self._b, int(on)), "dr_mppi_batch_set_graph")
@@ -455,6 +465,15 @@ class MPPIBatch:
     def kernel_times(self) -> dict[str, float]:
         return _kernel_times(lib().dr_mppi_batch_get_kernel_times, self._b)
 
+    def kernel_timeline(self) -> dict[str, tuple[float, float]]:
+        """(start, end) of each timed kernel in ms after the start of the step."""
+        names = (C.c_char_p * 16)()
+        st = (C.c_float * 16)()
+        en = (C.c_float * 16)()
+        cnt = C.c_int()
+        check(lib().dr_mppi_batch_get_kernel_timeline(self._b, names, st, en, 16, C.byref(cnt)), "get_kernel_timeline")
+        return {names[i].decode(): (float(st[i]), float(en[i])) for i in range(cnt.value)}
+
     def close(self) -> None:
         if self._b:
             lib().dr_mppi_batch_destroy(self._b)
@@ -475,15 +494,19 @@ class PRMPPIBatch:
         check(lib().dr_prmppi_batch_create(arr, len(controllers), C.c_void_p(stream) if stream else None, C.byref(b)), "dr_prmppi_batch_create")
         self._b = b
         self.infos = (abi.dr_prmppi_info * len(controllers))()
+        n = len(controllers)
+        self._st = (abi.dr_sim_state * n)()
+        self._bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
+        self._out = np.zeros((n, 2), np.float32)
+        self._args = (self._st, abi.fptr(self._bel), abi.fptr(self._out), self.infos)
 
     def step(self, states, beliefs: np.ndarray) -> np.ndarray:
-        n = len(self.ctls)
-        st = (abi.dr_sim_state * n)(*states)
-        bel = np.zeros((n, abi.DR_MAX_THETA), np.float32)
-        bel[:, : beliefs.shape[1]] = beliefs
-        out = np.zeros((n, 2), np.float32)
-        check(lib().dr_prmppi_batch_step(self._b, st, abi.fptr(bel), abi.fptr(out), self.infos), "dr_prmppi_batch_step")
-        return out
+        for i, s in enumerate(states):
+            self._st[i] = s
+        self._bel[:, : beliefs.shape[1]] = beliefs
+        self._bel[:, beliefs.shape[1]:] = 0.0
+        check(lib().dr_prmppi_batch_step(self._b, *self._args), "dr_prmppi_batch_step")
+        return self._out.copy()
 
     def step_dev(self, states_dev_ptr: int, beliefs_dev_ptr: int) -> None:
         check(lib().dr_prmppi_batch_step_dev(self._b, C.c_void_p(states_dev_ptr), C.c_void_p(beliefs_dev_ptr)), "dr_prmppi_batch_step_dev")

@@ -48,12 +48,14 @@ struct dr_mppi
     bool spl = false;
     // verification flavour: exact (per-sample parity with the oracle) or fast (default)
     bool exactVerify = false;
+    bool egoTableOn = true; // dr_mppi_set_ego_table
 
-    // The fast verification takes the ego's moves from the ego tables: they exist and no
-    // noise of the environment moves the ego.
+    // The fast verification takes the ego's moves from the ego tables: they exist, are
+    // switched on and no noise of the environment moves the ego.
     bool egoTableUsable() const
     {
-        return !exactVerify && desc.egoTab && env.action_noise_level == 0.0f && env.pos_noise_level == 0.0f && env.speed_noise_level == 0.0f;
+        return !exactVerify && egoTableOn && desc.egoTab && env.action_noise_level == 0.0f && env.pos_noise_level == 0.0f &&
+               env.speed_noise_level == 0.0f;
     }
     DevScratch predBuf; // dr_mppi_predict's inputs and outputs on the device
     Arena arena;
@@ -364,12 +366,24 @@ struct dr_mppi_batch
             timer->mark("prologue", ex);
         }
         CK(launchMppiPrologue(args(nullptr, 0, in), n, proSmem));
-        // The previous plan's verification needs only the prologue's shifted plan, so it
-        // runs on a second stream while the rollout (a few warps per SM) and the update
-        // run on the first; the new plan's verification follows the update.
+        // The previous plan's verification needs only the prologue's shifted plan and that
+        // plan's ego table, so it runs on a second stream while the rollout (a few warps per
+        // SM) and the update run on the first; the new plan's verification follows the
+        // update. The previous plan's table is computed here, on the critical stream, before
+        // the fork: alone on the device it takes a few tens of microseconds, beside the
+        // rollout several times longer (its single warp per table row issues behind the
+        // rollout's warps), and the side verification could not start before it ends.
         bool side = verify && overlap && nVerOld > 0;
         if (side)
-            CK(cudaEventRecord(evFork, ex)); // the side verification depends on the prologue only
+        {
+            if (egoTable())
+            {
+                if (profile)
+                    timer->mark("ego_table_old", ex);
+                CK(launchEgo(ex, in, 1));
+            }
+            CK(cudaEventRecord(evFork, ex)); // the side verification depends on the prologue and the table
+        }
         if (profile)
             timer->mark("rollout", ex);
         // the rollout is enqueued (captured) before the side verification, so that its
@@ -381,11 +395,8 @@ struct dr_mppi_batch
             if (profile)
             {
                 timerSide.begin();
-                timerSide.mark("ego_table_old", sideStream);
-            }
-            CK(launchEgo(sideStream, in, 1));
-            if (profile)
                 timerSide.mark("verify_old", sideStream);
+            }
             CK(launchQueued(qargs(dVerOld, nVerOld, in, Q_VER_OLD, sidePerSm, sideStream), true));
             if (profile)
             {
@@ -1857,6 +1868,18 @@ int dr_mppi_set_verify_exact(dr_mppi* h, int on)
     return DR_OK;
 }
 
+int dr_mppi_set_ego_table(dr_mppi* h, int on)
+{
+    if (!h)
+        return fail(DR_ERR_INVALID_ARG, "NULL handle");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    h->egoTableOn = on != 0;
+    h->self->dropGraph();
+    h->self->dropDevGraph();
+    return DR_OK;
+}
+
 int dr_mppi_debug_stage_timeout(dr_mppi* h, int on, int polls)
 {
     if (!h)
@@ -1894,6 +1917,14 @@ extern "C" int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** nam
         return fail(DR_ERR_INVALID_ARG, "NULL batch");
     CK(cudaSetDevice(b->device));
     return kernelTimes(b->timer, names, ms, n, count, &b->timerSide);
+}
+
+extern "C" int dr_mppi_batch_get_kernel_timeline(dr_mppi_batch* b, const char** names, float* start_ms, float* end_ms, int n, int* count)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    CK(cudaSetDevice(b->device));
+    return kernelTimeline(b->timer, names, start_ms, end_ms, n, count, &b->timerSide);
 }
 
 extern "C" int dr_mppi_batch_set_overlap(dr_mppi_batch* b, int on)

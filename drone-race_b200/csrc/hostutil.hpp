@@ -406,6 +406,29 @@ struct Timer
             ms[j] = (float)(sum / steps);
         }
     }
+    // Times of this timer's marks after the first mark of `ref` in the same step (the
+    // start of the step), averaged over the steps both timers recorded.
+    std::vector<float> offsets(const Timer& ref) const
+    {
+        const int n = std::min(steps, ref.steps);
+        std::vector<float> off(nm, 0.0f);
+        if (n == 0 || ref.nm == 0)
+            return off;
+        cudaEventSynchronize(ev[(size_t)(steps - 1) * MAXM + nm - 1]);
+        cudaEventSynchronize(ref.ev[(size_t)(ref.steps - 1) * MAXM + ref.nm - 1]);
+        for (int j = 0; j < nm; j++)
+        {
+            double sum = 0.0;
+            for (int s = 0; s < n; s++)
+            {
+                float x = 0.0f;
+                cudaEventElapsedTime(&x, ref.ev[(size_t)s * MAXM], ev[(size_t)s * MAXM + j]);
+                sum += x;
+            }
+            off[j] = (float)(sum / n);
+        }
+        return off;
+    }
     ~Timer()
     {
         for (auto e : ev)
@@ -433,6 +456,32 @@ inline int kernelTimes(Timer& t, const char** names, float* ms, int n, int* coun
                     names[c] = tm->names[i].c_str();
                 if (ms)
                     ms[c] = tm->ms[i];
+            }
+    }
+    if (count)
+        *count = c;
+    return DR_OK;
+}
+
+// Start and end of every timed kernel after the start of the step (the main timer's
+// first mark), averaged over the recorded steps: the schedule of the two streams.
+inline int kernelTimeline(Timer& t, const char** names, float* start, float* end, int n, int* count, Timer* side = nullptr)
+{
+    int c = 0;
+    for (Timer* tm : {&t, side})
+    {
+        if (!tm || tm->steps == 0)
+            continue;
+        const std::vector<float> off = tm->offsets(t);
+        for (int j = 0; j + 1 < tm->nm; j++, c++)
+            if (c < n)
+            {
+                if (names)
+                    names[c] = tm->names[j].c_str();
+                if (start)
+                    start[c] = off[j];
+                if (end)
+                    end[c] = off[j + 1];
             }
     }
     if (count)

@@ -335,6 +335,11 @@ typedef struct dr_tune_report
  * No counterpart in the reference. */
 int dr_mppi_batch_autotune(dr_mppi_batch* b, int reps, dr_tune_report* out);
 int dr_mppi_batch_get_kernel_times(dr_mppi_batch* b, const char** names, float* ms, int n, int* count);
+/* The schedule of the recorded steps: for each timed kernel (the critical-path stream's
+ * and the previous-plan verification stream's), its start and end in ms after the start
+ * of the step (CUDA events; averages over the recorded steps). Kernels of the two
+ * streams overlap where the device ran them concurrently. No counterpart in the reference. */
+int dr_mppi_batch_get_kernel_timeline(dr_mppi_batch* b, const char** names, float* start_ms, float* end_ms, int n, int* count);
 
 /* ---- gradient path (no counterpart in the reference) -----------------------------
  * The objective of an MPPI controller's noise-free rollout of the control sequence U
@@ -452,6 +457,14 @@ int dr_mppi_debug_verify(dr_mppi* h, const dr_sim_state* state, const float* bel
  * equal the CPU oracle's. Controllers of one batch need the same flavour, so set it before
  * batching the controller. */
 int dr_mppi_set_verify_exact(dr_mppi* h, int on);
+/* Whether the fast verification reads the ego's moves from the shared ego tables (on = 1,
+ * the default) or moves the ego in every sample (on = 0). The tables hold, per plan, the
+ * ego's trajectory without branching and for every branch and branching step; they are
+ * built only when no environment noise moves the ego and both plans' tables fit in 16 MiB
+ * (the library's build-time DR_EGO_TABLE_MAX_BYTES). The failure times are the same
+ * either way; off is slower. Set it before batching the controller. No counterpart in the
+ * reference. */
+int dr_mppi_set_ego_table(dr_mppi* h, int on);
 /* Test switch for the bounded device waits (no counterpart in the reference, whose
  * kernels have no device-side wait): while `on` is set, the rollout and verification CTAs
  * of this controller's own steps (dr_mppi_step, the dr_mppi_debug_* hooks) announce their

@@ -40,15 +40,18 @@ def _case(gap=1.2, noise=0.5, accel=6.0, V=2**17, nopp=1, nth=2):
     return sc, plan
 
 
-def _ours(sc, plan, exact):
+def _ours(sc, plan, exact, ego=True, belief=None):
     ctl = drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed)
     if exact:
         ctl.set_verify_exact(True)
+    if not ego:
+        ctl.set_ego_table(False)
     T, V = sc.mppi.n_timesteps, sc.mppi.n_verif_samples
     fc = np.zeros(T, np.uint32)
     ft = np.zeros(V, np.int32)
     th = np.zeros(V, np.int32)
-    abi.check(abi.lib().dr_mppi_debug_verify(ctl.handle, C.byref(sc.state), abi.fptr(sc.belief()), abi.fptr(plan), 0, abi.uptr(fc), abi.iptr(ft),
+    bel = sc.belief() if belief is None else np.asarray(belief, np.float32)
+    abi.check(abi.lib().dr_mppi_debug_verify(ctl.handle, C.byref(sc.state), abi.fptr(bel), abi.fptr(plan), 0, abi.uptr(fc), abi.iptr(ft),
                                              abi.iptr(th)), "debug_verify")
     return fc, ft, th
 
@@ -110,3 +113,19 @@ def test_fast_verification_is_deterministic(gpu):
     a, fa, _ = _ours(sc, plan, exact=False)
     b, fb, _ = _ours(sc, plan, exact=False)
     assert np.array_equal(a, b) and np.array_equal(fa, fb)
+
+
+@pytest.mark.parametrize("gap,noise,belief", [(1.2, 0.5, None), (2.0, 2.0, None), (1.2, 0.5, [0.05, 0.95])])
+def test_ego_table_changes_no_failure_time(gpu, gap, noise, belief):
+    """The fast verification reads the ego before and after each step from the shared ego
+    table (the trajectory without branching, and one per branch and branching step) or moves
+    the ego in every sample (dr_mppi_set_ego_table off): the per-sample failure times and
+    hypotheses are identical. Cases: samples that branch at many steps, and a confident
+    initial belief (the branch is taken before the first step)."""
+    sc, plan = _case(gap=gap, noise=noise, V=2**15)
+    a, fa, ta = _ours(sc, plan, exact=False, ego=True, belief=belief)
+    b, fb, tb = _ours(sc, plan, exact=False, ego=False, belief=belief)
+    assert a.sum() > 0
+    assert np.array_equal(ta, tb)
+    assert np.array_equal(fa, fb), f"{np.sum(fa != fb)} of {fa.size} failure times differ"
+    assert np.array_equal(a, b)
