@@ -126,9 +126,9 @@ def _ref_variant(O) -> str:
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture
 # of each kernel on this workload (--quick --no-overlap, 3 steps); grids, plans and tile
-# tables stay in L2, so DRAM traffic is spilled registers and first-touch reads, about a
-# megabyte per launch.
-TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 1365504.0, "rollout": 145152.0}
+# tables stay in L2, so DRAM traffic is spilled registers and first-touch reads, about 1.5
+# MB per verification launch (both plans, with the ego tables).
+TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 1544192.0, "rollout": 145152.0}
 
 
 def _package():
@@ -460,18 +460,29 @@ def run_ours(args) -> None:
 
     abi = drb.abi
     scs = workload(rank)
-    stream = torch.cuda.Stream()  # non-default stream: the batch captures a CUDA graph on it
-    ctls = [ctl_mod.MPPIController(s.env, s.mppi, s.seed, device=local, stream=stream.cuda_stream) for s in scs]
-    if WL["kind"] == "grad":
-        for c in ctls:
-            c.set_grad_refine(GRAD_STEPS, GRAD_STEP_SIZE, 0)
-    batch = ctl_mod.MPPIBatch(ctls, stream=stream.cuda_stream)
-    if args.no_overlap:
-        batch.set_overlap(False)
-    if args.side_verify is not None:
-        batch.set_side_verify(args.side_verify)
-    if args.pdl:
-        batch.set_pdl(True)
+
+    def make_set(shapes=None):
+        """A fresh batch of the workload's controllers (same scenarios and seeds). The
+        device-resident timing, the end-to-end timing and the per-kernel passes each run on
+        their own set, after the same number of warm-up steps, so that they all start from
+        the same controller state (the per-step work drifts as the plans evolve)."""
+        stream = torch.cuda.Stream()  # non-default stream: the batch captures a CUDA graph on it
+        ctls = [ctl_mod.MPPIController(s.env, s.mppi, s.seed, device=local, stream=stream.cuda_stream) for s in scs]
+        if WL["kind"] == "grad":
+            for c in ctls:
+                c.set_grad_refine(GRAD_STEPS, GRAD_STEP_SIZE, shapes["grad_ckpt"] if shapes else 0)
+        batch = ctl_mod.MPPIBatch(ctls, stream=stream.cuda_stream)
+        if args.no_overlap:
+            batch.set_overlap(False)
+        if args.side_verify is not None:
+            batch.set_side_verify(args.side_verify)
+        if args.pdl:
+            batch.set_pdl(True)
+        if shapes:
+            batch.set_persistent(shapes["rollout_ctas_per_sm"], shapes["verify_ctas_per_sm"], bool(shapes["rollout_lockstep"]))
+        return stream, ctls, batch
+
+    stream, ctls, batch = make_set()
     n = len(ctls)
     states = [s.state for s in scs]
     beliefs = np.stack([s.belief() for s in scs])
@@ -485,9 +496,9 @@ def run_ours(args) -> None:
     info_dev = torch.zeros(C.sizeof(abi.dr_mppi_info) * n, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
 
-    def dev_step():
+    def dev_step(b=None):
         # the whole control step on the device, its tail included (dr_mppi_batch_step_device)
-        batch.step_device(st_dev.data_ptr(), bel_dev.data_ptr(), act_dev.data_ptr(), info_dev.data_ptr())
+        (b or batch).step_device(st_dev.data_ptr(), bel_dev.data_ptr(), act_dev.data_ptr(), info_dev.data_ptr())
 
     # ---- device-resident throughput -------------------------------------------------------
     for _ in range(args.warmup):
@@ -514,58 +525,68 @@ def run_ours(args) -> None:
     _barrier(world)
     ms = e0.elapsed_time(e1)
     ms = _max_over_ranks(ms, world)
-    # per-kernel times and the two streams' schedule: a pass after the timed region with
-    # CUDA events between the kernels (launched directly, not replayed from the graph)
-    batch.set_profiling(True)
-    for _ in range(args.steps):
-        dev_step()
-    torch.cuda.synchronize()
-    kt = batch.kernel_times()
-    timeline = {k: [round(a, 4), round(b, 4)] for k, (a, b) in batch.kernel_timeline().items()}
-    batch.set_profiling(False)
     ms_per_step = ms / args.steps
     value = world * args.steps / (ms / 1e3)
 
     # ---- end to end through the C ABI with host buffers -----------------------------------
-    for c in ctls:
-        c.engine = object()
-    e2e_steps = 0 if args.quick else args.steps
-    for _ in range(0 if args.quick else args.warmup):
-        batch.step(states, beliefs)
-    torch.cuda.synchronize()
-    _barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        batch.step(states, beliefs)
-    t1 = time.perf_counter()
-    _barrier(world)
-    e2e_s = _max_over_ranks(max(t1 - t0, 1e-9), world)
+    # a second set of controllers, warmed up by as many steps as the first before its timed
+    # region and launched with the shapes the autotuner chose
+    e2e_s = None
     h2d = d2h = 0
-    for c in ctls:
-        a, b = C.c_size_t(), C.c_size_t()
-        abi.lib().dr_mppi_io_bytes(c.handle, C.byref(a), C.byref(b))
-        h2d += a.value
-        d2h += b.value
+    if not args.quick:
+        _, ctls_h, batch_h = make_set(tune)
+        for c in ctls_h:
+            c.engine = object()
+        for _ in range(2 * args.warmup):
+            batch_h.step(states, beliefs)
+        torch.cuda.synchronize()
+        _barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            batch_h.step(states, beliefs)
+        t1 = time.perf_counter()
+        _barrier(world)
+        e2e_s = _max_over_ranks(max(t1 - t0, 1e-9), world)
+        for c in ctls_h:
+            a, b = C.c_size_t(), C.c_size_t()
+            abi.lib().dr_mppi_io_bytes(c.handle, C.byref(a), C.byref(b))
+            h2d += a.value
+            d2h += b.value
+        batch_h.close()
+        for c in ctls_h:
+            c.close()
 
-    # ---- roofline of the dominant kernel --------------------------------------------------
-    # With the previous-plan verification beside the rollout, the two verification launches
-    # share the SMs with each other and with the rollout, so their event durations are not
-    # per-kernel times. A short pass after the timed region, with the verification of both
-    # plans in one launch on the main stream, measures the kernels one at a time.
-    kt_serial, serial_steps = kt, args.steps
+    # ---- per-kernel times, the streams' schedule and the roofline --------------------------
+    # A third set, warmed up like the first, with CUDA events between the kernels (launched
+    # directly, not replayed from the graph). First a pass with the verification of both
+    # plans in one launch on the main stream (the kernels one at a time: in the overlapped
+    # schedule the two verification launches share the SMs with each other and with the
+    # rollout, so their event durations are not per-kernel times), then the default
+    # overlapped schedule.
+    _, ctls_p, batch_p = make_set(tune)
+    for _ in range(2 * args.warmup):
+        dev_step(batch_p)
+    torch.cuda.synchronize()
+    serial_steps = max(10, min(50, args.steps))
+    kt_serial = None
     if not args.no_overlap:
-        batch.set_overlap(False)
-        serial_steps = max(10, min(50, args.steps))
-        for _ in range(3):
-            dev_step()
-        torch.cuda.synchronize()
-        batch.set_profiling(True)
+        batch_p.set_overlap(False)
+        batch_p.set_profiling(True)
         for _ in range(serial_steps):
-            dev_step()
+            dev_step(batch_p)
         torch.cuda.synchronize()
-        kt_serial = batch.kernel_times()
-        batch.set_profiling(False)
-        batch.set_overlap(True)
+        kt_serial = batch_p.kernel_times()
+        batch_p.set_profiling(False)
+        batch_p.set_overlap(True)
+    batch_p.set_profiling(True)
+    for _ in range(args.steps):
+        dev_step(batch_p)
+    torch.cuda.synchronize()
+    kt = batch_p.kernel_times()
+    timeline = {k: [round(a, 4), round(b, 4)] for k, (a, b) in batch_p.kernel_timeline().items()}
+    batch_p.set_profiling(False)
+    if kt_serial is None:
+        kt_serial, serial_steps = kt, args.steps
     units = {"rollout": AGENTS * _K() * N_THETA * H, "verify": AGENTS * 2 * V * VERIF_H}
     flops_unit = dict(zip(("rollout", "verify"), _flops()))
     dom = max(kt_serial, key=kt_serial.get) if kt_serial else None
@@ -610,8 +631,8 @@ def run_ours(args) -> None:
         "kernel_ms": kt,
         "kernel_timeline_ms": timeline,
         "kernel_ms_serial": kt_serial,
-        "e2e": None if args.quick else {"value": world * args.steps / e2e_s, "unit": "control steps/s", "h2d_bytes_per_step": h2d,
-                                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s / args.steps * 1e3},
+        "e2e": None if e2e_s is None else {"value": world * args.steps / e2e_s, "unit": "control steps/s", "h2d_bytes_per_step": h2d,
+                                           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s / args.steps * 1e3},
         "gpu_launches": len(kt) * args.steps,
         "autotune": {"rollout_ctas_per_sm": tune["rollout_ctas_per_sm"], "rollout_lockstep": tune["rollout_lockstep"],
                      "verify_ctas_per_sm": tune["verify_ctas_per_sm"], "grad_ckpt": tune["grad_ckpt"],
@@ -625,9 +646,10 @@ def run_ours(args) -> None:
         line["grad_vs_plain"] = closed_loop_compare()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    batch.close()
-    for c in ctls:
-        c.close()
+    for b_, cs_ in ((batch, ctls), (batch_p, ctls_p)):
+        b_.close()
+        for c in cs_:
+            c.close()
     if world > 1:
         import torch.distributed as dist
 

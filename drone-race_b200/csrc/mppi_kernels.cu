@@ -29,7 +29,17 @@
 namespace dr
 {
 
-constexpr int RB = 128; // rollout / verification block size
+// Rollout block size: RB / n_theta samples a CTA, one thread per (sample, hypothesis), up
+// to 128 registers a thread. 256: a rollout CTA takes the registers of one verification
+// CTA, so in the overlapped step the SMs that hold one run one verification CTA beside it
+// (128 CTAs for 4 x 4096 x 2 threads; 1.53 against 1.55 ms per step with 128-thread CTAs,
+// which spread over every SM; 512-thread CTAs: 1.55 ms, the rollout alone 0.39 against
+// 0.32 ms).
+#ifndef DR_ROLLOUT_BLOCK
+#define DR_ROLLOUT_BLOCK 256
+#endif
+constexpr int RB = DR_ROLLOUT_BLOCK;
+constexpr int RB_MIN_BLOCKS = RB <= 128 ? 4 : 512 / RB; // register budget of 128 a thread
 // Verification CTAs per SM that the register allocation is sized for (VERIFY_TILE = 512
 // threads a CTA: 2 -> 64 registers a thread). Measured on the 4 x 2^17 x 40 verification
 // (B200, 1965 MHz): 128-thread CTAs without the per-step barrier 3.14 ms (72 registers);
@@ -321,7 +331,7 @@ __device__ __forceinline__ void rolloutTile(const MppiDev& D, const MppiIn& I, c
 }
 
 template <int NOPP, int NTH, bool SPL, bool PQ, bool LOCK>
-__global__ void __launch_bounds__(RB, 4) mppi_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in,
+__global__ void __launch_bounds__(RB, RB_MIN_BLOCKS) mppi_rollout(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in,
                                                                        const Tile* __restrict__ tiles, int nTiles, unsigned* __restrict__ queue)
 {
     constexpr int NBP = NTH + 1;
