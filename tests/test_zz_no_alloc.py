@@ -23,15 +23,20 @@ def _regular_costs(ctl, sc, belief):
     return costs
 
 
-@pytest.mark.parametrize("spl", [False, True])
-def test_noalloc_rollout_matches_regular_entry_point(gpu, spl):
+@pytest.mark.parametrize("spl,confident", [(False, False), (True, False), (False, True)])
+def test_noalloc_rollout_matches_regular_entry_point(gpu, spl, confident):
+    """confident: a belief above the confidence threshold commits every sample to the
+    second hypothesis's branch, so the first branch has no compatible sample and its costs
+    are infinite: the non-finite costs reach the caller as the regular path reports them."""
     import torch
 
     sc = small_mppi(spl, K=1500, T=40, M=10, noise=True)
     rng = np.random.default_rng(21)
     ctl = mppi_ctl(sc, nominal=random_nominal(sc, rng))
-    belief = np.array([0.35, 0.65], np.float32)
+    belief = np.array([0.02, 0.98] if confident else [0.35, 0.65], np.float32)
     expect = _regular_costs(ctl, sc, belief)
+    if confident:
+        assert np.isinf(expect[1]).all()
     knots = torch.from_numpy(np.ascontiguousarray(ctl.knots())).cuda()
     for _ in range(2):
         out = torch.full((sc.n_theta + 1, sc.mppi.n_samples), float("nan"), dtype=torch.float32, device="cuda")
