@@ -101,7 +101,14 @@ __device__ __forceinline__ void storeGState(dr_gate_state& s, const GState& g)
     }
 }
 
-// sampleCenterline, env_dronerace.h:55-64
+// sampleCenterline, env_dronerace.h:55-64. The interpolation (1 - t) p0 + t p1 has two
+// products, and the compiler fuses one of them into the addition. The reference's PR-MPPI
+// kernels (prmppi_kernels.cu, built for the gate race) fuse the first,
+// fma(1 - t, p0, t p1): FUSE_FIRST states that explicitly (found by tracing one
+// PRMPPIfullRolloutKernel sample step by step: the PID target, and from it the opponent's
+// velocity, differed in the last bits from the other fusion). Without it the expression
+// is left to the compiler, which then evaluates it as the reference's MPPI kernels do.
+template <bool FUSE_FIRST = false>
 __device__ __forceinline__ void sampleCenterline(const float* __restrict__ tp, float s, float& o0, float& o1)
 {
     s = s - floorf(s);
@@ -109,8 +116,17 @@ __device__ __forceinline__ void sampleCenterline(const float* __restrict__ tp, f
     int idx0 = (int)idx_f;
     int idx1 = (idx0 + 1) % NTS;
     float t = idx_f - idx0;
-    o0 = (1.0f - t) * tp[idx0 * 2 + 0] + t * tp[idx1 * 2 + 0];
-    o1 = (1.0f - t) * tp[idx0 * 2 + 1] + t * tp[idx1 * 2 + 1];
+    if constexpr (FUSE_FIRST)
+    {
+        const float omt = 1.0f - t;
+        o0 = __fmaf_rn(omt, tp[idx0 * 2 + 0], __fmul_rn(t, tp[idx1 * 2 + 0]));
+        o1 = __fmaf_rn(omt, tp[idx0 * 2 + 1], __fmul_rn(t, tp[idx1 * 2 + 1]));
+    }
+    else
+    {
+        o0 = (1.0f - t) * tp[idx0 * 2 + 0] + t * tp[idx1 * 2 + 0];
+        o1 = (1.0f - t) * tp[idx0 * 2 + 1] + t * tp[idx1 * 2 + 1];
+    }
 }
 
 // sqDistToSample, :96-102
@@ -189,8 +205,9 @@ __device__ __forceinline__ float projectGreedy(const float* __restrict__ tp, flo
 }
 
 // computePIDAction, :473-541, for hypothesis th. The agent is a template parameter and
-// the raceline's arc length is selected, so that the state stays in registers.
-template <int AGENT>
+// the raceline's arc length is selected, so that the state stays in registers. PRK: as the
+// reference's PR-MPPI kernels evaluate it (sampleCenterline<true>).
+template <int AGENT, bool PRK = false>
 __device__ __forceinline__ void pidAction(const GState& s, const GateParams& G, const float* __restrict__ track, int th, float& out0, float& out1)
 {
     constexpr int agent = AGENT;
@@ -198,7 +215,7 @@ __device__ __forceinline__ void pidAction(const GState& s, const GateParams& G, 
     const int rl = G.pidRaceline[th];
     const float sRl = rl == 0 ? s.S[agent * G_NR] : s.S[agent * G_NR + 1];
     float tx, ty;
-    sampleCenterline(track + rl * NTS * 2, sRl + G.targetDistance, tx, ty);
+    sampleCenterline<PRK>(track + rl * NTS * 2, sRl + G.targetDistance, tx, ty);
     const float cx = s.pos[agent * 2], cy = s.pos[agent * 2 + 1];
     const float vx = s.vel[agent * 2], vy = s.vel[agent * 2 + 1];
     float sqError = 0.0f;
@@ -388,8 +405,9 @@ template <int AGENT> __device__ __forceinline__ float gateAdvance(const GState& 
 }
 
 // environmentStep<UPD, BR, ADDMARGIN, LOSE>, :546-680. The ego's action is (ego0, ego1);
-// the returned StepOut carries what the running cost needs.
-template <int NTH, bool UPD, bool BR, bool ADDMARGIN, bool LOSE, int ME>
+// the returned StepOut carries what the running cost needs. PRK: the PR-MPPI kernels'
+// evaluation of the PID target (sampleCenterline).
+template <int NTH, bool UPD, bool BR, bool ADDMARGIN, bool LOSE, int ME, bool PRK = false>
 __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* __restrict__ track, const GateParams& G, float ego0, float ego1,
                                             GState& s, BState<NTH>& bs, bool& branched, float minConf, EnvNoise& rng, float gateMargin)
 {
@@ -406,7 +424,7 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
     {
 #pragma unroll
         for (int th = 0; th < NTH; th++)
-            pidAction<opp>(s, G, track, th, nom0[th], nom1[th]);
+            pidAction<opp, PRK>(s, G, track, th, nom0[th], nom1[th]);
         u0 = nom0[0];
         u1 = nom1[0];
 #pragma unroll
@@ -418,7 +436,7 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
             }
     }
     else
-        pidAction<opp>(s, G, track, trueTheta, u0, u1);
+        pidAction<opp, PRK>(s, G, track, trueTheta, u0, u1);
     {
         float an = G.pidNoise[trueTheta];
         if (an != 0.0f)

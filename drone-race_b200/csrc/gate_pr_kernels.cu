@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(GPR_TILE, gatePrMinBlocks<NTH>()) gate_pr_roll
             float ego0 = sNom[t * 2] + scaled_normal(D.cfg.sigma0, r.x);
             float ego1 = sNom[t * 2 + 1] + scaled_normal(D.cfg.sigma1, r.y);
             bool branched = false;
-            StepOut o = gateStep<NTH, false, false, true, true, ME>(t, theta, sTrack, G, ego0, ego1, st, bs, branched, 0.0f, rng, D.cfg.gateMargin);
+            StepOut o = gateStep<NTH, false, false, true, true, ME, true>(t, theta, sTrack, G, ego0, ego1, st, bs, branched, 0.0f, rng, D.cfg.gateMargin);
             if (o.term != TERM_NONE)
                 active = false;
             running += decay * gatePrStateCost(o, G, D.cfg);
@@ -239,8 +239,8 @@ __global__ void __launch_bounds__(GPR_CAND) gate_pr_candidates(const PrDev* __re
         {
             rng.begin_step((uint32_t)t);
             bool branched = false;
-            StepOut o = gateStep<NTH, false, false, true, true, ME>(t, theta, sTrack, G, nominal[t * 2], nominal[t * 2 + 1], st, bs, branched, 0.0f, rng,
-                                                                    D.cfg.gateMargin);
+            StepOut o = gateStep<NTH, false, false, true, true, ME, true>(t, theta, sTrack, G, nominal[t * 2], nominal[t * 2 + 1], st, bs, branched, 0.0f,
+                                                                          rng, D.cfg.gateMargin);
             stop = (o.term != TERM_NONE);
             cost += decay * gatePrStateCost(o, G, D.cfg);
             decay *= DECAY;
