@@ -102,6 +102,9 @@ struct EnvParams
     // log-likelihood (env_stratrace.h:199-203), evaluated once per launch instead of
     // once per step with the same device logf.
     float logSqSigma[8][3];
+    // the fast flavour's Gaussian log-likelihood of an action error e: |e|^2 llScale + llConst,
+    // llScale = -1 / (2 sigma^2), llConst = -log(2 pi) - log(sigma^2) (two action dimensions)
+    float llScale[8][3], llConst[8][3];
     // 1 / trackLength and 1 / dt (the fast flavour multiplies by them)
     float invTrackLength, invDt;
     // Hypotheses that give opponent o the same action as an earlier one: dupAll[th][o] is
@@ -128,6 +131,8 @@ __device__ __forceinline__ void envDeviceTerms(EnvParams& dst, const EnvParams& 
     {
         const int th = i / 3, o = i % 3;
         dst.logSqSigma[th][o] = logf(beliefSqSigma(src.actionNoise[th][o]));
+        dst.llScale[th][o] = -0.5f / beliefSqSigma(src.actionNoise[th][o]);
+        dst.llConst[th][o] = -logf(2.0f * M_PIf32) - dst.logSqSigma[th][o];
         int all = -1, noBlock = -1;
         for (int j = th - 1; j >= 0; j--)
         {
@@ -945,8 +950,13 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
                     float dx1 = act1[o + 1] - n1 * scale;
                     sqDist += dx1 * dx1;
                     float an = E.actionNoise[th][o];
-                    float sqSigma = beliefSqSigma(an);
-                    logLikelihood += mdiv<F>(-0.5f * sqDist, sqSigma) - (float)2 * 0.5f * logf(2.0f * M_PIf32) - (float)2 * 0.5f * E.logSqSigma[th][o];
+                    if constexpr (F)
+                        logLikelihood += __fmaf_rn(sqDist, E.llScale[th][o], E.llConst[th][o]); // the same terms, constants folded
+                    else
+                    {
+                        float sqSigma = beliefSqSigma(an);
+                        logLikelihood += mdiv<F>(-0.5f * sqDist, sqSigma) - (float)2 * 0.5f * logf(2.0f * M_PIf32) - (float)2 * 0.5f * E.logSqSigma[th][o];
+                    }
                 }
                 bs.belief[th] *= mexp<F>(logLikelihood);
                 sum += bs.belief[th];

@@ -46,6 +46,12 @@ constexpr int RB_MIN_BLOCKS = RB <= 128 ? 4 : 512 / RB; // register budget of 12
 // 128 with the barrier 3.05; 256 x 3 CTAs 2.90; 512 x 2 2.73; 1024 x 1 2.74.
 // The larger models (two opponents, or eight hypotheses) spill heavily at 64 registers
 // and get one CTA per SM instead.
+// Steps between the verification CTA's barriers (measured on the 4 x 2 x 2^17 x 40 launch,
+// B200: a barrier every step 1.292 ms, every 2 steps 1.272, every 4 1.251).
+#ifndef DR_VERIFY_SYNC_STEPS
+#define DR_VERIFY_SYNC_STEPS 4
+#endif
+constexpr int VERIFY_SYNC_STEPS = DR_VERIFY_SYNC_STEPS;
 #ifndef VERIFY_MIN_BLOCKS
 #define VERIFY_MIN_BLOCKS 2
 #endif
@@ -1010,9 +1016,11 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
             bool failed = false;
             for (; t < H; t++)
             {
-                // every thread of the CTA takes this barrier once per step (H is uniform); it
-                // keeps the warps on the same step and ends the loop once all samples are done
-                if (!__syncthreads_or(active))
+                // every thread of the CTA takes this barrier every VERIFY_SYNC_STEPS steps (H
+                // is uniform, so all reach the same ones): it keeps the warps near the same
+                // step, where they fetch the same instructions, and ends the loop once all
+                // samples are done
+                if (t % VERIFY_SYNC_STEPS == 0 && !__syncthreads_or(active))
                     break;
                 if (!active)
                     continue;
