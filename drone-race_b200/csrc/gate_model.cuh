@@ -114,7 +114,7 @@ __device__ __forceinline__ void sampleCenterline(const float* __restrict__ tp, f
     s = s - floorf(s);
     float idx_f = s * NTS;
     int idx0 = (int)idx_f;
-    int idx1 = (idx0 + 1) % NTS;
+    int idx1 = wrapNts(idx0 + 1);
     float t = idx_f - idx0;
     if constexpr (FUSE_FIRST)
     {
@@ -127,6 +127,14 @@ __device__ __forceinline__ void sampleCenterline(const float* __restrict__ tp, f
         o0 = (1.0f - t) * tp[idx0 * 2 + 0] + t * tp[idx1 * 2 + 0];
         o1 = (1.0f - t) * tp[idx0 * 2 + 1] + t * tp[idx1 * 2 + 1];
     }
+}
+
+// (g + 1) % n for a gate index g >= 0: the remainder only when the index wraps, which a
+// gate index in [0, n) does at the last gate
+__device__ __forceinline__ int nextGateIndex(int g, int n)
+{
+    const int next = g + 1;
+    return next < n ? next : next % n;
 }
 
 // sqDistToSample, :96-102
@@ -167,13 +175,13 @@ __device__ __forceinline__ int walkMin(const float* __restrict__ tp, int i0, flo
 {
     int bestI = i0;
     bestSq = baseSq;
-    int cur = (i0 + delta + NTS) % NTS;
+    int cur = wrapNts(i0 + delta + NTS);
     float curSq = sqDistToSample(tp, cur, px, py);
     for (int n = 0; curSq < bestSq && n < NTS; n++)
     {
         bestI = cur;
         bestSq = curSq;
-        cur = (cur + delta + NTS) % NTS;
+        cur = wrapNts(cur + delta + NTS);
         curSq = sqDistToSample(tp, cur, px, py);
     }
     for (int i = 0; i < 10; i++)
@@ -184,7 +192,7 @@ __device__ __forceinline__ int walkMin(const float* __restrict__ tp, int i0, flo
             bestI = cur;
             bestSq = curSq;
         }
-        cur = (cur + delta + NTS) % NTS;
+        cur = wrapNts(cur + delta + NTS);
     }
     return bestI;
 }
@@ -194,7 +202,7 @@ __device__ __forceinline__ float projectGreedy(const float* __restrict__ tp, flo
 {
     if (prevS < 0)
         return projectFull(tp, px, py);
-    int baseI = (int)(prevS * NTS + 0.5f) % NTS;
+    int baseI = wrapNts((int)(prevS * NTS + 0.5f)); // prevS >= 0
     float baseSq = sqDistToSample(tp, baseI, px, py);
     float bSq, fSq;
     int bI = walkMin(tp, baseI, px, py, -1, baseSq, bSq);
@@ -282,7 +290,7 @@ __device__ __forceinline__ void updateGates(const GateParams& G, const float* __
 #pragma unroll
             for (int r = 0; r < G_NR; r++)
                 s.S[a * G_NR + r] = projectGreedy(track + r * NTS * 2, px, py, s.S[a * G_NR + r]);
-        const int next = (s.gates[a] + 1) % G.nGates;
+        const int next = nextGateIndex(s.gates[a], G.nGates);
         const float gc0 = G.gateCenters[next * 2], gc1 = G.gateCenters[next * 2 + 1];
         const float gv0 = G.gateVectors[next * 2], gv1 = G.gateVectors[next * 2 + 1];
         const float pp0 = prevPos[a * 2], pp1 = prevPos[a * 2 + 1];
@@ -392,7 +400,7 @@ template <int AGENT> __device__ __forceinline__ float gateAdvance(const GState& 
 {
     constexpr int agent = AGENT;
     float sqGateDist = 0.0f, sqConsGateDist = 0.0f;
-    int nextGate = (s.gates[agent] + 1) % G.nGates;
+    int nextGate = nextGateIndex(s.gates[agent], G.nGates);
     float scale = 0.8f;
     const float* prevC = G.gateCenters + s.gates[agent] * 2;
     const float* nextC = G.gateCenters + nextGate * 2;

@@ -293,7 +293,7 @@ __device__ __forceinline__ GPos gpos(Dv s, float L)
 
 __device__ __forceinline__ void gsample2(const float* __restrict__ arr, GPos q, Dv& o0, Dv& o1)
 {
-    const int i0 = q.i0, i1 = (i0 + 1) % NTS;
+    const int i0 = q.i0, i1 = wrapNts(i0 + 1);
     const Dv om = 1.0f - q.w;
     o0 = om * arr[i0 * 2 + 0] + q.w * arr[i1 * 2 + 0];
     o1 = om * arr[i0 * 2 + 1] + q.w * arr[i1 * 2 + 1];
@@ -301,7 +301,7 @@ __device__ __forceinline__ void gsample2(const float* __restrict__ arr, GPos q, 
 
 __device__ __forceinline__ Dv gsample1(const float* __restrict__ arr, GPos q)
 {
-    const int i0 = q.i0, i1 = (i0 + 1) % NTS;
+    const int i0 = q.i0, i1 = wrapNts(i0 + 1);
     return (1.0f - q.w) * arr[i0] + q.w * arr[i1];
 }
 
@@ -326,7 +326,7 @@ __device__ __forceinline__ Dv gproject(const Track& tr, float L, Dv px, Dv py, f
             bestJ = j;
         }
     }
-    const int bestInd = (bestJ + NTS) % NTS;
+    const int bestInd = wrapNts(bestJ + NTS); // bestJ >= -WIN
     Dv bestSq = cst(INFINITY), bestS = cst(0.0f), cx = cst(0.0f), cy = cst(0.0f);
 #pragma unroll
     for (int seg = -1; seg <= 0; ++seg)

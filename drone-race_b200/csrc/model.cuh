@@ -64,6 +64,13 @@ template <bool F> __device__ __forceinline__ float mexp(float x)
 }
 
 constexpr int NTS = 512;       // N_TRACK_SAMPLES (env_stratrace_defs.h:11)
+static_assert((NTS & (NTS - 1)) == 0, "the track sample count is a power of two");
+// x % NTS for x >= 0, which every track index taken modulo NTS here is (one AND instead of
+// the signed remainder's sequence)
+__host__ __device__ __forceinline__ int wrapNts(int x)
+{
+    return x & (NTS - 1);
+}
 constexpr int WIN = 10;        // WINDOW_SIZE (env_stratrace_defs.h:40)
 constexpr float DECAY = 0.97f; // include/config.h:30
 constexpr float MIN_COEFF = 0.01f; // MIN_COEFF_THRESHOLD, include/config.h:29
@@ -230,7 +237,7 @@ __device__ __forceinline__ Track trackIn(const float* grids)
 __device__ __forceinline__ void sampleAt2(const float* __restrict__ arr, TrackPos q, float& o0, float& o1)
 {
     const int idx0 = q.i0;
-    const int idx1 = (idx0 + 1) % NTS;
+    const int idx1 = wrapNts(idx0 + 1);
     const float t = q.w;
     o0 = (1.0f - t) * arr[idx0 * 2 + 0] + t * arr[idx1 * 2 + 0];
     o1 = (1.0f - t) * arr[idx0 * 2 + 1] + t * arr[idx1 * 2 + 1];
@@ -239,7 +246,7 @@ __device__ __forceinline__ void sampleAt2(const float* __restrict__ arr, TrackPo
 __device__ __forceinline__ float sampleAt1(const float* __restrict__ arr, TrackPos q)
 {
     const int idx0 = q.i0;
-    const int idx1 = (idx0 + 1) % NTS;
+    const int idx1 = wrapNts(idx0 + 1);
     const float t = q.w;
     return (1.0f - t) * arr[idx0] + t * arr[idx1];
 }
@@ -263,7 +270,7 @@ template <bool F>
 __device__ __forceinline__ float projectSegments(const Track& tr, float L, float invL, float px, float py, int bestJ, float& latDist, TrackPos& tpS)
 {
     const float2* __restrict__ P2 = reinterpret_cast<const float2*>(tr.p);
-    const int bestInd = (bestJ + NTS) % NTS;
+    const int bestInd = wrapNts(bestJ + NTS); // bestJ >= -WIN
     float bestSegSqDist = INFINITY;
     float bestS = 0.0f;
     float closestX = 0.0f, closestY = 0.0f;

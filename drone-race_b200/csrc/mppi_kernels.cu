@@ -42,16 +42,15 @@ constexpr int RB = DR_ROLLOUT_BLOCK;
 constexpr int RB_MIN_BLOCKS = RB <= 128 ? 4 : 512 / RB; // register budget of 128 a thread
 // Verification CTAs per SM that the register allocation is sized for (VERIFY_TILE = 512
 // threads a CTA: 2 -> 64 registers a thread). Measured on the 4 x 2^17 x 40 verification
-// (B200, 1965 MHz): 128-thread CTAs without the per-step barrier 3.14 ms (72 registers);
-// 128 with the barrier 3.05; 256 x 3 CTAs 2.90; 512 x 2 2.73; 1024 x 1 2.74.
+// of both plans (B200, 1965 MHz), exact arithmetic and a CTA barrier every step:
+// 128-thread CTAs without the barrier 3.14 ms (72 registers); 128 with the barrier 3.05;
+// 256 x 3 CTAs 2.90; 512 x 2 2.73; 1024 x 1 2.74. The barrier kept the warps of a CTA on
+// the same step, where they fetched the same instructions of the then 55 KB kernel. The
+// fast flavour with the ego tables is smaller and the barrier only held warps back: with
+// it every 1 / 2 / 4 / 16 / 32 steps 1.292 / 1.272 / 1.200 / 1.180 / 1.174 ms, without it
+// 1.171, so the warps now step on their own and leave the loop when their samples are done.
 // The larger models (two opponents, or eight hypotheses) spill heavily at 64 registers
 // and get one CTA per SM instead.
-// Steps between the verification CTA's barriers (measured on the 4 x 2 x 2^17 x 40 launch,
-// B200: a barrier every step 1.292 ms, every 2 steps 1.272, every 4 1.251).
-#ifndef DR_VERIFY_SYNC_STEPS
-#define DR_VERIFY_SYNC_STEPS 4
-#endif
-constexpr int VERIFY_SYNC_STEPS = DR_VERIFY_SYNC_STEPS;
 #ifndef VERIFY_MIN_BLOCKS
 #define VERIFY_MIN_BLOCKS 2
 #endif
@@ -1016,11 +1015,9 @@ __global__ void __launch_bounds__(VERIFY_TILE, (verifyMinBlocks<NOPP, NTH>())) m
             bool failed = false;
             for (; t < H; t++)
             {
-                // every thread of the CTA takes this barrier every VERIFY_SYNC_STEPS steps (H
-                // is uniform, so all reach the same ones): it keeps the warps near the same
-                // step, where they fetch the same instructions, and ends the loop once all
-                // samples are done
-                if (t % VERIFY_SYNC_STEPS == 0 && !__syncthreads_or(active))
+                // a warp leaves the loop once all its samples are done (no CTA barrier in
+                // the loop: see VERIFY_MIN_BLOCKS)
+                if (!__any_sync(0xffffffffu, active))
                     break;
                 if (!active)
                     continue;
