@@ -7,6 +7,8 @@
 // mppi_kernels.cu serve both environments (they see only costs, bookkeeping and plans).
 #include <cstdio>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "gate_model.cuh"
 #include "instance.cuh"
@@ -249,7 +251,10 @@ template <int NTH> constexpr int gateVerifyMinBlocks()
 {
     return NTH <= 4 ? GATE_VERIFY_MIN_BLOCKS : 1;
 }
-template <int NTH, int ME>
+// FAST: the verification's fast arithmetic flavour and noise source (the default; the
+// exact flavour reproduces the oracle's per-sample results and serves parity tests), as
+// in the strategic race's mppi_verify; its warps step without a CTA barrier.
+template <int NTH, int ME, bool FAST>
 __global__ void __launch_bounds__(VERIFY_TILE, (gateVerifyMinBlocks<NTH>())) gate_verify(const MppiDev* __restrict__ insts, const MppiIn* __restrict__ in, const Tile* __restrict__ tiles,
                                                              int* __restrict__ dbgFailTime, int* __restrict__ dbgTheta)
 {
@@ -319,14 +324,22 @@ __global__ void __launch_bounds__(VERIFY_TILE, (gateVerifyMinBlocks<NTH>())) gat
                 }
             }
         }
-        EnvNoise rng(k0, k1, (uint32_t)v, (uint32_t)plan << 16, step, S_VERIF_ENV);
+        using Noise = typename std::conditional<FAST, FastNoise, EnvNoise>::type;
+        Noise rng(k0, k1, (uint32_t)v, (uint32_t)plan << 16, step, S_VERIF_ENV);
         int tOrigin = 0, tEnd = H;
         bool failed = false;
         for (int t = 0; t < H; t++)
         {
-            // every thread takes this barrier once per step (H is uniform); it ends the
-            // loop once all samples of the CTA are done
-            if (!__syncthreads_or(active))
+            // exact flavour: every thread takes this barrier once per step (H is uniform),
+            // which keeps the warps on the same step, where they fetch the same
+            // instructions, and ends the loop once all samples of the CTA are done; fast
+            // flavour: a warp leaves once its samples are done
+            if constexpr (FAST)
+            {
+                if (!__any_sync(0xffffffffu, active))
+                    break;
+            }
+            else if (!__syncthreads_or(active))
                 break;
             if (!active)
                 continue;
@@ -335,7 +348,7 @@ __global__ void __launch_bounds__(VERIFY_TILE, (gateVerifyMinBlocks<NTH>())) gat
             int b = bs.predTheta;
             float e0 = sPlan[(b * T + local) * 2], e1 = sPlan[(b * T + local) * 2 + 1];
             bool branched = false;
-            StepOut o = gateStep<NTH, true, true, false, false, ME>(t, theta, sTrack, G, e0, e1, st, bs, branched, minConf, rng, gateMargin);
+            StepOut o = gateStep<NTH, true, true, false, false, ME, false, FAST, Noise>(t, theta, sTrack, G, e0, e1, st, bs, branched, minConf, rng, gateMargin);
             if (branched)
                 tOrigin = t + 1;
             if (o.term == TERM_LOSE)
@@ -485,7 +498,7 @@ template <int NTH, int ME> static cudaError_t launchGateRolloutT(const LaunchArg
 
 template <int NTH, int ME> static cudaError_t launchGateVerifyT(const LaunchArgs& a, size_t smem, int* ft, int* th)
 {
-    auto k = gate_verify<NTH, ME>;
+    auto k = a.exactVerify ? gate_verify<NTH, ME, false> : gate_verify<NTH, ME, true>;
     ensureSmem(k, smem);
     k<<<a.nTiles, VERIFY_TILE, smem, a.stream>>>(a.mppi, a.mppiIn, a.tiles, ft, th);
     return cudaGetLastError();

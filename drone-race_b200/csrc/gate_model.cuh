@@ -215,7 +215,7 @@ __device__ __forceinline__ float projectGreedy(const float* __restrict__ tp, flo
 // computePIDAction, :473-541, for hypothesis th. The agent is a template parameter and
 // the raceline's arc length is selected, so that the state stays in registers. PRK: as the
 // reference's PR-MPPI kernels evaluate it (sampleCenterline<true>).
-template <int AGENT, bool PRK = false>
+template <int AGENT, bool PRK = false, bool F = false>
 __device__ __forceinline__ void pidAction(const GState& s, const GateParams& G, const float* __restrict__ track, int th, float& out0, float& out1)
 {
     constexpr int agent = AGENT;
@@ -233,7 +233,7 @@ __device__ __forceinline__ void pidAction(const GState& s, const GateParams& G, 
         e = ty - cy;
         sqError += e * e;
     }
-    float invDist = 1.0f / sqrtf(sqError + 1e-5f);
+    float invDist = mdivsqrt<F>(1.0f, sqError + 1e-5f);
     float vParallelMag = 0.0f;
     {
         float dir = (tx - cx) * invDist;
@@ -258,10 +258,10 @@ __device__ __forceinline__ void pidAction(const GState& s, const GateParams& G, 
         float dist2 = 0.0f;
         dist2 += d0 * d0;
         dist2 += d1 * d1;
-        float dist = sqrtf(dist2) + 1e-8f;
+        float dist = msqrt<F>(dist2) + 1e-8f;
         if (dist < G.pidRepD[th] * G.droneRadius * 2.0f)
         {
-            float scale = repF / powf(dist * 0.5f / G.droneRadius, G.pidRepP[th] + 1.0f);
+            float scale = mdiv<F>(repF, powf(dist * 0.5f / G.droneRadius, G.pidRepP[th] + 1.0f));
             out0 -= scale * d0;
             out1 -= scale * d1;
         }
@@ -272,14 +272,14 @@ __device__ __forceinline__ void pidAction(const GState& s, const GateParams& G, 
     const float ma = G.maxAccel[agent];
     if (sqAccel > ma * ma)
     {
-        float fact = ma / sqrtf(sqAccel);
+        float fact = mdivsqrt<F>(ma, sqAccel);
         out0 *= fact;
         out1 *= fact;
     }
 }
 
 // updateGates<addMargin>, :412-470
-template <bool ADDMARGIN>
+template <bool ADDMARGIN, bool F = false>
 __device__ __forceinline__ void updateGates(const GateParams& G, const float* __restrict__ track, GState& s, const float* prevPos, float margin)
 {
 #pragma unroll
@@ -301,7 +301,7 @@ __device__ __forceinline__ void updateGates(const GateParams& G, const float* __
         denom += gv1 * (py - pp1);
         if (fabsf(denom) < 1e-10f)
             continue;
-        float lambda = num / denom;
+        float lambda = mdiv<F>(num, denom);
         if (lambda < 0.f || lambda > 1.f)
             continue;
         float sqDist = 0.f;
@@ -326,7 +326,7 @@ __device__ __forceinline__ void updateGates(const GateParams& G, const float* __
 
 // trackBoundaryDist<false>, :262-307 (the opponent-win shortcut is applied by callers);
 // ME is the ego's index (envConfig.iMppi)
-template <int ME> __device__ __forceinline__ float gateBoundaryDist(const GState& s, const GateParams& G)
+template <int ME, bool F = false> __device__ __forceinline__ float gateBoundaryDist(const GState& s, const GateParams& G)
 {
     constexpr int me = ME;
     const float c0 = s.pos[me * 2], c1 = s.pos[me * 2 + 1];
@@ -340,7 +340,7 @@ template <int ME> __device__ __forceinline__ float gateBoundaryDist(const GState
         sqDist += dist * dist;
         dist = fmaxf(0.0f, fmaxf(G.obstacles[i * 4 + 1] - c1, c1 - G.obstacles[(i * 2 + 1) * 2 + 1]));
         sqDist += dist * dist;
-        minDist = fminf(minDist, sqrtf(sqDist));
+        minDist = fminf(minDist, msqrt<F>(sqDist));
     }
     for (int i = 0; i < G.nRound; i++)
     {
@@ -349,14 +349,14 @@ template <int ME> __device__ __forceinline__ float gateBoundaryDist(const GState
         sqDist += dx * dx;
         dx = c1 - G.roundCenters[i * 2 + 1];
         sqDist += dx * dx;
-        minDist = fminf(minDist, sqrtf(sqDist) - G.roundRadius[i]);
+        minDist = fminf(minDist, msqrt<F>(sqDist) - G.roundRadius[i]);
     }
     float sqDist = 0.0f;
     float dx = s.pos[0] - s.pos[2];
     sqDist += dx * dx;
     dx = s.pos[1] - s.pos[3];
     sqDist += dx * dx;
-    minDist = fminf(minDist, sqrtf(sqDist) - G.droneRadius);
+    minDist = fminf(minDist, msqrt<F>(sqDist) - G.droneRadius);
     return minDist;
 }
 
@@ -414,12 +414,17 @@ template <int AGENT> __device__ __forceinline__ float gateAdvance(const GState& 
 
 // environmentStep<UPD, BR, ADDMARGIN, LOSE>, :546-680. The ego's action is (ego0, ego1);
 // the returned StepOut carries what the running cost needs. PRK: the PR-MPPI kernels'
-// evaluation of the PID target (sampleCenterline).
-template <int NTH, bool UPD, bool BR, bool ADDMARGIN, bool LOSE, int ME, bool PRK = false>
+// evaluation of the PID target (sampleCenterline). With BR, once the sample has committed
+// to a branch (predTheta != 0) its belief is read by nothing any more (the branch test
+// runs only while predTheta == 0, and the callers with BR return costs, branch records
+// and failure times, never the belief), so the belief update and the other hypotheses'
+// PID actions it needs are skipped; no output changes.
+template <int NTH, bool UPD, bool BR, bool ADDMARGIN, bool LOSE, int ME, bool PRK = false, bool F = false, class RNG = EnvNoise>
 __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* __restrict__ track, const GateParams& G, float ego0, float ego1,
-                                            GState& s, BState<NTH>& bs, bool& branched, float minConf, EnvNoise& rng, float gateMargin)
+                                            GState& s, BState<NTH>& bs, bool& branched, float minConf, RNG& rng, float gateMargin)
 {
     constexpr int me = ME, opp = 1 - ME;
+    const bool live = !BR || bs.predTheta == 0; // the belief is still read after this step
     float prevPos[G_NA * 2];
 #pragma unroll
     for (int i = 0; i < G_NA * 2; i++)
@@ -428,15 +433,15 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
     // of them; without the belief update only the true one is used)
     float nom0[UPD ? NTH : 1], nom1[UPD ? NTH : 1];
     float u0, u1;
-    if constexpr (UPD)
+    if (UPD && live)
     {
 #pragma unroll
-        for (int th = 0; th < NTH; th++)
-            pidAction<opp, PRK>(s, G, track, th, nom0[th], nom1[th]);
+        for (int th = 0; th < (UPD ? NTH : 1); th++)
+            pidAction<opp, PRK, F>(s, G, track, th, nom0[th], nom1[th]);
         u0 = nom0[0];
         u1 = nom1[0];
 #pragma unroll
-        for (int th = 1; th < NTH; th++)
+        for (int th = 1; th < (UPD ? NTH : 1); th++)
             if (th == trueTheta)
             {
                 u0 = nom0[th];
@@ -444,7 +449,7 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
             }
     }
     else
-        pidAction<opp, PRK>(s, G, track, trueTheta, u0, u1);
+        pidAction<opp, PRK, F>(s, G, track, trueTheta, u0, u1);
     {
         float an = G.pidNoise[trueTheta];
         if (an != 0.0f)
@@ -468,7 +473,7 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
         float factor = 1.0f;
         float maxSq = G.maxAccel[a] * G.maxAccel[a];
         if (sqNorm > maxSq)
-            factor = G.maxAccel[a] / sqrtf(sqNorm);
+            factor = mdivsqrt<F>(G.maxAccel[a], sqNorm);
 #pragma unroll
         for (int d = 0; d < 2; d++)
         {
@@ -491,10 +496,10 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
         float sq = 0.0f;
         sq += s.vel[a * 2] * s.vel[a * 2];
         sq += s.vel[a * 2 + 1] * s.vel[a * 2 + 1];
-        float spd = sqrtf(sq);
+        float spd = msqrt<F>(sq);
         if (spd > G.maxSpeed[a])
         {
-            float sc = G.maxSpeed[a] / spd;
+            float sc = mdiv<F>(G.maxSpeed[a], spd);
             s.vel[a * 2] *= sc;
             s.vel[a * 2 + 1] *= sc;
         }
@@ -512,42 +517,45 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
         }
     }
     // 8. gates
-    updateGates<ADDMARGIN>(G, track, s, prevPos, gateMargin);
+    updateGates<ADDMARGIN, F>(G, track, s, prevPos, gateMargin);
     // 9. belief (updateBelief, :212-258)
     if constexpr (UPD)
     {
-        const float maxPIDaccel = G.maxAccel[opp];
-        const float oa0 = me == 0 ? act[2] : act[0], oa1 = me == 0 ? act[3] : act[1];
-        float sum = 0.0f;
-#pragma unroll
-        for (int th = 0; th < NTH; th++)
+        if (live)
         {
-            float sqAccel = 0.f;
-            sqAccel += nom0[th] * nom0[th];
-            sqAccel += nom1[th] * nom1[th];
-            float scale = 1.0f;
-            if (sqAccel > maxPIDaccel * maxPIDaccel)
-                scale = maxPIDaccel / sqrtf(sqAccel);
-            float sqDist = 0.f;
-            float dx = oa0 - nom0[th] * scale;
-            sqDist += dx * dx;
-            dx = oa1 - nom1[th] * scale;
-            sqDist += dx * dx;
-            bs.belief[th] *= expf(-0.5f * sqDist / G.beliefSig2[th]) / G.beliefNorm[th];
-            sum += bs.belief[th];
-        }
-        if (sum < 1e-20f)
-        {
-            float uniform = 1.0f / NTH;
-#pragma unroll
-            for (int th = 0; th < NTH; ++th)
-                bs.belief[th] = uniform;
-        }
-        else
-        {
+            const float maxPIDaccel = G.maxAccel[opp];
+            const float oa0 = me == 0 ? act[2] : act[0], oa1 = me == 0 ? act[3] : act[1];
+            float sum = 0.0f;
 #pragma unroll
             for (int th = 0; th < NTH; th++)
-                bs.belief[th] /= sum;
+            {
+                float sqAccel = 0.f;
+                sqAccel += nom0[th] * nom0[th];
+                sqAccel += nom1[th] * nom1[th];
+                float scale = 1.0f;
+                if (sqAccel > maxPIDaccel * maxPIDaccel)
+                    scale = mdivsqrt<F>(maxPIDaccel, sqAccel);
+                float sqDist = 0.f;
+                float dx = oa0 - nom0[th] * scale;
+                sqDist += dx * dx;
+                dx = oa1 - nom1[th] * scale;
+                sqDist += dx * dx;
+                bs.belief[th] *= mdiv<F>(mexp<F>(mdiv<F>(-0.5f * sqDist, G.beliefSig2[th])), G.beliefNorm[th]);
+                sum += bs.belief[th];
+            }
+            if (sum < 1e-20f)
+            {
+                float uniform = 1.0f / NTH;
+#pragma unroll
+                for (int th = 0; th < NTH; ++th)
+                    bs.belief[th] = uniform;
+            }
+            else
+            {
+#pragma unroll
+                for (int th = 0; th < NTH; th++)
+                    bs.belief[th] = mdiv<F>(bs.belief[th], sum);
+            }
         }
     }
     if constexpr (BR)
@@ -563,7 +571,7 @@ __device__ __forceinline__ StepOut gateStep(int t, int trueTheta, const float* _
     // terminal checks (:672-679)
     StepOut r;
     bool oppWon = s.laps[opp] >= G.nWinLaps;
-    float bdRaw = gateBoundaryDist<ME>(s, G);
+    float bdRaw = gateBoundaryDist<ME, F>(s, G);
     bool winner = gateIsWinner<ME>(s, G);
     float bdTerm = (LOSE && oppWon) ? -1.0f : bdRaw;
     int term = TERM_NONE;

@@ -16,8 +16,13 @@ abi = drb.abi
 S = drb.scenarios
 
 
-def _ctl(sc, nominal=None):
-    return drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed, nominal=nominal)
+def _ctl(sc, nominal=None, exact_verify=False):
+    """exact_verify: the verification's exact flavour, whose per-sample results equal the
+    oracle's (the tests that compare failure times or plan choices with the oracle)."""
+    ctl = drb.controllers.MPPIController(sc.env, sc.mppi, sc.seed, nominal=nominal)
+    if exact_verify:
+        ctl.set_verify_exact(True)
+    return ctl
 
 
 def _dev_rollout(ctl, sc, belief):
@@ -129,7 +134,7 @@ def test_gate_rollout_matches_oracle_with_noise(gpu, spl):
 
 def test_gate_verification_matches_oracle(gpu):
     sc = small_gate(False, K=256, T=40, n_verif=4096, noise=True, agent=1, gap=0.02)
-    ctl = _ctl(sc)
+    ctl = _ctl(sc, exact_verify=True)
     plan = toward_opponent_plan(sc)
     belief = sc.belief()
     fc = np.zeros(sc.mppi.n_timesteps, np.uint32)
@@ -152,7 +157,7 @@ def test_gate_full_steps_match_oracle(gpu):
     sc = small_gate(True, K=1024, T=40, n_verif=2048, noise=True, agent=3)
     rng = np.random.default_rng(5)
     nominal = random_nominal(sc, rng, 0.5)
-    ctl = _ctl(sc, nominal=nominal)
+    ctl = _ctl(sc, nominal=nominal, exact_verify=True)
     ctl.engine = object()
     ref = OracleMPPI(sc, nominal=nominal)
     belief = sc.belief()
@@ -226,3 +231,43 @@ def test_cpp_adapter_on_the_gate_race(gpu):
         a = ctl.getControl(sc.state)
         assert np.array_equal(a, acts[k])
         assert np.array_equal(ctl.h_nominal, noms[k])
+
+
+
+def _gate_fail_counts(sc, plan, exact, seed_ref=None):
+    if seed_ref is not None:
+        fc = np.zeros(sc.mppi.n_timesteps, np.uint32)
+        rc = O.ref(O.gate_variant_name(False)).refc_mppi_verify(C.byref(sc.env), C.byref(sc.mppi), C.byref(sc.state), O._f(sc.belief()),
+                                                               O._f(plan), seed_ref, O._u(fc))
+        assert rc == 0
+        return fc
+    ctl = _ctl(sc, exact_verify=exact)
+    fc = np.zeros(sc.mppi.n_timesteps, np.uint32)
+    abi.check(abi.lib().dr_gate_mppi_debug_verify(ctl.handle, C.byref(sc.state), abi.fptr(sc.belief()), abi.fptr(plan), 0, abi.uptr(fc), None, None),
+              "debug_verify")
+    return fc
+
+
+def test_gate_fast_verification_matches_reference_in_distribution(gpu):
+    """The gate race's verification in the fast flavour (the default: the hardware's
+    approximate division, square root and exponential, Box-Muller PID noise) against the
+    reference's verifyNominalFailureKernel built for the gate race (curand hypotheses and
+    noise) and against this library's exact flavour: with V = 2^17 samples each, the
+    cumulative failure fractions differ by less than 5 standard deviations of a
+    difference of two binomial proportions at every step. The case: the ego driven at the
+    PID opponent (noise 0.5) from 2 % of a lap behind, so that a fair share collides."""
+    sc = small_gate(False, K=256, T=40, n_verif=2**17, noise=True, agent=1, gap=0.02)
+    plan = toward_opponent_plan(sc)
+    V = sc.mppi.n_verif_samples
+    fast = _gate_fail_counts(sc, plan, exact=False)
+    exact = _gate_fail_counts(sc, plan, exact=True)
+    ref = _gate_fail_counts(sc, plan, exact=False, seed_ref=31)
+    assert 0.05 < fast.sum() / V < 0.95, f"failure fraction {fast.sum() / V}"
+    for name, a, b in (("fast vs reference", fast, ref), ("fast vs exact", fast, exact), ("exact vs reference", exact, ref)):
+        Fa = np.cumsum(a.astype(np.float64)) / V
+        Fb = np.cumsum(b.astype(np.float64)) / V
+        p = 0.5 * (Fa + Fb)
+        sd = np.sqrt(np.maximum(p * (1 - p), 1.0 / V) * 2.0 / V)
+        z = np.abs(Fa - Fb) / sd
+        print(f"{name}: failure fraction {Fa[-1]:.4f} vs {Fb[-1]:.4f}, largest difference {z.max():.2f} sd")
+        assert z.max() < 5.0, f"{name}: {z.max():.2f} sd"
