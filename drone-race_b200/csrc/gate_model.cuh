@@ -21,9 +21,22 @@ constexpr int G_NA = DR_GATE_AGENTS;    // env_dronerace_defs.h:8
 constexpr int G_NR = DR_GATE_RACELINES; // env_dronerace_defs.h:17
 constexpr int G_MAXG = DR_GATE_MAX_GATES;
 constexpr int G_MAXO = DR_GATE_MAX_OBSTACLES;
-// racelines [G_NR][NTS][2] plus the sample read when s wraps to exactly 1.0f (the last
-// raceline's first sample), padded to 16 bytes
-constexpr int GATE_TRACK_FLOATS = G_NR * NTS * 2 + 4;
+// Track buffer: the racelines [G_NR][NTS][2] plus the sample read when s wraps to exactly
+// 1.0f (the last raceline's first sample), padded to 16 bytes; then every raceline again as
+// a row of x and a row of y with G_RPAD wrapped samples on each side (samples -G_RPAD ..
+// NTS + G_RPAD - 1, 8-byte aligned at even samples), read two samples at a time by the
+// raceline walk's margin scan.
+constexpr int G_RPAD = 16;
+constexpr int G_ROW = NTS + 2 * G_RPAD;
+constexpr int GATE_INTERLEAVED_FLOATS = G_NR * NTS * 2 + 4;
+constexpr int GATE_TRACK_FLOATS = GATE_INTERLEAVED_FLOATS + G_NR * 2 * G_ROW;
+static_assert(GATE_TRACK_FLOATS % 4 == 0 && G_ROW % 2 == 0 && G_RPAD % 2 == 0 && G_RPAD > 10, "gate track layout");
+
+// raceline r's x row at its sample 0 (the y row follows at + G_ROW)
+__host__ __device__ __forceinline__ const float* gateRowX(const float* track, int r)
+{
+    return track + GATE_INTERLEAVED_FLOATS + 2 * r * G_ROW + G_RPAD;
+}
 
 struct GateParams
 {
@@ -170,43 +183,74 @@ static __device__ __noinline__ float projectFull(const float* __restrict__ tp, f
 }
 
 // findMinAlongDirection, :105-140. The walk ends within NTS samples (the distance
-// decreases strictly along it); the bound only makes that explicit.
-__device__ __forceinline__ int walkMin(const float* __restrict__ tp, int i0, float px, float py, int delta, float baseSq, float& bestSq)
+// decreases strictly along it); the bound only makes that explicit. The margin's ten
+// samples (the walk's stop and the nine after it) are evaluated as pairs of consecutive
+// samples from the padded x / y rows with packed FP32x2 arithmetic (each lane rounds as
+// sqDistToSample's scalar sub, mul and fma do), then compared in the walk's order.
+template <int DELTA>
+__device__ __forceinline__ int walkMin(const float* __restrict__ tp, const float* __restrict__ rowX, int i0, float px, float py, float baseSq, float& bestSq)
 {
     int bestI = i0;
     bestSq = baseSq;
-    int cur = wrapNts(i0 + delta + NTS);
+    int cur = wrapNts(i0 + DELTA + NTS);
     float curSq = sqDistToSample(tp, cur, px, py);
     for (int n = 0; curSq < bestSq && n < NTS; n++)
     {
         bestI = cur;
         bestSq = curSq;
-        cur = wrapNts(cur + delta + NTS);
+        cur = wrapNts(cur + DELTA + NTS);
         curSq = sqDistToSample(tp, cur, px, py);
     }
-    for (int i = 0; i < 10; i++)
+    // samples cur + k DELTA, k = 0..9, lie in [lo, lo + 11] with lo even, inside the rows'
+    // padding (cur - 9 >= -9, cur + 9 <= 520)
+    const int lo = (DELTA > 0 ? cur : cur - 9) & ~1;
+    const int off = cur - lo; // DELTA > 0: 0 or 1; DELTA < 0: 9 or 10
+    // from sample -G_RPAD of the raceline's rows
+    const uint64_t* __restrict__ X2 = reinterpret_cast<const uint64_t*>(rowX - G_RPAD);
+    const uint64_t* __restrict__ Y2 = reinterpret_cast<const uint64_t*>(rowX - G_RPAD + G_ROW);
+    uint64_t pxx, pyy;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(pxx) : "f"(px));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(pyy) : "f"(py));
+    float d[12];
+#pragma unroll
+    for (int q = 0; q < 6; q++)
     {
-        curSq = sqDistToSample(tp, cur, px, py);
+        const int pi = (lo + G_RPAD) / 2 + q;
+        asm("{\n\t.reg .b64 d0, d1, s;\n\t"
+            "sub.rn.f32x2 d0, %2, %4;\n\t"
+            "sub.rn.f32x2 d1, %3, %5;\n\t"
+            "mul.rn.f32x2 s, d0, d0;\n\t"
+            "fma.rn.f32x2 s, d1, d1, s;\n\t"
+            "mov.b64 {%0, %1}, s;\n\t}"
+            : "=f"(d[2 * q]), "=f"(d[2 * q + 1])
+            : "l"(X2[pi]), "l"(Y2[pi]), "l"(pxx), "l"(pyy));
+    }
+#pragma unroll
+    for (int k = 0; k < 10; k++)
+    {
+        // the distance of sample cur + k DELTA: d[off + k DELTA], off taken from its two values
+        const int a = DELTA > 0 ? k : 9 - k;
+        curSq = (DELTA > 0 ? (off & 1) : (off == 10)) ? d[a + 1] : d[a];
         if (curSq < bestSq)
         {
-            bestI = cur;
+            bestI = wrapNts(cur + k * DELTA + NTS);
             bestSq = curSq;
         }
-        cur = wrapNts(cur + delta + NTS);
     }
     return bestI;
 }
 
-// fastProjectOnTrack, :143-209 (its distance output is unused on the path)
-__device__ __forceinline__ float projectGreedy(const float* __restrict__ tp, float px, float py, float prevS)
+// fastProjectOnTrack, :143-209 (its distance output is unused on the path); tp the
+// raceline's interleaved samples, rowX its padded x row (gateRowX)
+__device__ __forceinline__ float projectGreedy(const float* __restrict__ tp, const float* __restrict__ rowX, float px, float py, float prevS)
 {
     if (prevS < 0)
         return projectFull(tp, px, py);
     int baseI = wrapNts((int)(prevS * NTS + 0.5f)); // prevS >= 0
     float baseSq = sqDistToSample(tp, baseI, px, py);
     float bSq, fSq;
-    int bI = walkMin(tp, baseI, px, py, -1, baseSq, bSq);
-    int fI = walkMin(tp, baseI, px, py, +1, baseSq, fSq);
+    int bI = walkMin<-1>(tp, rowX, baseI, px, py, baseSq, bSq);
+    int fI = walkMin<+1>(tp, rowX, baseI, px, py, baseSq, fSq);
     if (fSq < bSq)
         return ((float)fI) / NTS;
     return ((float)bI) / NTS;
@@ -289,7 +333,7 @@ __device__ __forceinline__ void updateGates(const GateParams& G, const float* __
         if (s.S[a * G_NR] >= 0.0f)
 #pragma unroll
             for (int r = 0; r < G_NR; r++)
-                s.S[a * G_NR + r] = projectGreedy(track + r * NTS * 2, px, py, s.S[a * G_NR + r]);
+                s.S[a * G_NR + r] = projectGreedy(track + r * NTS * 2, gateRowX(track, r), px, py, s.S[a * G_NR + r]);
         const int next = nextGateIndex(s.gates[a], G.nGates);
         const float gc0 = G.gateCenters[next * 2], gc1 = G.gateCenters[next * 2 + 1];
         const float gv0 = G.gateVectors[next * 2], gv1 = G.gateVectors[next * 2 + 1];

@@ -254,7 +254,8 @@ inline GateParams toGateParams(const dr_gate_env_config& c)
     return g;
 }
 
-// racelines plus the sample the reference reads when s wraps to exactly 1.0f
+// racelines plus the sample the reference reads when s wraps to exactly 1.0f, then each
+// raceline's padded x and y rows (the gate track buffer's layout, gate_model.cuh)
 inline std::vector<float> packGateTrack(const dr_gate_env_config& c)
 {
     std::vector<float> t(GATE_TRACK_FLOATS, 0.0f);
@@ -263,6 +264,14 @@ inline std::vector<float> packGateTrack(const dr_gate_env_config& c)
         t[i] = c.track_points[i];
     t[n] = c.track_points[(size_t)(G_NR - 1) * NTS * 2];
     t[n + 1] = c.track_points[(size_t)(G_NR - 1) * NTS * 2 + 1];
+    for (int r = 0; r < G_NR; r++)
+        for (int j = -G_RPAD; j < NTS + G_RPAD; j++)
+        {
+            const int src = ((j % NTS) + NTS) % NTS;
+            const size_t row = (size_t)GATE_INTERLEAVED_FLOATS + (size_t)2 * r * G_ROW + G_RPAD + j;
+            t[row] = c.track_points[((size_t)r * NTS + src) * 2];
+            t[row + G_ROW] = c.track_points[((size_t)r * NTS + src) * 2 + 1];
+        }
     return t;
 }
 
