@@ -57,15 +57,21 @@ VERIF_H = 40
 # mppi_ego_table computes them once per plan): counting each distinct operation once per
 # step index over the samples (opcount dedup mode 2) leaves 337 FLOPs per sample-step,
 # the work the verification kernel has to do; 571 is a sample's own work in isolation.
+# Work whose result nothing reads (a committed sample's belief update and the other
+# hypotheses' actions, which the kernels skip) is left out too; on this workload's first
+# steps no sample commits within the horizon, so the counts stay 652 / 337.
+# `python oracle/count_flops.py` reproduces every count of this file.
 FLOPS_PER_ROLLOUT_STEP = 652.0    # MPPI rollout step (belief update over 2 hypotheses)
 FLOPS_PER_VERIFY_STEP = 337.0     # verification step, ego moves shared across samples
 
 # --workload gates: the same control step on the gate race (the reference's EnvDroneRace:
 # one PID opponent with 2 hypotheses, 8 gates on a 30 x 20 m ellipse, 2 racelines), FLOPs
-# per step counted the same way on oracle/port/gate_model.hpp (orc_gate_count_ops).
+# per step counted the same way on oracle/port/gate_model.hpp (orc_gate_count_ops): 405.7
+# per rollout step (487.0 with the committed samples' dead belief work), 328.4 per
+# verification step (475.7 as one sample's own work with that dead work).
 N_GATES = 8
-GATE_FLOPS_PER_ROLLOUT_STEP = 486.3
-GATE_FLOPS_PER_VERIFY_STEP = 473.4
+GATE_FLOPS_PER_ROLLOUT_STEP = 405.7
+GATE_FLOPS_PER_VERIFY_STEP = 328.4
 
 # --workload grad: gradient-refined MPPI on the strategic race, a quarter of the samples
 # (K = 1024) and one projected gradient step (--grad-steps) of the noise-free rollout objective after each

@@ -155,6 +155,9 @@ struct Flags
     bool loseOnOppWin;
     bool applyNoise;
     float gateMargin;
+    // operation counting only: with considerBranching, skip the belief update and the other
+    // hypotheses' PID actions once the sample has committed (nothing reads that belief)
+    bool skipDeadBelief = false;
 };
 
 // agentSpeed, env_dronerace.h:43-52
@@ -511,8 +514,10 @@ inline int environmentStep(int t, int trueTheta, const Env<R>& env, const R* ego
                 actions[a * DIM + d] = egoAction[d];
         else
         {
+            const bool dead = f.skipDeadBelief && f.considerBranching && bs.predTheta != 0;
             for (int th = 0; th < env.nth; th++)
-                pidAction(a, s, env, env.pid[th], nomPid + th * DIM);
+                if (!dead || th == trueTheta)
+                    pidAction(a, s, env, env.pid[th], nomPid + th * DIM);
             for (int d = 0; d < DIM; d++)
             {
                 R u = nomPid[trueTheta * DIM + d];
@@ -566,7 +571,7 @@ inline int environmentStep(int t, int trueTheta, const Env<R>& env, const R* ego
             }
     updateGates(env, s, prevPos, f.addMargin, (R)f.gateMargin);
     const int opp = 1 - env.iMppi;
-    if (f.updateBelief)
+    if (f.updateBelief && !(f.skipDeadBelief && f.considerBranching && bs.predTheta != 0))
         updateBelief(env, bs.belief, actions + opp * DIM, nomPid, env.maxAccel[opp]);
     if (f.considerBranching)
     {

@@ -597,6 +597,9 @@ struct StepFlags
     bool loseOnOppWin;
     bool applyNoise;
     bool allThetaOppActions; // compute the nominal opponent action for every theta (reference), or only the true one
+    // operation counting only: with considerBranching, skip the belief update and the other
+    // hypotheses' actions once the sample has committed (nothing reads that belief any more)
+    bool skipDeadBelief = false;
 };
 
 // environmentStep, :711-894. The noise source is any object with next().
@@ -613,10 +616,11 @@ inline int environmentStep(int t, int trueTheta, const Env<R>& env, const R* ego
     R nomOpp[DR_MAX_THETA * DR_MAX_OPP * DIM];
     for (int d = 0; d < DIM; d++)
         actions[d] = egoAction[d];
+    const bool dead = f.skipDeadBelief && f.considerBranching && bs.predTheta != 0;
     for (int o = 1; o <= env.nopp; o++)
     {
         for (int th = 0; th < env.nth; th++)
-            if (f.allThetaOppActions || th == trueTheta)
+            if ((f.allThetaOppActions && !dead) || th == trueTheta)
                 computeOpponentAction(o, s, env, &nomOpp[(th * env.nopp + o - 1) * DIM], th);
         for (int d = 0; d < DIM; d++)
         {
@@ -685,7 +689,7 @@ inline int environmentStep(int t, int trueTheta, const Env<R>& env, const R* ego
         if (s.S[a] > prevS[a] + env.trackLength * R(0.5))
             s.laps[a]--;
     }
-    if (f.updateBelief)
+    if (f.updateBelief && !dead)
         updateBelief(env, bs.belief, actions + DIM, nomOpp);
     if (f.considerBranching)
     {

@@ -11,7 +11,9 @@
 // an operation is counted once per step index over all the samples counted: the work of an
 // implementation that also shares what samples have in common at the same step (the
 // verification's ego moves, identical for samples that took the same branch at the same
-// step when the ego draws no noise).
+// step when the ego draws no noise). `dedup | 4` also leaves out work whose result nothing
+// reads: once a sample has committed to a branch, its belief update and the other
+// hypotheses' opponent actions (the kernels skip them; the reference does them).
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -200,6 +202,10 @@ template <typename EnvT, typename StateT, typename S0, typename MakeFlags>
 static int countOps(const EnvT& env, const dr_mppi_config* mc, const S0* s0, const float* belief0, const float* nominal, const float* noise,
                     uint64_t seed, uint64_t step, int nsamples, int kind, int dedup, double* out, MakeFlags makeFlags)
 {
+    // dedup | 4: skip the work whose result nothing reads (the belief update and the other
+    // hypotheses' actions once a sample has committed to a branch), as the kernels do
+    const bool skipDead = (dedup & 4) != 0;
+    dedup &= 3;
     CountCtx ctx;
     ctx.dedup = dedup != 0;
     if (dedup == 2)
@@ -247,7 +253,8 @@ static int countOps(const EnvT& env, const dr_mppi_config* mc, const S0* s0, con
             bool stop = false;
             int tOrigin = 0;
             EnvNoise rng(seed, (uint32_t)s, kind == 0 ? ((uint32_t)theta << 16) : 0u, step, kind == 0 ? S_MPPI_ROLL_ENV : S_VERIF_ENV);
-            const auto flags = makeFlags(kind);
+            auto flags = makeFlags(kind);
+            flags.skipDeadBelief = skipDead;
             int H = kind == 0 ? T : mc->verif_horizon;
             for (int t = 0; t < H && !stop; t++)
             {
