@@ -314,6 +314,7 @@ _PROTOS = {
     "dr_mppi_batch_get_kernel_timeline": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "dr_prmppi_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_prmppi_batch_get_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
+    "dr_prmppi_batch_set_rollout_slots": (C.c_int, [C.c_void_p, C.c_int]),
     "dr_mppi_debug_noise": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_size_t]),
     "dr_mppi_debug_rollout": (C.c_int, [C.c_void_p, C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "dr_mppi_debug_update": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),

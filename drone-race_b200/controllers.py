@@ -511,6 +511,11 @@ class PRMPPIBatch:
     def step_dev(self, states_dev_ptr: int, beliefs_dev_ptr: int) -> None:
         check(lib().dr_prmppi_batch_step_dev(self._b, C.c_void_p(states_dev_ptr), C.c_void_p(beliefs_dev_ptr)), "dr_prmppi_batch_step_dev")
 
+    def set_rollout_slots(self, slots: int) -> None:
+        """Hypothesis slots per rollout thread, sharing the ego's moves
+        (dr_prmppi_batch_set_rollout_slots); bit-identical costs for every choice."""
+        check(lib().dr_prmppi_batch_set_rollout_slots(self._b, int(slots)), "dr_prmppi_batch_set_rollout_slots")
+
     def set_profiling(self, on: bool) -> None:
         check(lib().dr_prmppi_batch_set_profiling(self._b, int(on)), "dr_prmppi_batch_set_profiling")
 

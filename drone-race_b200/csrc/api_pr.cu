@@ -121,6 +121,9 @@ struct dr_prmppi
     }
 };
 
+// Hypothesis slots per PR-MPPI rollout thread by default (dr_prmppi_batch_set_rollout_slots).
+constexpr int DEFAULT_PR_SLOTS = 1;
+
 struct dr_prmppi_batch
 {
     std::vector<dr_prmppi*> hs;
@@ -146,6 +149,21 @@ struct dr_prmppi_batch
     cudaGraphExec_t devGraphExec = nullptr;
     const void* devKey[2] = {nullptr, nullptr};
 
+    // hypothesis slots per rollout thread (dr_prmppi_batch_set_rollout_slots)
+    int prSlots = DEFAULT_PR_SLOTS;
+
+    // the slots a rollout thread may take: several only where every controller's ego
+    // draws no noise (its moves are then shared by the slots) and P is a multiple
+    int slotsFor(int want) const
+    {
+        if (envKind != 0 || want <= 1)
+            return 1;
+        for (auto* h : hs)
+            if (h->env.action_noise_level != 0.0f || h->env.pos_noise_level != 0.0f || h->env.speed_noise_level != 0.0f || h->P % want != 0)
+                return 1;
+        return want;
+    }
+
     LaunchArgs args(const Tile* tiles, int n, const PrIn* in) const
     {
         LaunchArgs a;
@@ -154,6 +172,7 @@ struct dr_prmppi_batch
         a.prIn = in;
         a.tiles = tiles;
         a.nTiles = n;
+        a.prSlots = slotsFor(prSlots);
         return a;
     }
 
@@ -285,6 +304,16 @@ struct dr_prmppi_batch
         CK(cudaStreamSynchronize(stream));
         hs[0]->finish(action, info);
         return hs[0]->lastTimeouts ? timedOut(hs[0]->lastTimeouts) : DR_OK;
+    }
+
+    void dropGraph()
+    {
+        if (graphExec)
+            cudaGraphExecDestroy(graphExec);
+        if (graph)
+            cudaGraphDestroy(graph);
+        graphExec = nullptr;
+        graph = nullptr;
     }
 
     void dropDevGraph()
@@ -1115,6 +1144,20 @@ extern "C" int dr_gate_env_step(const dr_gate_env_config* env, int true_theta, c
         belief[i] = io.belief[i];
     if (term)
         *term = io.term;
+    return DR_OK;
+}
+
+extern "C" int dr_prmppi_batch_set_rollout_slots(dr_prmppi_batch* b, int slots)
+{
+    if (!b)
+        return fail(DR_ERR_INVALID_ARG, "NULL batch");
+    if (slots != 1 && slots != 2 && slots != 4)
+        return fail(DR_ERR_INVALID_ARG, "slots must be 1, 2 or 4");
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->stream));
+    b->dropGraph();
+    b->dropDevGraph();
+    b->prSlots = slots;
     return DR_OK;
 }
 

@@ -35,6 +35,8 @@ struct LaunchArgs
     // fast verification: 1 = the ego's moves come from the instances' ego tables
     // (mppi_ego_table must have filled them for the plans verified)
     int egoTable = 0;
+    // PR-MPPI rollout: hypothesis slots per thread (1, 2, 4), sharing the ego's moves
+    int prSlots = 1;
 };
 
 inline int launchGrid(const LaunchArgs& a)

@@ -176,6 +176,7 @@ struct EnvNoise
     uint32_t k0, k1, c0, c1base, step, stream, t;
     int j;
     U4 cur;
+    EnvNoise() = default; // for arrays of streams, assigned before use
     __device__ __forceinline__ EnvNoise(uint32_t k0_, uint32_t k1_, uint32_t c0_, uint32_t c1base_, uint32_t step_, uint32_t stream_)
         : k0(k0_), k1(k1_), c0(c0_), c1base(c1base_), step(step_), stream(stream_), t(0), j(0), cur{0, 0, 0, 0}
     {

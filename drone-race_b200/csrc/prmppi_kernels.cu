@@ -133,10 +133,126 @@ __host__ __device__ inline PrRollSmem prLayout(int T)
     return L;
 }
 
+// pr_rollout's body for HPT > 1 slots per thread (see pr_rollout): thread i rolls out
+// slots pg HPT .. pg HPT + HPT - 1 of sample i / (P / HPT), pg = i % (P / HPT).
+template <int NOPP, int NTH, int HPT>
+__device__ __forceinline__ void prRolloutShared(const PrDev& D, const PrIn& I, const Tile& tile, const EnvParams& E, const Track& tr, const float* sNom,
+                                                float* red, int K, int T, int P, int robust, int spb)
+{
+    constexpr int NA = NOPP + 1;
+    const int G = P / HPT;
+    const int sl = threadIdx.x / G, pg = threadIdx.x % G;
+    const int s = tile.s0 + sl;
+    const bool valid = sl < spb && sl < tile.count;
+    const uint32_t k0 = D.cfg.k0, k1 = D.cfg.k1, step = I.step;
+    const SafetyMargin margin = safetyMargin(E, D.cfg.collDistFactor);
+    float running[HPT], safe[HPT];
+    bool active[HPT];
+    int theta[HPT];
+    DState<NA> st[HPT];
+    EnvNoise rng[HPT];
+    DState<1> ego;
+    {
+        DState<NA> s0;
+        loadState<NA>(s0, I.state);
+        s0.locate(E.trackLength);
+        ego.pos[0] = s0.pos[0];
+        ego.pos[1] = s0.pos[1];
+        ego.vel[0] = s0.vel[0];
+        ego.vel[1] = s0.vel[1];
+        ego.S[0] = s0.S[0];
+        ego.lat[0] = s0.lat[0];
+        ego.laps[0] = s0.laps[0];
+        ego.tp[0] = s0.tp[0];
+#pragma unroll
+        for (int h = 0; h < HPT; h++)
+        {
+            const int p = pg * HPT + h;
+            running[h] = 0.0f;
+            safe[h] = -INFINITY;
+            active[h] = valid;
+            theta[h] = D.thetas[p];
+            st[h] = s0;
+            rng[h] = EnvNoise(k0, k1, (uint32_t)s, ((((uint32_t)robust << 8) | (uint32_t)p) << 16), step, S_PR_ROLL_ENV);
+        }
+    }
+    BState<NTH> bs{};
+    float decay = 1.0f;
+    for (int t = 0; t < T; t++)
+    {
+        bool any = false;
+#pragma unroll
+        for (int h = 0; h < HPT; h++)
+            any = any || active[h];
+        // every thread of the CTA takes this barrier once per step (T is uniform)
+        if (!__syncthreads_or(any))
+            break;
+        if (!any)
+            continue;
+        U4 r = draw(k0, k1, (uint32_t)s, (uint32_t)t, step, S_PR_EPS, 0);
+        float ego0 = sNom[t * 2] + scaled_normal(D.cfg.sigma0, r.x);
+        float ego1 = sNom[t * 2 + 1] + scaled_normal(D.cfg.sigma1, r.y);
+        EgoRow row;
+        egoStep<false>(tr, E, ego0, ego1, ego, row);
+#pragma unroll
+        for (int h = 0; h < HPT; h++)
+        {
+            if (!active[h])
+                continue;
+            rng[h].begin_step((uint32_t)t);
+            bool branched = false;
+            StepOut o = envStep<NOPP, NTH, false, false, true, false, false, EnvNoise, true>(t, theta[h], tr, E, ego0, ego1, st[h], bs, branched, 0.0f,
+                                                                                           rng[h], &row);
+            if (o.term != TERM_NONE)
+                active[h] = false;
+            running[h] += decay * prStateCost(o, E, D.cfg.boundaryThresholdFactor, D.cfg.boundaryCost, D.cfg.winCost, D.cfg.oppWinCost);
+            safe[h] = fmaxf(safe[h], prSafetyCost(o, margin));
+        }
+        decay *= DECAY;
+    }
+#pragma unroll
+    for (int h = 0; h < HPT; h++)
+    {
+        const int p = pg * HPT + h;
+        if (valid)
+        {
+            running[h] += finalCost<NOPP>(st[h], E, D.cfg.finalAdvWeight, D.cfg.finalOppAdvWeight);
+            float* out = robust ? D.costRob : D.costNom;
+            out[((size_t)p * K + s) * 2 + 0] = running[h];
+            out[((size_t)p * K + s) * 2 + 1] = safe[h];
+        }
+        red[(sl * P + p) * 2] = running[h];
+        red[(sl * P + p) * 2 + 1] = safe[h];
+    }
+    __syncthreads();
+    // PRMPPIcostAvgKernel (prmppi_kernels.cu:134-166)
+    if (valid && pg == 0)
+    {
+        float avg = 0.0f, maxSafe = -INFINITY;
+        for (int q = 0; q < P; q++)
+        {
+            avg += red[(sl * P + q) * 2];
+            maxSafe = fmaxf(maxSafe, red[(sl * P + q) * 2 + 1]);
+        }
+        avg /= (float)P;
+        float full = avg + ((maxSafe > 0.0f) ? D.cfg.safetyWeight : 0.0f);
+        D.avg[((size_t)robust * K + s) * 2 + 0] = full;
+        D.avg[((size_t)robust * K + s) * 2 + 1] = maxSafe;
+        if (!isfinite(full))
+            atomicAdd(&D.stats[0], 1);
+    }
+}
+
 // tile: inst, s0 (first sample), count (samples), aux (0 nominal / 1 robust)
-template <int NOPP, int NTH>
-__global__ void __launch_bounds__(PR_ROLL_TILE, prRollMinBlocks<NOPP>()) pr_rollout(const PrDev* __restrict__ insts, const PrIn* __restrict__ in,
-                                                                              const Tile* __restrict__ tiles)
+// HPT hypothesis slots per thread (PR_ROLL_TILE / HPT threads a CTA, the same 512 slots):
+// with HPT > 1 a thread rolls out HPT of its sample's slots side by side and moves the
+// ego once for them (egoStep; envStep<..., EGO = true> then steps the opponents of each
+// slot): the ego's motion depends on its own action only, the sample's perturbed plan,
+// shared by every slot, so the costs are those of HPT = 1 bit for bit. Only for an ego
+// that draws no noise (egoNoiseFree on every instance of the launch).
+template <int NOPP, int NTH, int HPT = 1>
+__global__ void __launch_bounds__(PR_ROLL_TILE / HPT, prRollMinBlocks<NOPP>()) pr_rollout(const PrDev* __restrict__ insts, const PrIn* __restrict__ in,
+                                                                                    const Tile* __restrict__ tiles)
 {
     constexpr int NA = NOPP + 1;
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -170,6 +286,11 @@ __global__ void __launch_bounds__(PR_ROLL_TILE, prRollMinBlocks<NOPP>()) pr_roll
     const EnvParams& E = *sE;
     const Track tr = trackIn(sGrid);
     const int spb = PR_ROLL_TILE / P;
+    if constexpr (HPT > 1)
+    {
+        prRolloutShared<NOPP, NTH, HPT>(D, I, tile, E, tr, sNom, red, K, T, P, robust, spb);
+        return;
+    }
     const int sl = threadIdx.x / P, p = threadIdx.x % P;
     const int s = tile.s0 + sl;
     const bool valid = sl < spb && sl < tile.count;
@@ -645,12 +766,24 @@ cudaError_t launchPrPrologue(const LaunchArgs& a, int nInst)
     return cudaGetLastError();
 }
 
+template <int NOPP, int NTH, int HPT> static cudaError_t prRollH(const LaunchArgs& a, size_t smem)
+{
+    auto k = pr_rollout<NOPP, NTH, HPT>;
+    ensureSmem(k, smem);
+    k<<<a.nTiles, PR_ROLL_TILE / HPT, smem, a.stream>>>(a.pr, a.prIn, a.tiles);
+    return cudaGetLastError();
+}
+
+// a.prSlots hypothesis slots per thread (1, 2 or 4; the caller keeps it to 1 unless the
+// launch's egos draw no noise and P is a multiple of it)
 template <int NOPP, int NTH> static cudaError_t prRollT(const LaunchArgs& a, size_t smem)
 {
-    auto k = pr_rollout<NOPP, NTH>;
-    ensureSmem(k, smem);
-    k<<<a.nTiles, PR_ROLL_TILE, smem, a.stream>>>(a.pr, a.prIn, a.tiles);
-    return cudaGetLastError();
+    switch (a.prSlots)
+    {
+    case 2: return prRollH<NOPP, NTH, 2>(a, smem);
+    case 4: return prRollH<NOPP, NTH, 4>(a, smem);
+    default: return prRollH<NOPP, NTH, 1>(a, smem);
+    }
 }
 
 template <int NOPP, int NTH> static cudaError_t prCandT(const LaunchArgs& a, int nInst, int T)

@@ -131,3 +131,70 @@ def test_env_step_matches_reference(gpu):
         assert term == term_ref
         np.testing.assert_allclose(np.array(st.pos), np.array(st_ref.pos), rtol=1e-5, atol=1e-5)
         np.testing.assert_allclose(b, b_ref, rtol=1e-4, atol=1e-6)
+
+
+def _pr_agents(n=3, K=512, T=40, P=8):
+    return [S.robust_race(agent=a, seed=2, K=K, T=T, P=P, n_theta=8) for a in range(n)]
+
+
+def test_pr_batch_equals_single(gpu):
+    """dr_prmppi_batch_step (every agent's kernels in one launch each, graph replay after the
+    first step) against each controller stepped alone through dr_prmppi_step."""
+    scs = _pr_agents()
+    singles = [drb.controllers.PRMPPIController(s.env, s.prmppi, s.seed) for s in scs]
+    batched = [drb.controllers.PRMPPIController(s.env, s.prmppi, s.seed) for s in scs]
+    batch = drb.controllers.PRMPPIBatch(batched)
+    for c in singles:
+        c.engine = object()
+    beliefs = np.stack([s.belief() for s in scs])
+    for k in range(3):
+        a1 = np.stack([c.getControl(s.state) for c, s in zip(singles, scs)])
+        a2 = batch.step([s.state for s in scs], beliefs)
+        assert np.array_equal(a1, a2)
+        for c1, c2 in zip(singles, batched):
+            for x, y in zip(c1.nominals(), c2.nominals()):
+                assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("slots", [2, 4])
+def test_pr_rollout_slots_bit_identical(gpu, slots):
+    """Several hypothesis slots per rollout thread sharing the ego's moves (the benchmark's
+    PR workload: the ego draws no noise, P 8): actions and both plans identical to one slot
+    per thread, step after step."""
+    scs = _pr_agents()
+    assert all(s.env.action_noise_level == 0 and s.env.pos_noise_level == 0 and s.env.speed_noise_level == 0 for s in scs)
+    beliefs = np.stack([s.belief() for s in scs])
+    out = []
+    for n in (1, slots):
+        ctls = [drb.controllers.PRMPPIController(s.env, s.prmppi, s.seed) for s in scs]
+        b = drb.controllers.PRMPPIBatch(ctls)
+        b.set_rollout_slots(n)
+        acts = [b.step([s.state for s in scs], beliefs) for _ in range(3)]
+        out.append((acts, [c.nominals() for c in ctls]))
+        b.close()
+    (a1, n1), (a2, n2) = out
+    for x, y in zip(a1, a2):
+        assert np.array_equal(x, y)
+    for p, q in zip(n1, n2):
+        assert np.array_equal(p[0], q[0]) and np.array_equal(p[1], q[1])
+
+
+def test_pr_rollout_slots_fall_back_with_ego_noise(gpu):
+    """With ego noise the slots cannot share the ego's moves: the batch keeps one slot per
+    thread (same results), and an unsupported count is an error."""
+    scs = _pr_agents(n=2)
+    for s in scs:
+        s.env.action_noise_level = 0.1
+    beliefs = np.stack([s.belief() for s in scs])
+    res = []
+    for n in (1, 4):
+        ctls = [drb.controllers.PRMPPIController(s.env, s.prmppi, s.seed) for s in scs]
+        b = drb.controllers.PRMPPIBatch(ctls)
+        b.set_rollout_slots(n)
+        res.append([b.step([s.state for s in scs], beliefs) for _ in range(2)])
+        if n == 4:
+            with pytest.raises(abi.DrError):
+                b.set_rollout_slots(3)
+        b.close()
+    for x, y in zip(*res):
+        assert np.array_equal(x, y)
