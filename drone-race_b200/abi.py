@@ -363,6 +363,9 @@ _PROTOS = {
     "dr_debug_cp": (C.c_int, [C.POINTER(C.c_uint32), C.c_int, C.c_uint32, C.c_double, C.c_int, C.POINTER(C.c_double)]),
     "dr_debug_cp_host": (C.c_int, [C.POINTER(C.c_uint32), C.c_int, C.c_uint32, C.c_double, C.c_int, C.POINTER(C.c_double)]),
     "dr_env_step": (C.c_int, [C.POINTER(dr_env_config), C.c_int, C.POINTER(C.c_float), C.POINTER(dr_sim_state), C.POINTER(C.c_float), C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_int)]),
+    "dr_projection_certificate": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "dr_debug_project": (C.c_int, [C.POINTER(dr_env_config), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
     "dr_gate_mppi_create": (C.c_int, [C.POINTER(dr_gate_env_config), C.POINTER(dr_mppi_config), C.c_uint64, C.POINTER(C.c_float), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dr_gate_mppi_step": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_mppi_info)]),
     "dr_gate_mppi_batch_step": (C.c_int, [C.c_void_p, C.POINTER(dr_gate_state), C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(dr_mppi_info)]),

@@ -1052,6 +1052,103 @@ extern "C" int dr_env_step(const dr_env_config* env, int true_theta, const float
     return DR_OK;
 }
 
+// Test hook kernel of dr_debug_project: one point per thread.
+template <int MODE>
+__global__ void __launch_bounds__(256) debug_project_kernel(const float* __restrict__ grids, float L, float invL, const float* __restrict__ xy,
+                                                            const float* __restrict__ prevS, int n, float* __restrict__ outS, float* __restrict__ outLat,
+                                                            int* __restrict__ outIdx)
+{
+    __shared__ __align__(16) float sg[GRID_FLOATS];
+    for (int i = threadIdx.x; i < GRID_FLOATS; i += blockDim.x)
+        sg[i] = grids[i];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const Track tr = trackIn(sg);
+    float lat = 0.0f;
+    TrackPos tp{0, 0.0f};
+    float S;
+    if constexpr (MODE == 0)
+        S = projectOnTrack<true, true>(tr, L, invL, xy[2 * i], xy[2 * i + 1], prevS[i], lat, tp);
+    else if constexpr (MODE == 1)
+        S = projectOnTrack<true, false>(tr, L, invL, xy[2 * i], xy[2 * i + 1], prevS[i], lat, tp);
+    else
+        S = projectOnTrack<false>(tr, L, invL, xy[2 * i], xy[2 * i + 1], prevS[i], lat, tp);
+    outS[i] = S;
+    outLat[i] = lat;
+    outIdx[i] = tp.i0;
+}
+
+extern "C" int dr_debug_project(const dr_env_config* env, const float* xy, const float* prev_s, int n, int mode, float* s_out, float* lat_out,
+                                int32_t* idx_out)
+{
+    int rc = checkEnv(env);
+    if (rc)
+        return rc;
+    if (n < 0 || mode < 0 || mode > 2 || (n > 0 && (!xy || !prev_s || !s_out || !lat_out || !idx_out)))
+        return fail(DR_ERR_INVALID_ARG, "bad argument");
+    if (n == 0)
+        return DR_OK;
+    const std::vector<float> g = packGrids(*env);
+    const float L = env->track_length, invL = 1.0f / env->track_length;
+    float *dg = nullptr, *dxy = nullptr, *dps = nullptr, *dS = nullptr, *dLat = nullptr;
+    int* dIdx = nullptr;
+    auto release = [&]() {
+        cudaFree(dg);
+        cudaFree(dxy);
+        cudaFree(dps);
+        cudaFree(dS);
+        cudaFree(dLat);
+        cudaFree(dIdx);
+    };
+    const size_t nb = (size_t)n * 4;
+    cudaError_t e = cudaSuccess;
+    for (auto [ptr, bytes] : {std::pair<void**, size_t>{(void**)&dg, GRID_FLOATS * 4}, {(void**)&dxy, 2 * nb}, {(void**)&dps, nb}, {(void**)&dS, nb},
+                              {(void**)&dLat, nb}, {(void**)&dIdx, nb}})
+        if (e == cudaSuccess)
+            e = cudaMalloc(ptr, bytes);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dg, g.data(), GRID_FLOATS * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dxy, xy, 2 * nb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dps, prev_s, nb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+    {
+        const int blocks = (n + 255) / 256;
+        if (mode == 0)
+            debug_project_kernel<0><<<blocks, 256>>>(dg, L, invL, dxy, dps, n, dS, dLat, dIdx);
+        else if (mode == 1)
+            debug_project_kernel<1><<<blocks, 256>>>(dg, L, invL, dxy, dps, n, dS, dLat, dIdx);
+        else
+            debug_project_kernel<2><<<blocks, 256>>>(dg, L, invL, dxy, dps, n, dS, dLat, dIdx);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(s_out, dS, nb, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(lat_out, dLat, nb, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(idx_out, dIdx, nb, cudaMemcpyDeviceToHost);
+    release();
+    if (e != cudaSuccess)
+        return fail(DR_ERR_CUDA, std::string("dr_debug_project: ") + cudaGetErrorString(e));
+    return DR_OK;
+}
+
+extern "C" int dr_projection_certificate(const float* p_grid, float* cert)
+{
+    if (!p_grid || !cert)
+        return fail(DR_ERR_INVALID_ARG, "NULL argument");
+    for (int i = 0; i < 2 * NTS; i++)
+        if (!std::isfinite(p_grid[i]))
+            return fail(DR_ERR_INVALID_ARG, "track grids must be finite");
+    for (int c = 0; c < NTS; c++)
+        cert[c] = projectionCertificate(p_grid, c);
+    return DR_OK;
+}
+
 extern "C" int dr_track_grids(const double* q, int n_tracks, float* p_grid, float* dp_grid, float* t_grid, float* kappa_grid, float* track_length)
 {
     if (!q || n_tracks < 1 || !p_grid || !dp_grid || !t_grid || !kappa_grid || !track_length)

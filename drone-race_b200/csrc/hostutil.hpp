@@ -137,6 +137,74 @@ inline EnvParams toEnvParams(const dr_env_config& c)
 }
 
 // p[513][2] | t[513][2] | kappa[513] with the wrap-around sample appended.
+// Certificate of the fast projection's local search (windowLocalSearch) for sample c of the
+// centreline P ([NTS][2]): a squared radius r2 such that any point x with |x - q_c|^2 <= r2
+// at which c is a local minimum of the squared distances f(j) = |x - q_j|^2 (f(c -+ 1) >=
+// f(c) - EPS: what the search's truncated key comparisons establish) has f(k) > f(c) + EPS
+// for every sample k with 2 <= |k - c| <= 2 WIN, so that c is the minimum of every window
+// that holds it, by a margin far above the keys' resolution (2^-18 relative, at most 6e-5
+// within the 4 m cap). In y = x - q_c with d_k = q_k - q_c, f(k) - f(c) = |d_k|^2 - 2 d_k.y:
+// the points where sample k could win form the polygon
+//   (-d_k).y <= (EPS - |d_k|^2) / 2,  d_{c-1}.y <= (|d_{c-1}|^2 + EPS) / 2,
+//   d_{c+1}.y <= (|d_{c+1}|^2 + EPS) / 2,
+// and the radius is the distance from y = 0 to the nearest of these polygons (their nearest
+// point is the foot of 0 on an edge's line or a vertex that satisfies the other two), capped
+// at 4 m (points farther from the centreline than that are outside every track). Stored
+// shrunk by 1e-5 relative for the rounding of the kernel's distances.
+inline float projectionCertificate(const float* P, int c)
+{
+    constexpr double EPS = 1e-3, CAP = 4.0;
+    auto q = [&](int j, int d) { return (double)P[((j % NTS + NTS) % NTS) * 2 + d]; };
+    auto vec = [&](int k, double* v) {
+        v[0] = q(c + k, 0) - q(c, 0);
+        v[1] = q(c + k, 1) - q(c, 1);
+    };
+    double dm[2], dp[2];
+    vec(-1, dm);
+    vec(1, dp);
+    double r = CAP;
+    for (int k = -2 * WIN; k <= 2 * WIN; k++)
+    {
+        if (k >= -1 && k <= 1)
+            continue;
+        double dk[2];
+        vec(k, dk);
+        const double n[3][2] = {{-dk[0], -dk[1]}, {dm[0], dm[1]}, {dp[0], dp[1]}};
+        const double b[3] = {(EPS - (dk[0] * dk[0] + dk[1] * dk[1])) * 0.5, (dm[0] * dm[0] + dm[1] * dm[1] + EPS) * 0.5,
+                             (dp[0] * dp[0] + dp[1] * dp[1] + EPS) * 0.5};
+        auto feasible = [&](double y0, double y1) {
+            for (int i = 0; i < 3; i++)
+                if (n[i][0] * y0 + n[i][1] * y1 > b[i] + 1e-12 * (1.0 + std::fabs(b[i])))
+                    return false;
+            return true;
+        };
+        if (feasible(0.0, 0.0))
+            return -1.0f; // sample k may win next to q_c itself: always scan
+        double dist = INFINITY;
+        for (int i = 0; i < 3; i++)
+        {
+            const double nn = n[i][0] * n[i][0] + n[i][1] * n[i][1];
+            if (nn > 0.0)
+            {
+                const double y0 = n[i][0] * b[i] / nn, y1 = n[i][1] * b[i] / nn;
+                if (feasible(y0, y1))
+                    dist = std::min(dist, std::fabs(b[i]) / std::sqrt(nn));
+            }
+            for (int j = i + 1; j < 3; j++)
+            {
+                const double det = n[i][0] * n[j][1] - n[i][1] * n[j][0];
+                if (std::fabs(det) <= 1e-18)
+                    continue;
+                const double y0 = (b[i] * n[j][1] - n[i][1] * b[j]) / det, y1 = (n[i][0] * b[j] - b[i] * n[j][0]) / det;
+                if (feasible(y0, y1))
+                    dist = std::min(dist, std::sqrt(y0 * y0 + y1 * y1));
+            }
+        }
+        r = std::min(r, dist);
+    }
+    return r > 0.0 ? (float)(r * r * (1.0 - 1e-5)) : -1.0f;
+}
+
 inline std::vector<float> packGrids(const dr_env_config& c)
 {
     std::vector<float> g(GRID_FLOATS, 0.0f);
@@ -155,6 +223,8 @@ inline std::vector<float> packGrids(const dr_env_config& c)
         g[GRID_T + i * 2 + 1] = c.t_grid[k * 2 + 1];
         g[GRID_K + i] = c.kappa_grid[k];
     }
+    for (int i = 0; i < NTS; i++)
+        g[GRID_CERT + i] = projectionCertificate(c.p_grid, i);
     return g;
 }
 

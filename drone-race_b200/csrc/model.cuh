@@ -79,12 +79,16 @@ constexpr float MIN_COEFF = 0.01f; // MIN_COEFF_THRESHOLD, include/config.h:29
 //          side (p[j] for j in [-16, 528)), so that the projection window needs no modulo;
 //   t      unit tangent [513][2] and kappa curvature [513] (sample 512 = sample 0);
 //   px, py the padded centreline again as separate x and y rows (8-byte aligned at even
-//          indices), read two samples at a time by the projection window.
+//          indices), read two samples at a time by the projection window;
+//   cert   [512] per sample c, the squared radius within which a local minimum at c of the
+//          squared distances to the samples is their minimum over every window holding c
+//          (projectionCertificate, computed with the grids on the host).
 constexpr int GRID_PAD = 16;
 constexpr int GRID_ROW = NTS + 2 * GRID_PAD; // padded centreline samples
 constexpr int GRID_P = GRID_PAD * 2, GRID_T = GRID_ROW * 2, GRID_K = GRID_T + (NTS + 1) * 2;
 constexpr int GRID_PX = GRID_K + NTS + 1 + 1 + GRID_PAD, GRID_PY = GRID_PX + GRID_ROW;
-constexpr int GRID_FLOATS = GRID_PY - GRID_PAD + GRID_ROW;
+constexpr int GRID_CERT = GRID_PY - GRID_PAD + GRID_ROW;
+constexpr int GRID_FLOATS = GRID_CERT + NTS;
 static_assert(GRID_FLOATS % 4 == 0 && GRID_PX % 2 == 0 && GRID_PY % 2 == 0 && GRID_PAD > WIN + 1, "grid layout");
 
 enum Term
@@ -225,11 +229,12 @@ struct Track
     const float* k;  // [513]
     const float* px; // [-16, 528)
     const float* py; // [-16, 528)
+    const float* cert; // [512]
 };
 
 __device__ __forceinline__ Track trackIn(const float* grids)
 {
-    return Track{grids + GRID_P, grids + GRID_T, grids + GRID_K, grids + GRID_PX, grids + GRID_PY};
+    return Track{grids + GRID_P, grids + GRID_T, grids + GRID_K, grids + GRID_PX, grids + GRID_PY, grids + GRID_CERT};
 }
 
 // ---- track sampling (env_stratrace.h:44-85) ------------------------------------------
@@ -309,12 +314,67 @@ __device__ __forceinline__ float projectSegments(const Track& tr, float L, float
     return bestS;
 }
 
+// Key of the fast flavour's window search for window place k (sample j0 + k): the squared
+// distance with its low five mantissa bits dropped, then the place, so that the smaller of
+// two keys is the nearer sample and, at equal truncated distances, the earlier one. The
+// arithmetic rounds like each lane of the packed window scan below.
+__device__ __forceinline__ uint32_t windowKey(const Track& tr, int j0, int k, float px, float py)
+{
+    const int j = j0 + k;
+    const float d0 = __fsub_rn(tr.px[j], px), d1 = __fsub_rn(tr.py[j], py);
+    const float sq = __fmaf_rn(d1, d1, __fmul_rn(d0, d0));
+    return (__float_as_uint(sq) & ~31u) | (uint32_t)k;
+}
+
+// The fast flavour's local search: from the window's centre (the previous position's
+// sample), step to the neighbour with the smaller key while there is one. The sample it
+// stops at (a local minimum of the keys) is the window's minimum when the point lies within
+// the sample's certified radius (tr.cert) and is not at the window's edge; returns -1
+// otherwise, and the caller scans the whole window.
+__device__ __forceinline__ int windowLocalSearch(const Track& tr, int j0, float px, float py)
+{
+    int c = WIN;
+    uint32_t kc = windowKey(tr, j0, c, px, py);
+    uint32_t kl = windowKey(tr, j0, c - 1, px, py);
+    if (kl < kc)
+    {
+        for (int it = 0; it < WIN; it++) // down the window
+        {
+            c--;
+            kc = kl;
+            if (c == 0)
+                break;
+            kl = windowKey(tr, j0, c - 1, px, py);
+            if (!(kl < kc))
+                break;
+        }
+    }
+    else
+    {
+        uint32_t kr = windowKey(tr, j0, c + 1, px, py);
+        for (int it = 0; it < WIN && kr < kc; it++) // up the window
+        {
+            c++;
+            kc = kr;
+            if (c == 2 * WIN)
+                break;
+            kr = windowKey(tr, j0, c + 1, px, py);
+        }
+    }
+    const bool certified = c > 0 && c < 2 * WIN && __uint_as_float(kc & ~31u) <= tr.cert[wrapNts(j0 + c + NTS)];
+    return certified ? c : -1;
+}
+
 // fastProjectOnTrack<false> (env_stratrace.h:88-162): returns S, writes latDist and the
 // track position of S. The fast flavour takes the window's minimum on keys that pack the
 // squared distance (its low five mantissa bits dropped) with the sample's place in the
-// window, so one unsigned minimum per sample finds the first of the nearest samples; two
-// distances within 2^-18 relative of each other count as equal there.
-template <bool F>
+// window (windowKey), so one unsigned minimum per sample finds the first of the nearest
+// samples; two distances within 2^-18 relative of each other count as equal there. With
+// LOCAL (the verification's default) it first runs the certified local search
+// (windowLocalSearch), which evaluates three samples where the point moved less than a
+// sample's spacing, and scans the window only where that search cannot certify its
+// result; both give the same sample.
+template <bool F, bool LOCAL = F>
 __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float invL, float px, float py, float prevS, float& latDist, TrackPos& tpS)
 {
     if constexpr (F)
@@ -340,7 +400,12 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
     asm("mov.b64 %0, {%1, %1};" : "=l"(pxx) : "f"(px));
     asm("mov.b64 %0, {%1, %1};" : "=l"(pyy) : "f"(py));
     int bestJ = j0;
+    int local = -1;
+    if constexpr (F && LOCAL)
+        local = windowLocalSearch(tr, j0, px, py);
     if constexpr (F)
+        bestJ = j0 + local;
+    if (F && local < 0)
     {
         uint32_t best = 0xffffffffu;
         const uint32_t off = (uint32_t)(jp - j0); // place of the first pair's first sample
@@ -369,7 +434,7 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
         }
         bestJ = j0 + (int)(best & 31u);
     }
-    else
+    else if constexpr (!F)
     {
         float bestSqDist = INFINITY;
 #pragma unroll 5

@@ -590,6 +590,20 @@ int dr_track_grids(const double* q, int n_tracks, float* p_grid, float* dp_grid,
 int dr_env_step(const dr_env_config* env, int true_theta, const float* action, dr_sim_state* state, float* belief, int update_belief,
                 uint64_t seed, uint64_t step, int* term);
 
+/* Test hook: the projection onto the centreline (fastProjectOnTrack, env_stratrace.h:88-162)
+ * of n points xy[n][2], each from its previous arc length prev_s[n], as the kernels run it:
+ * mode 0 the verification's fast flavour (certified local search of the window, with the
+ * full window scan where the search cannot certify its sample), 1 the fast flavour's full
+ * window scan, 2 the exact flavour (the rollout's). Writes the arc length, the signed
+ * lateral distance and the track sample index of the arc length. */
+int dr_debug_project(const dr_env_config* env, const float* xy, const float* prev_s, int n, int mode, float* s_out, float* lat_out, int32_t* idx_out);
+/* The squared radii cert[512] of the fast projection's local search for the centreline
+ * p_grid[512][2] (host only, no GPU): within cert[c] of sample c, a point at which c is a
+ * local minimum of the squared distances to the samples is nearer to c than to every other
+ * sample of any window holding c, by more than 1e-3 m^2; negative where nothing is
+ * certified. Part of the packed track the kernels read. */
+int dr_projection_certificate(const float* p_grid, float* cert);
+
 /* ==== gate race (the reference's EnvDroneRace, include/environments/env_dronerace.h) ====
  * Two agents (the MPPI ego at index i_mppi, one PID opponent), gates crossed in order,
  * laps counted at the last gate, PID opponents following racelines. The reference fixes
