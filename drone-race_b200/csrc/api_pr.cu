@@ -1073,8 +1073,10 @@ __global__ void __launch_bounds__(256) debug_project_kernel(const float* __restr
         S = projectOnTrack<true, true>(tr, L, invL, xy[2 * i], xy[2 * i + 1], prevS[i], lat, tp);
     else if constexpr (MODE == 1)
         S = projectOnTrack<true, false>(tr, L, invL, xy[2 * i], xy[2 * i + 1], prevS[i], lat, tp);
+    else if constexpr (MODE == 2)
+        S = projectOnTrack<false, true>(tr, L, invL, xy[2 * i], xy[2 * i + 1], prevS[i], lat, tp);
     else
-        S = projectOnTrack<false>(tr, L, invL, xy[2 * i], xy[2 * i + 1], prevS[i], lat, tp);
+        S = projectOnTrack<false, false>(tr, L, invL, xy[2 * i], xy[2 * i + 1], prevS[i], lat, tp);
     outS[i] = S;
     outLat[i] = lat;
     outIdx[i] = tp.i0;
@@ -1086,7 +1088,7 @@ extern "C" int dr_debug_project(const dr_env_config* env, const float* xy, const
     int rc = checkEnv(env);
     if (rc)
         return rc;
-    if (n < 0 || mode < 0 || mode > 2 || (n > 0 && (!xy || !prev_s || !s_out || !lat_out || !idx_out)))
+    if (n < 0 || mode < 0 || mode > 3 || (n > 0 && (!xy || !prev_s || !s_out || !lat_out || !idx_out)))
         return fail(DR_ERR_INVALID_ARG, "bad argument");
     if (n == 0)
         return DR_OK;
@@ -1121,8 +1123,10 @@ extern "C" int dr_debug_project(const dr_env_config* env, const float* xy, const
             debug_project_kernel<0><<<blocks, 256>>>(dg, L, invL, dxy, dps, n, dS, dLat, dIdx);
         else if (mode == 1)
             debug_project_kernel<1><<<blocks, 256>>>(dg, L, invL, dxy, dps, n, dS, dLat, dIdx);
-        else
+        else if (mode == 2)
             debug_project_kernel<2><<<blocks, 256>>>(dg, L, invL, dxy, dps, n, dS, dLat, dIdx);
+        else
+            debug_project_kernel<3><<<blocks, 256>>>(dg, L, invL, dxy, dps, n, dS, dLat, dIdx);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess)

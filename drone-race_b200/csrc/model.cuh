@@ -314,29 +314,57 @@ __device__ __forceinline__ float projectSegments(const Track& tr, float L, float
     return bestS;
 }
 
-// Key of the fast flavour's window search for window place k (sample j0 + k): the squared
-// distance with its low five mantissa bits dropped, then the place, so that the smaller of
-// two keys is the nearer sample and, at equal truncated distances, the earlier one. The
-// arithmetic rounds like each lane of the packed window scan below.
-__device__ __forceinline__ uint32_t windowKey(const Track& tr, int j0, int k, float px, float py)
+// Squared distance from (px, py) to window sample j0 + k, rounded like each lane of the
+// packed window scans below (sub, mul, then fma).
+__device__ __forceinline__ float windowSqDist(const Track& tr, int j0, int k, float px, float py)
 {
     const int j = j0 + k;
     const float d0 = __fsub_rn(tr.px[j], px), d1 = __fsub_rn(tr.py[j], py);
-    const float sq = __fmaf_rn(d1, d1, __fmul_rn(d0, d0));
-    return (__float_as_uint(sq) & ~31u) | (uint32_t)k;
+    return __fmaf_rn(d1, d1, __fmul_rn(d0, d0));
 }
 
-// The fast flavour's local search: from the window's centre (the previous position's
-// sample), step to the neighbour with the smaller key while there is one. The sample it
-// stops at (a local minimum of the keys) is the window's minimum when the point lies within
-// the sample's certified radius (tr.cert) and is not at the window's edge; returns -1
-// otherwise, and the caller scans the whole window.
+// Key of window place k for the search of flavour F. Fast: the squared distance with its
+// low five mantissa bits dropped, then the place, as one unsigned word (the smaller key is
+// the nearer sample, at equal truncated distances the earlier one). Exact: the squared
+// distance itself, compared as the reference's scan compares it (strict '<' in increasing
+// place order: at equal distances the earlier place wins).
+template <bool F> struct WindowKey;
+template <> struct WindowKey<true>
+{
+    uint32_t v;
+    __device__ __forceinline__ WindowKey(const Track& tr, int j0, int k, float px, float py)
+    {
+        v = (__float_as_uint(windowSqDist(tr, j0, k, px, py)) & ~31u) | (uint32_t)k;
+    }
+    // this key (place k) before the key of place k + 1 / after the one of place k - 1
+    __device__ __forceinline__ bool beatsNext(const WindowKey& o) const { return v < o.v; }
+    __device__ __forceinline__ bool beatsPrev(const WindowKey& o) const { return v < o.v; }
+    __device__ __forceinline__ float dist() const { return __uint_as_float(v & ~31u); }
+};
+template <> struct WindowKey<false>
+{
+    float v;
+    __device__ __forceinline__ WindowKey(const Track& tr, int j0, int k, float px, float py) { v = windowSqDist(tr, j0, k, px, py); }
+    __device__ __forceinline__ bool beatsNext(const WindowKey& o) const { return v <= o.v; }
+    __device__ __forceinline__ bool beatsPrev(const WindowKey& o) const { return v < o.v; }
+    __device__ __forceinline__ float dist() const { return v; }
+};
+
+// The local search of the projection window: from the window's centre (the previous
+// position's sample), step to the neighbour whose key wins against the current one while
+// there is one. The sample it stops at is a local minimum of the keys and is the window's
+// first minimum when the point lies within the sample's certified radius (tr.cert: every
+// other sample of any window holding it is then farther by more than 1e-3 m^2, far above
+// the keys' truncation and the distances' rounding) and is not at the window's edge;
+// returns -1 otherwise, and the caller scans the whole window.
+template <bool F>
 __device__ __forceinline__ int windowLocalSearch(const Track& tr, int j0, float px, float py)
 {
+    using Key = WindowKey<F>;
     int c = WIN;
-    uint32_t kc = windowKey(tr, j0, c, px, py);
-    uint32_t kl = windowKey(tr, j0, c - 1, px, py);
-    if (kl < kc)
+    Key kc(tr, j0, c, px, py);
+    Key kl(tr, j0, c - 1, px, py);
+    if (kl.beatsNext(kc))
     {
         for (int it = 0; it < WIN; it++) // down the window
         {
@@ -344,37 +372,37 @@ __device__ __forceinline__ int windowLocalSearch(const Track& tr, int j0, float 
             kc = kl;
             if (c == 0)
                 break;
-            kl = windowKey(tr, j0, c - 1, px, py);
-            if (!(kl < kc))
+            kl = Key(tr, j0, c - 1, px, py);
+            if (!kl.beatsNext(kc))
                 break;
         }
     }
     else
     {
-        uint32_t kr = windowKey(tr, j0, c + 1, px, py);
-        for (int it = 0; it < WIN && kr < kc; it++) // up the window
+        Key kr(tr, j0, c + 1, px, py);
+        for (int it = 0; it < WIN && kr.beatsPrev(kc); it++) // up the window
         {
             c++;
             kc = kr;
             if (c == 2 * WIN)
                 break;
-            kr = windowKey(tr, j0, c + 1, px, py);
+            kr = Key(tr, j0, c + 1, px, py);
         }
     }
-    const bool certified = c > 0 && c < 2 * WIN && __uint_as_float(kc & ~31u) <= tr.cert[wrapNts(j0 + c + NTS)];
+    const bool certified = c > 0 && c < 2 * WIN && kc.dist() <= tr.cert[wrapNts(j0 + c + NTS)];
     return certified ? c : -1;
 }
 
 // fastProjectOnTrack<false> (env_stratrace.h:88-162): returns S, writes latDist and the
 // track position of S. The fast flavour takes the window's minimum on keys that pack the
 // squared distance (its low five mantissa bits dropped) with the sample's place in the
-// window (windowKey), so one unsigned minimum per sample finds the first of the nearest
+// window (WindowKey), so one unsigned minimum per sample finds the first of the nearest
 // samples; two distances within 2^-18 relative of each other count as equal there. With
-// LOCAL (the verification's default) it first runs the certified local search
+// LOCAL (the default, both flavours) it first runs the certified local search
 // (windowLocalSearch), which evaluates three samples where the point moved less than a
 // sample's spacing, and scans the window only where that search cannot certify its
-// result; both give the same sample.
-template <bool F, bool LOCAL = F>
+// result; both give the same sample, in the exact flavour the reference's.
+template <bool F, bool LOCAL = true>
 __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float invL, float px, float py, float prevS, float& latDist, TrackPos& tpS)
 {
     if constexpr (F)
@@ -399,12 +427,10 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
     uint64_t pxx, pyy;
     asm("mov.b64 %0, {%1, %1};" : "=l"(pxx) : "f"(px));
     asm("mov.b64 %0, {%1, %1};" : "=l"(pyy) : "f"(py));
-    int bestJ = j0;
     int local = -1;
-    if constexpr (F && LOCAL)
-        local = windowLocalSearch(tr, j0, px, py);
-    if constexpr (F)
-        bestJ = j0 + local;
+    if constexpr (LOCAL)
+        local = windowLocalSearch<F>(tr, j0, px, py);
+    int bestJ = j0 + local;
     if (F && local < 0)
     {
         uint32_t best = 0xffffffffu;
@@ -434,8 +460,9 @@ __device__ __forceinline__ float projectOnTrack(const Track& tr, float L, float 
         }
         bestJ = j0 + (int)(best & 31u);
     }
-    else if constexpr (!F)
+    else if (!F && local < 0)
     {
+        bestJ = j0;
         float bestSqDist = INFINITY;
 #pragma unroll 5
         for (int q = 0; q < WIN; q++)

@@ -593,9 +593,11 @@ int dr_env_step(const dr_env_config* env, int true_theta, const float* action, d
 /* Test hook: the projection onto the centreline (fastProjectOnTrack, env_stratrace.h:88-162)
  * of n points xy[n][2], each from its previous arc length prev_s[n], as the kernels run it:
  * mode 0 the verification's fast flavour (certified local search of the window, with the
- * full window scan where the search cannot certify its sample), 1 the fast flavour's full
- * window scan, 2 the exact flavour (the rollout's). Writes the arc length, the signed
- * lateral distance and the track sample index of the arc length. */
+ * full window scan where the search cannot certify its sample), 1 the fast flavour with
+ * the full window scan only, 2 the exact flavour (the rollout's: the same search on the
+ * unrounded distances), 3 the exact flavour with the full window scan only (the
+ * reference's algorithm as written). Writes the arc length, the signed lateral distance
+ * and the track sample index of the arc length. */
 int dr_debug_project(const dr_env_config* env, const float* xy, const float* prev_s, int n, int mode, float* s_out, float* lat_out, int32_t* idx_out);
 /* The squared radii cert[512] of the fast projection's local search for the centreline
  * p_grid[512][2] (host only, no GPU): within cert[c] of sample c, a point at which c is a

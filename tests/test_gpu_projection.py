@@ -1,7 +1,8 @@
-"""The verification's projection onto the centreline: the fast flavour's certified local
-search of the window (dr_debug_project mode 0, what mppi_verify runs) gives bit for bit
-the arc length, lateral distance and sample of the fast flavour's full window scan (mode 1)
-on smooth tracks, on a hairpin whose windows see both legs, for points on and far off the
+"""The projection onto the centreline: the certified local search of the window gives bit
+for bit the arc length, lateral distance and sample of the full window scan, in the fast
+flavour (dr_debug_project mode 0 against 1, what mppi_verify runs) and in the exact one
+(mode 2 against 3: the rollout's search against the reference's scan as written), on
+smooth tracks, on a hairpin whose windows see both legs, for points on and far off the
 track and for previous arc lengths up to nine samples away (walks to the window's edge,
 where the search hands over to the scan)."""
 from __future__ import annotations
@@ -58,9 +59,11 @@ def test_local_search_equals_window_scan(gpu, name):
     b = _project(env, xy, prev, 1)
     for x, y in zip(a, b):
         assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
-    # the exact flavour (the rollout's) agrees to within the fast flavour's arithmetic
-    # (arc lengths compared modulo the track length, on the track)
     e = _project(env, xy, prev, 2)
+    for x, y in zip(e, _project(env, xy, prev, 3)):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+    # the two flavours agree to within the fast flavour's arithmetic (arc lengths compared
+    # modulo the track length, on the track)
     on = np.abs(e[1]) < 2.0
     L = np.float64(grids.track_length)
     d = np.abs(np.mod(a[0][on].astype(np.float64) - e[0][on] + L / 2, L) - L / 2)
