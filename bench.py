@@ -409,7 +409,7 @@ def _race_cost_step(sc, st) -> float:
     return cost
 
 
-def closed_loop_compare(n_steps: int = 300) -> dict:
+def closed_loop_compare(n_steps: int = 500) -> dict:
     """Gradient-refined MPPI (K = K_GRAD, GRAD_STEPS steps) against plain MPPI (K = 4096)
     in closed loop: each of the 4 benchmark agents races its opponent for n_steps control
     steps (true dynamics on the device, true hypothesis 0, belief updated), the race cost

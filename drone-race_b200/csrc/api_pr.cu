@@ -416,7 +416,7 @@ int buildPrBatch(dr_prmppi* const* hs, int n, cudaStream_t stream, bool ownStrea
     {
         dr_prmppi* h = hs[i];
         descs.push_back(h->desc);
-        const int spb = prRolloutSamplesPerBlock() / h->P;
+        const int spb = (h->envKind ? gatePrRolloutSamplesPerBlock() : prRolloutSamplesPerBlock()) / h->P;
         for (int nr = 0; nr < 2; nr++)
             for (int s0 = h->sLo; s0 < h->sHi; s0 += spb)
                 roll.push_back(Tile{i, s0, std::min(spb, h->sHi - s0), nr});

@@ -26,12 +26,13 @@ namespace dr
 {
 
 constexpr int PRB = 128;
-// Rollout CTA: 512 threads, two CTAs per SM (64 registers a thread), whose warps take a
-// barrier every step (`__syncthreads_or` on the still-running samples) so the warps that
-// share an SM sub-partition fetch the same instructions; the benchmark's 4 x 2 x 8 x 2048
-// rollouts then fit in one wave of 296 CTAs.
+// Rollout CTA: 448 threads (56 samples x 8 hypotheses), two CTAs per SM (72 registers a
+// thread), whose warps take a barrier every step (`__syncthreads_or` on the still-running
+// samples) so the warps that share an SM sub-partition fetch the same instructions; the
+// benchmark's 4 x 2 x 8 x 2048 rollouts are then 296 CTAs, two on every SM in one wave
+// (with 512 threads they were 256 CTAs, which left 40 SMs with one: 0.53 against 0.49 ms).
 #ifndef PR_ROLL_TILE
-#define PR_ROLL_TILE 512
+#define PR_ROLL_TILE 448
 #endif
 // two CTAs a SM where one opponent keeps the state in 64 registers; one with two opponents
 template <int NOPP>
@@ -244,7 +245,7 @@ __device__ __forceinline__ void prRolloutShared(const PrDev& D, const PrIn& I, c
 }
 
 // tile: inst, s0 (first sample), count (samples), aux (0 nominal / 1 robust)
-// HPT hypothesis slots per thread (PR_ROLL_TILE / HPT threads a CTA, the same 512 slots):
+// HPT hypothesis slots per thread (PR_ROLL_TILE / HPT threads a CTA, the same PR_ROLL_TILE slots):
 // with HPT > 1 a thread rolls out HPT of its sample's slots side by side and moves the
 // ego once for them (egoStep; envStep<..., EGO = true> then steps the opponents of each
 // slot): the ego's motion depends on its own action only, the sample's perturbed plan,
