@@ -25,17 +25,25 @@ constexpr int G_MAXO = DR_GATE_MAX_OBSTACLES;
 // 1.0f (the last raceline's first sample), padded to 16 bytes; then every raceline again as
 // a row of x and a row of y with G_RPAD wrapped samples on each side (samples -G_RPAD ..
 // NTS + G_RPAD - 1, 8-byte aligned at even samples), read two samples at a time by the
-// raceline walk's margin scan.
+// raceline walk's margin scan; then per raceline the squared radii [NTS] of the
+// projection certificate (projectionCertificate, computed on the host with the track).
 constexpr int G_RPAD = 16;
 constexpr int G_ROW = NTS + 2 * G_RPAD;
 constexpr int GATE_INTERLEAVED_FLOATS = G_NR * NTS * 2 + 4;
-constexpr int GATE_TRACK_FLOATS = GATE_INTERLEAVED_FLOATS + G_NR * 2 * G_ROW;
+constexpr int GATE_CERT = GATE_INTERLEAVED_FLOATS + G_NR * 2 * G_ROW;
+constexpr int GATE_TRACK_FLOATS = GATE_CERT + G_NR * NTS;
 static_assert(GATE_TRACK_FLOATS % 4 == 0 && G_ROW % 2 == 0 && G_RPAD % 2 == 0 && G_RPAD > 10, "gate track layout");
 
 // raceline r's x row at its sample 0 (the y row follows at + G_ROW)
 __host__ __device__ __forceinline__ const float* gateRowX(const float* track, int r)
 {
     return track + GATE_INTERLEAVED_FLOATS + 2 * r * G_ROW + G_RPAD;
+}
+
+// raceline r's certified squared radii [NTS]
+__host__ __device__ __forceinline__ const float* gateCert(const float* track, int r)
+{
+    return track + GATE_CERT + r * NTS;
 }
 
 struct GateParams
@@ -187,20 +195,33 @@ static __device__ __noinline__ float projectFull(const float* __restrict__ tp, f
 // samples (the walk's stop and the nine after it) are evaluated as pairs of consecutive
 // samples from the padded x / y rows with packed FP32x2 arithmetic (each lane rounds as
 // sqDistToSample's scalar sub, mul and fma do), then compared in the walk's order.
+//
+// walkStop is the walk (moves: the samples it advanced), walkMargin the margin scan from
+// the walk's stop bestI, which it may replace.
 template <int DELTA>
-__device__ __forceinline__ int walkMin(const float* __restrict__ tp, const float* __restrict__ rowX, int i0, float px, float py, float baseSq, float& bestSq)
+__device__ __forceinline__ int walkStop(const float* __restrict__ tp, int i0, float px, float py, float baseSq, float& bestSq, int& moves)
 {
     int bestI = i0;
     bestSq = baseSq;
+    moves = 0;
     int cur = wrapNts(i0 + DELTA + NTS);
     float curSq = sqDistToSample(tp, cur, px, py);
     for (int n = 0; curSq < bestSq && n < NTS; n++)
     {
         bestI = cur;
         bestSq = curSq;
+        moves++;
         cur = wrapNts(cur + DELTA + NTS);
         curSq = sqDistToSample(tp, cur, px, py);
     }
+    return bestI;
+}
+
+template <int DELTA>
+__device__ __forceinline__ int walkMargin(const float* __restrict__ rowX, int bestI, float px, float py, float& bestSq)
+{
+    const int cur = wrapNts(bestI + DELTA + NTS);
+    float curSq;
     // samples cur + k DELTA, k = 0..9, lie in [lo, lo + 11] with lo even, inside the rows'
     // padding (cur - 9 >= -9, cur + 9 <= 520)
     const int lo = (DELTA > 0 ? cur : cur - 9) & ~1;
@@ -242,15 +263,27 @@ __device__ __forceinline__ int walkMin(const float* __restrict__ tp, const float
 
 // fastProjectOnTrack, :143-209 (its distance output is unused on the path); tp the
 // raceline's interleaved samples, rowX its padded x row (gateRowX)
-__device__ __forceinline__ float projectGreedy(const float* __restrict__ tp, const float* __restrict__ rowX, float px, float py, float prevS)
+__device__ __forceinline__ float projectGreedy(const float* __restrict__ tp, const float* __restrict__ rowX, const float* __restrict__ cert, float px, float py,
+                                              float prevS)
 {
     if (prevS < 0)
         return projectFull(tp, px, py);
     int baseI = wrapNts((int)(prevS * NTS + 0.5f)); // prevS >= 0
     float baseSq = sqDistToSample(tp, baseI, px, py);
     float bSq, fSq;
-    int bI = walkMin<-1>(tp, rowX, baseI, px, py, baseSq, bSq);
-    int fI = walkMin<+1>(tp, rowX, baseI, px, py, baseSq, fSq);
+    int nb, nf;
+    int bI = walkStop<-1>(tp, baseI, px, py, baseSq, bSq, nb);
+    int fI = walkStop<+1>(tp, baseI, px, py, baseSq, fSq, nf);
+    // The better stop c is a local minimum of the distances (the walks stopped on either
+    // side of it, or descended into it). Within its certified radius every other sample
+    // within 20 of it is farther by more than 1e-3 m^2, so no margin sample can win when
+    // both margins (bI - 10 .. bI - 1, fI + 1 .. fI + 10) lie within 20 of c.
+    const bool back = !(fSq < bSq);
+    const int c = back ? bI : fI;
+    if (nb + nf <= 10 && (back ? bSq : fSq) <= cert[c])
+        return ((float)c) / NTS;
+    bI = walkMargin<-1>(rowX, bI, px, py, bSq);
+    fI = walkMargin<+1>(rowX, fI, px, py, fSq);
     if (fSq < bSq)
         return ((float)fI) / NTS;
     return ((float)bI) / NTS;
@@ -333,7 +366,7 @@ __device__ __forceinline__ void updateGates(const GateParams& G, const float* __
         if (s.S[a * G_NR] >= 0.0f)
 #pragma unroll
             for (int r = 0; r < G_NR; r++)
-                s.S[a * G_NR + r] = projectGreedy(track + r * NTS * 2, gateRowX(track, r), px, py, s.S[a * G_NR + r]);
+                s.S[a * G_NR + r] = projectGreedy(track + r * NTS * 2, gateRowX(track, r), gateCert(track, r), px, py, s.S[a * G_NR + r]);
         const int next = nextGateIndex(s.gates[a], G.nGates);
         const float gc0 = G.gateCenters[next * 2], gc1 = G.gateCenters[next * 2 + 1];
         const float gv0 = G.gateVectors[next * 2], gv1 = G.gateVectors[next * 2 + 1];

@@ -342,6 +342,9 @@ inline std::vector<float> packGateTrack(const dr_gate_env_config& c)
             t[row] = c.track_points[((size_t)r * NTS + src) * 2];
             t[row + G_ROW] = c.track_points[((size_t)r * NTS + src) * 2 + 1];
         }
+    for (int r = 0; r < G_NR; r++)
+        for (int i = 0; i < NTS; i++)
+            t[(size_t)GATE_CERT + (size_t)r * NTS + i] = projectionCertificate(c.track_points + (size_t)r * NTS * 2, i);
     return t;
 }
 

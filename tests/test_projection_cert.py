@@ -38,11 +38,27 @@ def certificate(p_grid: np.ndarray) -> np.ndarray:
     return out
 
 
-@pytest.mark.parametrize("name", list(TRACKS))
+def _lines():
+    """(points [512][2], unit tangents [512][2]) of every track: the centrelines above and the
+    gate race's racelines (ellipse offsets, the raceline walk's samples)."""
+    out = {}
+    for name, f in TRACKS.items():
+        g = T.track_grids(f)
+        out[name] = (g.p_grid, g.t_grid)
+    for r, line in enumerate(drb.scenarios.ellipse_racelines()):
+        d = np.roll(line, -1, axis=0) - np.roll(line, 1, axis=0)
+        out[f"gate_raceline{r}"] = (np.ascontiguousarray(line, np.float32), (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32))
+    return out
+
+
+LINES = _lines()
+
+
+@pytest.mark.parametrize("name", list(LINES))
 def test_certificate_holds_by_brute_force(name):
-    g = T.track_grids(TRACKS[name])
-    cert = certificate(g.p_grid)
-    q = g.p_grid.astype(np.float64)
+    p_grid, t_grid = LINES[name]
+    cert = certificate(p_grid)
+    q = p_grid.astype(np.float64)
     rng = np.random.default_rng(7)
     checked = 0
     for c in range(512):
@@ -51,7 +67,7 @@ def test_certificate_holds_by_brute_force(name):
         r = np.sqrt(cert[c])
         # points of the certified disk near the slab where c can be a local minimum:
         # along-track offsets within a sample spacing, lateral offsets across the disk
-        t = g.t_grid[c].astype(np.float64)
+        t = t_grid[c].astype(np.float64)
         n = np.array([-t[1], t[0]])
         h = np.linalg.norm(q[(c + 1) % 512] - q[c])
         a = rng.uniform(-0.7 * h, 0.7 * h, 400)
