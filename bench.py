@@ -55,23 +55,26 @@ VERIF_H = 40
 # The verification shares the ego's moves across its samples (the ego draws no noise in
 # this workload, so samples that took the same branch at the same step move it alike;
 # mppi_ego_table computes them once per plan): counting each distinct operation once per
-# step index over the samples (opcount dedup mode 2) leaves 337 FLOPs per sample-step,
-# the work the verification kernel has to do; 571 is a sample's own work in isolation.
+# step index over the samples (opcount dedup mode 2) leaves 337 FLOPs per sample-step.
 # Work whose result nothing reads (a committed sample's belief update and the other
-# hypotheses' actions, which the kernels skip) is left out too; on this workload's first
-# steps no sample commits within the horizon, so the counts stay 652 / 337.
+# hypotheses' actions, which the kernels skip) is left out too, and the track projection
+# is counted as the kernels run it: the certified local search of its window, three to a
+# few distances where the reference's scan takes 21 (the same sample; this workload's
+# track certifies everywhere on it). That leaves 442.0 FLOPs per rollout step and 233.7
+# per verification step (652.4 / 337.0 with the window scanned as the reference does).
 # `python oracle/count_flops.py` reproduces every count of this file.
-FLOPS_PER_ROLLOUT_STEP = 652.0    # MPPI rollout step (belief update over 2 hypotheses)
-FLOPS_PER_VERIFY_STEP = 337.0     # verification step, ego moves shared across samples
+FLOPS_PER_ROLLOUT_STEP = 442.0    # MPPI rollout step (belief update over 2 hypotheses)
+FLOPS_PER_VERIFY_STEP = 233.7     # verification step, ego moves shared across samples
 
 # --workload gates: the same control step on the gate race (the reference's EnvDroneRace:
 # one PID opponent with 2 hypotheses, 8 gates on a 30 x 20 m ellipse, 2 racelines), FLOPs
-# per step counted the same way on oracle/port/gate_model.hpp (orc_gate_count_ops): 405.7
-# per rollout step (487.0 with the committed samples' dead belief work), 328.4 per
-# verification step (475.7 as one sample's own work with that dead work).
+# per step counted the same way on oracle/port/gate_model.hpp (orc_gate_count_ops), the
+# raceline walks without the margin scans the kernels skip where certified: 189.7 per
+# rollout step, 117.8 per verification step (405.7 / 328.4 with the margins scanned as
+# the reference does).
 N_GATES = 8
-GATE_FLOPS_PER_ROLLOUT_STEP = 405.7
-GATE_FLOPS_PER_VERIFY_STEP = 328.4
+GATE_FLOPS_PER_ROLLOUT_STEP = 189.7
+GATE_FLOPS_PER_VERIFY_STEP = 117.8
 
 # --workload grad: gradient-refined MPPI on the strategic race, a quarter of the samples
 # (K = 1024) and one projected gradient step (--grad-steps) of the noise-free rollout objective after each
@@ -83,9 +86,10 @@ GRAD_STEP_SIZE = 0.05
 # benchmark's PR configuration per agent: 8 opponent hypotheses (lateral aggressiveness
 # U(0, 2) m, speed scale U(0.8, 1.2), belief ~ Dirichlet(1)), P = 8 sampled hypotheses,
 # K = 2048, H = 64. FLOPs per PR rollout step (one hypothesis' policy, no belief update,
-# PRMPPIstateCost and PRMPPIsafetyCost) counted like the others (orc_pr_count_ops).
+# PRMPPIstateCost and PRMPPIsafetyCost) counted like the others (orc_pr_count_ops), the
+# projection as the kernels search it: 411.7 (623.5 with the window scanned as written).
 K_PR, P_PR, NTH_PR = 2048, 8, 8
-PR_FLOPS_PER_ROLLOUT_STEP = 623.5
+PR_FLOPS_PER_ROLLOUT_STEP = 411.7
 # --workload races: many independent races of uneven sizes in one batch per control mode
 # (scenarios.uneven_races: 256 races, U{1..8} agents each, K log-uniform [256, 16384],
 # H in {32, 48, 64, 96}, tracks through U{6..16} points, dense and spline controls by

@@ -252,9 +252,31 @@ template <typename R> inline R projectGreedy(const R* tp, const R* pos, R prevS)
         return projectFull(tp, pos);
     int baseI = (int)(prevS * (R)NTS + R(0.5)) % NTS;
     R baseSq = gate::sqDistToSample(tp, baseI, pos);
+    if (g_searchCount.local)
+    {
+        // counting only: the kernels' walks (walkStop in gate_model.cuh); their margin
+        // scans are skipped where the walks advanced at most 10 samples together
+        int moves = 0;
+        for (int delta = -1; delta <= 1; delta += 2)
+        {
+            R best = baseSq;
+            int cur = (baseI + delta + NTS) % NTS;
+            R curSq = gate::sqDistToSample(tp, cur, pos);
+            while (curSq < best)
+            {
+                best = curSq;
+                moves++;
+                cur = (cur + delta + NTS) % NTS;
+                curSq = gate::sqDistToSample(tp, cur, pos);
+            }
+        }
+        g_searchCount.pause(moves <= 10);
+    }
     R bSq, fSq;
     int bI = walkMin(tp, baseI, pos, -1, baseSq, bSq);
     int fI = walkMin(tp, baseI, pos, +1, baseSq, fSq);
+    if (g_searchCount.local)
+        g_searchCount.pause(false);
     if (fSq < bSq)
         return (R)fI / (R)NTS;
     return (R)bI / (R)NTS;

@@ -268,12 +268,64 @@ template <typename R> inline R sqDistToSample(const R* p_grid, int i, const R* p
     return sq;
 }
 
+// Operation counting only (opcount.cpp): with `local` set, the projections count the
+// searches the CUDA kernels run where their certificate holds (the local search of the
+// window from its centre; the gate race's walks without the margin scans) and take their
+// result from the searches as written below, evaluated with counting paused by `pause`.
+struct SearchCount
+{
+    bool local = false;
+    void (*pause)(bool) = nullptr;
+};
+inline thread_local SearchCount g_searchCount;
+
+// The kernels' local search of the window idxPrev -+ WINDOW_SIZE (windowLocalSearch in
+// model.cuh): from the centre, to the neighbour at no greater (below) or smaller (above)
+// distance while there is one; returns the sample it stops at.
+template <typename R> inline int localWindowSearch(const Env<R>& env, int idxPrev, const R* pos)
+{
+    auto f = [&](int k) { return sqDistToSample(env.p.data(), (idxPrev + k - WINDOW_SIZE + NTS) % NTS, pos); };
+    int c = WINDOW_SIZE;
+    R fc = f(c), fl = f(c - 1);
+    if (fl <= fc)
+    {
+        for (int it = 0; it < WINDOW_SIZE; it++)
+        {
+            c--;
+            fc = fl;
+            if (c == 0)
+                break;
+            fl = f(c - 1);
+            if (!(fl <= fc))
+                break;
+        }
+    }
+    else
+    {
+        R fr = f(c + 1);
+        for (int it = 0; it < WINDOW_SIZE && fr < fc; it++)
+        {
+            c++;
+            fc = fr;
+            if (c == 2 * WINDOW_SIZE)
+                break;
+            fr = f(c + 1);
+        }
+    }
+    return (idxPrev + c - WINDOW_SIZE + NTS) % NTS;
+}
+
 // fastProjectOnTrack<false>, :88-162. Returns S, writes latDist.
 template <typename R> inline R fastProjectOnTrack(const Env<R>& env, const R* pos, R prevS, R& latDist)
 {
     prevS /= env.trackLength;
     prevS = prevS - floor(prevS);
     int idxPrev = (int)(prevS * NTS);
+    if (g_searchCount.local)
+    {
+        localWindowSearch(env, idxPrev, pos);
+        g_searchCount.pause(true);
+    }
 
     int bestInd = (idxPrev - WINDOW_SIZE + NTS) % NTS;
     R bestSqDist = sqDistToSample(env.p.data(), bestInd, pos);
@@ -287,6 +339,8 @@ template <typename R> inline R fastProjectOnTrack(const Env<R>& env, const R* po
             bestInd = (idxPrev + offset) % NTS;
         }
     }
+    if (g_searchCount.local)
+        g_searchCount.pause(false);
 
     R bestSegSqDist = INFINITY;
     R bestS = R(0);

@@ -14,6 +14,10 @@
 // step when the ego draws no noise). `dedup | 4` also leaves out work whose result nothing
 // reads: once a sample has committed to a branch, its belief update and the other
 // hypotheses' opponent actions (the kernels skip them; the reference does them).
+// `dedup | 8` counts the projections' searches as the kernels run them where their
+// certificate holds (SearchCount in model.hpp: the local search of the window, the gate
+// race's walks without their margin scans), the results still taken from the searches
+// as the reference writes them.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -40,6 +44,37 @@ struct CountCtx
 };
 
 inline thread_local CountCtx* g_ctx = nullptr;
+inline thread_local CountCtx* g_paused = nullptr;
+
+// SearchCount::pause: suspends counting (on) and resumes it (off)
+inline void pauseCounting(bool on)
+{
+    if (on)
+    {
+        g_paused = g_ctx;
+        g_ctx = nullptr;
+    }
+    else if (g_paused)
+    {
+        g_ctx = g_paused;
+        g_paused = nullptr;
+    }
+}
+
+// sets SearchCount for one counting call and clears it on every return path
+struct SearchCountScope
+{
+    explicit SearchCountScope(bool local)
+    {
+        g_searchCount.local = local;
+        g_searchCount.pause = pauseCounting;
+    }
+    ~SearchCountScope()
+    {
+        g_searchCount.local = false;
+        g_paused = nullptr;
+    }
+};
 
 inline uint64_t dbits(double x)
 {
@@ -205,6 +240,7 @@ static int countOps(const EnvT& env, const dr_mppi_config* mc, const S0* s0, con
     // dedup | 4: skip the work whose result nothing reads (the belief update and the other
     // hypotheses' actions once a sample has committed to a branch), as the kernels do
     const bool skipDead = (dedup & 4) != 0;
+    const SearchCountScope searches((dedup & 8) != 0);
     dedup &= 3;
     CountCtx ctx;
     ctx.dedup = dedup != 0;
@@ -328,6 +364,8 @@ extern "C" int orc_pr_count_ops(const dr_env_config* ec, const dr_prmppi_config*
                                 int theta, uint64_t seed, uint64_t step, int nsamples, int dedup, double* out)
 {
     Env<CF> env(*ec);
+    const SearchCountScope searches((dedup & 8) != 0);
+    dedup &= 3;
     CountCtx ctx;
     ctx.dedup = dedup != 0;
     const int K = pc->n_samples, T = pc->n_timesteps;
