@@ -124,6 +124,9 @@ struct EnvParams
     // same s1, s2 and speedScale, so j's action is th's whenever the opponent blocks no
     // one (s3 is read only by the blocking term, env_stratrace.h:357-372).
     signed char dupAll[8][3], dupNoBlock[8][3];
+    // hypothesis th gives opponent o's action the noise level of hypothesis 0 (so the two
+    // have the same likelihood constants)
+    bool noiseAs0[8][3];
 };
 
 constexpr int ENV_HOST_WORDS = (int)(offsetof(EnvParams, logSqSigma) / 4);
@@ -155,6 +158,7 @@ __device__ __forceinline__ void envDeviceTerms(EnvParams& dst, const EnvParams& 
         }
         dst.dupAll[th][o] = (signed char)all;
         dst.dupNoBlock[th][o] = (signed char)noBlock;
+        dst.noiseAs0[th][o] = src.actionNoise[th][o] == src.actionNoise[0][o];
     }
     if (tid == 0)
     {
@@ -886,6 +890,9 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     act0[0] = ego0;
     act1[0] = ego1;
     float nom0[ALLTH ? NTH : 1][NOPP], nom1[ALLTH ? NTH : 1][NOPP];
+    // every hypothesis took hypothesis 0's action for every opponent, at its noise level:
+    // then their likelihoods are equal and the belief update only renormalises the belief
+    bool likeAs0 = true;
 #pragma unroll
     for (int o = 1; o <= NOPP; o++)
     {
@@ -903,6 +910,8 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
                 // an earlier hypothesis with the same action (all of them are evaluated
                 // while the belief is live, so that one's action is at hand)
                 const int src = live ? (blocks ? E.dupAll[th][o - 1] : E.dupNoBlock[th][o - 1]) : -1;
+                if (th > 0 && !(src == 0 && E.noiseAs0[th][o - 1]))
+                    likeAs0 = false;
                 bool copied = false;
 #pragma unroll
                 for (int j = 0; j < th; j++)
@@ -1026,7 +1035,11 @@ __device__ __forceinline__ StepOut envStep(int t, int trueTheta, const Track& tr
     // 10. belief update (env_stratrace.h:166-222)
     if constexpr (UPD)
     {
-        if (live)
+        // The fast flavour skips the update when the likelihoods are equal (ALLTH: every
+        // hypothesis' action is at hand), leaving the belief as it was where the update
+        // would renormalise it (a change of rounding only; the verification's results
+        // are checked in distribution).
+        if (live && !(F && ALLTH && likeAs0))
         {
             float sum = 0.0f;
 #pragma unroll
