@@ -1114,6 +1114,8 @@ def run_ours_mixed(args) -> None:
         else:
             ctls = [ctl_mod.PRMPPIController(s.env, s.prmppi, s.seed, device=local, stream=stream.cuda_stream) for s in g]
             r["batch"] = ctl_mod.PRMPPIBatch(ctls, stream=stream.cuda_stream)
+            if args.pr_slots is not None:
+                r["batch"].set_rollout_slots(args.pr_slots)
         r["ctls"] = ctls
         runs.append(r)
     torch.cuda.synchronize()
@@ -1376,7 +1378,7 @@ def main():
                     help="CTAs per SM of the previous plan's verification beside the rollout (0: one per tile; default: the library's)")
     ap.add_argument("--pdl", action="store_true", help="programmatic dependent launches of the update and the new plan's verification")
     ap.add_argument("--pr-slots", type=int, default=None, choices=[1, 2, 4],
-                    help="pr workload: hypothesis slots per rollout thread sharing the ego's moves (default: the library's)")
+                    help="pr and races workloads: hypothesis slots per PR-MPPI rollout thread sharing the ego's moves (default: the library's)")
     ap.add_argument("--grad-steps", type=int, default=GRAD_STEPS, help="grad workload: projected gradient steps after each update")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true", help="reference arm: skip timing the reference's CUDA path")
