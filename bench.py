@@ -136,9 +136,9 @@ def _ref_variant(O) -> str:
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture
 # of each kernel on this workload (--quick --no-overlap, 3 steps); grids, plans and tile
-# tables stay in L2, so DRAM traffic is spilled registers and first-touch reads, about 1.4
+# tables stay in L2, so DRAM traffic is spilled registers and first-touch reads, about 0.9
 # MB per verification launch (both plans, with the ego tables).
-TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 1402112.0, "rollout": 168960.0}
+TRAFFIC_PER_LAUNCH: dict[str, float] = {"verify": 855040.0, "rollout": 168960.0}
 
 
 def _package():
